@@ -1,0 +1,410 @@
+"""Benchmark of the Waltz B200 compressor hot path.
+
+Workload (N=1): float32 512x512x512 Gaussian random field with power
+spectrum k^-11/3 (unit variance, seed 1), REL 1e-3 bound resolved on the GPU
+(eb = 1e-3 * (max - min)), dyadic schedule with 5 levels per axis. A step is
+one compress of the field followed by one decompress of its archive; the
+metric is the field's bytes per second through that round trip (decimal GB/s),
+with compress and decompress throughput and their HBM-roofline fractions
+reported beside it. The 512 MiB input and output exceed the 126 MB L2, so no
+flush is needed between steps.
+
+N>1 (torchrun): one compressor per GPU on its own copy of the field
+(replicas, no collective on the data path); value = all ranks' bytes / max
+time over ranks.
+
+`--impl reference` times the reference's own CPU codec (compiled from its
+sources into oracle/_ref, AVX2 backend) on the host cores with one thread
+per core, on the same field split into its eight 256^3 octants.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "comp/decomp GB/s f32 512^3 REL1e-3, plain vs TC form at same bound; % HBM peak"
+SHAPE = (512, 512, 512)
+REL = 1e-3
+SEED = 1
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during timing."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append((time.time(), line.strip()))
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self, t0, t1):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for t, line in self.lines:
+            if not (t0 - 0.05 <= t <= t1 + 0.05):
+                continue
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() in ("active", "1", "yes"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------- GPU arm
+def gpu_arm(args, rank, world, local_rank):
+    import torch
+    import waltz_b200
+    from waltz_b200 import _lib
+    from waltz_b200.synthetic import power_law_field_device
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    lib = _lib.lib()
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    field = power_law_field_device(SHAPE, SEED, device=dev).contiguous()
+    n = field.numel()
+    nbytes = n * 4
+    lo, hi = waltz_b200.extrema(field)
+    eb = REL * (hi - lo)
+    cap = waltz_b200.compressed_capacity(n, 4)
+    archive = torch.empty(cap, dtype=torch.uint8, device=dev)
+    out = torch.empty_like(field)
+    nz, ny, nx = SHAPE
+    written = C.c_size_t()
+
+    def compress():
+        _lib.checked(lib.waltz_b200_compress(C.c_void_p(field.data_ptr()), 4, nx, ny, nz, eb,
+                                             C.c_void_p(archive.data_ptr()), cap, C.byref(written), sp))
+        return written.value
+
+    def decompress(size):
+        _lib.checked(lib.waltz_b200_decompress(C.c_void_p(archive.data_ptr()), size, 4, nx, ny, nz,
+                                               C.c_void_p(out.data_ptr()), nbytes, sp))
+
+    # correctness of the measured configuration (untimed)
+    size = compress()
+    decompress(size)
+    max_err = float((out.double() - field.double()).abs().max())
+    assert max_err <= eb, f"bound violated: {max_err} > {eb}"
+    first = archive[:size].clone()
+
+    for _ in range(args.warmup):
+        decompress(compress())
+
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    time.sleep(0.3)
+    dist_barrier(world)
+    torch.cuda.synchronize()
+    launches0 = lib.waltz_b200_launch_count()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps + 1)]
+    t_wall0 = time.time()
+    ev[0].record(stream)
+    for k in range(args.steps):
+        size = compress()
+        ev[2 * k + 1].record(stream)
+        decompress(size)
+        ev[2 * k + 2].record(stream)
+    torch.cuda.synchronize()
+    t_wall1 = time.time()
+    launches = lib.waltz_b200_launch_count() - launches0
+    dist_barrier(world)
+    sampler.stop()
+    comp_ms = [ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(args.steps)]
+    dec_ms = [ev[2 * k + 1].elapsed_time(ev[2 * k + 2]) for k in range(args.steps)]
+    total_ms = ev[0].elapsed_time(ev[-1])
+    total_ms = dist_max(total_ms, world)
+    assert torch.equal(archive[:size], first), "archive changed between steps"
+
+    # ---- per-kernel stage timing (separate, untimed pass)
+    lib.waltz_b200_profile(1)
+    stages = {}
+    for _ in range(3):
+        size = compress()
+        times = (C.c_double * 16)()
+        names = (C.c_char_p * 16)()
+        cnt = lib.waltz_b200_stage_times(times, names, 16)
+        for i in range(cnt):
+            stages.setdefault("compress:" + names[i].decode(), []).append(times[i])
+        decompress(size)
+        cnt = lib.waltz_b200_stage_times(times, names, 16)
+        for i in range(cnt):
+            stages.setdefault("decompress:" + names[i].decode(), []).append(times[i])
+    lib.waltz_b200_profile(0)
+    stage_ms = {k: statistics.median(v) for k, v in stages.items()}
+
+    # ---- end to end through the public API with host buffers
+    host_in = torch.empty(SHAPE, dtype=torch.float32, pin_memory=True)
+    host_in.copy_(field.cpu())
+    host_arch = torch.empty(cap, dtype=torch.uint8, pin_memory=True)
+    host_out = torch.empty(SHAPE, dtype=torch.float32, pin_memory=True)
+    e2e_ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    e2e = []
+    for k in range(max(2, min(args.steps, 5)) + 1):
+        dist_barrier(world)
+        torch.cuda.synchronize()
+        e2e_ev[0].record(stream)
+        field.copy_(host_in, non_blocking=True)
+        s = compress()
+        host_arch[:s].copy_(archive[:s], non_blocking=True)
+        e2e_ev[1].record(stream)
+        archive[:s].copy_(host_arch[:s], non_blocking=True)
+        decompress(s)
+        host_out.copy_(out, non_blocking=True)
+        e2e_ev[2].record(stream)
+        torch.cuda.synchronize()
+        if k:  # first pass warms the pinned paths
+            e2e.append((e2e_ev[0].elapsed_time(e2e_ev[1]), e2e_ev[1].elapsed_time(e2e_ev[2])))
+    e2e_c = statistics.median(x[0] for x in e2e)
+    e2e_d = statistics.median(x[1] for x in e2e)
+    e2e_step = dist_max(e2e_c + e2e_d, world)
+
+    hbm, peak_kind = peaks()
+    t_c = statistics.median(comp_ms) / 1e3
+    t_d = statistics.median(dec_ms) / 1e3
+    a_bytes = size
+    step_ms = total_ms / args.steps
+    value = world * nbytes / (step_ms / 1e3) / 1e9
+    algo = algorithmic_bytes(n, 4, a_bytes)
+    dom, dom_ms = max(((k, v) for k, v in stage_ms.items() if k in algo), key=lambda kv: kv[1])
+    achieved = algo[dom] / (dom_ms / 1e3) / 1e9
+    result = {
+        "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(step_ms, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded k^-11/3 Gaussian random field (stand-in for the reference's simulation fields)",
+        "config": {"workload": "f32 512^3 k^-11/3 GRF seed 1, REL 1e-3 (eb=%.6g), dyadic 5 levels, "
+                               "step = compress + decompress" % eb,
+                   "global_batch": world, "seq_len": None, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (512 MiB field)", "archive_bytes": a_bytes,
+                   "compression_ratio": round(nbytes / a_bytes, 4), "max_abs_error": max_err, "abs_bound": eb},
+        "compress_gbs": round(nbytes / t_c / 1e9, 3),
+        "decompress_gbs": round(nbytes / t_d / 1e9, 3),
+        "compress_hbm_frac": round((nbytes + a_bytes) / t_c / 1e9 / hbm, 4),
+        "decompress_hbm_frac": round((nbytes + a_bytes) / t_d / 1e9 / hbm, 4),
+        "stage_ms": {k: round(v, 4) for k, v in sorted(stage_ms.items())},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": hbm,
+                     "peak_source": peak_kind, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                     "algorithmic_bytes": algo[dom], "traffic": None},
+        "e2e": {"value": round(world * nbytes / (e2e_step / 1e3) / 1e9, 3), "unit": "GB/s",
+                "h2d_bytes_per_step": nbytes + a_bytes, "d2h_bytes_per_step": a_bytes + nbytes,
+                "compress_ms": round(e2e_c, 4), "decompress_ms": round(e2e_d, 4)},
+        "gpu_launches": int(launches),
+        "clocks": sampler.summary(t_wall0, t_wall1),
+    }
+    traffic = ROOT / "profiles" / "traffic.json"
+    if traffic.exists():
+        t = json.loads(traffic.read_text()).get(dom)
+        if t:
+            result["roofline"]["traffic"] = t
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(field.cpu().numpy(), eb)
+    return result
+
+
+def algorithmic_bytes(n, s, a):
+    """Bytes each timed stage must move at least (its inputs read once and its
+    outputs written once); a = archive bytes. Level kernels of the dyadic
+    schedule: level 0 dominates (7/8 of the samples)."""
+    w = a  # WZP stream is nearly the whole archive
+    return {
+        "compress:fwd_l0": 2 * n * s,
+        "compress:quantize": 2 * n * s + 2 * n + n // 8,
+        "compress:wzp_encode": 2 * n + n // 8 + w,
+        "compress:inv_l0_repair": 2 * n * s,
+        "decompress:wzp_decode": w + n * s,
+        "decompress:inv_l0": 2 * n * s,
+    }
+
+
+def dist_barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def dist_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------- CPU arms
+def _octants(field):
+    h = [s // 2 for s in field.shape]
+    out = []
+    for z in (0, 1):
+        for y in (0, 1):
+            for x in (0, 1):
+                out.append(np.ascontiguousarray(field[z * h[0]:(z + 1) * h[0], y * h[1]:(y + 1) * h[1],
+                                                      x * h[2]:(x + 1) * h[2]]))
+    return out
+
+
+def _codec(kind):
+    from oracle import oracle as O
+    if kind == "reference":
+        return O.RefCodec(O.AVX2)
+    class Port:
+        compress = staticmethod(O.compress)
+        decompress = staticmethod(O.decompress)
+    return Port()
+
+
+def cpu_baseline(field, eb, budget_s=12.0):
+    """Reference CPU codec (oracle/_ref, AVX2), one thread, on 256^3 octants of
+    the same field, repeated for about `budget_s` seconds."""
+    from oracle import oracle as O
+    kind = "reference" if O.ref_available() else "port"
+    codec = _codec(kind)
+    blocks = _octants(field)
+    done, t0, secs = 0, time.perf_counter(), 0.0
+    i = 0
+    while secs < budget_s and i < 8:
+        b = blocks[i]
+        a = codec.compress(b, eb)
+        codec.decompress(a, b.shape, b.dtype)
+        done += b.nbytes
+        i += 1
+        secs = time.perf_counter() - t0
+    return {"value": round(done / secs / 1e9, 4), "unit": "GB/s", "cores": 1, "kind": kind,
+            "sample": f"{i} of the field's eight 256^3 octants, compress + decompress each, "
+                      f"reference CPU codec AVX2 backend, 1 thread ({secs:.1f} s)"}
+
+
+def reference_arm(args):
+    """The reference's CPU implementation of the path, all host cores."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import oracle as O
+    from waltz_b200.synthetic import power_law_field
+    kind = "reference" if O.ref_available() else "port"
+    field = power_law_field(SHAPE, SEED)
+    eb = REL * (float(field.max()) - float(field.min()))
+    blocks = _octants(field)
+    cores = max(1, min(len(os.sched_getaffinity(0)), len(blocks)))
+    codecs = [_codec(kind) for _ in range(cores)]
+
+    def work(i):
+        codec = codecs[i % cores]
+        b = blocks[i]
+        a = codec.compress(b, eb)
+        codec.decompress(a, b.shape, b.dtype)
+        return b.nbytes
+
+    times = []
+    with ThreadPoolExecutor(cores) as pool:
+        for k in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            done = sum(pool.map(work, range(len(blocks))))
+            if k >= args.warmup:
+                times.append(time.perf_counter() - t0)
+    step = statistics.median(times)
+    value = done / step / 1e9
+    sample = (f"f32 512^3 field as eight 256^3 octants, compress + decompress each, reference CPU codec "
+              f"({'AVX2' if kind == 'reference' else 'C port'}), {cores} threads")
+    return {"metric": METRIC, "value": round(value, 4), "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(step * 1e3, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "f32 512^3 k^-11/3 GRF seed 1, REL 1e-3, split into 256^3 octants",
+                       "parallelism": f"{cores} host threads"},
+            "impl": "reference",
+            "cpu_baseline": {"value": round(value, 4), "unit": "GB/s", "cores": cores, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": round(value, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        print(json.dumps(reference_arm(args)))
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        result = gpu_arm(args, rank, world, local_rank)
+        if rank == 0:
+            print(json.dumps(result))
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,80 @@
+/*
+ * Waltz B200: C ABI of the GPU codec (one CUDA device per process, the
+ * calling thread's current device, the caller's stream).
+ *
+ * All pointers named d_* are device pointers. Every call is synchronous on
+ * its stream when it returns. Functions returning int give 0 on success and
+ * -1 on failure with the diagnostic in waltz_b200_last_error() (thread local).
+ * Archives are the reference's 32-byte-header native archives: in the default
+ * profile they are byte-identical to the reference CPU scalar codec.
+ *
+ * Reference interfaces these replace (paths inside the reference project):
+ *   waltz_b200_compressed_capacity  include/waltz.hpp:21-33 (compressed_buffer_capacity<T>)
+ *   waltz_b200_compress             include/waltz.hpp:51-61 (d_compress<T>) -> src/waltz.cu:327-609
+ *   waltz_b200_decompress           include/waltz.hpp:70-81 (d_decompress<T>) -> src/waltz.cu:612-834
+ *   waltz_b200_extrema              include/waltz.hpp:39-40 (d_extrema<T>) -> src/waltz.cu:867-876
+ * The reference's own C entry points keep their exact signatures in
+ * waltz_cuda.h and waltz_gpu_batch.h, exported by the same library.
+ */
+#ifndef WALTZ_B200_H
+#define WALTZ_B200_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Archive capacity the caller must provide for n samples of `width` bytes
+ * (4 or 8): one input volume plus the fixed side-record caps plus 1 MiB. */
+size_t waltz_b200_compressed_capacity(uint64_t n, int width);
+
+/* Compress nx*ny*nz samples (x fastest) of width 4 (float) or 8 (double) at
+ * the absolute pointwise bound abs_error. *written receives the archive size. */
+int waltz_b200_compress(const void* d_input, int width, uint32_t nx, uint32_t ny, uint32_t nz,
+                        double abs_error, void* d_archive, size_t capacity, size_t* written,
+                        void* stream);
+
+/* Decode an archive of `bytes` bytes into nx*ny*nz samples (the archive does
+ * not store its dimensions). */
+int waltz_b200_decompress(const void* d_archive, size_t bytes, int width, uint32_t nx, uint32_t ny,
+                          uint32_t nz, void* d_output, size_t output_bytes, void* stream);
+
+/* Minimum and maximum of n samples (the REL -> ABS bound resolution). */
+int waltz_b200_extrema(const void* d_input, int width, uint64_t n, double* min_out, double* max_out,
+                       void* stream);
+
+const char* waltz_b200_last_error(void);
+
+/* Diagnostic stage entry points (used by the parity tests).
+ * waltz_b200_transform: in-place all-level CDF 9/7 analysis (inverse = 0)
+ *   into the split-band coefficient layout, or synthesis (inverse = 1);
+ *   replaces allhalo::forward / allhalo::inverse
+ *   (include/transformers/all_halo.cuh:278-380 of the reference).
+ * waltz_b200_wzp_encode: WZP stream of n Morton-packed u16 magnitudes and a
+ *   natural sign bitmap (ceil(n/32) words); replaces lossless::wzp_enqueue
+ *   (src/lossless/wzp.cu:1102-1126 of the reference). */
+int waltz_b200_transform(void* d_data, int width, uint32_t nx, uint32_t ny, uint32_t nz, int inverse,
+                         void* stream);
+int waltz_b200_wzp_encode(const uint16_t* d_mag, const uint32_t* d_sign, uint32_t n, void* d_out,
+                          size_t capacity, size_t* written, void* stream);
+/* Test hook for the bounded-wait path: compress with chunk `skip_chunk`
+ * never publishing its lookback state and every wait capped at `spin_cap`
+ * polls (~0.5 us each). Must fail with a lookback-timeout diagnostic. */
+int waltz_b200_test_lookback_timeout(const void* d_input, int width, uint32_t nx, uint32_t ny, uint32_t nz,
+                                     double abs_error, void* d_archive, size_t capacity, uint32_t skip_chunk,
+                                     uint32_t spin_cap, void* stream);
+
+/* Instrumentation. waltz_b200_launch_count: kernels launched by this library
+ * since load. waltz_b200_profile(1) makes the calling thread record CUDA
+ * events between the pipeline stages of its next calls; after a call,
+ * waltz_b200_stage_times fills up to `cap` stage durations (ms) and names and
+ * returns how many stages were timed (the reference's per-stage GPUTimer
+ * report, include/utils/Timer.hpp:5-63). */
+unsigned long long waltz_b200_launch_count(void);
+void waltz_b200_profile(int enable);
+int waltz_b200_stage_times(double* ms, const char** names, int cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -258,7 +258,7 @@ long long wo_wzp_encode(const uint16_t* mag, const uint32_t* sign, uint32_t n,
     const size_t header = (size_t)groups * 4 + (size_t)chunks * 3;
     uint8_t* meta = out + (size_t)groups * 4;
     size_t cursor = header;
-    uint8_t planes[2 * CHUNK], packed[2 * CHUNK + 8];
+    uint8_t planes[2 * CHUNK], packed[2 * CHUNK + 2048 + 256 + 32 + 4 + 8]; /* worst case before the raw test */
     uint32_t g, c;
     if (n > 0x7fffffffu) { say(err, errlen, "WZP element count exceeds the GPU format limit"); return -1; }
     if (!n) return 0;

@@ -1,0 +1,266 @@
+"""GPU parity: the CUDA library, called through its C ABI, against the C
+oracle (bit/byte-exact) on the reference's own test shapes and patterns."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests import patterns as P
+
+pytestmark = pytest.mark.gpu
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _lib():
+    from waltz_b200 import _lib
+    return _lib.lib()
+
+
+def _stream():
+    return C.c_void_p(_torch().cuda.current_stream().cuda_stream)
+
+
+def gpu_transform(a: np.ndarray, inverse: bool) -> np.ndarray:
+    torch = _torch()
+    d = torch.from_numpy(np.ascontiguousarray(a).copy()).cuda()
+    nz, ny, nx = a.shape
+    rc = _lib().waltz_b200_transform(C.c_void_p(d.data_ptr()), a.itemsize, nx, ny, nz, int(inverse), _stream())
+    assert rc == 0, _lib().waltz_b200_last_error()
+    return d.cpu().numpy()
+
+
+def gpu_compress(a: np.ndarray, eb: float) -> bytes:
+    import waltz_b200
+    return waltz_b200.compress(a, abs_error=eb)
+
+
+def gpu_decompress(archive: bytes, shape, dtype) -> np.ndarray:
+    import waltz_b200
+    return waltz_b200.decompress(archive, shape=shape, dtype=dtype)
+
+
+TRANSFORM_SHAPES = P.CODEC_SHAPES + [(96, 40, 24), (130, 9, 70), (40, 44, 52), (100, 3, 33), (31, 64, 8),
+                                     (64, 65, 66), (200, 17, 9)]
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("nxyz", TRANSFORM_SHAPES)
+def test_transform_bit_exact(nxyz, dtype):
+    rng = np.random.default_rng(sum(nxyz) + 7)
+    a = rng.standard_normal(P.zyx(nxyz)).astype(dtype)
+    f = gpu_transform(a, inverse=False)
+    assert f.tobytes() == O.transform(a, inverse=False).tobytes()
+    i = gpu_transform(f, inverse=True)
+    assert i.tobytes() == O.transform(f, inverse=True).tobytes()
+
+
+def test_wzp_encode_byte_exact():
+    torch = _torch()
+    for n, pattern, mag, sign in P.wzp_cases():
+        if n == 0:
+            continue
+        expect = O.wzp_encode(mag, sign)
+        dm = torch.from_numpy(mag.astype(np.int16).view(np.int16)).cuda()
+        ds = torch.from_numpy(sign.view(np.int32)).cuda()
+        cap = O.oracle_lib().wo_wzp_max_bytes(n)
+        out = torch.zeros(cap, dtype=torch.uint8, device="cuda")
+        written = C.c_size_t()
+        rc = _lib().waltz_b200_wzp_encode(C.c_void_p(dm.data_ptr()), C.c_void_p(ds.data_ptr()), n,
+                                          C.c_void_p(out.data_ptr()), cap, C.byref(written), _stream())
+        assert rc == 0, _lib().waltz_b200_last_error()
+        got = out[:written.value].cpu().numpy().tobytes()
+        assert got == expect, (n, pattern)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("nxyz", P.CODEC_SHAPES)
+def test_archive_byte_exact_and_decode_bit_exact(nxyz, dtype):
+    for pattern in range(5):
+        a = P.codec_field(P.zyx(nxyz), pattern, 1e-3, dtype)
+        expect = O.compress(a, 1e-3)
+        got = gpu_compress(a, 1e-3)
+        assert got == expect, pattern
+        out = gpu_decompress(got, a.shape, dtype)
+        assert out.tobytes() == O.decompress(expect, a.shape, dtype).tobytes()
+        err = np.abs(out.astype(np.longdouble) - a.astype(np.longdouble)).max()
+        assert err <= np.longdouble(1e-3)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_side_channels_byte_exact(dtype):
+    cases = [((17, 19, 23), 5, 1e-5), ((9, 11, 17), 6, 1e-5), ((17, 19, 23), 2, 1e-7), ((64, 64, 64), 1, 1e-5),
+             ((23, 19, 17), 2, 1e-12)]
+    import waltz_b200
+    for nxyz, pattern, eb in cases:
+        a = P.codec_field(P.zyx(nxyz), pattern, eb, dtype)
+        try:
+            expect = O.compress(a, eb)
+        except O.CodecError:
+            with pytest.raises(waltz_b200.WaltzError):
+                gpu_compress(a, eb)
+            continue
+        got = gpu_compress(a, eb)
+        assert got == expect, (nxyz, pattern, eb)
+        assert gpu_decompress(got, a.shape, dtype).tobytes() == O.decompress(expect, a.shape, dtype).tobytes()
+
+
+def test_golden_fixtures_on_gpu():
+    from tests.golden import load_golden
+    import hashlib
+    for case in load_golden():
+        field = case["input"]
+        got = gpu_compress(field, case["abs_error"])
+        assert got == case["archive"], case["name"]
+        out = gpu_decompress(got, field.shape, field.dtype)
+        assert hashlib.sha256(out.tobytes()).hexdigest() == case["decoded_sha256"], case["name"]
+
+
+@pytest.mark.parametrize("case", ["powerlaw_f32", "front_f64_plane", "spiky_f32_plane"])
+def test_larger_fields_byte_exact(case):
+    from waltz_b200 import synthetic as S
+    if case == "powerlaw_f32":
+        a = S.power_law_field((96, 128, 160), 1)
+        eb = S.rel_to_abs(a, 1e-4)
+    elif case == "front_f64_plane":
+        a = S.front_field((48, 128, 96), 2)
+        eb = 1e-6
+    else:
+        a = S.spiky_field((40, 128, 128), 3)
+        eb = S.rel_to_abs(a, 1e-5)
+    expect = O.compress(a, eb)
+    got = gpu_compress(a, eb)
+    assert got == expect
+    out = gpu_decompress(got, a.shape, a.dtype)
+    assert out.tobytes() == O.decompress(expect, a.shape, a.dtype).tobytes()
+
+
+def test_invalid_inputs_rejected():
+    import waltz_b200
+    a = P.codec_field((17, 11, 9), 2, 1e-3, np.float32)
+    for bad in (np.nan, np.inf, -np.inf):
+        b = a.copy()
+        b.reshape(-1)[7] = bad
+        with pytest.raises(waltz_b200.WaltzError):
+            gpu_compress(b, 1e-3)
+    for eb in (0.0, -1.0, float("nan"), float("inf")):
+        with pytest.raises(ValueError):
+            gpu_compress(a, eb)
+
+
+def test_malformed_archives_rejected():
+    import waltz_b200
+    from tests.test_oracle import _mutations
+    a = P.codec_field((23, 19, 17), 3, 1e-5, np.float64)
+    archive = O.compress(a, 1e-5)
+    for bad in _mutations(archive, a.size):
+        with pytest.raises((waltz_b200.WaltzError, ValueError)):
+            gpu_decompress(bad, a.shape, np.float64)
+    # the untouched archive still decodes after all the rejections
+    assert gpu_decompress(archive, a.shape, np.float64).tobytes() == O.decompress(archive, a.shape, np.float64).tobytes()
+
+
+def test_unordered_side_records_accepted_duplicates_rejected():
+    """cpu/tests/test_codec.cpp:288-301: swapped side records decode to the same
+    bits; a duplicated index is rejected."""
+    import struct
+    import waltz_b200
+    a = P.codec_field((23, 19, 17), 3, 1e-5, np.float64)
+    archive = bytearray(O.compress(a, 1e-5))
+    expected = O.decompress(bytes(archive), a.shape, np.float64)
+    wzp = struct.unpack_from("<Q", archive, 16)[0]
+    np_ = struct.unpack_from("<I", archive, 24)[0]
+    assert np_ >= 2
+    pi = 32 + ((wzp + 7) & ~7)
+    pv = pi + ((np_ * 4 + 7) & ~7)
+    swapped = bytearray(archive)
+    for start, width in ((pi, 4), (pv, 8)):
+        first = bytes(swapped[start:start + width])
+        last = bytes(swapped[start + (np_ - 1) * width:start + np_ * width])
+        swapped[start:start + width] = last
+        swapped[start + (np_ - 1) * width:start + np_ * width] = first
+    out = gpu_decompress(bytes(swapped), a.shape, np.float64)
+    assert out.tobytes() == expected.tobytes()
+    dup = bytearray(swapped)
+    dup[pi + 4:pi + 8] = dup[pi:pi + 4]
+    with pytest.raises(waltz_b200.WaltzError):
+        gpu_decompress(bytes(dup), a.shape, np.float64)
+
+
+def test_extrema():
+    import waltz_b200
+    torch = _torch()
+    for dtype in (torch.float32, torch.float64):
+        t = torch.randn(3, 1000, 77, dtype=dtype, device="cuda") * 5
+        lo, hi = waltz_b200.extrema(t)
+        assert lo == float(t.min()) and hi == float(t.max())
+
+
+def test_decode_chunk_canonical():
+    torch = _torch()
+    a = P.codec_field((33, 31, 17), 2, 1e-3, np.float32)
+    archive = O.compress(a, 1e-3)
+    src = torch.from_numpy(np.frombuffer(archive, np.uint8).copy()).cuda()
+    out = torch.empty(a.shape, dtype=torch.float32, device="cuda")
+    err = _lib().waltz_cuda_decode_chunk(33, 31, 17, 4, C.c_void_p(src.data_ptr()), len(archive),
+                                         C.c_void_p(out.data_ptr()), out.numel() * 4, _stream())
+    assert err is None, err
+    assert out.cpu().numpy().tobytes() == O.decompress(archive, a.shape, np.float32).tobytes()
+    # wrong geometry / width / length are rejected with a diagnostic
+    assert _lib().waltz_cuda_decode_chunk(33, 31, 16, 4, C.c_void_p(src.data_ptr()), len(archive),
+                                          C.c_void_p(out.data_ptr()), 33 * 31 * 16 * 4, _stream()) is not None
+    assert _lib().waltz_cuda_decode_chunk(33, 31, 17, 4, C.c_void_p(src.data_ptr()), len(archive) - 8,
+                                          C.c_void_p(out.data_ptr()), out.numel() * 4, _stream()) is not None
+
+
+def test_lookback_wait_is_bounded():
+    """A chunk that never publishes its lookback state makes its successor's
+    bounded wait expire: the call fails with a diagnostic, without a hang."""
+    torch = _torch()
+    from waltz_b200 import synthetic as S
+    a = S.power_law_field((64, 64, 64), 5)
+    d = torch.from_numpy(a).cuda()
+    cap = _lib().waltz_b200_compressed_capacity(a.size, 4)
+    out = torch.empty(cap, dtype=torch.uint8, device="cuda")
+    rc = _lib().waltz_b200_test_lookback_timeout(C.c_void_p(d.data_ptr()), 4, 64, 64, 64, 1e-3,
+                                                 C.c_void_p(out.data_ptr()), cap, 3, 2000, _stream())
+    assert rc != 0
+    assert b"lookback" in _lib().waltz_b200_last_error()
+    # the context stays usable
+    assert gpu_compress(a, 1e-3) == O.compress(a, 1e-3)
+
+
+def test_batch_decode_matches_oracle():
+    """waltz_gpu_decode_batch: clipped edge tiles, two sides, a missing tile
+    (fill), against per-tile oracle decodes."""
+    torch = _torch()
+    from waltz_b200 import loader
+    from waltz_b200 import synthetic as S
+    tile, frame, samples = (16, 24, 20), (30, 40, 33), 2
+    fields = [[S.power_law_field(frame, 10 + 2 * s + side) for side in range(2)] for s in range(samples)]
+    batch_samples, expect = [], np.zeros((2, samples, *frame), np.float32)
+    for s in range(samples):
+        sample = []
+        for side in range(2):
+            blobs = loader.frame_to_archives(fields[s][side], tile, 1e-3, O.compress)
+            if s == 1 and side == 0:
+                blobs[1] = None  # missing tile -> fill
+            sample.append(blobs)
+            for k, origin in enumerate(loader.tile_origins(frame, tile)):
+                region = tuple(slice(o, min(o + t, n)) for o, t, n in zip(origin, tile, frame))
+                if blobs[k] is None:
+                    expect[(side, s, *region)] = -7.0
+                    continue
+                dec = O.decompress(blobs[k], tile, np.float32)
+                expect[(side, s, *region)] = dec[tuple(slice(0, r.stop - r.start) for r in region)]
+        batch_samples.append(sample)
+    batch = loader.pack(batch_samples, indexed=True)
+    out = loader.decode_batch(batch, tile=tile, frame=frame, width=4, sides=2, fill=-7.0)
+    torch.cuda.synchronize()
+    assert out.cpu().numpy().tobytes() == expect.tobytes()

@@ -1,0 +1,127 @@
+"""Waltz error-bounded 3-D compressor, B200-native.
+
+Host-side mirror of the reference's Python surface (python/pywaltz/codec.py:
+``compress(array, *, abs_error)`` / ``decompress(archive, *, shape, dtype)``),
+running on the GPU through the in-tree CUDA library, plus device-tensor
+entry points for callers whose data already lives in HBM. Archives are the
+reference's native 32-byte-header archives, byte-identical to the reference
+CPU scalar codec in the default profile.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import operator
+
+import numpy as np
+
+from ._lib import BatchShape, WaltzError, checked, lib
+
+__all__ = ["compress", "decompress", "compress_tensor", "decompress_tensor", "extrema",
+           "compressed_capacity", "rel_to_abs_bound", "WaltzError"]
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise WaltzError("a CUDA device is required (there is no CPU fallback)")
+    return torch
+
+
+def _geometry(shape, itemsize):
+    """(z,y,x) or (y,x) shape -> (nx, ny, nz), as python/pywaltz/codec.py:24-33."""
+    shape = tuple(operator.index(v) for v in shape)
+    if itemsize not in (4, 8):
+        raise TypeError("Waltz requires native float32 or float64")
+    if len(shape) not in (2, 3) or min(shape) <= 0:
+        raise ValueError("expected positive (y,x) or (z,y,x) dimensions")
+    if math.prod(shape) * itemsize > 0xffffffff:
+        raise ValueError("field exceeds the native Waltz archive limit")
+    return (*reversed(shape), 1)[:3]
+
+
+def _bound(value):
+    value = float(value)
+    if not math.isfinite(value) or value <= 0:
+        raise ValueError("abs_error must be finite and positive")
+    return value
+
+
+def compressed_capacity(n: int, itemsize: int) -> int:
+    return int(lib().waltz_b200_compressed_capacity(n, itemsize))
+
+
+def _stream(torch, stream):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def compress_tensor(field, abs_error: float, *, stream=None):
+    """Compress a contiguous float32/float64 CUDA tensor of shape (z,y,x) or
+    (y,x). Returns a uint8 CUDA tensor holding the archive."""
+    torch = _torch()
+    if not field.is_cuda or not field.is_contiguous():
+        raise ValueError("expected a contiguous CUDA tensor")
+    nx, ny, nz = _geometry(field.shape, field.element_size())
+    cap = compressed_capacity(field.numel(), field.element_size())
+    out = torch.empty(cap, dtype=torch.uint8, device=field.device)
+    written = C.c_size_t()
+    checked(lib().waltz_b200_compress(C.c_void_p(field.data_ptr()), field.element_size(), nx, ny, nz,
+                                      _bound(abs_error), C.c_void_p(out.data_ptr()), cap, C.byref(written),
+                                      _stream(torch, stream)))
+    return out[:written.value]
+
+
+def decompress_tensor(archive, shape, dtype, *, out=None, stream=None):
+    """Decode a uint8 CUDA tensor archive into a (z,y,x) CUDA tensor."""
+    torch = _torch()
+    dtype = {np.float32: torch.float32, np.float64: torch.float64}.get(dtype, dtype)
+    if dtype not in (torch.float32, torch.float64):
+        raise TypeError("Waltz requires float32 or float64")
+    itemsize = 4 if dtype == torch.float32 else 8
+    nx, ny, nz = _geometry(shape, itemsize)
+    if out is None:
+        out = torch.empty(tuple(shape), dtype=dtype, device=archive.device)
+    if not archive.is_cuda or not archive.is_contiguous():
+        raise ValueError("expected a contiguous CUDA archive tensor")
+    checked(lib().waltz_b200_decompress(C.c_void_p(archive.data_ptr()), archive.numel(), itemsize, nx, ny, nz,
+                                        C.c_void_p(out.data_ptr()), out.numel() * itemsize,
+                                        _stream(torch, stream)))
+    return out
+
+
+def extrema(field, *, stream=None):
+    """(min, max) of a CUDA tensor, as doubles."""
+    torch = _torch()
+    lo, hi = C.c_double(), C.c_double()
+    checked(lib().waltz_b200_extrema(C.c_void_p(field.data_ptr()), field.element_size(), field.numel(),
+                                     C.byref(lo), C.byref(hi), _stream(torch, stream)))
+    return lo.value, hi.value
+
+
+def rel_to_abs_bound(field, rel: float, *, stream=None) -> float:
+    """REL bound -> absolute bound: rel * (max - min) in double."""
+    lo, hi = extrema(field, stream=stream)
+    return float(rel) * (hi - lo)
+
+
+def compress(array, *, abs_error):
+    """Return canonical archive bytes of a float32/float64 (z,y,x) or (y,x)
+    numpy array, computed on the current CUDA device."""
+    torch = _torch()
+    a = np.ascontiguousarray(np.asarray(array))
+    if a.dtype not in (np.float32, np.float64):
+        raise TypeError("Waltz requires native float32 or float64")
+    dev = torch.from_numpy(a).cuda()
+    return bytes(compress_tensor(dev, abs_error).cpu().numpy().tobytes())
+
+
+def decompress(archive, *, shape, dtype):
+    """Decode archive bytes using the original numpy shape and dtype."""
+    torch = _torch()
+    src = np.frombuffer(archive, dtype=np.uint8)
+    if src.size < 32:
+        raise ValueError("truncated Waltz header")
+    dev = torch.from_numpy(src.copy()).cuda()
+    out = decompress_tensor(dev, tuple(shape), np.dtype(dtype).type)
+    return out.cpu().numpy()

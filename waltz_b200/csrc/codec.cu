@@ -1,0 +1,1009 @@
+// Waltz B200 pipeline driver and C ABI.
+//
+// Compress (default profile, src/waltz.cu:327-609 of the reference):
+//   forward all-level lifting -> quantise + Morton reorder -> WZP encode
+//   (decoupled lookback, writes the archive in place) -> inverse lifting with
+//   the repair emitter on the finest level -> ordered compaction of repairs
+//   and q-outliers straight into their archive sections -> header.
+// Decompress (src/waltz.cu:612-834): header checks -> WZP decode fused with
+// dequantisation and the row-major scatter -> q-outlier patches -> inverse
+// lifting -> repair patches. Every status is gathered in one device word and
+// read at the call's single synchronisation point.
+#include "common.cuh"
+#include "quantize.cuh"
+#include "transform.cuh"
+#include "wzp.cuh"
+
+#include "../../include/waltz_b200.h"
+#include "../../include/waltz_cuda.h"
+#include "../../include/waltz_gpu_batch.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <type_traits>
+#include <vector>
+
+namespace wb {
+
+// ---------------------------------------------------------------- workspace
+// Grow-only device arena per host thread (and device). Content never
+// outlives a call; geometry tables are cached separately.
+class Arena {
+    int device_ = -1;
+    char* base_ = nullptr;
+    size_t cap_ = 0;
+
+  public:
+    ~Arena() { release(); }
+    void release() {
+        if (base_) {
+            int prev = 0;
+            if (cudaGetDevice(&prev) == cudaSuccess) {
+                cudaSetDevice(device_);
+                cudaFree(base_);
+                cudaSetDevice(prev);
+            }
+        }
+        base_ = nullptr;
+        cap_ = 0;
+    }
+    char* reserve(size_t bytes) {
+        int dev = 0;
+        check(cudaGetDevice(&dev), "cudaGetDevice");
+        if (dev != device_ || bytes > cap_) {
+            release();
+            device_ = dev;
+            check(cudaMalloc(&base_, std::max<size_t>(bytes, 256)), "Waltz: cannot allocate device workspace");
+            cap_ = std::max<size_t>(bytes, 256);
+        }
+        return base_;
+    }
+};
+
+struct Carver {
+    char* base;
+    size_t used = 0;
+    template <class V> V* take(size_t count) {
+        used = (used + 255) & ~size_t(255);
+        V* p = reinterpret_cast<V*>(base ? base + used : nullptr);
+        used += std::max<size_t>(count, 1) * sizeof(V);
+        return p;
+    }
+};
+
+// ----------------------------------------------------------- Morton tables
+static uint32_t morton_rank(uint32_t x, uint32_t y, uint32_t z, uint32_t nx, uint32_t ny, uint32_t nz) {
+    uint32_t rank = 0;
+    while (nx > 1 || ny > 1 || nz > 1) {
+        const uint32_t lx = nx - nx / 2, ly = ny - ny / 2, lz = nz - nz / 2;
+        const bool ux = x >= lx, uy = y >= ly, uz = z >= lz;
+        const uint32_t hz = uz ? nz / 2 : lz, hy = uy ? ny / 2 : ly;
+        if (uz) rank += lz * nx * ny;
+        if (uy) rank += hz * ly * nx;
+        if (ux) rank += hz * hy * lx;
+        if (ux) x -= lx;
+        if (uy) y -= ly;
+        if (uz) z -= lz;
+        nx = ux ? nx / 2 : lx;
+        ny = hy;
+        nz = hz;
+    }
+    return rank;
+}
+
+// 8 slots x 256*bz entries; slot bits: short x edge, short y edge, short z
+// edge. forward: local row-major index -> rank; inverse: rank -> local index.
+static std::vector<uint16_t> morton_tables(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t bz, bool inverse) {
+    const uint32_t stride = 256 * bz;
+    std::vector<uint16_t> t(8 * stride, 0);
+    for (unsigned s = 0; s < 8; ++s) {
+        const uint32_t ex = (s & 1) ? nx % 16 : 16, ey = (s & 2) ? ny % 16 : 16, ez = (s & 4) ? nz % bz : bz;
+        for (uint32_t z = 0; z < ez; ++z)
+            for (uint32_t y = 0; y < ey; ++y)
+                for (uint32_t x = 0; x < ex; ++x) {
+                    const uint32_t local = (z * ey + y) * ex + x;
+                    const uint32_t r = morton_rank(x, y, z, ex, ey, ez);
+                    if (inverse) t[s * stride + r] = uint16_t(local);
+                    else t[s * stride + local] = uint16_t(r);
+                }
+    }
+    return t;
+}
+
+struct TableCache {
+    int device = -1;
+    uint32_t nx = 0, ny = 0, nz = 0, bz = 0;
+    bool inverse = false;
+    uint16_t* ptr = nullptr;
+    ~TableCache() {
+        if (ptr) cudaFree(ptr);
+    }
+    const uint16_t* get(uint32_t x, uint32_t y, uint32_t z, uint32_t b, bool inv, cudaStream_t stream) {
+        int dev = 0;
+        check(cudaGetDevice(&dev), "cudaGetDevice");
+        if (ptr && dev == device && x == nx && y == ny && z == nz && b == bz && inv == inverse) return ptr;
+        if (ptr && dev != device) ptr = nullptr; // belongs to another device's context; keep it alive
+        if (!ptr) check(cudaMalloc(&ptr, 8 * kChunk * sizeof(uint16_t)), "Waltz: cannot allocate Morton table");
+        const auto host = morton_tables(x, y, z, b, inv);
+        check(cudaMemcpyAsync(ptr, host.data(), host.size() * 2, cudaMemcpyHostToDevice, stream), "Morton table upload");
+        check(cudaStreamSynchronize(stream), "Morton table upload");
+        device = dev;
+        nx = x; ny = y; nz = z; bz = b; inverse = inv;
+        return ptr;
+    }
+};
+
+// ------------------------------------------------------------ level plans
+struct Geometry {
+    uint32_t nx, ny, nz;
+    uint64_t n;
+    unsigned lxy, lz, bz;
+    bool dyadic;
+    Dims dyad[5], xyl[5], zl[5];
+    static Geometry make(uint32_t nx, uint32_t ny, uint32_t nz) {
+        Geometry g{};
+        g.nx = nx; g.ny = ny; g.nz = nz;
+        g.n = uint64_t(nx) * ny * nz;
+        g.lxy = levels_of(std::min(nx, ny));
+        g.lz = levels_of(nz);
+        g.dyadic = g.lxy == g.lz;
+        g.bz = zband_of(nx, ny, nz, g.lz, g.dyadic);
+        Dims a{nx, ny, nz};
+        for (unsigned l = 0; l < 5; ++l) {
+            g.dyad[l] = a;
+            a = {half_len(a.x), half_len(a.y), half_len(a.z)};
+        }
+        a = {nx, ny, nz};
+        for (unsigned l = 0; l < 5; ++l) {
+            g.xyl[l] = a;
+            a = {half_len(a.x), half_len(a.y), a.z};
+        }
+        a = {nx, ny, nz};
+        for (unsigned l = 0; l < 5; ++l) {
+            g.zl[l] = a;
+            a = {a.x, a.y, half_len(a.z)};
+        }
+        return g;
+    }
+    uint8_t flags(unsigned width) const { return uint8_t((dyadic ? 1 : 0) | (width == 8 ? 4 : 0) | (3u << 3)); }
+};
+
+__host__ __device__ inline uint64_t vol(Dims d) { return uint64_t(d.x) * d.y * d.z; }
+static inline Dims halve(Dims d, int mask) {
+    return {(mask & AX) ? half_len(d.x) : d.x, (mask & AY) ? half_len(d.y) : d.y, (mask & AZ) ? half_len(d.z) : d.z};
+}
+
+// Tile shapes per schedule (UX, UY, UZ).
+template <class T> struct Tiles;
+template <> struct Tiles<float> {
+    static constexpr int XYZ[3] = {32, 8, 16};
+    static constexpr int XY[3] = {32, 16, 4};
+    static constexpr int Z[3] = {32, 8, 16};
+};
+template <> struct Tiles<double> {
+    static constexpr int XYZ[3] = {16, 8, 8};
+    static constexpr int XY[3] = {32, 16, 4};
+    static constexpr int Z[3] = {32, 8, 8};
+};
+
+template <class T, bool Inverse, int Mask, int UX, int UY, int UZ, class Src, class Out>
+static void launch_level(const Src& src, Dims a, const Out& out, cudaStream_t stream) {
+    auto kernel = level_kernel<T, Inverse, Mask, UX, UY, UZ, Src, Out>;
+    constexpr size_t smem = level_smem<T, Inverse, Mask, UX, UY, UZ>();
+    static thread_local int configured_device = -1;
+    int dev = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (configured_device != dev) {
+        check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+              "level kernel shared memory");
+        configured_device = dev;
+    }
+    const Dims grid{(a.x + UX - 1) / UX, (a.y + UY - 1) / UY, (a.z + UZ - 1) / UZ};
+    const uint64_t blocks = uint64_t(grid.x) * grid.y * grid.z;
+    need(blocks < (1ull << 31), "Waltz: level grid too large");
+    kernel<<<unsigned(blocks), 256, smem, stream>>>(src, a, grid, out); note_launch();
+    check(cudaGetLastError(), "level kernel launch");
+}
+
+template <class T, bool Inverse, int Mask, class Src, class Out>
+static void level(const Src& src, Dims a, const Out& out, cudaStream_t stream) {
+    if constexpr (Mask == (AX | AY | AZ))
+        launch_level<T, Inverse, Mask, Tiles<T>::XYZ[0], Tiles<T>::XYZ[1], Tiles<T>::XYZ[2]>(src, a, out, stream);
+    else if constexpr (Mask == (AX | AY))
+        launch_level<T, Inverse, Mask, Tiles<T>::XY[0], Tiles<T>::XY[1], Tiles<T>::XY[2]>(src, a, out, stream);
+    else
+        launch_level<T, Inverse, Mask, Tiles<T>::Z[0], Tiles<T>::Z[1], Tiles<T>::Z[2]>(src, a, out, stream);
+}
+
+template <class T, class Out>
+__global__ void identity_kernel(const T* in, Dims d, Out out) {
+    const uint64_t n = vol(d);
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t x = uint32_t(i % d.x), y = uint32_t((i / d.x) % d.y), z = uint32_t(i / (uint64_t(d.x) * d.y));
+        out(x, y, z, in[i]);
+    }
+}
+
+static unsigned grid_for(uint64_t n, unsigned threads = 256) {
+    uint64_t b = (n + threads - 1) / threads;
+    return unsigned(std::min<uint64_t>(std::max<uint64_t>(b, 1), 148ull * 64));
+}
+
+// Scratch element counts for the forward and inverse transforms.
+struct TransformScratch {
+    uint64_t low;   // each of two compact ping-pong buffers
+    uint64_t inter; // full-size intermediate (plane schedule with both stages)
+};
+static TransformScratch scratch_need(const Geometry& g) {
+    TransformScratch s{1, 0};
+    if (g.dyadic) {
+        for (unsigned l = 0; l < g.lxy; ++l) s.low = std::max(s.low, vol(halve(g.dyad[l], AX | AY | AZ)));
+        for (unsigned l = 0; l < g.lxy; ++l) s.low = std::max(s.low, vol(g.dyad[l]) * (l > 0));
+    } else {
+        for (unsigned l = 0; l < g.lz; ++l) s.low = std::max(s.low, vol(halve(g.zl[l], AZ)));
+        for (unsigned l = 0; l < g.lxy; ++l) s.low = std::max(s.low, vol(halve(g.xyl[l], AX | AY)));
+        for (unsigned l = 1; l < g.lz; ++l) s.low = std::max(s.low, vol(g.zl[l]));
+        for (unsigned l = 1; l < g.lxy; ++l) s.low = std::max(s.low, vol(g.xyl[l]));
+        if (g.lz && g.lxy) s.inter = g.n;
+    }
+    return s;
+}
+
+// Forward all-level transform of `in` into the coefficient array C.
+template <class T>
+static void forward(const Geometry& g, const T* in, T* C, T* lowA, T* lowB, T* inter, uint32_t* status,
+                    cudaStream_t stream) {
+    const size_t sy = g.nx, sz = size_t(g.nx) * g.ny;
+    T* lows[2] = {lowA, lowB};
+    if (g.lxy == 0 && g.lz == 0) {
+        copy_finite_kernel<T><<<grid_for(g.n), 256, 0, stream>>>(in, C, g.n, status); note_launch();
+        check(cudaGetLastError(), "copy launch");
+        return;
+    }
+    check_finite_kernel<T><<<grid_for(g.n), 256, 0, stream>>>(in, g.n, status); note_launch();
+    check(cudaGetLastError(), "finite check launch");
+    StageClock& clock = stage_clock();
+    clock.mark("finite_check", stream);
+    if (g.dyadic) {
+        FwdSrc<T> src{in, sy, sz};
+        for (unsigned l = 0; l < g.lxy; ++l) {
+            const Dims a = g.dyad[l], lo = halve(a, AX | AY | AZ);
+            const bool last = l + 1 == g.lxy;
+            FwdOut<T> out{C, sy, sz, last ? nullptr : lows[l & 1], lo, a, AX | AY | AZ};
+            level<T, false, AX | AY | AZ>(src, a, out, stream);
+            if (l == 0) clock.mark("fwd_l0", stream);
+            src = FwdSrc<T>{lows[l & 1], lo.x, size_t(lo.x) * lo.y};
+        }
+        if (g.lxy > 1) clock.mark("fwd_coarse", stream);
+        return;
+    }
+    FwdSrc<T> src{in, sy, sz};
+    T* zdst = g.lxy ? inter : C;
+    for (unsigned l = 0; l < g.lz; ++l) {
+        const Dims a = g.zl[l], lo = halve(a, AZ);
+        const bool last = l + 1 == g.lz;
+        FwdOut<T> out{zdst, sy, sz, last ? nullptr : lows[l & 1], lo, a, AZ};
+        level<T, false, AZ>(src, a, out, stream);
+        src = FwdSrc<T>{lows[l & 1], lo.x, size_t(lo.x) * lo.y};
+    }
+    if (g.lz) clock.mark("fwd_z", stream);
+    if (g.lz) src = FwdSrc<T>{inter, sy, sz};
+    for (unsigned l = 0; l < g.lxy; ++l) {
+        const Dims a = g.xyl[l], lo = halve(a, AX | AY);
+        const bool last = l + 1 == g.lxy;
+        FwdOut<T> out{C, sy, sz, last ? nullptr : lows[l & 1], lo, a, AX | AY};
+        level<T, false, AX | AY>(src, a, out, stream);
+        src = FwdSrc<T>{lows[l & 1], lo.x, size_t(lo.x) * lo.y};
+    }
+    if (g.lxy) clock.mark("fwd_xy", stream);
+}
+
+// Largest compact low band the inverse keeps between two levels of one stage.
+static uint64_t inverse_low_need(const Geometry& g) {
+    uint64_t m = 0;
+    if (g.dyadic) {
+        for (unsigned l = 1; l < g.lxy; ++l) m = std::max(m, vol(g.dyad[l]));
+    } else {
+        for (unsigned l = 1; l < g.lxy; ++l) m = std::max(m, vol(g.xyl[l]));
+    }
+    return m;
+}
+
+// Inverse all-level transform within three banks of n samples: C (the
+// coefficients, clobbered by the plane schedule once its XY stage is done),
+// bank1 and bank2. Dyadic and XY-stage low bands ping-pong between the two
+// halves of bank2; the plane schedule's XY output goes to bank1 and its Z
+// stage ping-pongs between bank2 and the freed C (or bank1). The finest level
+// hands every sample to `fin`.
+template <class T, class Final>
+static void inverse(const Geometry& g, T* C, T* bank1, T* bank2, const Final& fin, cudaStream_t stream,
+                    const char* final_stage = "inv_l0") {
+    StageClock& clock = stage_clock();
+    const size_t sy = g.nx, sz = size_t(g.nx) * g.ny;
+    const uint64_t half_off = ((g.n + 1) / 2 + 63) & ~uint64_t(63);
+    need(inverse_low_need(g) <= g.n - std::min(g.n, half_off), "Waltz: inverse scratch layout");
+    T* halves[2] = {bank2, bank2 + half_off};
+    if (g.lxy == 0 && g.lz == 0) {
+        identity_kernel<T, Final><<<grid_for(g.n), 256, 0, stream>>>(C, Dims{g.nx, g.ny, g.nz}, fin); note_launch();
+        check(cudaGetLastError(), "identity launch");
+        return;
+    }
+    if (g.dyadic) {
+        const T* low = nullptr;
+        for (int l = int(g.lxy) - 1; l >= 0; --l) {
+            const Dims a = g.dyad[l];
+            InvSrc<T> src{C, sy, sz, low, halve(a, AX | AY | AZ)};
+            if (l > 0) {
+                T* dst = halves[l & 1];
+                level<T, true, AX | AY | AZ>(src, a, StoreOut<T>{dst, a.x, size_t(a.x) * a.y}, stream);
+                low = dst;
+                if (l == 1) clock.mark("inv_coarse", stream);
+            } else {
+                level<T, true, AX | AY | AZ>(src, a, fin, stream);
+                clock.mark(final_stage, stream);
+            }
+        }
+        return;
+    }
+    const T* zbase = C;
+    T* zping[2] = {bank2, bank1};
+    if (g.lxy) {
+        const T* low = nullptr;
+        for (int l = int(g.lxy) - 1; l >= 0; --l) {
+            const Dims a = g.xyl[l];
+            InvSrc<T> src{C, sy, sz, low, halve(a, AX | AY)};
+            if (l > 0) {
+                T* dst = halves[l & 1];
+                level<T, true, AX | AY>(src, a, StoreOut<T>{dst, a.x, size_t(a.x) * a.y}, stream);
+                low = dst;
+            } else if (g.lz) {
+                level<T, true, AX | AY>(src, a, StoreOut<T>{bank1, sy, sz}, stream);
+                zbase = bank1;
+                zping[1] = C; // the coefficients are no longer read
+            } else {
+                level<T, true, AX | AY>(src, a, fin, stream);
+            }
+        }
+        clock.mark("inv_xy", stream);
+    }
+    if (g.lz) {
+        const T* low = nullptr;
+        for (int l = int(g.lz) - 1; l >= 0; --l) {
+            const Dims a = g.zl[l];
+            InvSrc<T> src{zbase, sy, sz, low, halve(a, AZ)};
+            if (l > 0) {
+                T* dst = zping[l & 1];
+                level<T, true, AZ>(src, a, StoreOut<T>{dst, a.x, size_t(a.x) * a.y}, stream);
+                low = dst;
+            } else {
+                level<T, true, AZ>(src, a, fin, stream);
+            }
+        }
+        clock.mark("inv_z", stream);
+    }
+}
+
+size_t capacity_for(uint64_t n, unsigned width) {
+    const uint64_t pwe = std::min<uint64_t>(n, 1ull << 22), qout = std::min<uint64_t>(n, 1ull << 20);
+    return size_t(n * width + pwe * (4 + width) + qout * 8 + (1ull << 20));
+}
+
+static thread_local Arena t_arena;
+static thread_local TableCache t_fwd_tables, t_inv_tables;
+static thread_local uint64_t* t_pinned = nullptr; // small pinned readback slots
+
+static uint64_t* pinned() {
+    if (!t_pinned) check(cudaMallocHost(&t_pinned, 64 * sizeof(uint64_t)), "pinned readback");
+    return t_pinned;
+}
+
+struct EncodeOptions {
+    uint32_t spin_cap = 1u << 22;
+    uint32_t skip_publish = 0xffffffffu;
+};
+
+// ------------------------------------------------------------------ encode
+template <class T>
+static size_t compress(const T* d_in, uint32_t nx, uint32_t ny, uint32_t nz, double eb, uint8_t* d_out,
+                       size_t capacity, cudaStream_t stream, const EncodeOptions& opt = EncodeOptions()) {
+    need(nx && ny && nz, "Waltz: nonzero dimensions required");
+    const uint64_t n = uint64_t(nx) * ny * nz;
+    need(n <= 0xffffffffull / sizeof(T), "Waltz: volume exceeds the archive section limits");
+    need(d_in && d_out, "Waltz: null buffer");
+    const double quantum = 1.5 * eb;
+    const T q = T(quantum), inv = T(1.0 / quantum);
+    need(eb > 0 && std::isfinite(eb) && std::isfinite(quantum) && q > T(0) && std::isfinite(q) && std::isfinite(inv),
+         "Waltz: invalid bound (positive finite, representable quantum required)");
+    {
+        const uintptr_t a = reinterpret_cast<uintptr_t>(d_in), b = reinterpret_cast<uintptr_t>(d_out);
+        need(!(a < b + capacity && b < a + n * sizeof(T)), "Waltz: input and output buffers overlap");
+    }
+    need(capacity >= 32 + wzp_header(uint32_t(n)), "Waltz: archive capacity too small");
+    const Geometry g = Geometry::make(nx, ny, nz);
+    const TransformScratch ts = scratch_need(g);
+    const uint32_t chunks = wzp_chunks(uint32_t(n));
+    const uint64_t words = (n + 31) / 32;
+    const uint64_t cblocks = (words + kCompactWords - 1) / kCompactWords;
+
+    Carver cv{nullptr};
+    auto plan = [&](Carver& c) {
+        struct P {
+            T *C, *lowA, *lowB, *inter, *bank2, *perr;
+            uint16_t* mag;
+            uint32_t *sign, *qbits, *qval, *pbits, *status, *ticket, *counts_p, *counts_q, *np, *nq;
+            uint64_t *state, *sizes, *wzp_total, *layout;
+        } p;
+        p.C = c.take<T>(n);
+        p.lowA = c.take<T>(ts.low);
+        p.lowB = c.take<T>(ts.low);
+        p.inter = c.take<T>(n);
+        p.bank2 = c.take<T>(n);
+        p.perr = c.take<T>(n);
+        p.mag = c.take<uint16_t>(n + 8);
+        p.sign = c.take<uint32_t>(words + 1);
+        p.qbits = c.take<uint32_t>(words + 1);
+        p.qval = c.take<uint32_t>(n);
+        p.pbits = c.take<uint32_t>(words + 1);
+        p.status = c.take<uint32_t>(1);
+        p.ticket = c.take<uint32_t>(1);
+        p.counts_p = c.take<uint32_t>(cblocks);
+        p.counts_q = c.take<uint32_t>(cblocks);
+        p.np = c.take<uint32_t>(1);
+        p.nq = c.take<uint32_t>(1);
+        p.state = c.take<uint64_t>(chunks);
+        p.sizes = c.take<uint64_t>(chunks);
+        p.wzp_total = c.take<uint64_t>(1);
+        p.layout = c.take<uint64_t>(8);
+        return p;
+    };
+    plan(cv);
+    Carver real{t_arena.reserve(cv.used)};
+    auto P = plan(real);
+    const uint16_t* rank = t_fwd_tables.get(nx, ny, nz, g.bz, false, stream);
+
+    check(cudaMemsetAsync(P.sign, 0, (words + 1) * 4, stream), "memset");
+    check(cudaMemsetAsync(P.qbits, 0, (words + 1) * 4, stream), "memset");
+    check(cudaMemsetAsync(P.pbits, 0, (words + 1) * 4, stream), "memset");
+    check(cudaMemsetAsync(P.status, 0, 4, stream), "memset");
+    check(cudaMemsetAsync(P.ticket, 0, 4, stream), "memset");
+    check(cudaMemsetAsync(P.state, 0, size_t(chunks) * 8, stream), "memset");
+
+    StageClock& clock = stage_clock();
+    clock.begin(stream);
+    // 1. forward transform
+    forward<T>(g, d_in, P.C, P.lowA, P.lowB, P.inter, P.status, stream);
+    // 2. quantisation + Morton reorder
+    {
+        QuantArgs<T> qa{P.C, Bricks::make(nx, ny, nz, g.bz), rank, q, inv, P.mag, P.sign, P.qbits, P.qval, P.status};
+        const uint64_t bricks = qa.b.count();
+        need(bricks < (1ull << 31), "Waltz: brick grid too large");
+        quantize_kernel<T><<<unsigned(bricks), kQuantThreads, 0, stream>>>(qa); note_launch();
+        check(cudaGetLastError(), "quantize launch");
+    }
+    clock.mark("quantize", stream);
+    // 3. WZP encode straight into the archive
+    {
+        static thread_local int cfg_dev = -1;
+        int dev = 0;
+        check(cudaGetDevice(&dev), "cudaGetDevice");
+        if (cfg_dev != dev) {
+            check(cudaFuncSetAttribute(wzp_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(sizeof(WzpEncodeSmem))), "wzp smem");
+            cfg_dev = dev;
+        }
+        WzpEncodeArgs wa{P.mag, P.sign, uint32_t(n), d_out + 32, capacity - 32, P.ticket, P.state, P.sizes,
+                         P.status, opt.spin_cap, opt.skip_publish};
+        wzp_encode_kernel<<<chunks, kWzpThreads, sizeof(WzpEncodeSmem), stream>>>(wa); note_launch();
+        check(cudaGetLastError(), "wzp encode launch");
+        const uint32_t groups = wzp_groups(uint32_t(n));
+        wzp_directory_kernel<<<(groups + 255) / 256, 256, 0, stream>>>(d_out + 32, uint32_t(n), P.state, P.sizes,
+                                                                       P.wzp_total); note_launch();
+        check(cudaGetLastError(), "wzp directory launch");
+    }
+    clock.mark("wzp_encode", stream);
+    // 4. inverse transform + repairs
+    {
+        RepairOut<T> fin{d_in, nx, size_t(nx) * ny, eb, T(eb), P.pbits, P.perr, P.status};
+        inverse<T>(g, P.C, P.inter, P.bank2, fin, stream, "inv_l0_repair");
+    }
+    // 5. ordered side records
+    compact_count_kernel<<<unsigned(cblocks), kCompactThreads, 0, stream>>>(P.pbits, words, P.counts_p); note_launch();
+    compact_count_kernel<<<unsigned(cblocks), kCompactThreads, 0, stream>>>(P.qbits, words, P.counts_q); note_launch();
+    compact_scan_kernel<<<1, kCompactThreads, 0, stream>>>(P.counts_p, uint32_t(cblocks), P.np); note_launch();
+    compact_scan_kernel<<<1, kCompactThreads, 0, stream>>>(P.counts_q, uint32_t(cblocks), P.nq); note_launch();
+    layout_kernel<<<1, 32, 0, stream>>>(d_out, capacity, P.wzp_total, P.np, P.nq, sizeof(T), g.flags(sizeof(T)),
+                                        uint8_t(g.lxy), uint8_t(g.lz), uint8_t(g.bz), quantum, P.layout); note_launch();
+    compact_write_kernel<T><<<unsigned(cblocks), kCompactThreads, 0, stream>>>(P.pbits, words, P.counts_p, P.perr,
+                                                                               d_out, P.layout, 0, 1, n); note_launch();
+    compact_write_kernel<uint32_t><<<unsigned(cblocks), kCompactThreads, 0, stream>>>(P.qbits, words, P.counts_q,
+                                                                                      P.qval, d_out, P.layout, 2, 3, n); note_launch();
+    check(cudaGetLastError(), "side record launch");
+    clock.mark("side_records", stream);
+    uint64_t* h = pinned();
+    check(cudaMemcpyAsync(h, P.layout, 8 * 8, cudaMemcpyDeviceToHost, stream), "readback");
+    check(cudaMemcpyAsync(h + 8, P.status, 4, cudaMemcpyDeviceToHost, stream), "readback");
+    check(cudaStreamSynchronize(stream), "compress");
+    const uint32_t status = uint32_t(h[8]);
+    const uint64_t np = h[5], nq = h[6];
+    if (status & ST_NONFINITE_INPUT) throw Error("nonfinite input is unsupported");
+    if (status & ST_QUANT_DOMAIN) throw Error("coefficient exceeds portable integer conversion domain");
+    if (status & ST_BOUND) throw Error("native repair cannot meet strict bound or nonfinite reconstruction");
+    if (status & ST_LOOKBACK_TIMEOUT) throw Error("Waltz: WZP lookback wait exceeded its bound");
+    if (status & ST_CAPACITY) throw Error("archive capacity too small");
+    if ((n > (1u << 20) && nq >= (1u << 20)) || (n > (1u << 22) && np >= (1u << 22)))
+        throw Error("portable GPU side-channel capacity reached");
+    if (h[7]) throw Error("archive capacity too small");
+    return size_t(h[4]);
+}
+
+// ------------------------------------------------------------------ decode
+struct Header {
+    uint8_t flags, lxy, lz, bz;
+    uint32_t pwe_bytes;
+    double q;
+    uint64_t wzp;
+    uint32_t np, nq;
+    static Header parse(const uint8_t* p) {
+        Header h;
+        h.flags = p[0]; h.lxy = p[1]; h.lz = p[2]; h.bz = p[3];
+        std::memcpy(&h.pwe_bytes, p + 4, 4);
+        std::memcpy(&h.q, p + 8, 8);
+        std::memcpy(&h.wzp, p + 16, 8);
+        std::memcpy(&h.np, p + 24, 4);
+        std::memcpy(&h.nq, p + 28, 4);
+        return h;
+    }
+};
+
+struct Layout {
+    uint64_t pi, pv, qi, qv, end;
+};
+
+// Header checks of the reference CPU decoder (cpu/src/codec.cpp:276-293);
+// `canonical` adds the exact-profile checks of src/waltz.cu:631-646.
+template <class T>
+static Layout validate_header(const Header& h, const Geometry& g, size_t bytes, bool canonical) {
+    const uint64_t n = g.n;
+    need(bytes >= 32, "invalid Waltz archive header");
+    need(!(h.flags & 0xe0) && (h.flags & 0x18) && ((h.flags & 4) ? 8u : 4u) == sizeof(T), "invalid Waltz archive header");
+    need(((h.flags >> 3) & 3) == 3, "unsupported Waltz synthesis mode");
+    need(!(h.flags & 2), "compact repair archives are not supported by this decoder");
+    const bool dyadic = h.flags & 1;
+    need(h.lxy <= 5 && h.lz <= 5 && h.bz >= 1 && h.bz <= 32 && !(dyadic && h.lxy != h.lz), "invalid levels or z band");
+    need(h.lxy == g.lxy && h.lz == g.lz, "dimensions/levels mismatch");
+    const T q = T(h.q);
+    need(h.q > 0 && std::isfinite(h.q) && q > T(0) && std::isfinite(q), "invalid quantum");
+    need(h.np <= n && h.nq <= n, "invalid section counts");
+    need(h.wzp <= (uint64_t(1) << 60), "Waltz archive size overflow");
+    Layout L;
+    L.pi = 32 + pad8(h.wzp);
+    L.pv = L.pi + pad8(uint64_t(h.np) * 4);
+    L.qi = L.pv + pad8(h.pwe_bytes);
+    L.qv = L.qi + pad8(uint64_t(h.nq) * 4);
+    L.end = L.qv + pad8(uint64_t(h.nq) * 4);
+    need(L.end == bytes, "truncated archive or trailing data");
+    need(uint64_t(h.pwe_bytes) == uint64_t(h.np) * sizeof(T), "invalid native correction section");
+    need(h.wzp >= wzp_header(uint32_t(n)) && h.wzp <= wzp_max_bytes(uint32_t(n)), "WZP archive size is outside its valid bounds");
+    need(h.bz == g.bz, "invalid Waltz reorder z-band");
+    if (canonical) {
+        need(h.flags == g.flags(sizeof(T)) && dyadic == g.dyadic, "invalid canonical Waltz chunk shape, header or length");
+    }
+    need(dyadic == g.dyadic, "dimensions/levels mismatch");
+    return L;
+}
+
+// Directory check: group spans must tile the payload exactly. The fast path
+// verifies canonical (increasing) order on the device; anything else is
+// checked on the host like cpu/src/wzp_cpu.cpp:720-761.
+__global__ void directory_check_kernel(const uint8_t* in, uint32_t n, uint64_t payload, uint32_t* status) {
+    __shared__ uint32_t tmp[40];
+    const uint32_t chunks = wzp_chunks(n), groups = wzp_groups(n);
+    const uint8_t* meta = in + size_t(groups) * 4;
+    uint64_t carry = 0;
+    uint32_t st = 0;
+    for (uint32_t base = 0; base < groups; base += 256) {
+        const uint32_t g = base + threadIdx.x;
+        uint32_t len = 0, off = 0;
+        if (g < groups) {
+            for (uint32_t c = g * kGroup; c < min(chunks, (g + 1) * kGroup); ++c) {
+                const WzpChunkInfo ci = wzp_meta(load_u24(meta + size_t(c) * 3), min(kChunk, n - c * kChunk));
+                if (!ci.ok) st |= ST_BAD_STREAM;
+                len += ci.mbytes + ci.sbytes;
+            }
+            off = load_u32(in + size_t(g) * 4);
+            if (off > payload || len > payload - off || (!len && off)) st |= ST_BAD_STREAM;
+        }
+        uint32_t sum;
+        const uint32_t ex = block_excl_scan<256>(len, tmp, sum);
+        if (g < groups && len && uint64_t(off) != carry + ex) st |= ST_DIRECTORY;
+        carry += sum;
+    }
+    if (threadIdx.x == 0 && carry != payload) st |= ST_DIRECTORY;
+    if (st) atomicOr(status, st);
+}
+
+static void host_directory_check(const uint8_t* in, uint32_t n, uint64_t payload) {
+    const uint32_t chunks = wzp_chunks(n), groups = wzp_groups(n);
+    std::vector<std::pair<uint32_t, uint32_t>> spans;
+    for (uint32_t g = 0; g < groups; ++g) {
+        uint32_t len = 0;
+        for (uint32_t c = g * kGroup; c < std::min(chunks, (g + 1) * kGroup); ++c) {
+            const uint8_t* m = in + size_t(groups) * 4 + size_t(c) * 3;
+            const uint32_t meta = m[0] | (m[1] << 8) | (m[2] << 16);
+            const uint32_t count = std::min(kChunk, n - c * kChunk), code = meta & kRawCode, sc = meta >> 14;
+            if (!code) {
+                need(!sc, "WZP zero chunk carries sign metadata");
+                continue;
+            }
+            const bool raw = code == kRawCode;
+            need(raw || (code >= 4 && code + 2 < 2 * count), "WZP invalid compressed magnitude length");
+            const uint32_t sb = sc ? sc : 1024;
+            need(sb <= (count + 7) / 8, "WZP sign stream exceeds the chunk size");
+            len += (raw ? 2 * count : code) + sb;
+        }
+        uint32_t off;
+        std::memcpy(&off, in + size_t(g) * 4, 4);
+        need(off <= payload && len <= payload - off && (len || !off), "WZP directory range is outside the payload");
+        if (len) spans.push_back({off, len});
+    }
+    std::sort(spans.begin(), spans.end());
+    uint64_t cursor = 0;
+    for (auto& s : spans) {
+        need(s.first == cursor, "WZP payload groups overlap or leave a gap");
+        cursor += s.second;
+    }
+    need(cursor == payload, "WZP trailing or missing payload bytes");
+}
+
+// Decoder kernels of one archive, launched without synchronising. Scratch:
+// C, bank1, bank2 of n samples each and the inverse Morton table.
+template <class T, class Final, class Patch>
+static void decode_launch(const uint8_t* d_in, const Header& h, const Layout& L, const Geometry& g,
+                          const uint16_t* irank, T* C, T* bank1, T* bank2, const Final& fin, const Patch& patch,
+                          uint32_t* status, cudaStream_t stream) {
+    const uint32_t n = uint32_t(g.n);
+    const uint8_t* wzp = d_in + 32;
+    const uint64_t header = wzp_header(n);
+    StageClock& clock = stage_clock();
+    clock.begin(stream);
+    directory_check_kernel<<<1, 256, 0, stream>>>(wzp, n, h.wzp - header, status); note_launch();
+    {
+        static thread_local int cfg_dev = -1;
+        int dev = 0;
+        check(cudaGetDevice(&dev), "cudaGetDevice");
+        if (cfg_dev != dev) {
+            check(cudaFuncSetAttribute(wzp_decode_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(sizeof(WzpDecodeSmem))), "wzp smem");
+            check(cudaFuncSetAttribute(wzp_decode_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(sizeof(WzpDecodeSmem))), "wzp smem");
+            cfg_dev = dev;
+        }
+        WzpDecodeArgs<T> da{wzp, h.wzp, n, BrickMap{g.nx, g.ny, g.nz, g.bz, irank}, T(h.q), C, status};
+        wzp_decode_kernel<T><<<wzp_chunks(n), kWzpThreads, sizeof(WzpDecodeSmem), stream>>>(da); note_launch();
+        check(cudaGetLastError(), "wzp decode launch");
+    }
+    clock.mark("wzp_decode", stream);
+    if (h.nq)
+        qpatch_kernel<T><<<(h.nq + 255) / 256, 256, 0, stream>>>(d_in + L.qi, d_in + L.qv, h.nq, g.n, T(h.q), C,
+                                                                 status); note_launch();
+    clock.mark("qpatch", stream);
+    inverse<T>(g, C, bank1, bank2, fin, stream);
+    if (h.np)
+        rpatch_kernel<T, Patch><<<(h.np + 255) / 256, 256, 0, stream>>>(d_in + L.pi, d_in + L.pv, h.np, g.n, patch,
+                                                                        status); note_launch();
+    check(cudaGetLastError(), "decode launch");
+    clock.mark("rpatch", stream);
+}
+
+// Status word -> exception, with the exact checks that need the host: a
+// non-canonical WZP directory order and unordered side-record lists.
+template <class T>
+static void decode_finish(uint32_t status, const uint8_t* d_in, const Header& h, const Layout& L, const Geometry& g,
+                          uint32_t* d_status, uint32_t* seen, cudaStream_t stream) {
+    uint64_t* pin = pinned();
+    const uint64_t header = wzp_header(uint32_t(g.n));
+    if (status & ST_DIRECTORY) {
+        std::vector<uint8_t> dir(header);
+        check(cudaMemcpy(dir.data(), d_in + 32, header, cudaMemcpyDeviceToHost), "directory readback");
+        host_directory_check(dir.data(), uint32_t(g.n), h.wzp - header);
+        status &= ~ST_DIRECTORY;
+    }
+    if (status & ST_UNORDERED) {
+        // Unsorted side records are valid when their indices are distinct.
+        const uint64_t words = (g.n + 31) / 32;
+        check(cudaMemsetAsync(d_status, 0, 4, stream), "memset");
+        for (int k = 0; k < 2; ++k) {
+            const uint32_t cnt = k ? h.nq : h.np;
+            if (cnt < 2) continue;
+            check(cudaMemsetAsync(seen, 0, (words + 1) * 4, stream), "memset");
+            duplicate_kernel<<<(cnt + 255) / 256, 256, 0, stream>>>(d_in + (k ? L.qi : L.pi), cnt, seen, d_status); note_launch();
+        }
+        check(cudaMemcpyAsync(pin + 9, d_status, 4, cudaMemcpyDeviceToHost, stream), "readback");
+        check(cudaStreamSynchronize(stream), "duplicate check");
+        status = (status & ~ST_UNORDERED) | uint32_t(pin[9]);
+    }
+    if (status & ST_BAD_STREAM) throw Error("malformed WZP stream");
+    if (status & ST_BAD_INDEX) throw Error("invalid or duplicate outlier index");
+    if (status & ST_BAD_QOUT) throw Error("invalid quantization outlier");
+    if (status & ST_BAD_REPAIR) throw Error("nonfinite correction");
+    if (status & ST_NONFINITE_INPUT) throw Error("nonfinite reconstruction");
+}
+
+template <class T>
+static void decompress(const uint8_t* d_in, size_t bytes, uint32_t nx, uint32_t ny, uint32_t nz, T* d_out,
+                       size_t out_bytes, cudaStream_t stream, bool canonical, const uint8_t* host_copy) {
+    need(nx && ny && nz, "Waltz: nonzero dimensions required");
+    const uint64_t n = uint64_t(nx) * ny * nz;
+    need(n <= 0xffffffffull / sizeof(T), "Waltz: volume exceeds the archive section limits");
+    need(d_in && d_out, "Waltz: null buffer");
+    need(out_bytes >= n * sizeof(T), "output capacity too small");
+    need(bytes >= 32, "invalid Waltz archive header");
+    {
+        const uintptr_t a = reinterpret_cast<uintptr_t>(d_in), b = reinterpret_cast<uintptr_t>(d_out);
+        need(!(a < b + n * sizeof(T) && b < a + bytes), "Waltz: input and output buffers overlap");
+    }
+    const Geometry g = Geometry::make(nx, ny, nz);
+    Header h;
+    uint64_t* pin = pinned();
+    if (host_copy) {
+        h = Header::parse(host_copy);
+    } else {
+        check(cudaMemcpyAsync(pin, d_in, 32, cudaMemcpyDeviceToHost, stream), "header readback");
+        check(cudaStreamSynchronize(stream), "header readback");
+        h = Header::parse(reinterpret_cast<const uint8_t*>(pin));
+    }
+    const Layout L = validate_header<T>(h, g, bytes, canonical);
+    const uint64_t words = (n + 31) / 32;
+    Carver cv{nullptr};
+    auto plan = [&](Carver& c) {
+        struct P {
+            T *C, *bank1, *bank2;
+            uint32_t *status, *seen;
+        } p;
+        p.C = c.take<T>(n);
+        p.bank1 = c.take<T>(n);
+        p.bank2 = c.take<T>(n);
+        p.status = c.take<uint32_t>(1);
+        p.seen = c.take<uint32_t>(words + 1);
+        return p;
+    };
+    plan(cv);
+    Carver real{t_arena.reserve(cv.used)};
+    auto P = plan(real);
+    const uint16_t* irank = t_inv_tables.get(nx, ny, nz, g.bz, true, stream);
+    check(cudaMemsetAsync(P.status, 0, 4, stream), "memset");
+    FinalOut<T> fin{d_out, nx, size_t(nx) * ny, P.status};
+    decode_launch<T>(d_in, h, L, g, irank, P.C, P.bank1, P.bank2, fin, RowPatch<T>{d_out}, P.status, stream);
+    check(cudaMemcpyAsync(pin + 8, P.status, 4, cudaMemcpyDeviceToHost, stream), "readback");
+    check(cudaStreamSynchronize(stream), "decompress");
+    decode_finish<T>(uint32_t(pin[8]), d_in, h, L, g, P.status, P.seen, stream);
+}
+
+template <class T>
+static void extrema(const T* d_in, uint64_t n, double* mn, double* mx, cudaStream_t stream) {
+    need(d_in && n, "extrema requires at least one element");
+    Carver cv{t_arena.reserve(256)};
+    auto* keys = cv.take<unsigned long long>(2);
+    const unsigned long long init[2] = {~0ull, 0ull};
+    uint64_t* pin = pinned();
+    std::memcpy(pin, init, 16);
+    check(cudaMemcpyAsync(keys, pin, 16, cudaMemcpyHostToDevice, stream), "extrema init");
+    extrema_kernel<T><<<grid_for(n, 256), 256, 0, stream>>>(d_in, n, keys); note_launch();
+    check(cudaGetLastError(), "extrema launch");
+    check(cudaMemcpyAsync(pin + 2, keys, 16, cudaMemcpyDeviceToHost, stream), "extrema readback");
+    check(cudaStreamSynchronize(stream), "extrema");
+    auto value = [](unsigned long long k) {
+        const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+        double d;
+        std::memcpy(&d, &b, 8);
+        return d;
+    };
+    *mn = value(pin[2]);
+    *mx = value(pin[3]);
+}
+
+static thread_local char t_error[256];
+static int fail(const std::exception& e) {
+    std::snprintf(t_error, sizeof(t_error), "%s", e.what());
+    return -1;
+}
+
+} // namespace wb
+
+using namespace wb;
+
+extern "C" {
+
+const char* waltz_b200_last_error(void) { return t_error; }
+
+size_t waltz_b200_compressed_capacity(uint64_t n, int width) {
+    if ((width != 4 && width != 8) || n > 0xffffffffull) return 0;
+    return capacity_for(n, unsigned(width));
+}
+
+int waltz_b200_compress(const void* d_input, int width, uint32_t nx, uint32_t ny, uint32_t nz, double abs_error,
+                        void* d_archive, size_t capacity, size_t* written, void* stream) {
+    try {
+        need(written != nullptr, "null argument");
+        *written = 0;
+        need(width == 4 || width == 8, "type must be FP32 or FP64");
+        auto s = reinterpret_cast<cudaStream_t>(stream);
+        auto* out = static_cast<uint8_t*>(d_archive);
+        *written = width == 4 ? compress(static_cast<const float*>(d_input), nx, ny, nz, abs_error, out, capacity, s)
+                              : compress(static_cast<const double*>(d_input), nx, ny, nz, abs_error, out, capacity, s);
+        t_error[0] = 0;
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+int waltz_b200_decompress(const void* d_archive, size_t bytes, int width, uint32_t nx, uint32_t ny, uint32_t nz,
+                          void* d_output, size_t output_bytes, void* stream) {
+    try {
+        need(width == 4 || width == 8, "type must be FP32 or FP64");
+        auto s = reinterpret_cast<cudaStream_t>(stream);
+        auto* in = static_cast<const uint8_t*>(d_archive);
+        if (width == 4) decompress(in, bytes, nx, ny, nz, static_cast<float*>(d_output), output_bytes, s, false, nullptr);
+        else decompress(in, bytes, nx, ny, nz, static_cast<double*>(d_output), output_bytes, s, false, nullptr);
+        t_error[0] = 0;
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+int waltz_b200_extrema(const void* d_input, int width, uint64_t n, double* min_out, double* max_out, void* stream) {
+    try {
+        need(min_out && max_out, "null argument");
+        need(width == 4 || width == 8, "type must be FP32 or FP64");
+        auto s = reinterpret_cast<cudaStream_t>(stream);
+        if (width == 4) extrema(static_cast<const float*>(d_input), n, min_out, max_out, s);
+        else extrema(static_cast<const double*>(d_input), n, min_out, max_out, s);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+const char* waltz_cuda_decode_chunk(uint32_t nx, uint32_t ny, uint32_t nz, int width, const void* archive,
+                                    size_t bytes, void* output, size_t out_bytes, void* stream) {
+    static std::mutex lock;
+    static thread_local char error[256];
+    try {
+        std::lock_guard<std::mutex> guard(lock);
+        need((width == 4 || width == 8) && nx && ny && nz && archive && output && bytes >= 32 &&
+                 uint64_t(nx) * ny <= 0xffffffffull / unsigned(width) / nz &&
+                 out_bytes == uint64_t(nx) * ny * nz * unsigned(width),
+             "invalid chunk dimensions or buffer sizes");
+        auto s = reinterpret_cast<cudaStream_t>(stream);
+        auto* in = static_cast<const uint8_t*>(archive);
+        if (width == 4) decompress(in, bytes, nx, ny, nz, static_cast<float*>(output), out_bytes, s, true, nullptr);
+        else decompress(in, bytes, nx, ny, nz, static_cast<double*>(output), out_bytes, s, true, nullptr);
+        return nullptr;
+    } catch (const std::exception& e) {
+        std::snprintf(error, sizeof(error), "%s", e.what());
+    }
+    (void)cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream));
+    return error;
+}
+
+} // extern "C"
+
+// Diagnostic stage entry points (declared in include/waltz_b200.h).
+extern "C" int waltz_b200_transform(void* d_data, int width, uint32_t nx, uint32_t ny, uint32_t nz, int inverse,
+                                    void* stream) {
+    try {
+        need(width == 4 || width == 8, "type must be FP32 or FP64");
+        need(nx && ny && nz && d_data, "invalid transform arguments");
+        auto s = reinterpret_cast<cudaStream_t>(stream);
+        const Geometry g = Geometry::make(nx, ny, nz);
+        const TransformScratch ts = scratch_need(g);
+        auto run = [&](auto* data) {
+            using T = std::remove_pointer_t<decltype(data)>;
+            Carver cv{nullptr};
+            auto plan = [&](Carver& c) {
+                struct P { T *C, *a, *b, *inter, *bank2; uint32_t* status; } p;
+                p.C = c.take<T>(g.n); p.a = c.take<T>(ts.low); p.b = c.take<T>(ts.low);
+                p.inter = c.take<T>(g.n); p.bank2 = c.take<T>(g.n); p.status = c.take<uint32_t>(1);
+                return p;
+            };
+            plan(cv);
+            Carver real{t_arena.reserve(cv.used)};
+            auto P = plan(real);
+            check(cudaMemsetAsync(P.status, 0, 4, s), "memset");
+            if (!inverse) {
+                forward<T>(g, data, P.C, P.a, P.b, P.inter, P.status, s);
+                check(cudaMemcpyAsync(data, P.C, g.n * sizeof(T), cudaMemcpyDeviceToDevice, s), "copy");
+            } else {
+                check(cudaMemcpyAsync(P.C, data, g.n * sizeof(T), cudaMemcpyDeviceToDevice, s), "copy");
+                wb::inverse<T>(g, P.C, P.inter, P.bank2, StoreOut<T>{data, nx, size_t(nx) * ny}, s);
+            }
+            check(cudaStreamSynchronize(s), "transform");
+        };
+        if (width == 4) run(static_cast<float*>(d_data));
+        else run(static_cast<double*>(d_data));
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+extern "C" int waltz_b200_wzp_encode(const uint16_t* d_mag, const uint32_t* d_sign, uint32_t n, void* d_out,
+                                     size_t capacity, size_t* written, void* stream) {
+    try {
+        need(written && d_mag && d_sign && d_out, "null argument");
+        need(n && n <= 0x7fffffffu, "WZP element count outside (0, 2^31)");
+        need(capacity >= wzp_header(n), "WZP output capacity is too small");
+        auto s = reinterpret_cast<cudaStream_t>(stream);
+        const uint32_t chunks = wzp_chunks(n);
+        Carver cv{nullptr};
+        auto plan = [&](Carver& c) {
+            struct P { uint32_t *status, *ticket; uint64_t *state, *sizes, *total; } p;
+            p.status = c.take<uint32_t>(1); p.ticket = c.take<uint32_t>(1);
+            p.state = c.take<uint64_t>(chunks); p.sizes = c.take<uint64_t>(chunks); p.total = c.take<uint64_t>(1);
+            return p;
+        };
+        plan(cv);
+        Carver real{t_arena.reserve(cv.used)};
+        auto P = plan(real);
+        check(cudaMemsetAsync(P.status, 0, 4, s), "memset");
+        check(cudaMemsetAsync(P.ticket, 0, 4, s), "memset");
+        check(cudaMemsetAsync(P.state, 0, size_t(chunks) * 8, s), "memset");
+        check(cudaFuncSetAttribute(wzp_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(sizeof(WzpEncodeSmem))), "wzp smem");
+        WzpEncodeArgs wa{d_mag, d_sign, n, static_cast<uint8_t*>(d_out), capacity, P.ticket, P.state, P.sizes,
+                         P.status, 1u << 22, 0xffffffffu};
+        wzp_encode_kernel<<<chunks, kWzpThreads, sizeof(WzpEncodeSmem), s>>>(wa); note_launch();
+        const uint32_t groups = wzp_groups(n);
+        wzp_directory_kernel<<<(groups + 255) / 256, 256, 0, s>>>(static_cast<uint8_t*>(d_out), n, P.state, P.sizes,
+                                                                  P.total); note_launch();
+        check(cudaGetLastError(), "wzp launch");
+        uint64_t* h = pinned();
+        check(cudaMemcpyAsync(h, P.total, 8, cudaMemcpyDeviceToHost, s), "readback");
+        check(cudaMemcpyAsync(h + 1, P.status, 4, cudaMemcpyDeviceToHost, s), "readback");
+        check(cudaStreamSynchronize(s), "wzp encode");
+        if (uint32_t(h[1]) & ST_CAPACITY) throw Error("WZP output capacity is too small");
+        if (uint32_t(h[1])) throw Error("WZP encode failed");
+        *written = size_t(h[0]);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+extern "C" unsigned long long waltz_b200_launch_count(void) { return launch_counter().load(); }
+
+extern "C" void waltz_b200_profile(int enable) { stage_clock().enabled = enable != 0; }
+
+extern "C" int waltz_b200_stage_times(double* ms, const char** names, int cap) {
+    const StageClock& c = stage_clock();
+    const int n = c.read(ms, cap);
+    for (int i = 0; i < n; ++i) names[i] = c.names[i];
+    return n;
+}
+
+// Test hook: compress with a bounded lookback cap and a chunk that never
+// publishes its state, to exercise the wait bound without a GPU fault.
+extern "C" int waltz_b200_test_lookback_timeout(const void* d_input, int width, uint32_t nx, uint32_t ny,
+                                                uint32_t nz, double abs_error, void* d_archive, size_t capacity,
+                                                uint32_t skip_chunk, uint32_t spin_cap, void* stream) {
+    try {
+        EncodeOptions opt;
+        opt.spin_cap = spin_cap;
+        opt.skip_publish = skip_chunk;
+        auto s = reinterpret_cast<cudaStream_t>(stream);
+        auto* out = static_cast<uint8_t*>(d_archive);
+        if (width == 4) compress(static_cast<const float*>(d_input), nx, ny, nz, abs_error, out, capacity, s, opt);
+        else compress(static_cast<const double*>(d_input), nx, ny, nz, abs_error, out, capacity, s, opt);
+        t_error[0] = 0;
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+#include "batch.cuh"

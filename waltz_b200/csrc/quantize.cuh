@@ -1,0 +1,349 @@
+// Uniform scalar quantisation fused with the block Morton reorder, and the
+// side-record kernels (ordered compaction, decode patches, extrema).
+#pragma once
+#include "common.cuh"
+#include "scan.cuh"
+
+namespace wb {
+
+// Brick grid of the coefficient array: 16 x 16 x bz bricks in raster order.
+struct Bricks {
+    uint32_t nx, ny, nz, bz;
+    uint32_t nbx, nby, nbz;
+    __host__ __device__ static Bricks make(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t bz) {
+        return {nx, ny, nz, bz, (nx + 15) / 16, (ny + 15) / 16, (nz + bz - 1) / bz};
+    }
+    __host__ __device__ uint64_t count() const { return uint64_t(nbx) * nby * nbz; }
+};
+
+// q = T(1.5 eb), inv = T(1 / (1.5 eb)); code = llrint(T(c * inv)) saturated to
+// +-INT32_MAX; the dequantised value T(+-|code|) * q replaces the coefficient
+// (cpu/src/codec.cpp:211-220). Magnitudes are clamped to 16 bits at their
+// Morton position; larger ones become q-outliers (index, magnitude).
+template <class T> struct QuantArgs {
+    T* coeff;                 // in: coefficients, out: dequantised values
+    Bricks b;
+    const uint16_t* rank;     // 8 slots x 256*bz: local row-major index -> rank
+    T q, inv;
+    uint16_t* mag;            // Morton-packed magnitudes
+    uint32_t* sign;           // Morton-packed sign bits (zeroed before launch)
+    uint32_t* qbits;          // row-major q-outlier bitmap (zeroed before launch)
+    uint32_t* qval;           // row-major q-outlier magnitudes (dense, sparse use)
+    uint32_t* status;
+};
+
+constexpr int kQuantThreads = 256;
+
+template <class T>
+__global__ void __launch_bounds__(kQuantThreads) quantize_kernel(QuantArgs<T> A) {
+    __shared__ uint16_t smag[kChunk];
+    __shared__ uint8_t ssign[kChunk];
+    const Bricks& B = A.b;
+    const uint64_t bi = blockIdx.x;
+    const uint32_t bxi = uint32_t(bi % B.nbx), byi = uint32_t((bi / B.nbx) % B.nby), bzi = uint32_t(bi / (uint64_t(B.nbx) * B.nby));
+    const uint32_t ex = min(16u, B.nx - bxi * 16), ey = min(16u, B.ny - byi * 16), ez = min(B.bz, B.nz - bzi * B.bz);
+    const uint32_t slot = (ex != 16) | ((ey != 16) << 1) | ((ez != B.bz) << 2);
+    const uint64_t plane = uint64_t(B.nx) * B.ny;
+    const uint64_t base = uint64_t(bzi) * B.bz * plane + uint64_t(byi) * 16 * B.nx * ez + uint64_t(bxi) * 16 * ey * ez;
+    const uint32_t size = ex * ey * ez;
+    const uint16_t* rank = A.rank + slot * 256 * B.bz;
+    uint32_t bad = 0;
+    for (uint32_t i = threadIdx.x; i < size; i += kQuantThreads) {
+        const uint32_t lx = i % ex, ly = (i / ex) % ey, lz = i / (ex * ey);
+        const uint64_t at = (uint64_t(bzi) * B.bz + lz) * plane + uint64_t(byi * 16 + ly) * B.nx + bxi * 16 + lx;
+        const T c = A.coeff[at];
+        const T scaled = Lift<T>::mul(c, A.inv);
+        int32_t m = 0;
+        bool neg = false;
+        if (!finite_bits(scaled) || fabs(double(scaled)) >= 9223372036854775808.0) {
+            bad = 1;
+        } else {
+            long long r;
+            if constexpr (sizeof(T) == 4) r = __float2ll_rn(scaled);
+            else r = __double2ll_rn(scaled);
+            neg = r < 0;
+            const unsigned long long m64 = neg ? (unsigned long long)(-r) : (unsigned long long)r;
+            m = m64 > 0x7fffffffull ? 0x7fffffff : int32_t(m64);
+        }
+        A.coeff[at] = m ? Lift<T>::mul(T(neg ? -m : m), A.q) : T(0);
+        const uint32_t rk = rank[i];
+        smag[rk] = uint16_t(m > 65535 ? 65535 : m);
+        ssign[rk] = neg && m;
+        if (m > 65535) {
+            atomicOr(&A.qbits[at >> 5], 1u << (at & 31));
+            A.qval[at] = uint32_t(m);
+        }
+    }
+    if (bad) atomicOr(A.status, ST_QUANT_DOMAIN);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < size; i += kQuantThreads) A.mag[base + i] = smag[i];
+    // sign words overlapping [base, base+size)
+    const uint64_t w0 = base >> 5, w1 = (base + size + 31) >> 5;
+    for (uint64_t w = w0 + threadIdx.x; w < w1; w += kQuantThreads) {
+        uint32_t bits = 0;
+        for (int k = 0; k < 32; ++k) {
+            const uint64_t p = w * 32 + k;
+            if (p >= base && p < base + size && ssign[p - base]) bits |= 1u << k;
+        }
+        if (bits) atomicOr(&A.sign[w], bits);
+    }
+}
+
+// Copy with a finiteness check (zero-level transform: coefficients = input).
+template <class T>
+__global__ void copy_finite_kernel(const T* in, T* out, uint64_t n, uint32_t* status) {
+    bool bad = false;
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        const T v = in[i];
+        bad |= !finite_bits(v);
+        out[i] = v;
+    }
+    if (bad) atomicOr(status, ST_NONFINITE_INPUT);
+}
+
+template <class T>
+__global__ void check_finite_kernel(const T* in, uint64_t n, uint32_t* status) {
+    bool bad = false;
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+        bad |= !finite_bits(in[i]);
+    if (bad) atomicOr(status, ST_NONFINITE_INPUT);
+}
+
+// Encoder repair emitter for the finest synthesis: err = T(value - orig);
+// a sample is patched iff |err| > T(eb); the corrected value must be finite
+// and strictly within eb of the original (cpu/src/repair_avx2.cpp:57-74).
+template <class T> struct RepairOut {
+    const T* orig;
+    size_t sy, sz;
+    double bound;
+    T nb;
+    uint32_t* pbits;  // row-major bitmap of patched samples
+    T* perr;          // dense errors (sparse use)
+    uint32_t* status;
+    __device__ __forceinline__ void operator()(uint32_t x, uint32_t y, uint32_t z, T v) const {
+        const size_t i = size_t(z) * sz + size_t(y) * sy + x;
+        const T o = orig[i];
+        const T err = Lift<T>::sub(v, o);
+        uint32_t st = 0;
+        if (!finite_bits(v) || !finite_bits(err)) st |= ST_BOUND;
+        T w = v;
+        if (fabs(double(err)) > double(nb)) {
+            atomicOr(&pbits[i >> 5], 1u << (i & 31));
+            perr[i] = err;
+            w = Lift<T>::sub(v, err);
+        }
+        if (!finite_bits(w) || !strictly_within(double(w), double(o), bound)) st |= ST_BOUND;
+        if (st) atomicOr(status, st);
+    }
+};
+
+// Decoder final store with the finiteness check fused in.
+template <class T> struct FinalOut {
+    T* dst;
+    size_t sy, sz;
+    uint32_t* status;
+    __device__ __forceinline__ void operator()(uint32_t x, uint32_t y, uint32_t z, T v) const {
+        dst[size_t(z) * sz + size_t(y) * sy + x] = v;
+        if (!finite_bits(v)) atomicOr(status, ST_NONFINITE_INPUT);
+    }
+};
+
+// ----------------------------------------------- ordered bitmap compaction
+// Set bits of a row-major bitmap, in ascending index order, become
+// (index, value) records: pass 1 counts per block, pass 2 scans the block
+// counts (single CTA), pass 3 writes. Ordered by construction, no sort.
+constexpr int kCompactThreads = 256;
+constexpr int kCompactWords = kCompactThreads * 4; // bitmap words per block
+
+__global__ void compact_count_kernel(const uint32_t* bits, uint64_t words, uint32_t* counts) {
+    __shared__ uint32_t tmp[40];
+    const uint64_t w0 = uint64_t(blockIdx.x) * kCompactWords + threadIdx.x * 4;
+    uint32_t c = 0;
+    for (int k = 0; k < 4; ++k)
+        if (w0 + k < words) c += __popc(bits[w0 + k]);
+    const uint32_t total = block_sum<kCompactThreads>(c, tmp);
+    if (threadIdx.x == 0) counts[blockIdx.x] = total;
+}
+
+// Exclusive scan of `count` block counts in place; writes the grand total.
+__global__ void compact_scan_kernel(uint32_t* counts, uint32_t count, uint32_t* total) {
+    __shared__ uint32_t tmp[40];
+    uint32_t carry = 0;
+    for (uint32_t base = 0; base < count; base += kCompactThreads) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t v = i < count ? counts[i] : 0;
+        uint32_t sum;
+        const uint32_t ex = block_excl_scan<kCompactThreads>(v, tmp, sum);
+        if (i < count) counts[i] = carry + ex;
+        carry += sum;
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+// Record sink: indices as u32 LE, values of `VB` bytes, both at device-side
+// offsets inside the archive (given by `layout`).
+template <class V>
+__global__ void compact_write_kernel(const uint32_t* bits, uint64_t words, const uint32_t* offsets,
+                                     const V* values, uint8_t* archive, const uint64_t* layout, int idx_slot,
+                                     int val_slot, uint64_t cap_records) {
+    __shared__ uint32_t tmp[40];
+    const uint64_t w0 = uint64_t(blockIdx.x) * kCompactWords + threadIdx.x * 4;
+    uint32_t wv[4];
+    uint32_t c = 0;
+    for (int k = 0; k < 4; ++k) {
+        wv[k] = w0 + k < words ? bits[w0 + k] : 0;
+        c += __popc(wv[k]);
+    }
+    uint32_t total;
+    uint32_t r = offsets[blockIdx.x] + block_excl_scan<kCompactThreads>(c, tmp, total);
+    if (layout[7]) return; // layout overflow: nothing is written
+    uint8_t* idx = archive + layout[idx_slot];
+    uint8_t* val = archive + layout[val_slot];
+    for (int k = 0; k < 4; ++k)
+        for (uint32_t b = wv[k]; b; b &= b - 1) {
+            const uint64_t i = (w0 + k) * 32 + (__ffs(b) - 1);
+            if (r < cap_records) {
+                const uint32_t ii = uint32_t(i);
+                idx[4 * uint64_t(r) + 0] = uint8_t(ii);
+                idx[4 * uint64_t(r) + 1] = uint8_t(ii >> 8);
+                idx[4 * uint64_t(r) + 2] = uint8_t(ii >> 16);
+                idx[4 * uint64_t(r) + 3] = uint8_t(ii >> 24);
+                const V v = values[i];
+                const uint8_t* vb = reinterpret_cast<const uint8_t*>(&v);
+                for (int j = 0; j < int(sizeof(V)); ++j) val[sizeof(V) * uint64_t(r) + j] = vb[j];
+            }
+            ++r;
+        }
+}
+
+// Archive layout from device-side counts. layout[]: 0 pi, 1 pv, 2 qi, 3 qv,
+// 4 end, 5 np, 6 nq, 7 overflow flag. Also writes the 32-byte header and
+// zeroes every padding byte between sections.
+__global__ void layout_kernel(uint8_t* archive, size_t capacity, const uint64_t* wzp_total, const uint32_t* np_p,
+                              const uint32_t* nq_p, uint32_t width, uint8_t flags, uint8_t lxy, uint8_t lz,
+                              uint8_t bz, double quantum, uint64_t* layout) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const uint64_t wb = *wzp_total; // includes the WZP header
+    const uint32_t np = *np_p, nq = *nq_p;
+    const uint64_t pi = 32 + pad8(wb);
+    const uint64_t pv = pi + pad8(uint64_t(np) * 4);
+    const uint64_t qi = pv + pad8(uint64_t(np) * width);
+    const uint64_t qv = qi + pad8(uint64_t(nq) * 4);
+    const uint64_t end = qv + pad8(uint64_t(nq) * 4);
+    layout[0] = pi;
+    layout[1] = pv;
+    layout[2] = qi;
+    layout[3] = qv;
+    layout[4] = end;
+    layout[5] = np;
+    layout[6] = nq;
+    layout[7] = end > capacity;
+    if (end > capacity) return;
+    archive[0] = flags;
+    archive[1] = lxy;
+    archive[2] = lz;
+    archive[3] = bz;
+    const uint32_t pb = np * width;
+    for (int k = 0; k < 4; ++k) archive[4 + k] = uint8_t(pb >> (8 * k));
+    uint64_t qb;
+    memcpy(&qb, &quantum, 8);
+    for (int k = 0; k < 8; ++k) archive[8 + k] = uint8_t(qb >> (8 * k));
+    for (int k = 0; k < 8; ++k) archive[16 + k] = uint8_t(wb >> (8 * k));
+    for (int k = 0; k < 4; ++k) archive[24 + k] = uint8_t(np >> (8 * k));
+    for (int k = 0; k < 4; ++k) archive[28 + k] = uint8_t(nq >> (8 * k));
+    // zero padding: after WZP, after each section
+    for (uint64_t p = 32 + wb; p < pi; ++p) archive[p] = 0;
+    for (uint64_t p = pi + uint64_t(np) * 4; p < pv; ++p) archive[p] = 0;
+    for (uint64_t p = pv + uint64_t(np) * width; p < qi; ++p) archive[p] = 0;
+    for (uint64_t p = qi + uint64_t(nq) * 4; p < qv; ++p) archive[p] = 0;
+    for (uint64_t p = qv + uint64_t(nq) * 4; p < end; ++p) archive[p] = 0;
+}
+
+// ------------------------------------------------------------ decode patches
+// Validates ascending/in-range indices (flags unordered lists for an exact
+// duplicate check) and patches q-outliers: coeff = +-T(v) * q with the sign of
+// the clamped value already in place.
+template <class T>
+__global__ void qpatch_kernel(const uint8_t* qi, const uint8_t* qv, uint32_t nq, uint64_t n, T q, T* coeff,
+                              uint32_t* status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nq) return;
+    uint32_t at, v, prev = 0;
+    memcpy(&at, qi + 4 * uint64_t(i), 4);
+    memcpy(&v, qv + 4 * uint64_t(i), 4);
+    if (i) memcpy(&prev, qi + 4 * uint64_t(i - 1), 4);
+    if (at >= n) { atomicOr(status, ST_BAD_INDEX); return; }
+    if (i && prev >= at) atomicOr(status, ST_UNORDERED);
+    if (v <= 65535u || v > 0x7fffffffu) { atomicOr(status, ST_BAD_QOUT); return; }
+    const T x = Lift<T>::mul(T(v), q);
+    coeff[at] = coeff[at] < T(0) ? -x : x;
+}
+
+// Repair patch targets: a row-major output, or a tile clipped into a frame.
+template <class T> struct RowPatch {
+    T* out;
+    __device__ __forceinline__ T* at(uint32_t i) const { return out + i; }
+};
+
+// Repair records: validate, then out[i] -= err (after synthesis).
+template <class T, class Patch>
+__global__ void rpatch_kernel(const uint8_t* pi, const uint8_t* pv, uint32_t np, uint64_t n, Patch patch,
+                              uint32_t* status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= np) return;
+    uint32_t at, prev = 0;
+    T err;
+    memcpy(&at, pi + 4 * uint64_t(i), 4);
+    memcpy(&err, pv + sizeof(T) * uint64_t(i), sizeof(T));
+    if (i) memcpy(&prev, pi + 4 * uint64_t(i - 1), 4);
+    if (at >= n) { atomicOr(status, ST_BAD_INDEX); return; }
+    if (i && prev >= at) atomicOr(status, ST_UNORDERED);
+    if (!finite_bits(err)) { atomicOr(status, ST_BAD_REPAIR); return; }
+    T* p = patch.at(at);
+    if (!p) return;
+    const T r = Lift<T>::sub(*p, err);
+    *p = r;
+    if (!finite_bits(r)) atomicOr(status, ST_NONFINITE_INPUT);
+}
+
+// Exact duplicate test of an unordered index list (test-and-set bitmap).
+__global__ void duplicate_kernel(const uint8_t* idx, uint32_t count, uint32_t* seen, uint32_t* status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    uint32_t at;
+    memcpy(&at, idx + 4 * uint64_t(i), 4);
+    const uint32_t old = atomicOr(&seen[at >> 5], 1u << (at & 31));
+    if (old & (1u << (at & 31))) atomicOr(status, ST_BAD_INDEX);
+}
+
+// ------------------------------------------------------------------ extrema
+// Min/max through order-preserving integer keys (sign-magnitude -> two's
+// complement style flip), one atomic pair per CTA.
+__device__ __forceinline__ unsigned long long order_key(double v) {
+    const unsigned long long b = __double_as_longlong(v);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double key_value(unsigned long long k) {
+    const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+    return __longlong_as_double(b);
+}
+
+template <class T>
+__global__ void extrema_kernel(const T* in, uint64_t n, unsigned long long* keys) {
+    double lo = 1.0 / 0.0, hi = -1.0 / 0.0;
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        const double v = double(in[i]);
+        lo = fmin(lo, v);
+        hi = fmax(hi, v);
+    }
+    for (int d = 16; d; d >>= 1) {
+        lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, d));
+        hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, d));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&keys[0], order_key(lo));
+        atomicMax(&keys[1], order_key(hi));
+    }
+}
+
+} // namespace wb

@@ -1,0 +1,600 @@
+// WZP magnitude/sign codec on the GPU.
+//
+// Stream format (byte-exact with cpu/src/wzp_cpu.cpp:769-867):
+//   [u32 LE group offset x groups][u24 LE metadata x chunks][payload]
+// 8192 magnitudes per chunk, 16 chunks per directory group. A nonzero chunk
+// stores its magnitude bytes (bit-plane transpose + zero/repetition
+// elimination, or verbatim when that is not at least 3 bytes smaller) and
+// then its compacted sign bits, one per nonzero magnitude, LSB first.
+//
+// Encoder: one CTA per chunk, chunks taken from a ticket counter so that
+// every chunk's predecessors are already resident; the payload offset is
+// found by decoupled lookback over per-chunk states and the chunk writes
+// straight into the archive. Every wait is bounded: a wait that hits its cap
+// records ST_LOOKBACK_TIMEOUT and the kernel still terminates.
+// Decoder: one CTA per chunk, fused with dequantisation and the inverse
+// Morton scatter into the row-major coefficient array.
+#pragma once
+#include "common.cuh"
+#include "scan.cuh"
+
+namespace wb {
+
+constexpr int kWzpThreads = 512;
+
+__device__ __forceinline__ void store_u24(uint8_t* p, uint32_t v) {
+    p[0] = uint8_t(v);
+    p[1] = uint8_t(v >> 8);
+    p[2] = uint8_t(v >> 16);
+}
+__device__ __forceinline__ uint32_t load_u24(const uint8_t* p) {
+    return uint32_t(p[0]) | (uint32_t(p[1]) << 8) | (uint32_t(p[2]) << 16);
+}
+__device__ __forceinline__ uint32_t load_u32(const uint8_t* p) {
+    return load_u24(p) | (uint32_t(p[3]) << 24);
+}
+__device__ __forceinline__ void store_u32(uint8_t* p, uint32_t v) {
+    store_u24(p, v);
+    p[3] = uint8_t(v >> 24);
+}
+
+// chunk lookback state: bits 62-63 flag, low 62 bits value
+constexpr uint64_t kAggregate = 1ull << 62;
+constexpr uint64_t kInclusive = 2ull << 62;
+constexpr uint64_t kValueMask = (1ull << 62) - 1;
+
+struct WzpEncodeSmem {
+    uint16_t m[kChunk];                // magnitudes
+    uint8_t planes[2 * kChunk];        // bit-plane transposed chunk
+    uint8_t enc[2 * kChunk];           // zero/repetition-eliminated bytes
+    uint8_t lv[2048 + 256 + 32 + 4];   // nonzero bitmap and its reductions
+    uint32_t sgn[kChunk / 32];         // compacted sign bits
+    uint32_t gcount[kChunk / 32];      // nonzero magnitudes per 32-group
+    uint32_t tmp[40];
+    uint32_t chunk, excl;
+};
+
+struct WzpEncodeArgs {
+    const uint16_t* mag;
+    const uint32_t* sign;
+    uint32_t n;
+    uint8_t* out;       // start of the WZP stream
+    size_t capacity;    // bytes available from `out`
+    uint32_t* ticket;   // zeroed before launch
+    uint64_t* state;    // per chunk, zeroed before launch
+    uint64_t* sizes;    // per chunk byte count (output)
+    uint32_t* status;
+    uint32_t spin_cap;  // lookback wait bound (iterations of ~0.5 us)
+    uint32_t skip_publish; // test hook: this chunk never publishes (0xffffffff = none)
+};
+
+__global__ void __launch_bounds__(kWzpThreads) wzp_encode_kernel(WzpEncodeArgs A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    WzpEncodeSmem& S = *reinterpret_cast<WzpEncodeSmem*>(smem_raw);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = kWzpThreads / 32;
+    const uint32_t chunks = wzp_chunks(A.n), groups = wzp_groups(A.n);
+    if (tid == 0) S.chunk = atomicAdd(A.ticket, 1u);
+    __syncthreads();
+    const uint32_t c = S.chunk;
+    if (c >= chunks) return;
+    const uint32_t first = c * kChunk;
+    const uint32_t count = min(kChunk, A.n - first);
+    const uint32_t blocks = count / 16;
+
+    // ---- magnitudes (16-byte loads when the chunk is whole)
+    if (count == kChunk) {
+        const uint4* src = reinterpret_cast<const uint4*>(A.mag + first);
+        for (int i = tid; i < int(kChunk / 8); i += kWzpThreads) reinterpret_cast<uint4*>(S.m)[i] = src[i];
+    } else {
+        for (int i = tid; i < int(kChunk); i += kWzpThreads) S.m[i] = i < int(count) ? A.mag[first + i] : 0;
+    }
+    for (int i = tid; i < int(kChunk / 32); i += kWzpThreads) S.sgn[i] = 0;
+    __syncthreads();
+
+    // ---- per 32-group nonzero counts, bit planes (warp ballots)
+    for (int g = warp; g < int(kChunk / 32); g += NW) {
+        const int e = g * 32 + lane;
+        const uint32_t v = S.m[e];
+        const uint32_t nzmask = __ballot_sync(0xffffffffu, v != 0);
+        if (lane == 0) S.gcount[g] = __popc(nzmask);
+        if (uint32_t(g * 32) < blocks * 16) {
+            uint32_t mine = 0;
+#pragma unroll
+            for (int p = 0; p < 16; ++p) {
+                const uint32_t r = __brev(__ballot_sync(0xffffffffu, (v >> (15 - p)) & 1u));
+                if (lane == p) mine = r;
+            }
+            uint16_t* pl = reinterpret_cast<uint16_t*>(S.planes);
+            if (lane < 16) {
+                pl[lane * blocks + 2 * g] = uint16_t(mine >> 16);
+                if (uint32_t(2 * g + 1) < blocks) pl[lane * blocks + 2 * g + 1] = uint16_t(mine & 0xffffu);
+            }
+        }
+    }
+    // verbatim tail after the planes
+    for (uint32_t i = blocks * 16 + tid; i < count; i += kWzpThreads)
+        reinterpret_cast<uint16_t*>(S.planes)[i] = S.m[i];
+    __syncthreads();
+
+    // ---- signs: rank of every nonzero magnitude inside the chunk
+    uint32_t nnz;
+    {
+        const uint32_t gc = tid < int(kChunk / 32) ? S.gcount[tid] : 0;
+        const uint32_t gp = block_excl_scan<kWzpThreads>(gc, S.tmp, nnz);
+        __syncthreads();
+        if (tid < int(kChunk / 32)) S.gcount[tid] = gp; // now the group prefix
+        __syncthreads();
+    }
+    const uint32_t* natural = A.sign + (first >> 5);
+    for (int g = warp; g < int(kChunk / 32); g += NW) {
+        if (uint32_t(g * 32) >= count) break;
+        const int e = g * 32 + lane;
+        const uint32_t v = S.m[e];
+        const uint32_t nzmask = __ballot_sync(0xffffffffu, v != 0);
+        const uint32_t word = natural[g];
+        if (v != 0 && ((word >> lane) & 1u)) {
+            const uint32_t rank = S.gcount[g] + __popc(nzmask & ((1u << lane) - 1u));
+            atomicOr(&S.sgn[rank >> 5], 1u << (rank & 31));
+        }
+    }
+
+    // ---- zero elimination of the plane bytes
+    const uint32_t raw_bytes = 2 * count;
+    uint32_t nzb, c1 = 0, c2 = 0, c3 = 0;
+    {
+        const uint32_t b0 = tid * 32;
+        uint32_t bits = 0;
+        const uint4* q = reinterpret_cast<const uint4*>(S.planes + b0);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const uint4 w = q[h];
+            const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                const uint32_t byte = (ws[k >> 2] >> (8 * (k & 3))) & 0xffu;
+                const uint32_t at = b0 + h * 16 + k;
+                if (byte && at < raw_bytes) bits |= 1u << (h * 16 + k);
+            }
+        }
+        const uint32_t off = block_excl_scan<kWzpThreads>(__popc(bits), S.tmp, nzb);
+        uint32_t o = off;
+        for (uint32_t b = bits; b; b &= b - 1) {
+            const int k = __ffs(b) - 1;
+            if (o < 2 * kChunk) S.enc[o] = S.planes[b0 + k];
+            ++o;
+        }
+        S.lv[4 * tid + 0] = uint8_t(bits);
+        S.lv[4 * tid + 1] = uint8_t(bits >> 8);
+        S.lv[4 * tid + 2] = uint8_t(bits >> 16);
+        S.lv[4 * tid + 3] = uint8_t(bits >> 24);
+    }
+    __syncthreads();
+    // ---- repetition elimination: 2048 -> 256 -> 32 -> 4 bytes
+    {
+        // level 1: thread t < 256 owns bitmap bytes 8t..8t+7
+        uint32_t flags = 0, cnt = 0;
+        if (tid < 256) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int i = tid * 8 + k;
+                const uint8_t prev = i ? S.lv[i - 1] : 0;
+                if (S.lv[i] != prev) flags |= 1u << k;
+            }
+            cnt = __popc(flags);
+        }
+        uint32_t off = block_excl_scan<kWzpThreads>(cnt, S.tmp, c1);
+        if (tid < 256) {
+            for (uint32_t b = flags; b; b &= b - 1) {
+                const int k = __ffs(b) - 1;
+                const uint32_t o = nzb + off++;
+                if (o < 2 * kChunk) S.enc[o] = S.lv[tid * 8 + k];
+            }
+            S.lv[2048 + tid] = uint8_t(flags);
+        }
+        __syncthreads();
+        // level 2: warp 0, lane owns level-1 bytes 8l..8l+7
+        if (warp == 0) {
+            uint32_t f2 = 0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int i = lane * 8 + k;
+                const uint8_t prev = i ? S.lv[2048 + i - 1] : 0;
+                if (S.lv[2048 + i] != prev) f2 |= 1u << k;
+            }
+            const uint32_t n2 = __popc(f2);
+            const uint32_t inc = warp_incl_scan(n2);
+            c2 = __shfl_sync(0xffffffffu, inc, 31);
+            uint32_t o2 = inc - n2;
+            for (uint32_t b = f2; b; b &= b - 1) {
+                const int k = __ffs(b) - 1;
+                const uint32_t o = nzb + c1 + o2++;
+                if (o < 2 * kChunk) S.enc[o] = S.lv[2048 + lane * 8 + k];
+            }
+            S.lv[2048 + 256 + lane] = uint8_t(f2);
+            __syncwarp();
+            // level 3: lanes 0..3 own level-2 bytes 8l..8l+7
+            uint32_t f3 = 0;
+            if (lane < 4) {
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const int i = lane * 8 + k;
+                    const uint8_t prev = i ? S.lv[2048 + 256 + i - 1] : 0;
+                    if (S.lv[2048 + 256 + i] != prev) f3 |= 1u << k;
+                }
+            }
+            const uint32_t n3 = __popc(f3);
+            const uint32_t inc3 = warp_incl_scan(n3);
+            c3 = __shfl_sync(0xffffffffu, inc3, 31);
+            uint32_t o3 = inc3 - n3;
+            for (uint32_t b = f3; b; b &= b - 1) {
+                const int k = __ffs(b) - 1;
+                const uint32_t o = nzb + c1 + c2 + o3++;
+                if (o < 2 * kChunk) S.enc[o] = S.lv[2048 + 256 + lane * 8 + k];
+            }
+            if (lane < 4) {
+                const uint32_t o = nzb + c1 + c2 + c3 + lane;
+                if (o < 2 * kChunk) S.enc[o] = uint8_t(f3);
+            }
+            if (lane == 0) {
+                S.tmp[34] = c2;
+                S.tmp[35] = c3;
+            }
+        }
+        __syncthreads();
+        c2 = S.tmp[34];
+        c3 = S.tmp[35];
+    }
+    const uint32_t rze = nzb ? nzb + c1 + c2 + c3 + 4 : 0;
+    const bool raw = rze + 2 >= raw_bytes;
+    const uint32_t mbytes = raw ? raw_bytes : rze;
+    const uint32_t sbytes = (nnz + 7) / 8;
+    const uint64_t chunk_bytes = nnz ? uint64_t(mbytes) + sbytes : 0;
+
+    // ---- decoupled lookback (thread 0), bounded waits
+    if (tid == 0) {
+        uint64_t excl = 0;
+        const bool publish = c != A.skip_publish;
+        if (c == 0) {
+            if (publish) atomicExch(reinterpret_cast<unsigned long long*>(&A.state[0]),
+                                    (unsigned long long)(kInclusive | chunk_bytes));
+        } else {
+            if (publish) atomicExch(reinterpret_cast<unsigned long long*>(&A.state[c]),
+                                    (unsigned long long)(kAggregate | chunk_bytes));
+            int64_t j = int64_t(c) - 1;
+            while (j >= 0) {
+                uint64_t s;
+                uint32_t spins = 0;
+                for (;;) {
+                    s = *reinterpret_cast<volatile uint64_t*>(&A.state[j]);
+                    if (s >> 62) break;
+                    if (++spins >= A.spin_cap) break;
+                    __nanosleep(500);
+                }
+                if (!(s >> 62)) { // predecessor never published: give up, flag it
+                    atomicOr(A.status, ST_LOOKBACK_TIMEOUT);
+                    break;
+                }
+                excl += s & kValueMask;
+                if ((s >> 62) == 2) break;
+                --j;
+            }
+            if (publish) atomicExch(reinterpret_cast<unsigned long long*>(&A.state[c]),
+                                    (unsigned long long)(kInclusive | (excl + chunk_bytes)));
+        }
+        A.sizes[c] = chunk_bytes;
+        S.excl = uint32_t(excl);
+        const size_t header = size_t(groups) * 4 + size_t(chunks) * 3;
+        if (header + excl + chunk_bytes > A.capacity || excl + chunk_bytes > 0xffffffffull) {
+            atomicOr(A.status, ST_CAPACITY);
+            S.excl = 0xffffffffu;
+        }
+        const uint32_t meta = nnz ? ((raw ? kRawCode : mbytes) | ((sbytes == 1024 ? 0u : sbytes) << 14)) : 0u;
+        store_u24(A.out + size_t(groups) * 4 + size_t(c) * 3, meta);
+    }
+    __syncthreads();
+    if (!nnz || S.excl == 0xffffffffu) return;
+    uint8_t* dst = A.out + size_t(groups) * 4 + size_t(chunks) * 3 + S.excl;
+    const uint8_t* msrc = raw ? reinterpret_cast<const uint8_t*>(S.m) : S.enc;
+    for (uint32_t i = tid; i < mbytes; i += kWzpThreads) dst[i] = msrc[i];
+    const uint8_t* sb = reinterpret_cast<const uint8_t*>(S.sgn);
+    for (uint32_t i = tid; i < sbytes; i += kWzpThreads) dst[mbytes + i] = sb[i];
+}
+
+// Group directory: payload offset of the first byte of every nonempty group.
+__global__ void wzp_directory_kernel(uint8_t* out, uint32_t n, const uint64_t* state, const uint64_t* sizes,
+                                     uint64_t* total) {
+    const uint32_t chunks = wzp_chunks(n), groups = wzp_groups(n);
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= groups) return;
+    const uint32_t f = g * kGroup, l = min(f + kGroup, chunks) - 1;
+    const uint64_t start = (state[f] & kValueMask) - sizes[f];
+    const uint64_t end = state[l] & kValueMask;
+    store_u32(out + size_t(g) * 4, end > start ? uint32_t(start) : 0u);
+    if (g == groups - 1) *total = size_t(groups) * 4 + size_t(chunks) * 3 + end;
+}
+
+// ------------------------------------------------------------------ decode
+
+// Brick geometry of the Morton-packed stream (bricks of 16 x 16 x bz, raster
+// order z, y, x; edge bricks shrink): packed index -> row-major index.
+struct BrickMap {
+    uint32_t nx, ny, nz, bz;
+    const uint16_t* local; // 8 slots x 256*bz: rank -> local row-major index
+    __device__ __forceinline__ size_t rowmajor(uint64_t k) const {
+        const uint64_t plane = uint64_t(nx) * ny;
+        const uint64_t slab_sz = plane * bz;
+        const uint64_t slab = k / slab_sz;
+        uint64_t r = k - slab * slab_sz;
+        const uint32_t ez = min(uint64_t(bz), uint64_t(nz) - slab * bz);
+        const uint64_t row_sz = uint64_t(16) * nx * ez;
+        const uint64_t row = r / row_sz;
+        r -= row * row_sz;
+        const uint32_t ey = min(uint64_t(16), uint64_t(ny) - row * 16);
+        const uint64_t brick_sz = uint64_t(16) * ey * ez;
+        const uint64_t bxi = r / brick_sz;
+        const uint32_t rk = uint32_t(r - bxi * brick_sz);
+        const uint32_t ex = min(uint64_t(16), uint64_t(nx) - bxi * 16);
+        const uint32_t slot = (ex != 16) | ((ey != 16) << 1) | ((ez != bz) << 2);
+        const uint32_t loc = local[slot * 256 * bz + rk];
+        const uint32_t lx = loc % ex, ly = (loc / ex) % ey, lz = loc / (ex * ey);
+        return (slab * bz + lz) * plane + (row * 16 + ly) * uint64_t(nx) + bxi * 16 + lx;
+    }
+};
+
+struct WzpDecodeSmem {
+    uint16_t m[kChunk];
+    uint8_t planes[2 * kChunk];
+    uint8_t lv[2048 + 256 + 32 + 4];
+    uint32_t gprefix[kChunk / 32];
+    uint32_t tmp[40];
+    uint32_t off, mbytes, sbytes, raw, bad;
+};
+
+struct WzpChunkInfo {
+    uint32_t mbytes, sbytes;
+    bool raw, ok;
+};
+__device__ __forceinline__ WzpChunkInfo wzp_meta(uint32_t meta, uint32_t count) {
+    WzpChunkInfo r{0, 0, false, true};
+    const uint32_t code = meta & kRawCode, scode = meta >> 14;
+    if (!code) {
+        r.ok = scode == 0;
+        return r;
+    }
+    r.raw = code == kRawCode;
+    if (!r.raw && (code < 4 || code + 2 >= 2 * count)) r.ok = false;
+    r.sbytes = scode ? scode : 1024;
+    if (r.sbytes > (count + 7) / 8) r.ok = false;
+    r.mbytes = r.raw ? 2 * count : code;
+    return r;
+}
+
+template <class T> struct WzpDecodeArgs {
+    const uint8_t* in;  // start of the WZP stream
+    size_t bytes;       // stream length (header + payload)
+    uint32_t n;
+    BrickMap map;
+    T q;
+    T* coeff;           // row-major dequantised coefficients (output)
+    uint32_t* status;
+};
+
+template <class T>
+__global__ void __launch_bounds__(kWzpThreads) wzp_decode_kernel(WzpDecodeArgs<T> A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    WzpDecodeSmem& S = *reinterpret_cast<WzpDecodeSmem*>(smem_raw);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = kWzpThreads / 32;
+    const uint32_t chunks = wzp_chunks(A.n), groups = wzp_groups(A.n);
+    const uint32_t c = blockIdx.x;
+    const uint32_t first = c * kChunk, count = min(kChunk, A.n - first);
+    const size_t header = size_t(groups) * 4 + size_t(chunks) * 3;
+    const uint8_t* meta = A.in + size_t(groups) * 4;
+    const uint8_t* payload = A.in + header;
+    const size_t payload_bytes = A.bytes - header;
+
+    if (tid == 0) {
+        const uint32_t g = c / kGroup;
+        uint64_t off = load_u32(A.in + size_t(g) * 4);
+        bool ok = true;
+        for (uint32_t k = g * kGroup; k < c; ++k) {
+            const WzpChunkInfo ci = wzp_meta(load_u24(meta + size_t(k) * 3), min(kChunk, A.n - k * kChunk));
+            ok &= ci.ok;
+            off += ci.mbytes + ci.sbytes;
+        }
+        const WzpChunkInfo me = wzp_meta(load_u24(meta + size_t(c) * 3), count);
+        ok &= me.ok;
+        if (ok && off + me.mbytes + me.sbytes > payload_bytes) ok = false;
+        S.off = uint32_t(off);
+        S.mbytes = me.mbytes;
+        S.sbytes = me.sbytes;
+        S.raw = me.raw;
+        S.bad = !ok;
+        if (!ok) atomicOr(A.status, ST_BAD_STREAM);
+    }
+    __syncthreads();
+    if (S.bad) return;
+    const uint8_t* src = payload + S.off;
+    const uint32_t mbytes = S.mbytes, sbytes = S.sbytes;
+    const uint32_t raw_bytes = 2 * count;
+    const uint32_t blocks = count / 16;
+    bool bad = false;
+
+    if (mbytes == 0) {
+        for (int i = tid; i < int(kChunk); i += kWzpThreads) S.m[i] = 0;
+    } else if (S.raw) {
+        for (int i = tid; i < int(kChunk); i += kWzpThreads)
+            S.m[i] = i < int(count) ? uint16_t(src[2 * i] | (src[2 * i + 1] << 8)) : 0;
+    } else {
+        // ---- undo repetition elimination from the back of the stream
+        uint32_t pos = mbytes - 4;
+        uint8_t* L3 = S.lv + 2048 + 256 + 32;
+        uint8_t* L2 = S.lv + 2048 + 256;
+        uint8_t* L1 = S.lv + 2048;
+        uint8_t* L0 = S.lv;
+        if (tid < 4) L3[tid] = src[pos + tid];
+        __syncthreads();
+        // level 2 (32 bytes) from L3
+        if (warp == 0) {
+            const uint32_t mark = uint32_t(L3[0]) | (uint32_t(L3[1]) << 8) | (uint32_t(L3[2]) << 16) | (uint32_t(L3[3]) << 24);
+            const uint32_t cnt = __popc(mark);
+            const bool under = cnt > pos;
+            const uint32_t base = under ? 0 : pos - cnt;
+            const uint32_t rank = __popc(mark & ((2u << lane) - 1u)); // inclusive (lane 31 ok: 2u<<31 == 0)
+            const uint32_t r = lane == 31 ? cnt : rank;
+            uint8_t v = 0;
+            if (!under && r) v = src[base + r - 1];
+            if (!under && ((mark >> lane) & 1u)) {
+                const uint8_t prev = r > 1 ? src[base + r - 2] : 0;
+                if (v == prev) bad = true;
+            }
+            L2[lane] = v;
+            if (under) bad = true;
+            if (lane == 0) S.tmp[36] = base;
+        }
+        __syncthreads();
+        pos = S.tmp[36];
+        // level 1 (256 bytes) from L2
+        {
+            uint32_t bit = 0;
+            if (tid < 256) bit = (L2[tid >> 3] >> (tid & 7)) & 1u;
+            uint32_t cnt;
+            const uint32_t ex = block_excl_scan<kWzpThreads>(bit, S.tmp, cnt);
+            const bool under = cnt > pos;
+            const uint32_t base = under ? 0 : pos - cnt;
+            if (tid < 256) {
+                const uint32_t r = ex + bit;
+                uint8_t v = 0;
+                if (!under && r) v = src[base + r - 1];
+                if (!under && bit) {
+                    const uint8_t prev = r > 1 ? src[base + r - 2] : 0;
+                    if (v == prev) bad = true;
+                }
+                L1[tid] = v;
+            }
+            if (under) bad = true;
+            pos = base;
+        }
+        __syncthreads();
+        // level 0 (2048 bytes) from L1: four entries per thread
+        {
+            uint32_t bits4 = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int i = tid * 4 + k;
+                bits4 |= ((L1[i >> 3] >> (i & 7)) & 1u) << k;
+            }
+            uint32_t cnt;
+            const uint32_t ex = block_excl_scan<kWzpThreads>(__popc(bits4), S.tmp, cnt);
+            const bool under = cnt > pos;
+            const uint32_t base = under ? 0 : pos - cnt;
+            uint32_t r = ex;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const uint32_t bit = (bits4 >> k) & 1u;
+                r += bit;
+                uint8_t v = 0;
+                if (!under && r) v = src[base + r - 1];
+                if (!under && bit) {
+                    const uint8_t prev = r > 1 ? src[base + r - 2] : 0;
+                    if (v == prev) bad = true;
+                }
+                L0[tid * 4 + k] = v;
+            }
+            if (under) bad = true;
+            pos = base;
+        }
+        __syncthreads();
+        // nonzero bytes: 32 per thread
+        {
+            const uint32_t bits = uint32_t(L0[4 * tid]) | (uint32_t(L0[4 * tid + 1]) << 8) |
+                                  (uint32_t(L0[4 * tid + 2]) << 16) | (uint32_t(L0[4 * tid + 3]) << 24);
+            uint32_t cnt;
+            const uint32_t ex = block_excl_scan<kWzpThreads>(__popc(bits), S.tmp, cnt);
+            if (cnt == 0 || cnt != pos) bad = true;
+            const uint32_t b0 = tid * 32;
+            // bitmap beyond the chunk's bytes must be empty
+            if (b0 + 32 > raw_bytes) {
+                const uint32_t keep = b0 >= raw_bytes ? 0u : (raw_bytes - b0 >= 32 ? 32u : raw_bytes - b0);
+                const uint32_t allowed = keep == 32 ? 0xffffffffu : ((1u << keep) - 1u);
+                if (bits & ~allowed) bad = true;
+            }
+            uint32_t r = ex;
+            uint32_t* out32 = reinterpret_cast<uint32_t*>(S.planes + b0);
+#pragma unroll
+            for (int w = 0; w < 8; ++w) {
+                uint32_t word = 0;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int i = w * 4 + k;
+                    uint32_t v = 0;
+                    if ((bits >> i) & 1u) {
+                        v = (!bad && r < pos) ? src[r] : 0;
+                        if (!v) bad = true;
+                        ++r;
+                    }
+                    word |= v << (8 * k);
+                }
+                out32[w] = word;
+            }
+        }
+        __syncthreads();
+        // ---- inverse bit planes (warp shuffles of the plane words)
+        const uint16_t* pl = reinterpret_cast<const uint16_t*>(S.planes);
+        for (int g = warp; g < int(kChunk / 32); g += NW) {
+            if (uint32_t(g * 32) >= blocks * 16) break;
+            uint32_t mine = 0;
+            if (lane < 16) {
+                mine = uint32_t(pl[lane * blocks + 2 * g]) << 16;
+                if (uint32_t(2 * g + 1) < blocks) mine |= pl[lane * blocks + 2 * g + 1];
+            }
+            uint32_t v = 0;
+#pragma unroll
+            for (int p = 0; p < 16; ++p) {
+                const uint32_t r = __shfl_sync(0xffffffffu, mine, p);
+                v |= ((r >> (31 - lane)) & 1u) << (15 - p);
+            }
+            const int e = g * 32 + lane;
+            if (uint32_t(e) < blocks * 16) S.m[e] = uint16_t(v);
+        }
+        for (uint32_t i = blocks * 16 + tid; i < kChunk; i += kWzpThreads)
+            S.m[i] = i < count ? pl[i] : 0;
+    }
+    __syncthreads();
+
+    // ---- signs and dequantisation
+    uint32_t nnz = 0;
+    {
+        uint32_t gc = 0;
+        if (tid < int(kChunk / 32)) {
+            for (int k = 0; k < 32; ++k) gc += S.m[tid * 32 + k] != 0;
+        }
+        const uint32_t gp = block_excl_scan<kWzpThreads>(gc, S.tmp, nnz);
+        if (tid < int(kChunk / 32)) S.gprefix[tid] = gp;
+    }
+    if (mbytes != 0) {
+        if (nnz == 0 || (nnz + 7) / 8 != sbytes) bad = true;
+        else if ((nnz & 7) && (src[mbytes + sbytes - 1] >> (nnz & 7))) bad = true;
+    }
+    __syncthreads();
+    const uint8_t* sgn = src + mbytes;
+    for (int g = warp; g < int(kChunk / 32); g += NW) {
+        if (uint32_t(g * 32) >= count) break;
+        const int e = g * 32 + lane;
+        const uint32_t v = S.m[e];
+        const uint32_t nzmask = __ballot_sync(0xffffffffu, v != 0);
+        bool neg = false;
+        if (v && !bad) {
+            const uint32_t rank = S.gprefix[g] + __popc(nzmask & ((1u << lane) - 1u));
+            if (rank < 8 * sbytes) neg = (sgn[rank >> 3] >> (rank & 7)) & 1u;
+        }
+        if (uint32_t(e) < count) {
+            const T mag = Lift<T>::mul(T(v), A.q);
+            A.coeff[A.map.rowmajor(uint64_t(first) + e)] = neg ? -mag : mag;
+        }
+    }
+    if (bad) atomicOr(A.status, ST_BAD_STREAM);
+}
+
+} // namespace wb
