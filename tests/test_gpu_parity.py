@@ -204,18 +204,22 @@ def test_extrema():
 
 def test_decode_chunk_canonical():
     torch = _torch()
-    a = P.codec_field((33, 31, 17), 2, 1e-3, np.float32)
+    nx, ny, nz = 33, 31, 17
+    a = P.codec_field(P.zyx((nx, ny, nz)), 2, 1e-3, np.float32)
     archive = O.compress(a, 1e-3)
     src = torch.from_numpy(np.frombuffer(archive, np.uint8).copy()).cuda()
     out = torch.empty(a.shape, dtype=torch.float32, device="cuda")
-    err = _lib().waltz_cuda_decode_chunk(33, 31, 17, 4, C.c_void_p(src.data_ptr()), len(archive),
+    err = _lib().waltz_cuda_decode_chunk(nx, ny, nz, 4, C.c_void_p(src.data_ptr()), len(archive),
                                          C.c_void_p(out.data_ptr()), out.numel() * 4, _stream())
     assert err is None, err
     assert out.cpu().numpy().tobytes() == O.decompress(archive, a.shape, np.float32).tobytes()
     # wrong geometry / width / length are rejected with a diagnostic
-    assert _lib().waltz_cuda_decode_chunk(33, 31, 16, 4, C.c_void_p(src.data_ptr()), len(archive),
-                                          C.c_void_p(out.data_ptr()), 33 * 31 * 16 * 4, _stream()) is not None
-    assert _lib().waltz_cuda_decode_chunk(33, 31, 17, 4, C.c_void_p(src.data_ptr()), len(archive) - 8,
+    assert _lib().waltz_cuda_decode_chunk(nx, ny, 8, 4, C.c_void_p(src.data_ptr()), len(archive),
+                                          C.c_void_p(out.data_ptr()), nx * ny * 8 * 4, _stream()) is not None
+    wide = torch.empty(a.shape, dtype=torch.float64, device="cuda")
+    assert _lib().waltz_cuda_decode_chunk(nx, ny, nz, 8, C.c_void_p(src.data_ptr()), len(archive),
+                                          C.c_void_p(wide.data_ptr()), wide.numel() * 8, _stream()) is not None
+    assert _lib().waltz_cuda_decode_chunk(nx, ny, nz, 4, C.c_void_p(src.data_ptr()), len(archive) - 8,
                                           C.c_void_p(out.data_ptr()), out.numel() * 4, _stream()) is not None
 
 

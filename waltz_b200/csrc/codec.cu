@@ -263,12 +263,9 @@ static void forward(const Geometry& g, const T* in, T* C, T* lowA, T* lowB, T* i
         check(cudaGetLastError(), "copy launch");
         return;
     }
-    check_finite_kernel<T><<<grid_for(g.n), 256, 0, stream>>>(in, g.n, status); note_launch();
-    check(cudaGetLastError(), "finite check launch");
     StageClock& clock = stage_clock();
-    clock.mark("finite_check", stream);
     if (g.dyadic) {
-        FwdSrc<T> src{in, sy, sz};
+        FwdSrc<T> src{in, sy, sz, status};
         for (unsigned l = 0; l < g.lxy; ++l) {
             const Dims a = g.dyad[l], lo = halve(a, AX | AY | AZ);
             const bool last = l + 1 == g.lxy;
@@ -280,7 +277,7 @@ static void forward(const Geometry& g, const T* in, T* C, T* lowA, T* lowB, T* i
         if (g.lxy > 1) clock.mark("fwd_coarse", stream);
         return;
     }
-    FwdSrc<T> src{in, sy, sz};
+    FwdSrc<T> src{in, sy, sz, status};
     T* zdst = g.lxy ? inter : C;
     for (unsigned l = 0; l < g.lz; ++l) {
         const Dims a = g.zl[l], lo = halve(a, AZ);

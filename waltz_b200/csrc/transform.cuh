@@ -20,14 +20,20 @@ namespace wb {
 
 enum Axes : int { AX = 1, AY = 2, AZ = 4 };
 
-// Forward source: a compact or strided box, reflected at its edges.
+// Forward source: a compact or strided box, reflected at its edges. With
+// `status` set, every staged sample is also checked for finiteness (the
+// finest level stages every input sample at least once).
 template <class T> struct FwdSrc {
     const T* p;
     size_t sy, sz; // element strides
+    uint32_t* status = nullptr;
     __device__ __forceinline__ T at(uint32_t x, uint32_t y, uint32_t z) const {
         return p[size_t(z) * sz + size_t(y) * sy + x];
     }
 };
+
+template <class Src> __device__ __forceinline__ uint32_t* finite_status(const Src&) { return nullptr; }
+template <class T> __device__ __forceinline__ uint32_t* finite_status(const FwdSrc<T>& s) { return s.status; }
 
 // Inverse source: coefficient box whose low corner (lo dims) may come from a
 // separately reconstructed compact array, the rest from `base`.
@@ -163,6 +169,14 @@ __global__ void __launch_bounds__(256) level_kernel(Src src, Dims a, Dims grid, 
             sz = mirror(pz, a.z);
         }
         A[(size_t(fz) * S::FY + fy) * S::FPX + fx] = src.at(sx, sy, sz);
+    }
+    if (uint32_t* st = finite_status(src)) {
+        bool bad = false;
+        for (int i = threadIdx.x; i < S::FOOT; i += blockDim.x) {
+            const int fx = i % S::FX, fy = (i / S::FX) % S::FY, fz = i / (S::FX * S::FY);
+            bad |= !finite_bits(A[(size_t(fz) * S::FY + fy) * S::FPX + fx]);
+        }
+        if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(st, ST_NONFINITE_INPUT);
     }
     __syncthreads();
 
