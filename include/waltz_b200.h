@@ -57,6 +57,19 @@ int waltz_b200_transform(void* d_data, int width, uint32_t nx, uint32_t ny, uint
                          void* stream);
 int waltz_b200_wzp_encode(const uint16_t* d_mag, const uint32_t* d_sign, uint32_t n, void* d_out,
                           size_t capacity, size_t* written, void* stream);
+/* Allocation-free variant of waltz_b200_wzp_encode (same arguments, same
+ * stream bytes), for callers that cannot allocate device memory when they
+ * call: a framework whose allocator owns the device budget, a plugin or filter
+ * callback, or a loop that cannot take cudaMalloc's device synchronisation.
+ * No counterpart in the reference. Its working state lives in one static
+ * device array of about 256 KiB that every GPU loading the library holds
+ * until exit; n is limited to 134217728 magnitudes (16384 chunks) and larger
+ * n is rejected with an error. The first call on a device looks up the
+ * array's device address (make that first call before any stream capture).
+ * Calls share the array, so calls that overlap on the GPU (other streams,
+ * threads or processes sharing a context) race: serialise them. */
+int waltz_b200_wzp_encode_noalloc(const uint16_t* d_mag, const uint32_t* d_sign, uint32_t n, void* d_out,
+                                  size_t capacity, size_t* written, void* stream);
 /* Test hook for the bounded-wait path: compress with chunk `skip_chunk`
  * never publishing its lookback state and every wait capped at `spin_cap`
  * polls (~0.5 us each). Must fail with a lookback-timeout diagnostic. */

@@ -972,6 +972,81 @@ extern "C" int waltz_b200_wzp_encode(const uint16_t* d_mag, const uint32_t* d_si
     }
 }
 
+// ------------------------------------------------ allocation-free WZP encode
+// Some callers cannot allocate device memory at the point of call: a host
+// framework whose caching allocator owns the whole device budget, a plugin or
+// filter callback with no device-memory lifetime of its own, or a hot loop
+// that cannot afford the device-wide synchronisation of cudaMalloc/cudaFree.
+// For them the WZP encoder keeps its working state (ticket, status, total and
+// the per-chunk lookback states and sizes) in one file-scope device array,
+// loaded with the library on every GPU that uses it and held until exit.
+namespace wb {
+constexpr uint32_t kNoAllocMaxChunks = 16384; // 134,217,728 magnitudes
+constexpr size_t kNoAllocWords = 32 + 2 * size_t(kNoAllocMaxChunks); // u64 words: header, states, sizes
+static __device__ __align__(256) uint64_t g_wzp_noalloc_scratch[kNoAllocWords];
+
+// Device address of the array for the current device. The first call on a
+// device resolves it with cudaGetSymbolAddress (with that device current);
+// later calls reuse it. The host-side name of the array is only a stand-in
+// and must never reach a kernel.
+static uint64_t* noalloc_scratch() {
+    constexpr int kMaxDevices = 64;
+    static std::mutex lock;
+    static uint64_t* addr[kMaxDevices] = {};
+    int dev = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    need(dev >= 0 && dev < kMaxDevices, "Waltz: device ordinal outside the scratch table");
+    std::lock_guard<std::mutex> guard(lock);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        check(cudaGetSymbolAddress(&p, g_wzp_noalloc_scratch), "Waltz: scratch symbol address");
+        addr[dev] = static_cast<uint64_t*>(p);
+    }
+    return addr[dev];
+}
+} // namespace wb
+
+extern "C" int waltz_b200_wzp_encode_noalloc(const uint16_t* d_mag, const uint32_t* d_sign, uint32_t n, void* d_out,
+                                             size_t capacity, size_t* written, void* stream) {
+    try {
+        need(written && d_mag && d_sign && d_out, "null argument");
+        *written = 0;
+        need(n > 0, "WZP element count must be positive");
+        need(wzp_chunks(n) <= kNoAllocMaxChunks,
+             "WZP element count exceeds the allocation-free limit of 134217728 magnitudes");
+        need(capacity >= wzp_header(n), "WZP output capacity is too small");
+        auto s = reinterpret_cast<cudaStream_t>(stream);
+        const uint32_t chunks = wzp_chunks(n), groups = wzp_groups(n);
+        uint64_t* base = noalloc_scratch();
+        auto* ticket = reinterpret_cast<uint32_t*>(base);      // word 0, low half
+        auto* status = reinterpret_cast<uint32_t*>(base) + 1;  // word 0, high half
+        uint64_t* total = base + 1;
+        uint64_t* state = base + 32;
+        uint64_t* sizes = state + kNoAllocMaxChunks;
+        // The array keeps the previous call's contents: clear what must start at zero.
+        check(cudaMemsetAsync(base, 0, 16, s), "memset");
+        check(cudaMemsetAsync(state, 0, size_t(chunks) * 8, s), "memset");
+        check(cudaFuncSetAttribute(wzp_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(sizeof(WzpEncodeSmem))), "wzp smem");
+        WzpEncodeArgs wa{d_mag, d_sign, n, static_cast<uint8_t*>(d_out), capacity, ticket, state, sizes,
+                         status, 1u << 22, 0xffffffffu};
+        wzp_encode_kernel<<<chunks, kWzpThreads, sizeof(WzpEncodeSmem), s>>>(wa); note_launch();
+        wzp_directory_kernel<<<(groups + 255) / 256, 256, 0, s>>>(static_cast<uint8_t*>(d_out), n, state, sizes,
+                                                                  total); note_launch();
+        check(cudaGetLastError(), "wzp launch");
+        uint64_t host[2] = {0, 0}; // pageable: the copy completes before cudaMemcpyAsync returns
+        check(cudaMemcpyAsync(host, base, 16, cudaMemcpyDeviceToHost, s), "readback");
+        check(cudaStreamSynchronize(s), "wzp encode");
+        const uint32_t st = uint32_t(host[0] >> 32);
+        if (st & ST_CAPACITY) throw Error("WZP output capacity is too small");
+        if (st) throw Error("WZP encode failed");
+        *written = size_t(host[1]);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
 extern "C" unsigned long long waltz_b200_launch_count(void) { return launch_counter().load(); }
 
 extern "C" void waltz_b200_profile(int enable) { stage_clock().enabled = enable != 0; }
