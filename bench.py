@@ -117,7 +117,8 @@ def gpu_arm(args, rank, world, local_rank):
     lib = _lib.lib()
     stream = torch.cuda.current_stream()
     sp = C.c_void_p(stream.cuda_stream)
-    field = power_law_field_device(SHAPE, SEED, device=dev).contiguous()
+    shape = tuple(args.shape)
+    field = power_law_field_device(shape, SEED, device=dev).contiguous()
     n = field.numel()
     nbytes = n * 4
     lo, hi = waltz_b200.extrema(field)
@@ -125,7 +126,7 @@ def gpu_arm(args, rank, world, local_rank):
     cap = waltz_b200.compressed_capacity(n, 4)
     archive = torch.empty(cap, dtype=torch.uint8, device=dev)
     out = torch.empty_like(field)
-    nz, ny, nx = SHAPE
+    nz, ny, nx = shape
     written = C.c_size_t()
 
     def compress():
@@ -190,10 +191,10 @@ def gpu_arm(args, rank, world, local_rank):
     stage_ms = {k: statistics.median(v) for k, v in stages.items()}
 
     # ---- end to end through the public API with host buffers
-    host_in = torch.empty(SHAPE, dtype=torch.float32, pin_memory=True)
+    host_in = torch.empty(shape, dtype=torch.float32, pin_memory=True)
     host_in.copy_(field.cpu())
     host_arch = torch.empty(cap, dtype=torch.uint8, pin_memory=True)
-    host_out = torch.empty(SHAPE, dtype=torch.float32, pin_memory=True)
+    host_out = torch.empty(shape, dtype=torch.float32, pin_memory=True)
     e2e_ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
     e2e = []
     for k in range(max(2, min(args.steps, 5)) + 1):
@@ -229,8 +230,8 @@ def gpu_arm(args, rank, world, local_rank):
         "warmup": args.warmup, "ms_per_step": round(step_ms, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: seeded k^-11/3 Gaussian random field (stand-in for the reference's simulation fields)",
-        "config": {"workload": "f32 512^3 k^-11/3 GRF seed 1, REL 1e-3 (eb=%.6g), dyadic 5 levels, "
-                               "step = compress + decompress" % eb,
+        "config": {"workload": "f32 %dx%dx%d (z,y,x) k^-11/3 GRF seed 1, REL 1e-3 (eb=%.6g), "
+                               "step = compress + decompress" % (*shape, eb),
                    "global_batch": world, "seq_len": None, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (512 MiB field)", "archive_bytes": a_bytes,
                    "compression_ratio": round(nbytes / a_bytes, 4), "max_abs_error": max_err, "abs_bound": eb},
@@ -380,6 +381,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shape", type=int, nargs=3, default=list(SHAPE), metavar=("NZ", "NY", "NX"),
+                    help="field shape (z y x); smaller shapes serve profiler captures")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

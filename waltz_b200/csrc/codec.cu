@@ -95,7 +95,8 @@ static uint32_t morton_rank(uint32_t x, uint32_t y, uint32_t z, uint32_t nx, uin
 }
 
 // 8 slots x 256*bz entries; slot bits: short x edge, short y edge, short z
-// edge. forward: local row-major index -> rank; inverse: rank -> local index.
+// edge. forward: local row-major index -> rank; inverse: rank -> packed local
+// coordinates x | y << 4 | z << 8.
 static std::vector<uint16_t> morton_tables(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t bz, bool inverse) {
     const uint32_t stride = 256 * bz;
     std::vector<uint16_t> t(8 * stride, 0);
@@ -106,7 +107,7 @@ static std::vector<uint16_t> morton_tables(uint32_t nx, uint32_t ny, uint32_t nz
                 for (uint32_t x = 0; x < ex; ++x) {
                     const uint32_t local = (z * ey + y) * ex + x;
                     const uint32_t r = morton_rank(x, y, z, ex, ey, ez);
-                    if (inverse) t[s * stride + r] = uint16_t(local);
+                    if (inverse) t[s * stride + r] = uint16_t(x | (y << 4) | (z << 8));
                     else t[s * stride + local] = uint16_t(r);
                 }
     }

@@ -22,14 +22,17 @@ enum Axes : int { AX = 1, AY = 2, AZ = 4 };
 
 // Forward source: a compact or strided box, reflected at its edges. With
 // `status` set, every staged sample is also checked for finiteness (the
-// finest level stages every input sample at least once).
+// finest level stages every input sample at least once). Samples are staged
+// row by row: `row(y, z)` resolves a row once, `get(row, x)` reads one sample.
 template <class T> struct FwdSrc {
     const T* p;
     size_t sy, sz; // element strides
     uint32_t* status = nullptr;
-    __device__ __forceinline__ T at(uint32_t x, uint32_t y, uint32_t z) const {
-        return p[size_t(z) * sz + size_t(y) * sy + x];
-    }
+    struct Row {
+        const T* p;
+    };
+    __device__ __forceinline__ Row row(uint32_t y, uint32_t z) const { return {p + size_t(z) * sz + size_t(y) * sy}; }
+    __device__ __forceinline__ T get(const Row& r, uint32_t x) const { return r.p[x]; }
 };
 
 template <class Src> __device__ __forceinline__ uint32_t* finite_status(const Src&) { return nullptr; }
@@ -42,10 +45,15 @@ template <class T> struct InvSrc {
     size_t sy, sz;
     const T* low; // nullable
     Dims lo;
-    __device__ __forceinline__ T at(uint32_t x, uint32_t y, uint32_t z) const {
-        if (low && x < lo.x && y < lo.y && z < lo.z) return low[(size_t(z) * lo.y + y) * lo.x + x];
-        return base[size_t(z) * sz + size_t(y) * sy + x];
+    struct Row {
+        const T* b;
+        const T* l; // the row's low-corner part, or null
+    };
+    __device__ __forceinline__ Row row(uint32_t y, uint32_t z) const {
+        const T* l = (low && y < lo.y && z < lo.z) ? low + (size_t(z) * lo.y + y) * lo.x : nullptr;
+        return {base + size_t(z) * sz + size_t(y) * sy, l};
     }
+    __device__ __forceinline__ T get(const Row& r, uint32_t x) const { return (r.l && x < lo.x) ? r.l[x] : r.b[x]; }
 };
 
 // Forward output: high bands to `dst` at split positions; the all-even low
@@ -154,29 +162,53 @@ __global__ void __launch_bounds__(256) level_kernel(Src src, Dims a, Dims grid, 
     const uint32_t ox = bx * UX, oy = by * UY, oz = bz * UZ;
     const int hx = (Mask & AX) ? 4 : 0, hy = (Mask & AY) ? 4 : 0, hz = (Mask & AZ) ? 4 : 0;
 
-    // ---- stage the footprint
-    for (int i = threadIdx.x; i < S::FOOT; i += blockDim.x) {
-        const int fx = i % S::FX, fy = (i / S::FX) % S::FY, fz = i / (S::FX * S::FY);
-        const int64_t px = int64_t(ox) + fx - hx, py = int64_t(oy) + fy - hy, pz = int64_t(oz) + fz - hz;
-        uint32_t sx, sy, sz;
-        if (Inverse) {
-            sx = (Mask & AX) ? coeff_at(px, a.x) : mirror(px, a.x);
-            sy = (Mask & AY) ? coeff_at(py, a.y) : mirror(py, a.y);
-            sz = (Mask & AZ) ? coeff_at(pz, a.z) : mirror(pz, a.z);
-        } else {
-            sx = mirror(px, a.x);
-            sy = mirror(py, a.y);
-            sz = mirror(pz, a.z);
-        }
-        A[(size_t(fz) * S::FY + fy) * S::FPX + fx] = src.at(sx, sy, sz);
-    }
-    if (uint32_t* st = finite_status(src)) {
+    // ---- stage the footprint: warp w takes rows w, w+8, ...; a lane covers
+    // x = lane and lane + 32 of every row. Source positions are reflected
+    // (forward) or coefficient-mapped (inverse) once per lane and per row, and
+    // each lane keeps kBatch rows of loads in flight before storing them.
+    static_assert(S::FX <= 64, "footprint rows wider than two warps");
+    {
+        auto map = [&](int64_t p, uint32_t n, bool lifted) -> uint32_t {
+            return (Inverse && lifted) ? coeff_at(p, n) : mirror(p, n);
+        };
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        constexpr int NW = 256 / 32;
+        const bool has0 = lane < S::FX, has1 = lane + 32 < S::FX;
+        const uint32_t x0 = map(int64_t(ox) + lane - hx, a.x, Mask & AX);
+        const uint32_t x1 = map(int64_t(ox) + lane + 32 - hx, a.x, Mask & AX);
+        constexpr int ROWS = S::FY * S::FZ;
+        constexpr int kBatch = 8;
         bool bad = false;
-        for (int i = threadIdx.x; i < S::FOOT; i += blockDim.x) {
-            const int fx = i % S::FX, fy = (i / S::FX) % S::FY, fz = i / (S::FX * S::FY);
-            bad |= !finite_bits(A[(size_t(fz) * S::FY + fy) * S::FPX + fx]);
+        for (int r0 = warp; r0 < ROWS; r0 += NW * kBatch) {
+            T v0[kBatch], v1[kBatch];
+#pragma unroll
+            for (int u = 0; u < kBatch; ++u) {
+                const int r = r0 + u * NW;
+                v0[u] = T(0);
+                v1[u] = T(0);
+                if (r < ROWS) {
+                    const int fy = r % S::FY, fz = r / S::FY;
+                    const auto row = src.row(map(int64_t(oy) + fy - hy, a.y, Mask & AY),
+                                             map(int64_t(oz) + fz - hz, a.z, Mask & AZ));
+                    if (has0) v0[u] = src.get(row, x0);
+                    if (has1) v1[u] = src.get(row, x1);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kBatch; ++u) {
+                const int r = r0 + u * NW;
+                if (r < ROWS) {
+                    const int fy = r % S::FY, fz = r / S::FY;
+                    T* dst = A + (size_t(fz) * S::FY + fy) * S::FPX;
+                    if (has0) dst[lane] = v0[u];
+                    if (has1) dst[lane + 32] = v1[u];
+                    bad |= !finite_bits(v0[u]) || !finite_bits(v1[u]);
+                }
+            }
         }
-        if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(st, ST_NONFINITE_INPUT);
+        if (uint32_t* st = finite_status(src)) {
+            if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(st, ST_NONFINITE_INPUT);
+        }
     }
     __syncthreads();
 

@@ -126,6 +126,8 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_encode_kernel(WzpEncodeArgs A
         if (tid < int(kChunk / 32)) S.gcount[tid] = gp; // now the group prefix
         __syncthreads();
     }
+    // Each 32-group packs its nonzero magnitudes' sign bits with one warp OR
+    // reduction and merges them at its bit offset (at most two words).
     const uint32_t* natural = A.sign + (first >> 5);
     for (int g = warp; g < int(kChunk / 32); g += NW) {
         if (uint32_t(g * 32) >= count) break;
@@ -133,9 +135,12 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_encode_kernel(WzpEncodeArgs A
         const uint32_t v = S.m[e];
         const uint32_t nzmask = __ballot_sync(0xffffffffu, v != 0);
         const uint32_t word = natural[g];
-        if (v != 0 && ((word >> lane) & 1u)) {
-            const uint32_t rank = S.gcount[g] + __popc(nzmask & ((1u << lane) - 1u));
-            atomicOr(&S.sgn[rank >> 5], 1u << (rank & 31));
+        const uint32_t pos = __popc(nzmask & ((1u << lane) - 1u));
+        const uint32_t packed = __reduce_or_sync(0xffffffffu, (v != 0 && ((word >> lane) & 1u)) ? 1u << pos : 0u);
+        if (lane == 0 && packed) {
+            const uint32_t r = S.gcount[g], sh = r & 31;
+            atomicOr(&S.sgn[r >> 5], packed << sh);
+            if (sh && (packed >> (32 - sh))) atomicOr(&S.sgn[(r >> 5) + 1], packed >> (32 - sh));
         }
     }
 
@@ -320,25 +325,26 @@ __global__ void wzp_directory_kernel(uint8_t* out, uint32_t n, const uint64_t* s
 // order z, y, x; edge bricks shrink): packed index -> row-major index.
 struct BrickMap {
     uint32_t nx, ny, nz, bz;
-    const uint16_t* local; // 8 slots x 256*bz: rank -> local row-major index
-    __device__ __forceinline__ size_t rowmajor(uint64_t k) const {
-        const uint64_t plane = uint64_t(nx) * ny;
-        const uint64_t slab_sz = plane * bz;
-        const uint64_t slab = k / slab_sz;
-        uint64_t r = k - slab * slab_sz;
-        const uint32_t ez = min(uint64_t(bz), uint64_t(nz) - slab * bz);
-        const uint64_t row_sz = uint64_t(16) * nx * ez;
-        const uint64_t row = r / row_sz;
+    const uint16_t* local; // 8 slots x 256*bz: rank -> packed brick-local (x | y << 4 | z << 8)
+    // Every index fits 32 bits: archives hold at most 2^32 - 1 sample bytes.
+    __device__ __forceinline__ uint32_t rowmajor(uint32_t k) const {
+        const uint32_t plane = nx * ny;
+        const uint32_t slab_sz = plane * bz;
+        const uint32_t slab = k / slab_sz;
+        uint32_t r = k - slab * slab_sz;
+        const uint32_t ez = min(bz, nz - slab * bz);
+        const uint32_t row_sz = 16 * nx * ez;
+        const uint32_t row = r / row_sz;
         r -= row * row_sz;
-        const uint32_t ey = min(uint64_t(16), uint64_t(ny) - row * 16);
-        const uint64_t brick_sz = uint64_t(16) * ey * ez;
-        const uint64_t bxi = r / brick_sz;
-        const uint32_t rk = uint32_t(r - bxi * brick_sz);
-        const uint32_t ex = min(uint64_t(16), uint64_t(nx) - bxi * 16);
+        const uint32_t ey = min(16u, ny - row * 16);
+        const uint32_t brick_sz = 16 * ey * ez;
+        const uint32_t bxi = r / brick_sz;
+        const uint32_t rk = r - bxi * brick_sz;
+        const uint32_t ex = min(16u, nx - bxi * 16);
         const uint32_t slot = (ex != 16) | ((ey != 16) << 1) | ((ez != bz) << 2);
         const uint32_t loc = local[slot * 256 * bz + rk];
-        const uint32_t lx = loc % ex, ly = (loc / ex) % ey, lz = loc / (ex * ey);
-        return (slab * bz + lz) * plane + (row * 16 + ly) * uint64_t(nx) + bxi * 16 + lx;
+        const uint32_t lx = loc & 15, ly = (loc >> 4) & 15, lz = loc >> 8;
+        return (slab * bz + lz) * plane + (row * 16 + ly) * nx + bxi * 16 + lx;
     }
 };
 
@@ -394,24 +400,29 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_decode_kernel(WzpDecodeArgs<T
     const uint8_t* payload = A.in + header;
     const size_t payload_bytes = A.bytes - header;
 
-    if (tid == 0) {
-        const uint32_t g = c / kGroup;
-        uint64_t off = load_u32(A.in + size_t(g) * 4);
-        bool ok = true;
-        for (uint32_t k = g * kGroup; k < c; ++k) {
-            const WzpChunkInfo ci = wzp_meta(load_u24(meta + size_t(k) * 3), min(kChunk, A.n - k * kChunk));
-            ok &= ci.ok;
-            off += ci.mbytes + ci.sbytes;
+    if (warp == 0) {
+        // Lane k reads the metadata of the group's chunk k; the chunk's payload
+        // offset is the group offset plus its predecessors' lengths.
+        const uint32_t g = c / kGroup, k = g * kGroup + lane;
+        WzpChunkInfo ci{0, 0, false, true};
+        if (lane < int(kGroup) && k <= c) ci = wzp_meta(load_u24(meta + size_t(k) * 3), min(kChunk, A.n - k * kChunk));
+        const uint32_t len = (lane < int(kGroup) && k < c) ? ci.mbytes + ci.sbytes : 0u;
+        const uint32_t before = __reduce_add_sync(0xffffffffu, len);
+        const bool ok_all = __all_sync(0xffffffffu, ci.ok);
+        const int me = int(c - g * kGroup);
+        const uint32_t mb = __shfl_sync(0xffffffffu, ci.mbytes, me);
+        const uint32_t sb = __shfl_sync(0xffffffffu, ci.sbytes, me);
+        const bool raw = __shfl_sync(0xffffffffu, ci.raw ? 1u : 0u, me) != 0;
+        if (lane == 0) {
+            const uint64_t off = uint64_t(load_u32(A.in + size_t(g) * 4)) + before;
+            const bool ok = ok_all && off + mb + sb <= payload_bytes;
+            S.off = uint32_t(off);
+            S.mbytes = mb;
+            S.sbytes = sb;
+            S.raw = raw;
+            S.bad = !ok;
+            if (!ok) atomicOr(A.status, ST_BAD_STREAM);
         }
-        const WzpChunkInfo me = wzp_meta(load_u24(meta + size_t(c) * 3), count);
-        ok &= me.ok;
-        if (ok && off + me.mbytes + me.sbytes > payload_bytes) ok = false;
-        S.off = uint32_t(off);
-        S.mbytes = me.mbytes;
-        S.sbytes = me.sbytes;
-        S.raw = me.raw;
-        S.bad = !ok;
-        if (!ok) atomicOr(A.status, ST_BAD_STREAM);
     }
     __syncthreads();
     if (S.bad) return;
@@ -591,7 +602,7 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_decode_kernel(WzpDecodeArgs<T
         }
         if (uint32_t(e) < count) {
             const T mag = Lift<T>::mul(T(v), A.q);
-            A.coeff[A.map.rowmajor(uint64_t(first) + e)] = neg ? -mag : mag;
+            A.coeff[A.map.rowmajor(first + uint32_t(e))] = neg ? -mag : mag;
         }
     }
     if (bad) atomicOr(A.status, ST_BAD_STREAM);
