@@ -11,6 +11,7 @@
 // read at the call's single synchronisation point.
 #include "common.cuh"
 #include "quantize.cuh"
+#include "stream.cuh"
 #include "transform.cuh"
 #include "wzp.cuh"
 
@@ -219,6 +220,68 @@ static void level(const Src& src, Dims a, const Out& out, cudaStream_t stream) {
         launch_level<T, Inverse, Mask, Tiles<T>::Z[0], Tiles<T>::Z[1], Tiles<T>::Z[2]>(src, a, out, stream);
 }
 
+// Resident CTAs of a kernel per SM times the SM count, cached per device.
+template <class K> static uint64_t resident_slots(K kernel, size_t smem) {
+    static thread_local int cached_dev = -1;
+    static thread_local uint64_t slots = 0;
+    int dev = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (cached_dev != dev) {
+        int sms = 0, occ = 0;
+        check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+        check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, 256, smem), "occupancy");
+        slots = uint64_t(sms) * uint64_t(occ > 0 ? occ : 1);
+        cached_dev = dev;
+    }
+    return slots;
+}
+
+// One dyadic forward level as a z-march: XY tiles, and the z axis split into
+// ranges only as far as needed to give every resident CTA slot work. Planes
+// are staged by TMA when the source rows meet the copy engine's alignment.
+template <class T>
+static void level_fwd_stream(const FwdSrc<T>& src, Dims a, const FwdOut<T>& out, uint32_t* status,
+                             cudaStream_t stream) {
+    constexpr int UX = StreamTile<T>::UX, UY = StreamTile<T>::UY, Q = StreamTile<T>::Q;
+    using S = StreamShape<T, UX, UY, Q>;
+    CUtensorMap map{};
+    const bool tma = make_map_3d<T>(&map, src.p, a.x, a.y, a.z, src.sy, src.sz, S::FX, S::FY, 1);
+    auto kernel = tma ? fwd_stream_kernel<T, UX, UY, Q, true> : fwd_stream_kernel<T, UX, UY, Q, false>;
+    static thread_local int configured_device = -1;
+    int dev = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (configured_device != dev) {
+        check(cudaFuncSetAttribute(fwd_stream_kernel<T, UX, UY, Q, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(S::smem)), "stream kernel shared memory");
+        check(cudaFuncSetAttribute(fwd_stream_kernel<T, UX, UY, Q, false>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(S::smem)),
+              "stream kernel shared memory");
+        configured_device = dev;
+    }
+    const uint32_t tx = (a.x + UX - 1) / UX, ty = (a.y + UY - 1) / UY;
+    const uint64_t tiles = uint64_t(tx) * ty, slots = resident_slots(kernel, S::smem);
+    // z ranges: maximise (filled share of the last wave) x (planes kept out of
+    // the 8-plane halo a range re-reads), over up to 16 ranges of >= 16 planes
+    uint32_t zrange = a.z + (a.z & 1);
+    double best = -1;
+    for (uint32_t k = 1; k <= 16; ++k) {
+        uint32_t r = (a.z + k - 1) / k;
+        r += r & 1;
+        if (k > 1 && r < 16) break;
+        const uint64_t blocks = tiles * ((a.z + r - 1) / r);
+        const double waves = double((blocks + slots - 1) / slots);
+        const double score = double(blocks) / (waves * double(slots)) * double(r) / double(r + 8);
+        if (score > best + 1e-9) {
+            best = score;
+            zrange = r;
+        }
+    }
+    const uint64_t blocks = tiles * ((a.z + zrange - 1) / zrange);
+    need(blocks < (1ull << 31), "Waltz: level grid too large");
+    kernel<<<unsigned(blocks), 256, S::smem, stream>>>(src, map, a, tx, ty, zrange, out, status); note_launch();
+    check(cudaGetLastError(), "stream level launch");
+}
+
 template <class T, class Out>
 __global__ void identity_kernel(const T* in, Dims d, Out out) {
     const uint64_t n = vol(d);
@@ -271,7 +334,7 @@ static void forward(const Geometry& g, const T* in, T* C, T* lowA, T* lowB, T* i
             const Dims a = g.dyad[l], lo = halve(a, AX | AY | AZ);
             const bool last = l + 1 == g.lxy;
             FwdOut<T> out{C, sy, sz, last ? nullptr : lows[l & 1], lo, a, AX | AY | AZ};
-            level<T, false, AX | AY | AZ>(src, a, out, stream);
+            level_fwd_stream<T>(src, a, out, status, stream);
             if (l == 0) clock.mark("fwd_l0", stream);
             src = FwdSrc<T>{lows[l & 1], lo.x, size_t(lo.x) * lo.y};
         }
@@ -530,6 +593,7 @@ static size_t compress(const T* d_in, uint32_t nx, uint32_t ny, uint32_t nz, dou
     if (status & ST_QUANT_DOMAIN) throw Error("coefficient exceeds portable integer conversion domain");
     if (status & ST_BOUND) throw Error("native repair cannot meet strict bound or nonfinite reconstruction");
     if (status & ST_LOOKBACK_TIMEOUT) throw Error("Waltz: WZP lookback wait exceeded its bound");
+    if (status & ST_WAIT_TIMEOUT) throw Error("Waltz: asynchronous copy wait exceeded its bound");
     if (status & ST_CAPACITY) throw Error("archive capacity too small");
     if ((n > (1u << 20) && nq >= (1u << 20)) || (n > (1u << 22) && np >= (1u << 22)))
         throw Error("portable GPU side-channel capacity reached");
@@ -920,7 +984,10 @@ extern "C" int waltz_b200_transform(void* d_data, int width, uint32_t nx, uint32
                 check(cudaMemcpyAsync(P.C, data, g.n * sizeof(T), cudaMemcpyDeviceToDevice, s), "copy");
                 wb::inverse<T>(g, P.C, P.inter, P.bank2, StoreOut<T>{data, nx, size_t(nx) * ny}, s);
             }
+            uint32_t st = 0;
+            check(cudaMemcpyAsync(&st, P.status, 4, cudaMemcpyDeviceToHost, s), "readback");
             check(cudaStreamSynchronize(s), "transform");
+            if (st & ST_WAIT_TIMEOUT) throw Error("Waltz: asynchronous copy wait exceeded its bound");
         };
         if (width == 4) run(static_cast<float*>(d_data));
         else run(static_cast<double*>(d_data));

@@ -89,6 +89,7 @@ enum Status : uint32_t {
     ST_BAD_QOUT = 1u << 8,          // q-outlier value outside (65535, INT32_MAX]
     ST_BAD_REPAIR = 1u << 9,        // nonfinite repair value
     ST_DIRECTORY = 1u << 10,        // WZP directory not in canonical order
+    ST_WAIT_TIMEOUT = 1u << 11,     // a bounded wait for an asynchronous copy expired
 };
 
 // ------------------------------------------------------------ geometry

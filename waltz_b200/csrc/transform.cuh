@@ -73,6 +73,12 @@ template <class T> struct FwdOut {
         if (low && ex && ey && ez) low[(size_t(cz) * lo.y + cy) * lo.x + cx] = v;
         else dst[size_t(cz) * sz + size_t(cy) * sy + cx] = v;
     }
+    // All-axes form with the column's split (cx, cy) resolved by the caller.
+    __device__ __forceinline__ void put(uint32_t cx, uint32_t cy, bool even_xy, uint32_t z, T v) const {
+        const uint32_t cz = split_of(z, a.z);
+        if (low && even_xy && !(z & 1)) low[(size_t(cz) * lo.y + cy) * lo.x + cx] = v;
+        else dst[size_t(cz) * sz + size_t(cy) * sy + cx] = v;
+    }
 };
 
 // Inverse output into a compact or strided array.

@@ -256,46 +256,54 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_encode_kernel(WzpEncodeArgs A
     const uint32_t sbytes = (nnz + 7) / 8;
     const uint64_t chunk_bytes = nnz ? uint64_t(mbytes) + sbytes : 0;
 
-    // ---- decoupled lookback (thread 0), bounded waits
-    if (tid == 0) {
-        uint64_t excl = 0;
+    // ---- decoupled lookback by warp 0: 32 predecessor states per step; the
+    // closest inclusive prefix ends the walk. Every wait is bounded.
+    if (warp == 0) {
         const bool publish = c != A.skip_publish;
-        if (c == 0) {
-            if (publish) atomicExch(reinterpret_cast<unsigned long long*>(&A.state[0]),
-                                    (unsigned long long)(kInclusive | chunk_bytes));
-        } else {
-            if (publish) atomicExch(reinterpret_cast<unsigned long long*>(&A.state[c]),
-                                    (unsigned long long)(kAggregate | chunk_bytes));
-            int64_t j = int64_t(c) - 1;
-            while (j >= 0) {
-                uint64_t s;
-                uint32_t spins = 0;
-                for (;;) {
-                    s = *reinterpret_cast<volatile uint64_t*>(&A.state[j]);
-                    if (s >> 62) break;
-                    if (++spins >= A.spin_cap) break;
-                    __nanosleep(500);
-                }
-                if (!(s >> 62)) { // predecessor never published: give up, flag it
-                    atomicOr(A.status, ST_LOOKBACK_TIMEOUT);
+        if (lane == 0 && publish)
+            atomicExch(reinterpret_cast<unsigned long long*>(&A.state[c]),
+                       (unsigned long long)((c == 0 ? kInclusive : kAggregate) | chunk_bytes));
+        uint64_t excl = 0;
+        bool timed_out = false;
+        int64_t top = int64_t(c) - 1; // predecessor examined by lane 0
+        uint32_t spins = 0;
+        while (top >= 0) {
+            const int64_t j = top - lane;
+            const uint64_t st = j >= 0 ? *reinterpret_cast<volatile uint64_t*>(&A.state[j]) : uint64_t(2ull << 62);
+            const uint32_t pub = __ballot_sync(0xffffffffu, (st >> 62) != 0);
+            const uint32_t inc = __ballot_sync(0xffffffffu, (st >> 62) == 2);
+            const int last = inc ? __ffs(inc) - 1 : 31; // lanes 0..last are needed
+            const uint32_t need = last == 31 ? 0xffffffffu : ((2u << last) - 1u);
+            if ((pub & need) != need) {
+                if (++spins >= A.spin_cap) {
+                    timed_out = true;
                     break;
                 }
-                excl += s & kValueMask;
-                if ((s >> 62) == 2) break;
-                --j;
+                __nanosleep(200);
+                continue;
             }
-            if (publish) atomicExch(reinterpret_cast<unsigned long long*>(&A.state[c]),
-                                    (unsigned long long)(kInclusive | (excl + chunk_bytes)));
+            uint64_t v = lane <= last ? (st & kValueMask) : 0;
+#pragma unroll
+            for (int d = 16; d; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+            excl += v;
+            if (inc) break;
+            top -= 32;
         }
-        A.sizes[c] = chunk_bytes;
-        S.excl = uint32_t(excl);
-        const size_t header = size_t(groups) * 4 + size_t(chunks) * 3;
-        if (header + excl + chunk_bytes > A.capacity || excl + chunk_bytes > 0xffffffffull) {
-            atomicOr(A.status, ST_CAPACITY);
-            S.excl = 0xffffffffu;
+        if (lane == 0) {
+            if (timed_out) atomicOr(A.status, ST_LOOKBACK_TIMEOUT);
+            if (c > 0 && publish)
+                atomicExch(reinterpret_cast<unsigned long long*>(&A.state[c]),
+                           (unsigned long long)(kInclusive | (excl + chunk_bytes)));
+            A.sizes[c] = chunk_bytes;
+            S.excl = uint32_t(excl);
+            const size_t header = size_t(groups) * 4 + size_t(chunks) * 3;
+            if (header + excl + chunk_bytes > A.capacity || excl + chunk_bytes > 0xffffffffull) {
+                atomicOr(A.status, ST_CAPACITY);
+                S.excl = 0xffffffffu;
+            }
+            const uint32_t meta = nnz ? ((raw ? kRawCode : mbytes) | ((sbytes == 1024 ? 0u : sbytes) << 14)) : 0u;
+            store_u24(A.out + size_t(groups) * 4 + size_t(c) * 3, meta);
         }
-        const uint32_t meta = nnz ? ((raw ? kRawCode : mbytes) | ((sbytes == 1024 ? 0u : sbytes) << 14)) : 0u;
-        store_u24(A.out + size_t(groups) * 4 + size_t(c) * 3, meta);
     }
     __syncthreads();
     if (!nnz || S.excl == 0xffffffffu) return;
