@@ -134,6 +134,7 @@ static void decode_batch(const waltz_batch_shape& d, const uint8_t* host, const 
     if (word & ST_BAD_QOUT) throw Error("invalid quantization outlier");
     if (word & ST_BAD_REPAIR) throw Error("nonfinite correction");
     if (word & ST_NONFINITE_INPUT) throw Error("nonfinite reconstruction");
+    if (word & ST_WAIT_TIMEOUT) throw Error("Waltz: asynchronous copy wait exceeded its bound");
 }
 
 } // namespace wb

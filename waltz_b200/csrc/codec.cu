@@ -10,6 +10,7 @@
 // lifting -> repair patches. Every status is gathered in one device word and
 // read at the call's single synchronisation point.
 #include "common.cuh"
+#include "inverse.cuh"
 #include "quantize.cuh"
 #include "stream.cuh"
 #include "transform.cuh"
@@ -282,6 +283,39 @@ static void level_fwd_stream(const FwdSrc<T>& src, Dims a, const FwdOut<T>& out,
     check(cudaGetLastError(), "stream level launch");
 }
 
+// One dyadic inverse level from TMA-staged parity boxes when the coefficient
+// rows meet the copy engine's alignment; the generic level kernel otherwise.
+template <class T, class Out>
+static void level_inv(const InvSrc<T>& src, Dims a, const Out& out, uint32_t* status, cudaStream_t stream) {
+    constexpr int UX = InvTile<T>::UX, UY = InvTile<T>::UY, UZ = InvTile<T>::UZ;
+    using S = InvShape<T, UX, UY, UZ>;
+    CUtensorMap cmap{}, lmap{};
+    bool tma = half_len(a.x) % S::V == 0 &&
+               make_map_3d<T>(&cmap, src.base, a.x, a.y, a.z, src.sy, src.sz, S::BX, S::HY, S::HZ);
+    if (tma && src.low)
+        tma = make_map_3d<T>(&lmap, src.low, src.lo.x, src.lo.y, src.lo.z, src.lo.x, uint64_t(src.lo.x) * src.lo.y,
+                             S::BX, S::HY, S::HZ);
+    if (!tma) {
+        level<T, true, AX | AY | AZ>(src, a, out, stream);
+        return;
+    }
+    auto kernel = inv_tile_kernel<T, UX, UY, UZ, Out>;
+    static thread_local int configured_device = -1;
+    int dev = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (configured_device != dev) {
+        check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(S::smem)),
+              "inverse tile shared memory");
+        configured_device = dev;
+    }
+    const uint32_t tx = (a.x + UX - 1) / UX, ty = (a.y + UY - 1) / UY, tz = (a.z + UZ - 1) / UZ;
+    const uint64_t blocks = uint64_t(tx) * ty * tz;
+    need(blocks < (1ull << 31), "Waltz: level grid too large");
+    const InvLevel<T> lv{src.base, src.sy, src.sz, src.low, src.lo, a};
+    kernel<<<unsigned(blocks), 256, S::smem, stream>>>(lv, cmap, lmap, tx, ty, out, status); note_launch();
+    check(cudaGetLastError(), "inverse tile launch");
+}
+
 template <class T, class Out>
 __global__ void identity_kernel(const T* in, Dims d, Out out) {
     const uint64_t n = vol(d);
@@ -380,8 +414,8 @@ static uint64_t inverse_low_need(const Geometry& g) {
 // stage ping-pongs between bank2 and the freed C (or bank1). The finest level
 // hands every sample to `fin`.
 template <class T, class Final>
-static void inverse(const Geometry& g, T* C, T* bank1, T* bank2, const Final& fin, cudaStream_t stream,
-                    const char* final_stage = "inv_l0") {
+static void inverse(const Geometry& g, T* C, T* bank1, T* bank2, const Final& fin, uint32_t* status,
+                    cudaStream_t stream, const char* final_stage = "inv_l0") {
     StageClock& clock = stage_clock();
     const size_t sy = g.nx, sz = size_t(g.nx) * g.ny;
     const uint64_t half_off = ((g.n + 1) / 2 + 63) & ~uint64_t(63);
@@ -399,11 +433,11 @@ static void inverse(const Geometry& g, T* C, T* bank1, T* bank2, const Final& fi
             InvSrc<T> src{C, sy, sz, low, halve(a, AX | AY | AZ)};
             if (l > 0) {
                 T* dst = halves[l & 1];
-                level<T, true, AX | AY | AZ>(src, a, StoreOut<T>{dst, a.x, size_t(a.x) * a.y}, stream);
+                level_inv<T>(src, a, StoreOut<T>{dst, a.x, size_t(a.x) * a.y}, status, stream);
                 low = dst;
                 if (l == 1) clock.mark("inv_coarse", stream);
             } else {
-                level<T, true, AX | AY | AZ>(src, a, fin, stream);
+                level_inv<T>(src, a, fin, status, stream);
                 clock.mark(final_stage, stream);
             }
         }
@@ -568,7 +602,7 @@ static size_t compress(const T* d_in, uint32_t nx, uint32_t ny, uint32_t nz, dou
     // 4. inverse transform + repairs
     {
         RepairOut<T> fin{d_in, nx, size_t(nx) * ny, eb, T(eb), P.pbits, P.perr, P.status};
-        inverse<T>(g, P.C, P.inter, P.bank2, fin, stream, "inv_l0_repair");
+        inverse<T>(g, P.C, P.inter, P.bank2, fin, P.status, stream, "inv_l0_repair");
     }
     // 5. ordered side records
     compact_count_kernel<<<unsigned(cblocks), kCompactThreads, 0, stream>>>(P.pbits, words, P.counts_p); note_launch();
@@ -752,7 +786,7 @@ static void decode_launch(const uint8_t* d_in, const Header& h, const Layout& L,
         qpatch_kernel<T><<<(h.nq + 255) / 256, 256, 0, stream>>>(d_in + L.qi, d_in + L.qv, h.nq, g.n, T(h.q), C,
                                                                  status); note_launch();
     clock.mark("qpatch", stream);
-    inverse<T>(g, C, bank1, bank2, fin, stream);
+    inverse<T>(g, C, bank1, bank2, fin, status, stream);
     if (h.np)
         rpatch_kernel<T, Patch><<<(h.np + 255) / 256, 256, 0, stream>>>(d_in + L.pi, d_in + L.pv, h.np, g.n, patch,
                                                                         status); note_launch();
@@ -792,6 +826,7 @@ static void decode_finish(uint32_t status, const uint8_t* d_in, const Header& h,
     if (status & ST_BAD_QOUT) throw Error("invalid quantization outlier");
     if (status & ST_BAD_REPAIR) throw Error("nonfinite correction");
     if (status & ST_NONFINITE_INPUT) throw Error("nonfinite reconstruction");
+    if (status & ST_WAIT_TIMEOUT) throw Error("Waltz: asynchronous copy wait exceeded its bound");
 }
 
 template <class T>
@@ -982,7 +1017,7 @@ extern "C" int waltz_b200_transform(void* d_data, int width, uint32_t nx, uint32
                 check(cudaMemcpyAsync(data, P.C, g.n * sizeof(T), cudaMemcpyDeviceToDevice, s), "copy");
             } else {
                 check(cudaMemcpyAsync(P.C, data, g.n * sizeof(T), cudaMemcpyDeviceToDevice, s), "copy");
-                wb::inverse<T>(g, P.C, P.inter, P.bank2, StoreOut<T>{data, nx, size_t(nx) * ny}, s);
+                wb::inverse<T>(g, P.C, P.inter, P.bank2, StoreOut<T>{data, nx, size_t(nx) * ny}, P.status, s);
             }
             uint32_t st = 0;
             check(cudaMemcpyAsync(&st, P.status, 4, cudaMemcpyDeviceToHost, s), "readback");

@@ -1,0 +1,208 @@
+// Inverse dyadic level (synthesis Z, X, Y) from TMA-staged parity boxes.
+//
+// The coefficients of one level live in the reference's split-band layout:
+// along each axis the even spatial positions are the low half [0, ceil(n/2))
+// and the odd positions the high half. The footprint of a spatial tile
+// (UX x UY x UZ outputs plus a 4-sample halo per side) therefore maps to eight
+// coefficient boxes, one per parity combination (x, y, z even or odd), each
+// (UX/2+4) x (UY/2+4) x (UZ/2+4). A CTA loads the eight boxes with tensor-map
+// copies (the all-even box from the separately reconstructed low band when
+// there is one), so every lifting pass reads its even samples from one box
+// and its odd samples from the other, and writes its outputs back in place.
+//
+// Inverse windows fold their endpoint normalisations along Y and Z, so those
+// results depend on the window (cpu/src/transform.cpp:110-147): the tile's Z
+// extent is exactly one canonical Z window (16 f32 / 8 f64 outputs at a
+// multiple of it) and its Y extent two canonical Y windows of 8. X does not
+// fold and takes the tile's whole row as one window.
+//
+// Edge tiles (footprint crossing the array) first fix every out-of-range cell
+// from its reflected position, coefficient-mapped like
+// include/transformers/halo3d.cuh:23-28 of the reference: copied from inside
+// the staged footprint when the reflected cell is there, else loaded.
+#pragma once
+#include "common.cuh"
+#include "tma.cuh"
+#include "transform.cuh"
+
+namespace wb {
+
+template <class T> struct InvTile;
+template <> struct InvTile<float> {
+    static constexpr int UX = 32, UY = 16, UZ = 16;
+};
+template <> struct InvTile<double> {
+    static constexpr int UX = 16, UY = 16, UZ = 8;
+};
+
+template <class T, int UX, int UY, int UZ> struct InvShape {
+    static constexpr int V = 16 / int(sizeof(T));       // elements per 16 bytes
+    static constexpr int HX = UX / 2 + 4, HY = UY / 2 + 4, HZ = UZ / 2 + 4;
+    static constexpr int PADX = (V - 2 % V) % V;         // box x origin = ox/2 - 2 - PADX (16-byte aligned)
+    static constexpr int BX = (HX + PADX + V - 1) / V * V;
+    static constexpr int BOX = HZ * HY * BX;             // elements per parity box
+    static constexpr int FX = UX + 8, FY = UY + 8, FZ = UZ + 8;
+    static constexpr size_t smem = size_t(8) * BOX * sizeof(T) + 128 + 16;
+    static_assert((BOX * sizeof(T)) % 128 == 0, "parity boxes must stay 128-byte aligned");
+    static_assert(UX % (2 * V) == 0 && UZ == (sizeof(T) == 4 ? 16 : 8) && UY % 8 == 0, "tile shape");
+};
+
+// Emission and source description of one inverse level.
+template <class T> struct InvLevel {
+    const T* base;  // coefficients (split layout), strides sy, sz
+    size_t sy, sz;
+    const T* low;   // reconstructed low band (compact, dims lo) or null
+    Dims lo;
+    Dims a;         // level dims
+};
+
+template <class T, int UX, int UY, int UZ, class Out>
+__global__ void __launch_bounds__(256, 2)
+    inv_tile_kernel(InvLevel<T> lv, const __grid_constant__ CUtensorMap cmap, const __grid_constant__ CUtensorMap lmap,
+                    uint32_t tiles_x, uint32_t tiles_y, Out out, uint32_t* status) {
+    using S = InvShape<T, UX, UY, UZ>;
+    extern __shared__ __align__(128) unsigned char inv_smem[];
+    T* Bx = reinterpret_cast<T*>(inv_smem + ((128 - (smem_u32(inv_smem) & 127)) & 127));
+    uint64_t* bar = reinterpret_cast<uint64_t*>(Bx + 8 * S::BOX);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const Dims a = lv.a;
+    const uint32_t bx = blockIdx.x % tiles_x, by = (blockIdx.x / tiles_x) % tiles_y, bz = blockIdx.x / (tiles_x * tiles_y);
+    const uint32_t ox = bx * UX, oy = by * UY, oz = bz * UZ;
+    const uint32_t hx = half_len(a.x), hy = half_len(a.y), hz = half_len(a.z);
+
+    // staged cell of spatial footprint position (fx, fy, fz)
+    auto cell = [&](int fx, int fy, int fz) -> T* {
+        return Bx + ((fz & 1) * 4 + (fy & 1) * 2 + (fx & 1)) * S::BOX + ((fz >> 1) * S::HY + (fy >> 1)) * S::BX +
+               (fx >> 1) + S::PADX;
+    };
+
+    // ---- stage the eight parity boxes
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        fence_barrier_init();
+        mbar_expect_tx(bar, uint32_t(8 * S::BOX * sizeof(T)));
+        const int x0 = int(ox / 2) - 2 - S::PADX, y0 = int(oy / 2) - 2, z0 = int(oz / 2) - 2;
+#pragma unroll 1
+        for (int b = 0; b < 8; ++b) {
+            const int xp = b & 1, yp = (b >> 1) & 1, zp = b >> 2;
+            const bool from_low = b == 0 && lv.low != nullptr;
+            tma_load_3d(Bx + b * S::BOX, from_low ? &lmap : &cmap, x0 + (xp ? int(hx) : 0), y0 + (yp ? int(hy) : 0),
+                        z0 + (zp ? int(hz) : 0), bar);
+        }
+    }
+    {
+        const bool ok = __syncthreads_and(warp != 0 || mbar_wait(bar, 0, kWaitBound));
+        if (!ok) {
+            if (tid == 0) atomicOr(status, ST_WAIT_TIMEOUT);
+            return;
+        }
+    }
+    // ---- edge tiles: out-of-range cells from their reflections
+    const bool edge = ox < 4 || ox + UX + 4 > a.x || oy < 4 || oy + UY + 4 > a.y || oz < 4 || oz + UZ + 4 > a.z;
+    if (edge) {
+        for (int r = warp; r < S::FY * S::FZ; r += 8) {
+            const int fy = r % S::FY, fz = r / S::FY;
+            const int64_t py = int64_t(oy) + fy - 4, pz = int64_t(oz) + fz - 4;
+            const bool row_in = py >= 0 && py < int64_t(a.y) && pz >= 0 && pz < int64_t(a.z);
+            for (int fx = lane; fx < S::FX; fx += 32) {
+                const int64_t px = int64_t(ox) + fx - 4;
+                if (row_in && px >= 0 && px < int64_t(a.x)) continue;
+                const uint32_t mx = mirror(px, a.x), my = mirror(py, a.y), mz = mirror(pz, a.z);
+                const int64_t gx = int64_t(mx) - (int64_t(ox) - 4), gy = int64_t(my) - (int64_t(oy) - 4),
+                              gz = int64_t(mz) - (int64_t(oz) - 4);
+                T v;
+                if (gx >= 0 && gx < S::FX && gy >= 0 && gy < S::FY && gz >= 0 && gz < S::FZ) {
+                    v = *cell(int(gx), int(gy), int(gz));
+                } else {
+                    const uint32_t cx = split_of(mx, a.x), cy = split_of(my, a.y), cz = split_of(mz, a.z);
+                    if (lv.low && cx < lv.lo.x && cy < lv.lo.y && cz < lv.lo.z)
+                        v = lv.low[(size_t(cz) * lv.lo.y + cy) * lv.lo.x + cx];
+                    else
+                        v = lv.base[size_t(cz) * lv.sz + size_t(cy) * lv.sy + cx];
+                }
+                *cell(fx, fy, fz) = v;
+            }
+        }
+        __syncthreads();
+    }
+
+    // ---- Z: every (x, y) footprint column, one canonical window, in place
+    {
+        constexpr int P = UZ / 2 + 4;
+        for (int L = tid; L < S::FX * S::FY; L += 256) {
+            // lines enumerated x-index fastest inside one (x parity, y parity)
+            // box, so a warp reads consecutive words of one box
+            const int i = L % (S::FX / 2), k = (L / (S::FX / 2)) % (S::FY / 2);
+            const int par = L / ((S::FX / 2) * (S::FY / 2)); // 0..3: x parity, y parity
+            const int fx = 2 * i + (par & 1), fy = 2 * k + (par >> 1);
+            T e[P], o[P];
+#pragma unroll
+            for (int j = 0; j < P; ++j) {
+                e[j] = *cell(fx, fy, 2 * j);
+                o[j] = *cell(fx, fy, 2 * j + 1);
+            }
+            lift_inverse<T, P, true>(e, o);
+#pragma unroll
+            for (int j = 2; j < P - 2; ++j) {
+                const int u = 2 * (j - 2); // output z = oz + u at footprint z = u + 4
+                *cell(fx, fy, u + 4) = e[j];
+                *cell(fx, fy, u + 5) = o[j];
+            }
+        }
+    }
+    __syncthreads();
+    // ---- X: every (y, z) row of the Z outputs, one window over the row
+    {
+        constexpr int P = UX / 2 + 4;
+        for (int L = tid; L < S::FY * UZ; L += 256) {
+            const int fy = L % S::FY, fz = 4 + L / S::FY;
+            T e[P], o[P];
+#pragma unroll
+            for (int j = 0; j < P; ++j) {
+                e[j] = *cell(2 * j, fy, fz);
+                o[j] = *cell(2 * j + 1, fy, fz);
+            }
+            lift_inverse<T, P, false>(e, o);
+#pragma unroll
+            for (int j = 2; j < P - 2; ++j) {
+                const int u = 2 * (j - 2);
+                *cell(u + 4, fy, fz) = e[j];
+                *cell(u + 5, fy, fz) = o[j];
+            }
+        }
+    }
+    __syncthreads();
+    // ---- Y: every (x, z) column of the tile, two canonical windows of 8,
+    // emitted from registers. Lanes 0-15 take even x, 16-31 odd x, so a warp
+    // covers 32 consecutive x.
+    {
+        constexpr int P = 8 / 2 + 4;
+        constexpr int WIN = UY / 8;
+        for (int L = tid; L < UX * UZ; L += 256) {
+            const int zrow = L / UX, xr = L % UX;
+            const int u_x = 2 * (xr % (UX / 2)) + xr / (UX / 2); // first half of a row: even x
+            const int fx = u_x + 4, fz = zrow + 4;
+            T e[P], o[P];
+#pragma unroll
+            for (int win = 0; win < WIN; ++win) {
+#pragma unroll
+                for (int j = 0; j < P; ++j) {
+                    e[j] = *cell(fx, win * 8 + 2 * j, fz);
+                    o[j] = *cell(fx, win * 8 + 2 * j + 1, fz);
+                }
+                lift_inverse<T, P, true>(e, o);
+                const uint32_t gx = ox + u_x, gz = oz + zrow;
+                if (gx < a.x && gz < a.z) {
+#pragma unroll
+                    for (int j = 2; j < P - 2; ++j) {
+                        const uint32_t gy = oy + win * 8 + 2 * (j - 2);
+                        if (gy < a.y) out(gx, gy, gz, e[j]);
+                        if (gy + 1 < a.y) out(gx, gy + 1, gz, o[j]);
+                    }
+                }
+            }
+        }
+    }
+}
+
+} // namespace wb
