@@ -43,13 +43,21 @@ constexpr uint64_t kAggregate = 1ull << 62;
 constexpr uint64_t kInclusive = 2ull << 62;
 constexpr uint64_t kValueMask = (1ull << 62) - 1;
 
+// Payload bytes one chunk can stage: RZE output (at most the 2 * 8192 plane
+// bytes plus 2048 + 256 + 32 + 4 bitmap bytes) or the raw magnitudes, then up
+// to 1024 sign bytes, plus slack for the word-wide copy.
+constexpr uint32_t kEncBytes = 2 * kChunk + 2048 + 256 + 32 + 4 + 1024 + 60;
+
 struct WzpEncodeSmem {
-    uint16_t m[kChunk];                // magnitudes
+    union {
+        uint16_t m[kChunk];            // magnitudes (until the sign pass)
+        uint8_t enc[kEncBytes];        // the chunk's payload as written
+    };
     uint8_t planes[2 * kChunk];        // bit-plane transposed chunk
-    uint8_t enc[2 * kChunk];           // zero/repetition-eliminated bytes
     uint8_t lv[2048 + 256 + 32 + 4];   // nonzero bitmap and its reductions
     uint32_t sgn[kChunk / 32];         // compacted sign bits
     uint32_t gcount[kChunk / 32];      // nonzero magnitudes per 32-group
+    uint32_t sel[16];                  // byte_perm selectors: compact the bytes of a 4-bit mask
     uint32_t tmp[40];
     uint32_t chunk, excl;
 };
@@ -64,9 +72,48 @@ struct WzpEncodeArgs {
     uint64_t* state;    // per chunk, zeroed before launch
     uint64_t* sizes;    // per chunk byte count (output)
     uint32_t* status;
-    uint32_t spin_cap;  // lookback wait bound (iterations of ~0.5 us)
+    uint32_t spin_cap;  // lookback wait bound (polls of ~0.2 us)
     uint32_t skip_publish; // test hook: this chunk never publishes (0xffffffff = none)
 };
+
+// 4-bit mask of the nonzero bytes of w (bit k = byte k).
+__device__ __forceinline__ uint32_t nonzero_nibble(uint32_t w) { return (__vsetne4(w, 0u) * 0x01020408u) >> 24; }
+// 4-bit mask of the bytes of w that differ from the byte before them
+// (`prev` is the byte preceding w).
+__device__ __forceinline__ uint32_t changed_nibble(uint32_t w, uint32_t prev) {
+    return (__vsetne4(w, (w << 8) | (prev & 0xffu)) * 0x01020408u) >> 24;
+}
+// Appends the bytes of w selected by the 4-bit mask to dst + o; returns how many.
+__device__ __forceinline__ uint32_t put_selected(uint8_t* dst, uint32_t o, uint32_t w, uint32_t mask,
+                                                 const uint32_t* sel) {
+    const uint32_t c = __popc(mask), cw = __byte_perm(w, 0u, sel[mask]);
+    if (c > 0) dst[o] = uint8_t(cw);
+    if (c > 1) dst[o + 1] = uint8_t(cw >> 8);
+    if (c > 2) dst[o + 2] = uint8_t(cw >> 16);
+    if (c > 3) dst[o + 3] = uint8_t(cw >> 24);
+    return c;
+}
+
+// Copies len bytes from 4-byte aligned shared memory to any global address:
+// aligned 32-bit stores for whole destination words, byte stores at the two
+// ends. src must stay readable 4 bytes past len.
+__device__ __forceinline__ void copy_to_global(uint8_t* dst, const uint8_t* src, uint32_t len, int tid, int nthreads) {
+    const uint32_t mis = uint32_t(reinterpret_cast<uintptr_t>(dst) & 3u);
+    uint32_t* base = reinterpret_cast<uint32_t*>(dst - mis);
+    const uint32_t* sw = reinterpret_cast<const uint32_t*>(src);
+    const uint32_t total = mis + len, words = (total + 3) / 4;
+    for (uint32_t j = tid; j < words; j += nthreads) {
+        const int64_t r0 = int64_t(4 * j) - mis; // source offset of the word's first byte
+        if (r0 >= 0 && r0 + 4 <= int64_t(len)) {
+            base[j] = mis ? __funnelshift_r(sw[j - 1], sw[j], 8 * (4 - mis)) : sw[j];
+        } else {
+            for (int t = 0; t < 4; ++t) {
+                const int64_t r = r0 + t;
+                if (r >= 0 && r < int64_t(len)) dst[r] = src[r];
+            }
+        }
+    }
+}
 
 __global__ void __launch_bounds__(kWzpThreads) wzp_encode_kernel(WzpEncodeArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -75,6 +122,15 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_encode_kernel(WzpEncodeArgs A
     constexpr int NW = kWzpThreads / 32;
     const uint32_t chunks = wzp_chunks(A.n), groups = wzp_groups(A.n);
     if (tid == 0) S.chunk = atomicAdd(A.ticket, 1u);
+    if (tid < 16) {
+        uint32_t sel = 0x4444u, k = 0;
+        for (int b = 0; b < 4; ++b)
+            if ((tid >> b) & 1) {
+                sel = (sel & ~(0xfu << (4 * k))) | (uint32_t(b) << (4 * k));
+                ++k;
+            }
+        S.sel[tid] = sel;
+    }
     __syncthreads();
     const uint32_t c = S.chunk;
     if (c >= chunks) return;
@@ -92,18 +148,22 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_encode_kernel(WzpEncodeArgs A
     for (int i = tid; i < int(kChunk / 32); i += kWzpThreads) S.sgn[i] = 0;
     __syncthreads();
 
-    // ---- per 32-group nonzero counts, bit planes (warp ballots)
+    // ---- per 32-group nonzero counts, bit planes (warp ballots; planes above
+    // the group's highest set bit are zero and skip their ballots)
     for (int g = warp; g < int(kChunk / 32); g += NW) {
         const int e = g * 32 + lane;
         const uint32_t v = S.m[e];
         const uint32_t nzmask = __ballot_sync(0xffffffffu, v != 0);
         if (lane == 0) S.gcount[g] = __popc(nzmask);
         if (uint32_t(g * 32) < blocks * 16) {
+            const int top = 32 - __clz(__reduce_or_sync(0xffffffffu, v)); // planes 16-top .. 15 may be set
             uint32_t mine = 0;
 #pragma unroll
             for (int p = 0; p < 16; ++p) {
-                const uint32_t r = __brev(__ballot_sync(0xffffffffu, (v >> (15 - p)) & 1u));
-                if (lane == p) mine = r;
+                if (15 - p < top) {
+                    const uint32_t r = __brev(__ballot_sync(0xffffffffu, (v >> (15 - p)) & 1u));
+                    if (lane == p) mine = r;
+                }
             }
             uint16_t* pl = reinterpret_cast<uint16_t*>(S.planes);
             if (lane < 16) {
@@ -143,103 +203,77 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_encode_kernel(WzpEncodeArgs A
             if (sh && (packed >> (32 - sh))) atomicOr(&S.sgn[(r >> 5) + 1], packed >> (32 - sh));
         }
     }
+    __syncthreads(); // S.m is dead from here on: S.enc reuses its bytes
 
-    // ---- zero elimination of the plane bytes
+    // ---- zero elimination of the plane bytes: thread t owns bytes 32t..32t+31
     const uint32_t raw_bytes = 2 * count;
     uint32_t nzb, c1 = 0, c2 = 0, c3 = 0;
     {
         const uint32_t b0 = tid * 32;
-        uint32_t bits = 0;
+        uint32_t w[8];
         const uint4* q = reinterpret_cast<const uint4*>(S.planes + b0);
+        const uint4 q0 = q[0], q1 = q[1];
+        w[0] = q0.x; w[1] = q0.y; w[2] = q0.z; w[3] = q0.w;
+        w[4] = q1.x; w[5] = q1.y; w[6] = q1.z; w[7] = q1.w;
+        uint32_t bits = 0;
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const uint4 w = q[h];
-            const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+        for (int k = 0; k < 8; ++k) bits |= nonzero_nibble(w[k]) << (4 * k);
+        if (b0 + 32 > raw_bytes) bits &= b0 >= raw_bytes ? 0u : ((1u << (raw_bytes - b0)) - 1u);
+        uint32_t o = block_excl_scan<kWzpThreads>(__popc(bits), S.tmp, nzb);
 #pragma unroll
-            for (int k = 0; k < 16; ++k) {
-                const uint32_t byte = (ws[k >> 2] >> (8 * (k & 3))) & 0xffu;
-                const uint32_t at = b0 + h * 16 + k;
-                if (byte && at < raw_bytes) bits |= 1u << (h * 16 + k);
-            }
-        }
-        const uint32_t off = block_excl_scan<kWzpThreads>(__popc(bits), S.tmp, nzb);
-        uint32_t o = off;
-        for (uint32_t b = bits; b; b &= b - 1) {
-            const int k = __ffs(b) - 1;
-            if (o < 2 * kChunk) S.enc[o] = S.planes[b0 + k];
-            ++o;
-        }
-        S.lv[4 * tid + 0] = uint8_t(bits);
-        S.lv[4 * tid + 1] = uint8_t(bits >> 8);
-        S.lv[4 * tid + 2] = uint8_t(bits >> 16);
-        S.lv[4 * tid + 3] = uint8_t(bits >> 24);
+        for (int k = 0; k < 8; ++k) o += put_selected(S.enc, o, w[k], (bits >> (4 * k)) & 15u, S.sel);
+        reinterpret_cast<uint32_t*>(S.lv)[tid] = bits; // bitmap bytes 4t..4t+3
     }
     __syncthreads();
-    // ---- repetition elimination: 2048 -> 256 -> 32 -> 4 bytes
+    // ---- repetition elimination: 2048 -> 256 -> 32 -> 4 bytes; a byte is
+    // kept iff it differs from the byte before it (before the first: 0)
     {
         // level 1: thread t < 256 owns bitmap bytes 8t..8t+7
-        uint32_t flags = 0, cnt = 0;
+        uint32_t flags = 0, w0 = 0, w1 = 0;
         if (tid < 256) {
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const int i = tid * 8 + k;
-                const uint8_t prev = i ? S.lv[i - 1] : 0;
-                if (S.lv[i] != prev) flags |= 1u << k;
-            }
-            cnt = __popc(flags);
+            const uint32_t* lw = reinterpret_cast<const uint32_t*>(S.lv);
+            w0 = lw[2 * tid];
+            w1 = lw[2 * tid + 1];
+            const uint32_t prev = tid ? (lw[2 * tid - 1] >> 24) : 0u;
+            flags = changed_nibble(w0, prev) | (changed_nibble(w1, w0 >> 24) << 4);
         }
-        uint32_t off = block_excl_scan<kWzpThreads>(cnt, S.tmp, c1);
+        uint32_t o = nzb + block_excl_scan<kWzpThreads>(__popc(flags), S.tmp, c1);
         if (tid < 256) {
-            for (uint32_t b = flags; b; b &= b - 1) {
-                const int k = __ffs(b) - 1;
-                const uint32_t o = nzb + off++;
-                if (o < 2 * kChunk) S.enc[o] = S.lv[tid * 8 + k];
-            }
+            o += put_selected(S.enc, o, w0, flags & 15u, S.sel);
+            put_selected(S.enc, o, w1, flags >> 4, S.sel);
             S.lv[2048 + tid] = uint8_t(flags);
         }
         __syncthreads();
-        // level 2: warp 0, lane owns level-1 bytes 8l..8l+7
+        // levels 2 and 3 by warp 0
         if (warp == 0) {
-            uint32_t f2 = 0;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const int i = lane * 8 + k;
-                const uint8_t prev = i ? S.lv[2048 + i - 1] : 0;
-                if (S.lv[2048 + i] != prev) f2 |= 1u << k;
-            }
+            const uint32_t* l1 = reinterpret_cast<const uint32_t*>(S.lv + 2048);
+            const uint32_t v0 = l1[2 * lane], v1 = l1[2 * lane + 1];
+            const uint32_t pv = lane ? (l1[2 * lane - 1] >> 24) : 0u;
+            const uint32_t f2 = changed_nibble(v0, pv) | (changed_nibble(v1, v0 >> 24) << 4);
             const uint32_t n2 = __popc(f2);
             const uint32_t inc = warp_incl_scan(n2);
             c2 = __shfl_sync(0xffffffffu, inc, 31);
-            uint32_t o2 = inc - n2;
-            for (uint32_t b = f2; b; b &= b - 1) {
-                const int k = __ffs(b) - 1;
-                const uint32_t o = nzb + c1 + o2++;
-                if (o < 2 * kChunk) S.enc[o] = S.lv[2048 + lane * 8 + k];
-            }
+            uint32_t o2 = nzb + c1 + inc - n2;
+            o2 += put_selected(S.enc, o2, v0, f2 & 15u, S.sel);
+            put_selected(S.enc, o2, v1, f2 >> 4, S.sel);
             S.lv[2048 + 256 + lane] = uint8_t(f2);
             __syncwarp();
-            // level 3: lanes 0..3 own level-2 bytes 8l..8l+7
-            uint32_t f3 = 0;
+            const uint32_t* l2 = reinterpret_cast<const uint32_t*>(S.lv + 2048 + 256);
+            uint32_t f3 = 0, u0 = 0, u1 = 0;
             if (lane < 4) {
-#pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    const int i = lane * 8 + k;
-                    const uint8_t prev = i ? S.lv[2048 + 256 + i - 1] : 0;
-                    if (S.lv[2048 + 256 + i] != prev) f3 |= 1u << k;
-                }
+                u0 = l2[2 * lane];
+                u1 = l2[2 * lane + 1];
+                const uint32_t pu = lane ? (l2[2 * lane - 1] >> 24) : 0u;
+                f3 = changed_nibble(u0, pu) | (changed_nibble(u1, u0 >> 24) << 4);
             }
             const uint32_t n3 = __popc(f3);
             const uint32_t inc3 = warp_incl_scan(n3);
             c3 = __shfl_sync(0xffffffffu, inc3, 31);
-            uint32_t o3 = inc3 - n3;
-            for (uint32_t b = f3; b; b &= b - 1) {
-                const int k = __ffs(b) - 1;
-                const uint32_t o = nzb + c1 + c2 + o3++;
-                if (o < 2 * kChunk) S.enc[o] = S.lv[2048 + 256 + lane * 8 + k];
-            }
             if (lane < 4) {
-                const uint32_t o = nzb + c1 + c2 + c3 + lane;
-                if (o < 2 * kChunk) S.enc[o] = uint8_t(f3);
+                uint32_t o3 = nzb + c1 + c2 + inc3 - n3;
+                o3 += put_selected(S.enc, o3, u0, f3 & 15u, S.sel);
+                put_selected(S.enc, o3, u1, f3 >> 4, S.sel);
+                S.enc[nzb + c1 + c2 + c3 + lane] = uint8_t(f3);
             }
             if (lane == 0) {
                 S.tmp[34] = c2;
@@ -305,13 +339,25 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_encode_kernel(WzpEncodeArgs A
             store_u24(A.out + size_t(groups) * 4 + size_t(c) * 3, meta);
         }
     }
+    if (!nnz) return; // uniform: no payload, and no barrier follows
+    // ---- payload: magnitude bytes (raw: reloaded), then the sign bytes
+    if (raw) {
+        if (count == kChunk) {
+            const uint4* src = reinterpret_cast<const uint4*>(A.mag + first);
+            for (int i = tid; i < int(kChunk / 8); i += kWzpThreads) reinterpret_cast<uint4*>(S.enc)[i] = src[i];
+        } else {
+            for (int i = tid; i < int(count); i += kWzpThreads) reinterpret_cast<uint16_t*>(S.enc)[i] = A.mag[first + i];
+        }
+        __syncthreads();
+    }
+    {
+        const uint8_t* sb = reinterpret_cast<const uint8_t*>(S.sgn);
+        for (uint32_t i = tid; i < sbytes; i += kWzpThreads) S.enc[mbytes + i] = sb[i];
+    }
     __syncthreads();
-    if (!nnz || S.excl == 0xffffffffu) return;
-    uint8_t* dst = A.out + size_t(groups) * 4 + size_t(chunks) * 3 + S.excl;
-    const uint8_t* msrc = raw ? reinterpret_cast<const uint8_t*>(S.m) : S.enc;
-    for (uint32_t i = tid; i < mbytes; i += kWzpThreads) dst[i] = msrc[i];
-    const uint8_t* sb = reinterpret_cast<const uint8_t*>(S.sgn);
-    for (uint32_t i = tid; i < sbytes; i += kWzpThreads) dst[mbytes + i] = sb[i];
+    if (S.excl == 0xffffffffu) return;
+    copy_to_global(A.out + size_t(groups) * 4 + size_t(chunks) * 3 + S.excl, S.enc, uint32_t(chunk_bytes), tid,
+                   kWzpThreads);
 }
 
 // Group directory: payload offset of the first byte of every nonempty group.
