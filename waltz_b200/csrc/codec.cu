@@ -777,7 +777,14 @@ static void decode_launch(const uint8_t* d_in, const Header& h, const Layout& L,
                                        int(sizeof(WzpDecodeSmem))), "wzp smem");
             cfg_dev = dev;
         }
-        WzpDecodeArgs<T> da{wzp, h.wzp, n, BrickMap{g.nx, g.ny, g.nz, g.bz, irank}, T(h.q), C, status};
+        BrickMap map{g.nx, g.ny, g.nz, g.bz, irank, false, 0};
+        const uint32_t bsz = 256 * g.bz;
+        if (g.nx % 16 == 0 && g.ny % 16 == 0 && g.nz % g.bz == 0 && (bsz & (bsz - 1)) == 0 && bsz <= kChunk &&
+            kChunk / bsz <= 32) {
+            map.fast = true;
+            while ((1u << map.lb) < bsz) ++map.lb;
+        }
+        WzpDecodeArgs<T> da{wzp, h.wzp, n, map, T(h.q), C, status};
         wzp_decode_kernel<T><<<wzp_chunks(n), kWzpThreads, sizeof(WzpDecodeSmem), stream>>>(da); note_launch();
         check(cudaGetLastError(), "wzp decode launch");
     }

@@ -380,6 +380,19 @@ __global__ void wzp_directory_kernel(uint8_t* out, uint32_t n, const uint64_t* s
 struct BrickMap {
     uint32_t nx, ny, nz, bz;
     const uint16_t* local; // 8 slots x 256*bz: rank -> packed brick-local (x | y << 4 | z << 8)
+    // Fast map: every brick whole (16 | nx, 16 | ny, bz | nz) and 256*bz a power
+    // of two (lb = its log2), so a chunk is a run of whole bricks.
+    bool fast;
+    uint32_t lb;
+    __device__ __forceinline__ uint32_t brick_base(uint32_t b) const {
+        const uint32_t nbx = nx / 16, nby = ny / 16;
+        const uint32_t bxi = b % nbx, t = b / nbx, byi = t % nby, slab = t / nby;
+        return slab * bz * (nx * ny) + byi * 16 * nx + bxi * 16;
+    }
+    __device__ __forceinline__ uint32_t in_full_brick(uint32_t base, uint32_t rk) const {
+        const uint32_t loc = __ldg(local + rk);
+        return base + (loc >> 8) * (nx * ny) + ((loc >> 4) & 15u) * nx + (loc & 15u);
+    }
     // Every index fits 32 bits: archives hold at most 2^32 - 1 sample bytes.
     __device__ __forceinline__ uint32_t rowmajor(uint32_t k) const {
         const uint32_t plane = nx * ny;
@@ -403,6 +416,7 @@ struct BrickMap {
 };
 
 struct WzpDecodeSmem {
+    uint32_t bbase[32];                // row-major base of each whole brick of the chunk (fast map)
     uint16_t m[kChunk];
     uint8_t planes[2 * kChunk];
     uint8_t lv[2048 + 256 + 32 + 4];
@@ -605,23 +619,27 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_decode_kernel(WzpDecodeArgs<T
             }
         }
         __syncthreads();
-        // ---- inverse bit planes (warp shuffles of the plane words)
+        // ---- inverse bit planes: lane p < 16 holds plane p of the group's 32
+        // magnitudes (bit e = magnitude e's bit 15-p); a 32x32 bit transpose
+        // across the warp (five butterfly exchanges) leaves magnitude e in lane e
         const uint16_t* pl = reinterpret_cast<const uint16_t*>(S.planes);
         for (int g = warp; g < int(kChunk / 32); g += NW) {
             if (uint32_t(g * 32) >= blocks * 16) break;
-            uint32_t mine = 0;
+            uint32_t x = 0;
             if (lane < 16) {
-                mine = uint32_t(pl[lane * blocks + 2 * g]) << 16;
-                if (uint32_t(2 * g + 1) < blocks) mine |= pl[lane * blocks + 2 * g + 1];
+                uint32_t w = uint32_t(pl[lane * blocks + 2 * g]) << 16;
+                if (uint32_t(2 * g + 1) < blocks) w |= pl[lane * blocks + 2 * g + 1];
+                x = __brev(w);
             }
-            uint32_t v = 0;
 #pragma unroll
-            for (int p = 0; p < 16; ++p) {
-                const uint32_t r = __shfl_sync(0xffffffffu, mine, p);
-                v |= ((r >> (31 - lane)) & 1u) << (15 - p);
+            for (int j = 16; j >= 1; j >>= 1) {
+                const uint32_t m = j == 16 ? 0x0000ffffu : j == 8 ? 0x00ff00ffu : j == 4 ? 0x0f0f0f0fu
+                                 : j == 2  ? 0x33333333u : 0x55555555u;
+                const uint32_t y = __shfl_xor_sync(0xffffffffu, x, j);
+                x = (lane & j) ? ((x & ~m) | ((y >> j) & m)) : ((x & m) | ((y << j) & ~m));
             }
             const int e = g * 32 + lane;
-            if (uint32_t(e) < blocks * 16) S.m[e] = uint16_t(v);
+            if (uint32_t(e) < blocks * 16) S.m[e] = uint16_t(__brev(x) >> 16);
         }
         for (uint32_t i = blocks * 16 + tid; i < kChunk; i += kWzpThreads)
             S.m[i] = i < count ? pl[i] : 0;
@@ -629,12 +647,15 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_decode_kernel(WzpDecodeArgs<T
     __syncthreads();
 
     // ---- signs and dequantisation
+    for (int g = warp; g < int(kChunk / 32); g += NW) {
+        const uint32_t nzm = __ballot_sync(0xffffffffu, S.m[g * 32 + lane] != 0);
+        if (lane == 0) S.gprefix[g] = __popc(nzm);
+    }
+    if (A.map.fast && tid < int(kChunk >> A.map.lb)) S.bbase[tid] = A.map.brick_base((first >> A.map.lb) + tid);
+    __syncthreads();
     uint32_t nnz = 0;
     {
-        uint32_t gc = 0;
-        if (tid < int(kChunk / 32)) {
-            for (int k = 0; k < 32; ++k) gc += S.m[tid * 32 + k] != 0;
-        }
+        const uint32_t gc = tid < int(kChunk / 32) ? S.gprefix[tid] : 0;
         const uint32_t gp = block_excl_scan<kWzpThreads>(gc, S.tmp, nnz);
         if (tid < int(kChunk / 32)) S.gprefix[tid] = gp;
     }
@@ -656,7 +677,10 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_decode_kernel(WzpDecodeArgs<T
         }
         if (uint32_t(e) < count) {
             const T mag = Lift<T>::mul(T(v), A.q);
-            A.coeff[A.map.rowmajor(first + uint32_t(e))] = neg ? -mag : mag;
+            const uint32_t at = A.map.fast ? A.map.in_full_brick(S.bbase[uint32_t(e) >> A.map.lb],
+                                                                 uint32_t(e) & ((1u << A.map.lb) - 1u))
+                                           : A.map.rowmajor(first + uint32_t(e));
+            A.coeff[at] = neg ? -mag : mag;
         }
     }
     if (bad) atomicOr(A.status, ST_BAD_STREAM);
