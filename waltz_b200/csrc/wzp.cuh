@@ -417,7 +417,9 @@ struct BrickMap {
 
 struct WzpDecodeSmem {
     uint32_t bbase[32];                // row-major base of each whole brick of the chunk (fast map)
-    uint16_t m[kChunk];
+    uint16_t m[kChunk + 16];           // staged magnitude bytes, then the decoded magnitudes
+    uint8_t sb[1024 + 32];             // staged sign bytes
+    uint32_t xsel[16];                 // byte_perm selectors: spread 4-bit-mask bytes into place
     uint8_t planes[2 * kChunk];
     uint8_t lv[2048 + 256 + 32 + 4];
     uint32_t gprefix[kChunk / 32];
@@ -442,6 +444,27 @@ __device__ __forceinline__ WzpChunkInfo wzp_meta(uint32_t meta, uint32_t count) 
     if (r.sbytes > (count + 7) / 8) r.ok = false;
     r.mbytes = r.raw ? 2 * count : code;
     return r;
+}
+
+// Copies src[0, len) to dst[mis, mis + len), mis = src mod 16 (dst 16-byte
+// aligned): 16-byte loads for granules wholly inside the range, bytes at its
+// ends. Returns mis.
+__device__ __forceinline__ uint32_t stage_bytes(uint8_t* dst, const uint8_t* src, uint32_t len, int tid, int nt) {
+    const uint32_t mis = uint32_t(reinterpret_cast<uintptr_t>(src) & 15u);
+    const uint8_t* a0 = src - mis;
+    const uint32_t n16 = (mis + len + 15) / 16;
+    for (uint32_t i = tid; i < n16; i += nt) {
+        const uint32_t lo = 16 * i;
+        if (lo >= mis && lo + 16 <= mis + len) {
+            reinterpret_cast<uint4*>(dst)[i] = reinterpret_cast<const uint4*>(a0)[i];
+        } else {
+            for (uint32_t k = 0; k < 16; ++k) {
+                const uint32_t r = lo + k;
+                if (r >= mis && r < mis + len) dst[r] = a0[r];
+            }
+        }
+    }
+    return mis;
 }
 
 template <class T> struct WzpDecodeArgs {
@@ -494,17 +517,30 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_decode_kernel(WzpDecodeArgs<T
     }
     __syncthreads();
     if (S.bad) return;
-    const uint8_t* src = payload + S.off;
+    const uint8_t* gsrc = payload + S.off;
     const uint32_t mbytes = S.mbytes, sbytes = S.sbytes;
     const uint32_t raw_bytes = 2 * count;
     const uint32_t blocks = count / 16;
     bool bad = false;
+    // stage the chunk's compressed magnitude bytes and its sign bytes
+    uint8_t* mstage = reinterpret_cast<uint8_t*>(S.m);
+    uint32_t mis_m = 0, mis_s = 0;
+    if (mbytes && !S.raw) mis_m = stage_bytes(mstage, gsrc, mbytes, tid, kWzpThreads);
+    if (sbytes) mis_s = stage_bytes(S.sb, gsrc + mbytes, sbytes, tid, kWzpThreads);
+    if (tid < 16) {
+        uint32_t sel = 0, k = 0;
+        for (int b = 0; b < 4; ++b) sel |= (((tid >> b) & 1) ? k++ : 4u) << (4 * b);
+        S.xsel[tid] = sel;
+    }
+    __syncthreads();
+    const uint8_t* src = mstage + mis_m; // compressed magnitude bytes (RZE chunks)
+    const uint8_t* sgn = S.sb + mis_s;
 
     if (mbytes == 0) {
         for (int i = tid; i < int(kChunk); i += kWzpThreads) S.m[i] = 0;
     } else if (S.raw) {
         for (int i = tid; i < int(kChunk); i += kWzpThreads)
-            S.m[i] = i < int(count) ? uint16_t(src[2 * i] | (src[2 * i + 1] << 8)) : 0;
+            S.m[i] = i < int(count) ? uint16_t(gsrc[2 * i] | (gsrc[2 * i + 1] << 8)) : 0;
     } else {
         // ---- undo repetition elimination from the back of the stream
         uint32_t pos = mbytes - 4;
@@ -599,24 +635,26 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_decode_kernel(WzpDecodeArgs<T
                 const uint32_t allowed = keep == 32 ? 0xffffffffu : ((1u << keep) - 1u);
                 if (bits & ~allowed) bad = true;
             }
+            // spread the next popc(mask) stream bytes over each word's set
+            // bytes; every one of them must be nonzero and inside the stream
             uint32_t r = ex;
-            uint32_t* out32 = reinterpret_cast<uint32_t*>(S.planes + b0);
+            if (r + __popc(bits) > pos) bad = true;
+            const uint32_t* sw = reinterpret_cast<const uint32_t*>(mstage);
+            uint32_t words[8];
 #pragma unroll
             for (int w = 0; w < 8; ++w) {
-                uint32_t word = 0;
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const int i = w * 4 + k;
-                    uint32_t v = 0;
-                    if ((bits >> i) & 1u) {
-                        v = (!bad && r < pos) ? src[r] : 0;
-                        if (!v) bad = true;
-                        ++r;
-                    }
-                    word |= v << (8 * k);
-                }
-                out32[w] = word;
+                const uint32_t m4 = (bits >> (4 * w)) & 15u;
+                const uint32_t b = mis_m + r, wi = b >> 2;
+                const uint32_t val = __funnelshift_r(sw[wi], sw[wi + 1], 8 * (b & 3u));
+                const uint32_t word = __byte_perm(val, 0u, S.xsel[m4]);
+                if (nonzero_nibble(word) != m4) bad = true;
+                words[w] = bad ? 0u : word;
+                r += __popc(m4);
             }
+            __syncthreads(); // every thread has read the staged bytes it needs
+            uint4* out = reinterpret_cast<uint4*>(S.planes + b0);
+            out[0] = make_uint4(words[0], words[1], words[2], words[3]);
+            out[1] = make_uint4(words[4], words[5], words[6], words[7]);
         }
         __syncthreads();
         // ---- inverse bit planes: lane p < 16 holds plane p of the group's 32
@@ -661,10 +699,9 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_decode_kernel(WzpDecodeArgs<T
     }
     if (mbytes != 0) {
         if (nnz == 0 || (nnz + 7) / 8 != sbytes) bad = true;
-        else if ((nnz & 7) && (src[mbytes + sbytes - 1] >> (nnz & 7))) bad = true;
+        else if ((nnz & 7) && (sgn[sbytes - 1] >> (nnz & 7))) bad = true;
     }
     __syncthreads();
-    const uint8_t* sgn = src + mbytes;
     for (int g = warp; g < int(kChunk / 32); g += NW) {
         if (uint32_t(g * 32) >= count) break;
         const int e = g * 32 + lane;
