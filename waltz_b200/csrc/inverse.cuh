@@ -126,48 +126,66 @@ __global__ void __launch_bounds__(256, 2)
         __syncthreads();
     }
 
-    // ---- Z: every (x, y) footprint column, one canonical window, in place
+    // ---- Z: every (x, y) footprint column, one canonical window, in place.
+    // Pair j of a line sits at slot j of the z-even and z-odd boxes, and the
+    // outputs of pair j overwrite exactly those two slots.
+    constexpr int ZS = S::HY * S::BX; // z-slot stride inside a box
     {
         constexpr int P = UZ / 2 + 4;
         for (int L = tid; L < S::FX * S::FY; L += 256) {
-            // lines enumerated x-index fastest inside one (x parity, y parity)
-            // box, so a warp reads consecutive words of one box
+            // x index fastest inside one (x parity, y parity) box
             const int i = L % (S::FX / 2), k = (L / (S::FX / 2)) % (S::FY / 2);
-            const int par = L / ((S::FX / 2) * (S::FY / 2)); // 0..3: x parity, y parity
-            const int fx = 2 * i + (par & 1), fy = 2 * k + (par >> 1);
+            const int par = L / ((S::FX / 2) * (S::FY / 2)); // x parity + 2 * y parity
+            T* pe = Bx + par * S::BOX + k * S::BX + i + S::PADX;
+            T* po = pe + 4 * S::BOX;
             T e[P], o[P];
 #pragma unroll
             for (int j = 0; j < P; ++j) {
-                e[j] = *cell(fx, fy, 2 * j);
-                o[j] = *cell(fx, fy, 2 * j + 1);
+                e[j] = pe[j * ZS];
+                o[j] = po[j * ZS];
             }
             lift_inverse<T, P, true>(e, o);
 #pragma unroll
             for (int j = 2; j < P - 2; ++j) {
-                const int u = 2 * (j - 2); // output z = oz + u at footprint z = u + 4
-                *cell(fx, fy, u + 4) = e[j];
-                *cell(fx, fy, u + 5) = o[j];
+                pe[j * ZS] = e[j];
+                po[j * ZS] = o[j];
             }
         }
     }
     __syncthreads();
-    // ---- X: every (y, z) row of the Z outputs, one window over the row
+    // ---- X: every (y, z) row of the Z outputs, one window over the row; the
+    // x-even and x-odd halves of a row are read and written as 16-byte vectors
     {
         constexpr int P = UX / 2 + 4;
+        constexpr int NV = S::BX / S::V; // 16-byte vectors per box row
         for (int L = tid; L < S::FY * UZ; L += 256) {
             const int fy = L % S::FY, fz = 4 + L / S::FY;
+            T* re = Bx + ((fz & 1) * 4 + (fy & 1) * 2) * S::BOX + ((fz >> 1) * S::HY + (fy >> 1)) * S::BX;
+            T* ro = re + S::BOX;
+            T ve[S::BX], vo[S::BX];
+#pragma unroll
+            for (int q = 0; q < NV; ++q) {
+                *reinterpret_cast<uint4*>(ve + q * S::V) = reinterpret_cast<const uint4*>(re)[q];
+                *reinterpret_cast<uint4*>(vo + q * S::V) = reinterpret_cast<const uint4*>(ro)[q];
+            }
             T e[P], o[P];
 #pragma unroll
             for (int j = 0; j < P; ++j) {
-                e[j] = *cell(2 * j, fy, fz);
-                o[j] = *cell(2 * j + 1, fy, fz);
+                e[j] = ve[S::PADX + j];
+                o[j] = vo[S::PADX + j];
             }
             lift_inverse<T, P, false>(e, o);
 #pragma unroll
             for (int j = 2; j < P - 2; ++j) {
-                const int u = 2 * (j - 2);
-                *cell(u + 4, fy, fz) = e[j];
-                *cell(u + 5, fy, fz) = o[j];
+                ve[S::PADX + j] = e[j];
+                vo[S::PADX + j] = o[j];
+            }
+            // slots PADX+2 .. PADX+P-3 changed: whole vectors from (PADX+2)/V on
+            static_assert((S::PADX + 2) % S::V == 0, "X outputs start on a vector");
+#pragma unroll
+            for (int q = (S::PADX + 2) / S::V; q < (S::PADX + P - 2 + S::V - 1) / S::V; ++q) {
+                reinterpret_cast<uint4*>(re)[q] = *reinterpret_cast<const uint4*>(ve + q * S::V);
+                reinterpret_cast<uint4*>(ro)[q] = *reinterpret_cast<const uint4*>(vo + q * S::V);
             }
         }
     }
@@ -178,21 +196,31 @@ __global__ void __launch_bounds__(256, 2)
     {
         constexpr int P = 8 / 2 + 4;
         constexpr int WIN = UY / 8;
+        constexpr int K = S::HY; // y slots per parity
         for (int L = tid; L < UX * UZ; L += 256) {
             const int zrow = L / UX, xr = L % UX;
             const int u_x = 2 * (xr % (UX / 2)) + xr / (UX / 2); // first half of a row: even x
             const int fx = u_x + 4, fz = zrow + 4;
-            T e[P], o[P];
+            const T* pe = Bx + ((fz & 1) * 4 + (fx & 1)) * S::BOX + (fz >> 1) * ZS + (fx >> 1) + S::PADX;
+            const T* po = pe + 2 * S::BOX;
+            T ye[K], yo[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                ye[k] = pe[k * S::BX];
+                yo[k] = po[k * S::BX];
+            }
+            const uint32_t gx = ox + u_x, gz = oz + zrow;
+            const bool live = gx < a.x && gz < a.z;
 #pragma unroll
             for (int win = 0; win < WIN; ++win) {
+                T e[P], o[P];
 #pragma unroll
                 for (int j = 0; j < P; ++j) {
-                    e[j] = *cell(fx, win * 8 + 2 * j, fz);
-                    o[j] = *cell(fx, win * 8 + 2 * j + 1, fz);
+                    e[j] = ye[4 * win + j];
+                    o[j] = yo[4 * win + j];
                 }
                 lift_inverse<T, P, true>(e, o);
-                const uint32_t gx = ox + u_x, gz = oz + zrow;
-                if (gx < a.x && gz < a.z) {
+                if (live) {
 #pragma unroll
                     for (int j = 2; j < P - 2; ++j) {
                         const uint32_t gy = oy + win * 8 + 2 * (j - 2);
