@@ -144,6 +144,8 @@ def gpu_arm(args, rank, world, local_rank):
     max_err = float((out.double() - field.double()).abs().max())
     assert max_err <= eb, f"bound violated: {max_err} > {eb}"
     first = archive[:size].clone()
+    header = first[:32].cpu().numpy().tobytes()
+    n_repairs, n_qout = int.from_bytes(header[24:28], "little"), int.from_bytes(header[28:32], "little")
 
     for _ in range(args.warmup):
         decompress(compress())
@@ -234,7 +236,8 @@ def gpu_arm(args, rank, world, local_rank):
                                "step = compress + decompress" % (*shape, eb),
                    "global_batch": world, "seq_len": None, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (512 MiB field)", "archive_bytes": a_bytes,
-                   "compression_ratio": round(nbytes / a_bytes, 4), "max_abs_error": max_err, "abs_bound": eb},
+                   "compression_ratio": round(nbytes / a_bytes, 4), "max_abs_error": max_err, "abs_bound": eb,
+                   "repair_records": n_repairs, "q_outliers": n_qout},
         "compress_gbs": round(nbytes / t_c / 1e9, 3),
         "decompress_gbs": round(nbytes / t_d / 1e9, 3),
         "compress_hbm_frac": round((nbytes + a_bytes) / t_c / 1e9 / hbm, 4),

@@ -9,6 +9,7 @@ namespace wb {
 
 // A tile's samples clipped into its place inside the (z, y, x) frame.
 template <class T> struct FrameOut {
+    static constexpr bool kPrefetch = false;
     T* dst;                 // frame base of this job's (side, sample)
     uint32_t fx, fy, fz;    // frame dims
     uint32_t ox, oy, oz;    // tile origin inside the frame

@@ -601,7 +601,10 @@ static size_t compress(const T* d_in, uint32_t nx, uint32_t ny, uint32_t nz, dou
     clock.mark("wzp_encode", stream);
     // 4. inverse transform + repairs
     {
-        RepairOut<T> fin{d_in, nx, size_t(nx) * ny, eb, T(eb), P.pbits, P.perr, P.status};
+        // fast-accept threshold of the repair check (float): eb * (1 - 2^-21), rounded down
+        T safe = T(eb * (1.0 - std::ldexp(1.0, -21)));
+        if (double(safe) > eb * (1.0 - std::ldexp(1.0, -21))) safe = std::nextafter(safe, T(0));
+        RepairOut<T> fin{d_in, nx, size_t(nx) * ny, eb, T(eb), P.pbits, P.perr, P.status, safe};
         inverse<T>(g, P.C, P.inter, P.bank2, fin, P.status, stream, "inv_l0_repair");
     }
     // 5. ordered side records

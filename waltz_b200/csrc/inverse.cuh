@@ -211,6 +211,13 @@ __global__ void __launch_bounds__(256, 2)
             }
             const uint32_t gx = ox + u_x, gz = oz + zrow;
             const bool live = gx < a.x && gz < a.z;
+            // operands the emitter needs (the originals, for repairs) are
+            // fetched before the synthesis so their latency overlaps it
+            T pre[UY];
+            if constexpr (Out::kPrefetch) {
+#pragma unroll
+                for (int k = 0; k < UY; ++k) pre[k] = (live && oy + k < a.y) ? out.fetch(gx, oy + k, gz) : T(0);
+            }
 #pragma unroll
             for (int win = 0; win < WIN; ++win) {
                 T e[P], o[P];
@@ -224,8 +231,13 @@ __global__ void __launch_bounds__(256, 2)
 #pragma unroll
                     for (int j = 2; j < P - 2; ++j) {
                         const uint32_t gy = oy + win * 8 + 2 * (j - 2);
-                        if (gy < a.y) out(gx, gy, gz, e[j]);
-                        if (gy + 1 < a.y) out(gx, gy + 1, gz, o[j]);
+                        if constexpr (Out::kPrefetch) {
+                            if (gy < a.y) out.emit(gx, gy, gz, e[j], pre[win * 8 + 2 * (j - 2)]);
+                            if (gy + 1 < a.y) out.emit(gx, gy + 1, gz, o[j], pre[win * 8 + 2 * (j - 2) + 1]);
+                        } else {
+                            if (gy < a.y) out(gx, gy, gz, e[j]);
+                            if (gy + 1 < a.y) out(gx, gy + 1, gz, o[j]);
+                        }
                     }
                 }
             }

@@ -112,6 +112,10 @@ __global__ void check_finite_kernel(const T* in, uint64_t n, uint32_t* status) {
 // Encoder repair emitter for the finest synthesis: err = T(value - orig);
 // a sample is patched iff |err| > T(eb); the corrected value must be finite
 // and strictly within eb of the original (cpu/src/repair_avx2.cpp:57-74).
+// The original is fetched ahead of the synthesis (kPrefetch). A corrected
+// value whose rounded float difference is at most `safe` (eb shrunk by
+// 2^-21, rounded down) passes the strict double check for certain, so only
+// values near the bound take the two-difference test; float only.
 template <class T> struct RepairOut {
     const T* orig;
     size_t sy, sz;
@@ -120,25 +124,38 @@ template <class T> struct RepairOut {
     uint32_t* pbits;  // row-major bitmap of patched samples
     T* perr;          // dense errors (sparse use)
     uint32_t* status;
-    __device__ __forceinline__ void operator()(uint32_t x, uint32_t y, uint32_t z, T v) const {
-        const size_t i = size_t(z) * sz + size_t(y) * sy + x;
-        const T o = orig[i];
+    T safe;           // float: fast-accept threshold; double: unused
+    static constexpr bool kPrefetch = true;
+    __device__ __forceinline__ T fetch(uint32_t x, uint32_t y, uint32_t z) const {
+        return __ldg(orig + size_t(z) * sz + size_t(y) * sy + x);
+    }
+    __device__ __forceinline__ void emit(uint32_t x, uint32_t y, uint32_t z, T v, T o) const {
         const T err = Lift<T>::sub(v, o);
-        uint32_t st = 0;
-        if (!finite_bits(v) || !finite_bits(err)) st |= ST_BOUND;
-        T w = v;
-        if (fabs(double(err)) > double(nb)) {
+        const bool patched = fabs(err) > nb;
+        const T w = patched ? Lift<T>::sub(v, err) : v;
+        bool ok = finite_bits(v) && finite_bits(err) && finite_bits(w);
+        if (ok) {
+            if constexpr (sizeof(T) == 4) {
+                if (!(fabsf(Lift<T>::sub(w, o)) <= safe)) ok = strictly_within(double(w), double(o), bound);
+            } else {
+                ok = strictly_within(double(w), double(o), bound);
+            }
+        }
+        if (patched) {
+            const size_t i = size_t(z) * sz + size_t(y) * sy + x;
             atomicOr(&pbits[i >> 5], 1u << (i & 31));
             perr[i] = err;
-            w = Lift<T>::sub(v, err);
         }
-        if (!finite_bits(w) || !strictly_within(double(w), double(o), bound)) st |= ST_BOUND;
-        if (st) atomicOr(status, st);
+        if (!ok) atomicOr(status, ST_BOUND);
+    }
+    __device__ __forceinline__ void operator()(uint32_t x, uint32_t y, uint32_t z, T v) const {
+        emit(x, y, z, v, fetch(x, y, z));
     }
 };
 
 // Decoder final store with the finiteness check fused in.
 template <class T> struct FinalOut {
+    static constexpr bool kPrefetch = false;
     T* dst;
     size_t sy, sz;
     uint32_t* status;

@@ -83,6 +83,7 @@ template <class T> struct FwdOut {
 
 // Inverse output into a compact or strided array.
 template <class T> struct StoreOut {
+    static constexpr bool kPrefetch = false;
     T* dst;
     size_t sy, sz;
     __device__ __forceinline__ void operator()(uint32_t x, uint32_t y, uint32_t z, T v) const {
