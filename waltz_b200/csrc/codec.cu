@@ -369,10 +369,10 @@ static void forward(const Geometry& g, const T* in, T* C, T* lowA, T* lowB, T* i
             const bool last = l + 1 == g.lxy;
             FwdOut<T> out{C, sy, sz, last ? nullptr : lows[l & 1], lo, a, AX | AY | AZ};
             level_fwd_stream<T>(src, a, out, status, stream);
-            if (l == 0) clock.mark("fwd_l0", stream);
+            static const char* const kFwdNames[5] = {"fwd_l0", "fwd_l1", "fwd_l2", "fwd_l3", "fwd_l4"};
+            clock.mark(kFwdNames[l], stream);
             src = FwdSrc<T>{lows[l & 1], lo.x, size_t(lo.x) * lo.y};
         }
-        if (g.lxy > 1) clock.mark("fwd_coarse", stream);
         return;
     }
     FwdSrc<T> src{in, sy, sz, status};
@@ -435,7 +435,8 @@ static void inverse(const Geometry& g, T* C, T* bank1, T* bank2, const Final& fi
                 T* dst = halves[l & 1];
                 level_inv<T>(src, a, StoreOut<T>{dst, a.x, size_t(a.x) * a.y}, status, stream);
                 low = dst;
-                if (l == 1) clock.mark("inv_coarse", stream);
+                static const char* const kInvNames[5] = {"inv_l0", "inv_l1", "inv_l2", "inv_l3", "inv_l4"};
+                clock.mark(kInvNames[l], stream);
             } else {
                 level_inv<T>(src, a, fin, status, stream);
                 clock.mark(final_stage, stream);

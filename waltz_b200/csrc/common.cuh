@@ -103,6 +103,10 @@ __host__ __device__ inline uint32_t half_len(uint32_t n) { return n - n / 2; }
 __host__ __device__ inline uint32_t mirror(int64_t p, uint32_t n) {
     if (n <= 1) return 0;
     if (p >= 0 && p < (int64_t)n) return (uint32_t)p;
+    // one reflection at either end covers every halo of an array longer
+    // than the halo; the general periodic form is the fallback
+    const int64_t once = p < 0 ? -p : 2 * (int64_t)n - 2 - p;
+    if (once >= 0 && once < (int64_t)n) return (uint32_t)once;
     const int64_t period = 2 * (int64_t)n - 2;
     int64_t r = p % period;
     if (r < 0) r += period;
