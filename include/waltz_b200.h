@@ -50,8 +50,8 @@ const char* waltz_b200_last_error(void);
  *   into the split-band coefficient layout, or synthesis (inverse = 1);
  *   replaces allhalo::forward / allhalo::inverse
  *   (include/transformers/all_halo.cuh:278-380 of the reference).
- * waltz_b200_wzp_encode: WZP stream of n Morton-packed u16 magnitudes and a
- *   natural sign bitmap (ceil(n/32) words); replaces lossless::wzp_enqueue
+ * waltz_b200_wzp_encode: WZP stream of n Morton-packed u16 magnitudes (16-byte
+ *   aligned) and a natural sign bitmap (ceil(n/32) words); replaces lossless::wzp_enqueue
  *   (src/lossless/wzp.cu:1102-1126 of the reference). */
 int waltz_b200_transform(void* d_data, int width, uint32_t nx, uint32_t ny, uint32_t nz, int inverse,
                          void* stream);

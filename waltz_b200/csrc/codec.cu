@@ -1048,6 +1048,7 @@ extern "C" int waltz_b200_wzp_encode(const uint16_t* d_mag, const uint32_t* d_si
     try {
         need(written && d_mag && d_sign && d_out, "null argument");
         need(n && n <= 0x7fffffffu, "WZP element count outside (0, 2^31)");
+        need(!(reinterpret_cast<uintptr_t>(d_mag) & 15), "WZP magnitudes must be 16-byte aligned");
         need(capacity >= wzp_header(n), "WZP output capacity is too small");
         auto s = reinterpret_cast<cudaStream_t>(stream);
         const uint32_t chunks = wzp_chunks(n);
@@ -1126,6 +1127,7 @@ extern "C" int waltz_b200_wzp_encode_noalloc(const uint16_t* d_mag, const uint32
         need(written && d_mag && d_sign && d_out, "null argument");
         *written = 0;
         need(n > 0, "WZP element count must be positive");
+        need(!(reinterpret_cast<uintptr_t>(d_mag) & 15), "WZP magnitudes must be 16-byte aligned");
         need(wzp_chunks(n) <= kNoAllocMaxChunks,
              "WZP element count exceeds the allocation-free limit of 134217728 magnitudes");
         need(capacity >= wzp_header(n), "WZP output capacity is too small");

@@ -34,10 +34,31 @@ template <class T> struct QuantArgs {
 
 constexpr int kQuantThreads = 256;
 
+// Rounds x (|x| below kFastQuant) to the nearest integer, ties to even,
+// with one add of 1.5 * 2^(mantissa bits): the sum's low bits then hold the
+// rounded value. Returns the integer; `back` receives it as T exactly.
+template <class T> struct FastRound;
+template <> struct FastRound<float> {
+    static constexpr float kLimit = 4194304.0f; // 2^22
+    static __device__ __forceinline__ int32_t round(float x, float& back) {
+        const float t = __fadd_rn(x, 12582912.0f); // 1.5 * 2^23
+        back = __fsub_rn(t, 12582912.0f);
+        return int32_t(__float_as_uint(t) & 0x7fffffu) - 0x400000;
+    }
+};
+template <> struct FastRound<double> {
+    static constexpr double kLimit = 1073741824.0; // 2^30
+    static __device__ __forceinline__ int32_t round(double x, double& back) {
+        const double t = __dadd_rn(x, 6755399441055744.0); // 1.5 * 2^52
+        back = __dsub_rn(t, 6755399441055744.0);
+        return int32_t(int64_t(uint64_t(__double_as_longlong(t)) & 0xfffffffffffffull) - (int64_t(1) << 51));
+    }
+};
+
 template <class T>
 __global__ void __launch_bounds__(kQuantThreads) quantize_kernel(QuantArgs<T> A) {
-    __shared__ uint16_t smag[kChunk];
-    __shared__ uint8_t ssign[kChunk];
+    __shared__ __align__(16) uint16_t smag[kChunk];
+    __shared__ __align__(16) uint8_t ssign[kChunk];
     const Bricks& B = A.b;
     const uint64_t bi = blockIdx.x;
     const uint32_t bxi = uint32_t(bi % B.nbx), byi = uint32_t((bi / B.nbx) % B.nby), bzi = uint32_t(bi / (uint64_t(B.nbx) * B.nby));
@@ -46,17 +67,33 @@ __global__ void __launch_bounds__(kQuantThreads) quantize_kernel(QuantArgs<T> A)
     const uint64_t plane = uint64_t(B.nx) * B.ny;
     const uint64_t base = uint64_t(bzi) * B.bz * plane + uint64_t(byi) * 16 * B.nx * ez + uint64_t(bxi) * 16 * ey * ez;
     const uint32_t size = ex * ey * ez;
+    const bool full = ex == 16 && ey == 16;
     const uint16_t* rank = A.rank + slot * 256 * B.bz;
+    const T* corner = A.coeff + (uint64_t(bzi) * B.bz) * plane + uint64_t(byi) * 16 * B.nx + bxi * 16;
     uint32_t bad = 0;
     for (uint32_t i = threadIdx.x; i < size; i += kQuantThreads) {
-        const uint32_t lx = i % ex, ly = (i / ex) % ey, lz = i / (ex * ey);
-        const uint64_t at = (uint64_t(bzi) * B.bz + lz) * plane + uint64_t(byi * 16 + ly) * B.nx + bxi * 16 + lx;
-        const T c = A.coeff[at];
-        const T scaled = Lift<T>::mul(c, A.inv);
+        uint32_t lx, ly, lz;
+        if (full) {
+            lx = i & 15u;
+            ly = (i >> 4) & 15u;
+            lz = i >> 8;
+        } else {
+            lx = i % ex;
+            ly = (i / ex) % ey;
+            lz = i / (ex * ey);
+        }
+        T* cp = const_cast<T*>(corner) + lz * plane + uint64_t(ly) * B.nx + lx;
+        const T scaled = Lift<T>::mul(*cp, A.inv);
         int32_t m = 0;
         bool neg = false;
-        if (!finite_bits(scaled) || fabs(double(scaled)) >= 9223372036854775808.0) {
+        T deq;
+        if (fabs(scaled) < FastRound<T>::kLimit) {
+            const int32_t r = FastRound<T>::round(scaled, deq);
+            neg = r < 0;
+            m = neg ? -r : r;
+        } else if (!finite_bits(scaled) || fabs(double(scaled)) >= 9223372036854775808.0) {
             bad = 1;
+            deq = T(0);
         } else {
             long long r;
             if constexpr (sizeof(T) == 4) r = __float2ll_rn(scaled);
@@ -64,18 +101,35 @@ __global__ void __launch_bounds__(kQuantThreads) quantize_kernel(QuantArgs<T> A)
             neg = r < 0;
             const unsigned long long m64 = neg ? (unsigned long long)(-r) : (unsigned long long)r;
             m = m64 > 0x7fffffffull ? 0x7fffffff : int32_t(m64);
+            deq = Lift<T>::mul(T(neg ? -m : m), A.q);
         }
-        A.coeff[at] = m ? Lift<T>::mul(T(neg ? -m : m), A.q) : T(0);
+        if (m < int32_t(FastRound<T>::kLimit)) deq = m ? Lift<T>::mul(deq, A.q) : T(0);
+        *cp = deq;
         const uint32_t rk = rank[i];
         smag[rk] = uint16_t(m > 65535 ? 65535 : m);
         ssign[rk] = neg && m;
         if (m > 65535) {
+            const uint64_t at = uint64_t(cp - A.coeff);
             atomicOr(&A.qbits[at >> 5], 1u << (at & 31));
             A.qval[at] = uint32_t(m);
         }
     }
     if (bad) atomicOr(A.status, ST_QUANT_DOMAIN);
     __syncthreads();
+    if (base % 32 == 0 && size % 32 == 0) {
+        // brick on whole sign words: 16-byte magnitude stores (base is a
+        // multiple of 8 magnitudes), sign words owned outright
+        for (uint32_t i = threadIdx.x; i < size / 8; i += kQuantThreads)
+            reinterpret_cast<uint4*>(A.mag + base)[i] = reinterpret_cast<const uint4*>(smag)[i];
+        for (uint32_t w = threadIdx.x; w < size / 32; w += kQuantThreads) {
+            const uint32_t* sw = reinterpret_cast<const uint32_t*>(ssign + 32 * w);
+            uint32_t bits = 0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) bits |= (((sw[k] & 0x01010101u) * 0x01020408u) >> 24) << (4 * k);
+            if (bits) A.sign[(base >> 5) + w] = bits;
+        }
+        return;
+    }
     for (uint32_t i = threadIdx.x; i < size; i += kQuantThreads) A.mag[base + i] = smag[i];
     // sign words overlapping [base, base+size)
     const uint64_t w0 = base >> 5, w1 = (base + size + 31) >> 5;
