@@ -316,6 +316,22 @@ static void level_inv(const InvSrc<T>& src, Dims a, const Out& out, uint32_t* st
     check(cudaGetLastError(), "inverse tile launch");
 }
 
+// WZP encoder launch for one magnitude source (shared memory set up once per
+// device and source type).
+template <class Src>
+static void launch_wzp_encode(const WzpEncodeArgs& wa, const Src& src, uint32_t chunks, cudaStream_t stream) {
+    static thread_local int cfg_dev = -1;
+    int dev = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (cfg_dev != dev) {
+        check(cudaFuncSetAttribute(wzp_encode_kernel<Src>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(sizeof(WzpEncodeSmem))), "wzp smem");
+        cfg_dev = dev;
+    }
+    wzp_encode_kernel<Src><<<chunks, kWzpThreads, sizeof(WzpEncodeSmem), stream>>>(wa, src); note_launch();
+    check(cudaGetLastError(), "wzp encode launch");
+}
+
 template <class T, class Out>
 __global__ void identity_kernel(const T* in, Dims d, Out out) {
     const uint64_t n = vol(d);
@@ -572,28 +588,31 @@ static size_t compress(const T* d_in, uint32_t nx, uint32_t ny, uint32_t nz, dou
     // 1. forward transform
     forward<T>(g, d_in, P.C, P.lowA, P.lowB, P.inter, P.status, stream);
     // 2. quantisation + Morton reorder
-    {
+    // A field made of whole bricks (2^k samples each) is quantised inside the
+    // WZP encoder, chunk by chunk; otherwise a separate pass writes the
+    // Morton-packed magnitudes and signs first.
+    const uint32_t bsz = 256 * g.bz;
+    const bool fused = nx % 16 == 0 && ny % 16 == 0 && nz % g.bz == 0 && (bsz & (bsz - 1)) == 0 && bsz <= kChunk;
+    if (!fused) {
         QuantArgs<T> qa{P.C, Bricks::make(nx, ny, nz, g.bz), rank, q, inv, P.mag, P.sign, P.qbits, P.qval, P.status};
         const uint64_t bricks = qa.b.count();
         need(bricks < (1ull << 31), "Waltz: brick grid too large");
         quantize_kernel<T><<<unsigned(bricks), kQuantThreads, 0, stream>>>(qa); note_launch();
         check(cudaGetLastError(), "quantize launch");
+        clock.mark("quantize", stream);
     }
-    clock.mark("quantize", stream);
     // 3. WZP encode straight into the archive
     {
-        static thread_local int cfg_dev = -1;
-        int dev = 0;
-        check(cudaGetDevice(&dev), "cudaGetDevice");
-        if (cfg_dev != dev) {
-            check(cudaFuncSetAttribute(wzp_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       int(sizeof(WzpEncodeSmem))), "wzp smem");
-            cfg_dev = dev;
+        WzpEncodeArgs wa{uint32_t(n), d_out + 32, capacity - 32, P.ticket, P.state, P.sizes, P.status, opt.spin_cap,
+                         opt.skip_publish};
+        if (fused) {
+            uint32_t lb = 0;
+            while ((1u << lb) < bsz) ++lb;
+            launch_wzp_encode(wa, QuantBricks<T>{P.C, nx, ny, g.bz, lb, rank, q, inv, P.qbits, P.qval, P.status},
+                              chunks, stream);
+        } else {
+            launch_wzp_encode(wa, MagArrays{P.mag, P.sign}, chunks, stream);
         }
-        WzpEncodeArgs wa{P.mag, P.sign, uint32_t(n), d_out + 32, capacity - 32, P.ticket, P.state, P.sizes,
-                         P.status, opt.spin_cap, opt.skip_publish};
-        wzp_encode_kernel<<<chunks, kWzpThreads, sizeof(WzpEncodeSmem), stream>>>(wa); note_launch();
-        check(cudaGetLastError(), "wzp encode launch");
         const uint32_t groups = wzp_groups(uint32_t(n));
         wzp_directory_kernel<<<(groups + 255) / 256, 256, 0, stream>>>(d_out + 32, uint32_t(n), P.state, P.sizes,
                                                                        P.wzp_total); note_launch();
@@ -1065,11 +1084,9 @@ extern "C" int waltz_b200_wzp_encode(const uint16_t* d_mag, const uint32_t* d_si
         check(cudaMemsetAsync(P.status, 0, 4, s), "memset");
         check(cudaMemsetAsync(P.ticket, 0, 4, s), "memset");
         check(cudaMemsetAsync(P.state, 0, size_t(chunks) * 8, s), "memset");
-        check(cudaFuncSetAttribute(wzp_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   int(sizeof(WzpEncodeSmem))), "wzp smem");
-        WzpEncodeArgs wa{d_mag, d_sign, n, static_cast<uint8_t*>(d_out), capacity, P.ticket, P.state, P.sizes,
-                         P.status, 1u << 22, 0xffffffffu};
-        wzp_encode_kernel<<<chunks, kWzpThreads, sizeof(WzpEncodeSmem), s>>>(wa); note_launch();
+        WzpEncodeArgs wa{n, static_cast<uint8_t*>(d_out), capacity, P.ticket, P.state, P.sizes, P.status, 1u << 22,
+                         0xffffffffu};
+        launch_wzp_encode(wa, MagArrays{d_mag, d_sign}, chunks, s);
         const uint32_t groups = wzp_groups(n);
         wzp_directory_kernel<<<(groups + 255) / 256, 256, 0, s>>>(static_cast<uint8_t*>(d_out), n, P.state, P.sizes,
                                                                   P.total); note_launch();
@@ -1142,11 +1159,9 @@ extern "C" int waltz_b200_wzp_encode_noalloc(const uint16_t* d_mag, const uint32
         // The array keeps the previous call's contents: clear what must start at zero.
         check(cudaMemsetAsync(base, 0, 16, s), "memset");
         check(cudaMemsetAsync(state, 0, size_t(chunks) * 8, s), "memset");
-        check(cudaFuncSetAttribute(wzp_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   int(sizeof(WzpEncodeSmem))), "wzp smem");
-        WzpEncodeArgs wa{d_mag, d_sign, n, static_cast<uint8_t*>(d_out), capacity, ticket, state, sizes,
-                         status, 1u << 22, 0xffffffffu};
-        wzp_encode_kernel<<<chunks, kWzpThreads, sizeof(WzpEncodeSmem), s>>>(wa); note_launch();
+        WzpEncodeArgs wa{n, static_cast<uint8_t*>(d_out), capacity, ticket, state, sizes, status, 1u << 22,
+                         0xffffffffu};
+        launch_wzp_encode(wa, MagArrays{d_mag, d_sign}, chunks, s);
         wzp_directory_kernel<<<(groups + 255) / 256, 256, 0, s>>>(static_cast<uint8_t*>(d_out), n, state, sizes,
                                                                   total); note_launch();
         check(cudaGetLastError(), "wzp launch");

@@ -55,6 +55,34 @@ template <> struct FastRound<double> {
     }
 };
 
+// Quantisation of one coefficient: code = llrint(T(c * inv)) saturated to
+// +-INT32_MAX (magnitude m, sign neg); returns the dequantised T(+-m) * q.
+// Sets bad for a non-finite or out-of-range scaled value (then m = 0).
+template <class T>
+__device__ __forceinline__ T quantize_one(T c, T inv, T q, int32_t& m, bool& neg, uint32_t& bad) {
+    const T scaled = Lift<T>::mul(c, inv);
+    m = 0;
+    neg = false;
+    if (fabs(scaled) < FastRound<T>::kLimit) {
+        T back;
+        const int32_t r = FastRound<T>::round(scaled, back);
+        neg = r < 0;
+        m = neg ? -r : r;
+        return m ? Lift<T>::mul(back, q) : T(0);
+    }
+    if (!finite_bits(scaled) || fabs(double(scaled)) >= 9223372036854775808.0) {
+        bad = 1;
+        return T(0);
+    }
+    long long r;
+    if constexpr (sizeof(T) == 4) r = __float2ll_rn(scaled);
+    else r = __double2ll_rn(scaled);
+    neg = r < 0;
+    const unsigned long long m64 = neg ? (unsigned long long)(-r) : (unsigned long long)r;
+    m = m64 > 0x7fffffffull ? 0x7fffffff : int32_t(m64);
+    return Lift<T>::mul(T(neg ? -m : m), q);
+}
+
 template <class T>
 __global__ void __launch_bounds__(kQuantThreads) quantize_kernel(QuantArgs<T> A) {
     __shared__ __align__(16) uint16_t smag[kChunk];
@@ -83,28 +111,9 @@ __global__ void __launch_bounds__(kQuantThreads) quantize_kernel(QuantArgs<T> A)
             lz = i / (ex * ey);
         }
         T* cp = const_cast<T*>(corner) + lz * plane + uint64_t(ly) * B.nx + lx;
-        const T scaled = Lift<T>::mul(*cp, A.inv);
-        int32_t m = 0;
-        bool neg = false;
-        T deq;
-        if (fabs(scaled) < FastRound<T>::kLimit) {
-            const int32_t r = FastRound<T>::round(scaled, deq);
-            neg = r < 0;
-            m = neg ? -r : r;
-        } else if (!finite_bits(scaled) || fabs(double(scaled)) >= 9223372036854775808.0) {
-            bad = 1;
-            deq = T(0);
-        } else {
-            long long r;
-            if constexpr (sizeof(T) == 4) r = __float2ll_rn(scaled);
-            else r = __double2ll_rn(scaled);
-            neg = r < 0;
-            const unsigned long long m64 = neg ? (unsigned long long)(-r) : (unsigned long long)r;
-            m = m64 > 0x7fffffffull ? 0x7fffffff : int32_t(m64);
-            deq = Lift<T>::mul(T(neg ? -m : m), A.q);
-        }
-        if (m < int32_t(FastRound<T>::kLimit)) deq = m ? Lift<T>::mul(deq, A.q) : T(0);
-        *cp = deq;
+        int32_t m;
+        bool neg;
+        *cp = quantize_one<T>(*cp, A.inv, A.q, m, neg, bad);
         const uint32_t rk = rank[i];
         smag[rk] = uint16_t(m > 65535 ? 65535 : m);
         ssign[rk] = neg && m;

@@ -16,6 +16,7 @@
 // Morton scatter into the row-major coefficient array.
 #pragma once
 #include "common.cuh"
+#include "quantize.cuh"
 #include "scan.cuh"
 
 namespace wb {
@@ -43,28 +44,28 @@ constexpr uint64_t kAggregate = 1ull << 62;
 constexpr uint64_t kInclusive = 2ull << 62;
 constexpr uint64_t kValueMask = (1ull << 62) - 1;
 
-// Payload bytes one chunk can stage: RZE output (at most the 2 * 8192 plane
-// bytes plus 2048 + 256 + 32 + 4 bitmap bytes) or the raw magnitudes, then up
-// to 1024 sign bytes, plus slack for the word-wide copy.
-constexpr uint32_t kEncBytes = 2 * kChunk + 2048 + 256 + 32 + 4 + 1024 + 60;
+// Bytes of the plane / payload buffer: the 2 * 8192 plane bytes, which the
+// zero and repetition elimination overwrite in place with at most
+// 16384 + 2048 + 256 + 32 + 4 payload bytes, plus slack for word-wide copies.
+constexpr uint32_t kEncBytes = 2 * kChunk + 2048 + 256 + 32 + 4 + 28;
 
 struct WzpEncodeSmem {
+    uint16_t m[kChunk + 8];            // magnitudes (+ slack for word-wide copies)
     union {
-        uint16_t m[kChunk];            // magnitudes (until the sign pass)
-        uint8_t enc[kEncBytes];        // the chunk's payload as written
+        uint8_t planes[kEncBytes];     // bit planes, then the eliminated payload in place
+        uint8_t sneg[kChunk];          // negative-code flags while a source quantises
     };
-    uint8_t planes[2 * kChunk];        // bit-plane transposed chunk
-    uint8_t lv[2048 + 256 + 32 + 4];   // nonzero bitmap and its reductions
-    uint32_t sgn[kChunk / 32];         // compacted sign bits
+    uint8_t lv[2048 + 256 + 32 + 4 + 4]; // nonzero bitmap and its reductions
+    uint32_t sgn[kChunk / 32 + 1];     // compacted sign bits (+ slack)
     uint32_t gcount[kChunk / 32];      // nonzero magnitudes per 32-group
+    uint32_t nsign[kChunk / 32];       // natural sign words of the chunk
+    uint32_t bbase[32];                // row-major bases of the chunk's bricks (quantising source)
     uint32_t sel[16];                  // byte_perm selectors: compact the bytes of a 4-bit mask
     uint32_t tmp[40];
     uint32_t chunk, excl;
 };
 
 struct WzpEncodeArgs {
-    const uint16_t* mag;
-    const uint32_t* sign;
     uint32_t n;
     uint8_t* out;       // start of the WZP stream
     size_t capacity;    // bytes available from `out`
@@ -115,7 +116,79 @@ __device__ __forceinline__ void copy_to_global(uint8_t* dst, const uint8_t* src,
     }
 }
 
-__global__ void __launch_bounds__(kWzpThreads) wzp_encode_kernel(WzpEncodeArgs A) {
+// Magnitude sources of the encoder. Each fills S.m[0, 8192) (zeros past
+// the chunk's end) and S.nsign (the chunk's natural sign words).
+
+// Morton-packed u16 magnitudes and a natural sign bitmap in global memory.
+struct MagArrays {
+    const uint16_t* mag;
+    const uint32_t* sign;
+    __device__ __forceinline__ void load(WzpEncodeSmem& S, uint32_t first, uint32_t count, int tid) const {
+        if (count == kChunk) {
+            const uint4* src = reinterpret_cast<const uint4*>(mag + first);
+            for (int i = tid; i < int(kChunk / 8); i += kWzpThreads) reinterpret_cast<uint4*>(S.m)[i] = src[i];
+        } else {
+            for (int i = tid; i < int(kChunk); i += kWzpThreads) S.m[i] = i < int(count) ? mag[first + i] : 0;
+        }
+        for (uint32_t g = tid; g < kChunk / 32; g += kWzpThreads)
+            S.nsign[g] = g * 32 < count ? sign[(first >> 5) + g] : 0u;
+    }
+};
+
+// The coefficients themselves, quantised by the encoder (quantize_kernel
+// fused in): the chunk is a run of whole 16 x 16 x bz bricks (2^lb samples
+// each, the field made of whole bricks only); every brick is read and
+// rewritten (dequantised) row by row, its magnitudes and negative flags placed
+// at their Morton ranks, and q-outliers recorded as in quantize_kernel.
+template <class T> struct QuantBricks {
+    T* coeff;
+    uint32_t nx, ny, bz, lb;
+    const uint16_t* rank; // full-brick slot: brick-local row-major index -> rank
+    T q, inv;
+    uint32_t* qbits;
+    uint32_t* qval;
+    uint32_t* status;
+    __device__ __forceinline__ void load(WzpEncodeSmem& S, uint32_t first, uint32_t count, int tid) const {
+        const uint32_t bsz = 1u << lb, nb = count >> lb, plane = nx * ny;
+        if (tid < int(nb)) {
+            const uint32_t b = (first >> lb) + tid, nbx = nx / 16, nby = ny / 16;
+            const uint32_t bxi = b % nbx, t = b / nbx, byi = t % nby, slab = t / nby;
+            S.bbase[tid] = slab * bz * plane + byi * 16 * nx + bxi * 16;
+        }
+        for (uint32_t e = nb * bsz + tid; e < kChunk; e += kWzpThreads) {
+            S.m[e] = 0;
+            S.sneg[e] = 0;
+        }
+        __syncthreads();
+        uint32_t bad = 0;
+        for (uint32_t e = tid; e < nb * bsz; e += kWzpThreads) {
+            const uint32_t j = e >> lb, i = e & (bsz - 1u);
+            const uint32_t at = S.bbase[j] + (i >> 8) * plane + ((i >> 4) & 15u) * nx + (i & 15u);
+            int32_t m;
+            bool neg;
+            coeff[at] = quantize_one<T>(coeff[at], inv, q, m, neg, bad);
+            const uint32_t slot = (j << lb) + rank[i];
+            S.m[slot] = uint16_t(m > 65535 ? 65535 : m);
+            S.sneg[slot] = neg && m;
+            if (m > 65535) {
+                atomicOr(&qbits[at >> 5], 1u << (at & 31));
+                qval[at] = uint32_t(m);
+            }
+        }
+        if (bad) atomicOr(status, ST_QUANT_DOMAIN);
+        __syncthreads();
+        for (uint32_t g = tid; g < kChunk / 32; g += kWzpThreads) {
+            const uint32_t* f = reinterpret_cast<const uint32_t*>(S.sneg + 32 * g);
+            uint32_t bits = 0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) bits |= (((f[k] & 0x01010101u) * 0x01020408u) >> 24) << (4 * k);
+            S.nsign[g] = bits;
+        }
+    }
+};
+
+template <class Src>
+__global__ void __launch_bounds__(kWzpThreads) wzp_encode_kernel(WzpEncodeArgs A, Src src) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WzpEncodeSmem& S = *reinterpret_cast<WzpEncodeSmem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -138,14 +211,9 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_encode_kernel(WzpEncodeArgs A
     const uint32_t count = min(kChunk, A.n - first);
     const uint32_t blocks = count / 16;
 
-    // ---- magnitudes (16-byte loads when the chunk is whole)
-    if (count == kChunk) {
-        const uint4* src = reinterpret_cast<const uint4*>(A.mag + first);
-        for (int i = tid; i < int(kChunk / 8); i += kWzpThreads) reinterpret_cast<uint4*>(S.m)[i] = src[i];
-    } else {
-        for (int i = tid; i < int(kChunk); i += kWzpThreads) S.m[i] = i < int(count) ? A.mag[first + i] : 0;
-    }
-    for (int i = tid; i < int(kChunk / 32); i += kWzpThreads) S.sgn[i] = 0;
+    // ---- magnitudes and natural sign words of the chunk
+    src.load(S, first, count, tid);
+    for (int i = tid; i < int(kChunk / 32) + 1; i += kWzpThreads) S.sgn[i] = 0;
     __syncthreads();
 
     // ---- per 32-group nonzero counts, bit planes (warp ballots; planes above
@@ -188,13 +256,12 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_encode_kernel(WzpEncodeArgs A
     }
     // Each 32-group packs its nonzero magnitudes' sign bits with one warp OR
     // reduction and merges them at its bit offset (at most two words).
-    const uint32_t* natural = A.sign + (first >> 5);
     for (int g = warp; g < int(kChunk / 32); g += NW) {
         if (uint32_t(g * 32) >= count) break;
         const int e = g * 32 + lane;
         const uint32_t v = S.m[e];
         const uint32_t nzmask = __ballot_sync(0xffffffffu, v != 0);
-        const uint32_t word = natural[g];
+        const uint32_t word = S.nsign[g];
         const uint32_t pos = __popc(nzmask & ((1u << lane) - 1u));
         const uint32_t packed = __reduce_or_sync(0xffffffffu, (v != 0 && ((word >> lane) & 1u)) ? 1u << pos : 0u);
         if (lane == 0 && packed) {
@@ -203,7 +270,7 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_encode_kernel(WzpEncodeArgs A
             if (sh && (packed >> (32 - sh))) atomicOr(&S.sgn[(r >> 5) + 1], packed >> (32 - sh));
         }
     }
-    __syncthreads(); // S.m is dead from here on: S.enc reuses its bytes
+    __syncthreads();
 
     // ---- zero elimination of the plane bytes: thread t owns bytes 32t..32t+31
     const uint32_t raw_bytes = 2 * count;
@@ -221,7 +288,7 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_encode_kernel(WzpEncodeArgs A
         if (b0 + 32 > raw_bytes) bits &= b0 >= raw_bytes ? 0u : ((1u << (raw_bytes - b0)) - 1u);
         uint32_t o = block_excl_scan<kWzpThreads>(__popc(bits), S.tmp, nzb);
 #pragma unroll
-        for (int k = 0; k < 8; ++k) o += put_selected(S.enc, o, w[k], (bits >> (4 * k)) & 15u, S.sel);
+        for (int k = 0; k < 8; ++k) o += put_selected(S.planes, o, w[k], (bits >> (4 * k)) & 15u, S.sel);
         reinterpret_cast<uint32_t*>(S.lv)[tid] = bits; // bitmap bytes 4t..4t+3
     }
     __syncthreads();
@@ -239,8 +306,8 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_encode_kernel(WzpEncodeArgs A
         }
         uint32_t o = nzb + block_excl_scan<kWzpThreads>(__popc(flags), S.tmp, c1);
         if (tid < 256) {
-            o += put_selected(S.enc, o, w0, flags & 15u, S.sel);
-            put_selected(S.enc, o, w1, flags >> 4, S.sel);
+            o += put_selected(S.planes, o, w0, flags & 15u, S.sel);
+            put_selected(S.planes, o, w1, flags >> 4, S.sel);
             S.lv[2048 + tid] = uint8_t(flags);
         }
         __syncthreads();
@@ -254,8 +321,8 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_encode_kernel(WzpEncodeArgs A
             const uint32_t inc = warp_incl_scan(n2);
             c2 = __shfl_sync(0xffffffffu, inc, 31);
             uint32_t o2 = nzb + c1 + inc - n2;
-            o2 += put_selected(S.enc, o2, v0, f2 & 15u, S.sel);
-            put_selected(S.enc, o2, v1, f2 >> 4, S.sel);
+            o2 += put_selected(S.planes, o2, v0, f2 & 15u, S.sel);
+            put_selected(S.planes, o2, v1, f2 >> 4, S.sel);
             S.lv[2048 + 256 + lane] = uint8_t(f2);
             __syncwarp();
             const uint32_t* l2 = reinterpret_cast<const uint32_t*>(S.lv + 2048 + 256);
@@ -271,9 +338,9 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_encode_kernel(WzpEncodeArgs A
             c3 = __shfl_sync(0xffffffffu, inc3, 31);
             if (lane < 4) {
                 uint32_t o3 = nzb + c1 + c2 + inc3 - n3;
-                o3 += put_selected(S.enc, o3, u0, f3 & 15u, S.sel);
-                put_selected(S.enc, o3, u1, f3 >> 4, S.sel);
-                S.enc[nzb + c1 + c2 + c3 + lane] = uint8_t(f3);
+                o3 += put_selected(S.planes, o3, u0, f3 & 15u, S.sel);
+                put_selected(S.planes, o3, u1, f3 >> 4, S.sel);
+                S.planes[nzb + c1 + c2 + c3 + lane] = uint8_t(f3);
             }
             if (lane == 0) {
                 S.tmp[34] = c2;
@@ -339,25 +406,13 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_encode_kernel(WzpEncodeArgs A
             store_u24(A.out + size_t(groups) * 4 + size_t(c) * 3, meta);
         }
     }
-    if (!nnz) return; // uniform: no payload, and no barrier follows
-    // ---- payload: magnitude bytes (raw: reloaded), then the sign bytes
-    if (raw) {
-        if (count == kChunk) {
-            const uint4* src = reinterpret_cast<const uint4*>(A.mag + first);
-            for (int i = tid; i < int(kChunk / 8); i += kWzpThreads) reinterpret_cast<uint4*>(S.enc)[i] = src[i];
-        } else {
-            for (int i = tid; i < int(count); i += kWzpThreads) reinterpret_cast<uint16_t*>(S.enc)[i] = A.mag[first + i];
-        }
-        __syncthreads();
-    }
-    {
-        const uint8_t* sb = reinterpret_cast<const uint8_t*>(S.sgn);
-        for (uint32_t i = tid; i < sbytes; i += kWzpThreads) S.enc[mbytes + i] = sb[i];
-    }
     __syncthreads();
-    if (S.excl == 0xffffffffu) return;
-    copy_to_global(A.out + size_t(groups) * 4 + size_t(chunks) * 3 + S.excl, S.enc, uint32_t(chunk_bytes), tid,
-                   kWzpThreads);
+    if (!nnz || S.excl == 0xffffffffu) return;
+    // ---- payload: magnitude bytes (eliminated, or the raw magnitudes), then
+    // the sign bytes, each copied with word-wide stores
+    uint8_t* dst = A.out + size_t(groups) * 4 + size_t(chunks) * 3 + S.excl;
+    copy_to_global(dst, raw ? reinterpret_cast<const uint8_t*>(S.m) : S.planes, mbytes, tid, kWzpThreads);
+    copy_to_global(dst + mbytes, reinterpret_cast<const uint8_t*>(S.sgn), sbytes, tid, kWzpThreads);
 }
 
 // Group directory: payload offset of the first byte of every nonempty group.
