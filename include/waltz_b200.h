@@ -57,6 +57,13 @@ int waltz_b200_transform(void* d_data, int width, uint32_t nx, uint32_t ny, uint
                          void* stream);
 int waltz_b200_wzp_encode(const uint16_t* d_mag, const uint32_t* d_sign, uint32_t n, void* d_out,
                           size_t capacity, size_t* written, void* stream);
+/* waltz_b200_zmatrix: the precision form's Z transform in place on a z-major
+ *   float field (nx*ny a multiple of 4, 1 <= nz <= 64): all Z levels of the
+ *   CDF 9/7 analysis (inverse = 0, coefficients in split-band order) or
+ *   synthesis (inverse = 1) as one nz x nz matrix on the tensor cores (TF32
+ *   hi/lo halves, FP32 accumulation). Counterpart of the reference's plane
+ *   schedule Z stage, include/transformers/all_halo.cuh:143-224. */
+int waltz_b200_zmatrix(float* d_data, uint32_t nx, uint32_t ny, uint32_t nz, int inverse, void* stream);
 /* Allocation-free variant of waltz_b200_wzp_encode (same arguments, same
  * stream bytes), for callers that cannot allocate device memory when they
  * call: a framework whose allocator owns the device budget, a plugin or filter

@@ -268,3 +268,35 @@ def test_batch_decode_matches_oracle():
     out = loader.decode_batch(batch, tile=tile, frame=frame, width=4, sides=2, fill=-7.0)
     torch.cuda.synchronize()
     assert out.cpu().numpy().tobytes() == expect.tobytes()
+
+
+def _z_matrix_f64(nz: int, inverse: bool) -> np.ndarray:
+    """The all-levels Z analysis of a column as a matrix, from the oracle's
+    float64 plane-schedule transform of unit columns (nx = ny = 1)."""
+    m = np.empty((nz, nz))
+    for k in range(nz):
+        e = np.zeros((nz, 1, 1))
+        e[k] = 1.0
+        m[:, k] = O.transform(e, inverse=False).reshape(nz)
+    return np.linalg.inv(m) if inverse else m
+
+
+@pytest.mark.parametrize("nxyz", [(64, 64, 64), (32, 24, 40), (16, 20, 33), (256, 4, 17), (20, 20, 9)])
+def test_tensor_core_z_transform_matches_float64(nxyz):
+    """The precision form's tensor-core Z transform (TF32 hi/lo halves, FP32
+    accumulation) against the float64 matrix of the lifting transform; the
+    coefficient error is a few 2^-20 of the row-weighted input."""
+    torch = _torch()
+    nx, ny, nz = nxyz
+    rng = np.random.default_rng(nx * 7 + nz)
+    a = rng.standard_normal((nz, ny, nx)).astype(np.float32)
+    for inverse in (False, True):
+        m = _z_matrix_f64(nz, inverse)
+        expect = (m @ a.reshape(nz, -1).astype(np.float64)).reshape(a.shape)
+        d = torch.from_numpy(a.copy()).cuda()
+        rc = _lib().waltz_b200_zmatrix(C.c_void_p(d.data_ptr()), nx, ny, nz, int(inverse), _stream())
+        assert rc == 0, _lib().waltz_b200_last_error()
+        got = d.cpu().numpy().astype(np.float64)
+        scale = np.abs(m).sum(axis=1).max() * np.abs(a).max()
+        err = np.abs(got - expect).max()
+        assert err <= 4e-6 * scale, (inverse, err, scale)

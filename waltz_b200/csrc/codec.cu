@@ -15,6 +15,7 @@
 #include "stream.cuh"
 #include "transform.cuh"
 #include "wzp.cuh"
+#include "zmatrix.cuh"
 
 #include "../../include/waltz_b200.h"
 #include "../../include/waltz_cuda.h"
@@ -496,6 +497,165 @@ static void inverse(const Geometry& g, T* C, T* bank1, T* bank2, const Final& fi
         }
         clock.mark("inv_z", stream);
     }
+}
+
+// ------------------------------------------------ precision form: Z matrices
+// Mz[n][k]: all Z levels of the forward transform of a unit column e_k, in
+// double (the lifting of the symmetrically reflected line, the exact
+// counterpart of the window lifting), coefficients in split-band order. Its
+// inverse (the synthesis matrix) comes from Gauss-Jordan elimination.
+static void lift_line_forward(std::vector<double>& v, uint32_t n) {
+    constexpr int H = 8;
+    const double A = -1.586134342059924, B = -0.052980118572961, G = 0.882911075530934, D = 0.443506852043971,
+                 K = 1.1496043988602418;
+    std::vector<double> x(n + 2 * H);
+    for (int i = -H; i < int(n) + H; ++i) x[i + H] = v[mirror(i, n)];
+    auto step = [&](int parity, double c) {
+        for (int i = -H + 1; i < int(n) + H - 1; ++i)
+            if (((i % 2) + 2) % 2 == parity) x[i + H] += c * (x[i + H - 1] + x[i + H + 1]);
+    };
+    step(1, A);
+    step(0, B);
+    step(1, G);
+    step(0, D);
+    const uint32_t h = half_len(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const double y = (i & 1) ? x[i + H] * (-1.0 / K) : x[i + H] * K;
+        v[(i >> 1) + ((i & 1) ? h : 0)] = y;
+    }
+}
+
+static std::vector<double> z_analysis_matrix(uint32_t nz) {
+    const unsigned levels = levels_of(nz);
+    std::vector<double> M(size_t(nz) * nz);
+    for (uint32_t k = 0; k < nz; ++k) {
+        std::vector<double> v(nz, 0.0);
+        v[k] = 1.0;
+        uint32_t len = nz;
+        for (unsigned l = 0; l < levels; ++l) {
+            std::vector<double> part(v.begin(), v.begin() + len);
+            lift_line_forward(part, len);
+            std::copy(part.begin(), part.end(), v.begin());
+            len = half_len(len);
+        }
+        for (uint32_t r = 0; r < nz; ++r) M[size_t(r) * nz + k] = v[r];
+    }
+    return M;
+}
+
+static std::vector<double> invert_matrix(std::vector<double> a, uint32_t n) {
+    std::vector<double> inv(size_t(n) * n, 0.0);
+    for (uint32_t i = 0; i < n; ++i) inv[size_t(i) * n + i] = 1.0;
+    for (uint32_t c = 0; c < n; ++c) {
+        uint32_t piv = c;
+        for (uint32_t r = c + 1; r < n; ++r)
+            if (std::fabs(a[size_t(r) * n + c]) > std::fabs(a[size_t(piv) * n + c])) piv = r;
+        need(std::fabs(a[size_t(piv) * n + c]) > 1e-12, "Waltz: singular Z transform matrix");
+        for (uint32_t j = 0; j < n; ++j) {
+            std::swap(a[size_t(c) * n + j], a[size_t(piv) * n + j]);
+            std::swap(inv[size_t(c) * n + j], inv[size_t(piv) * n + j]);
+        }
+        const double d = a[size_t(c) * n + c];
+        for (uint32_t j = 0; j < n; ++j) {
+            a[size_t(c) * n + j] /= d;
+            inv[size_t(c) * n + j] /= d;
+        }
+        for (uint32_t r = 0; r < n; ++r) {
+            if (r == c) continue;
+            const double f = a[size_t(r) * n + c];
+            if (f == 0.0) continue;
+            for (uint32_t j = 0; j < n; ++j) {
+                a[size_t(r) * n + j] -= f * a[size_t(c) * n + j];
+                inv[size_t(r) * n + j] -= f * inv[size_t(c) * n + j];
+            }
+        }
+    }
+    return inv;
+}
+
+// TF32 halves of a matrix in the K-major no-swizzle core layout of zmatrix_kernel.
+static void pack_tf32_halves(const std::vector<double>& m, uint32_t nz, std::vector<float>& hi,
+                             std::vector<float>& lo) {
+    const ZmPlan P = ZmPlan::make(nz);
+    hi.assign(size_t(P.np) * P.kp, 0.f);
+    lo.assign(size_t(P.np) * P.kp, 0.f);
+    for (uint32_t n = 0; n < P.np; ++n)
+        for (uint32_t k = 0; k < P.kp; ++k) {
+            const float v = (n < nz && k < nz) ? float(m[size_t(n) * nz + k]) : 0.f;
+            uint32_t bits;
+            std::memcpy(&bits, &v, 4);
+            bits &= 0xffffe000u;
+            float h;
+            std::memcpy(&h, &bits, 4);
+            const size_t at = (size_t(n / 8) * (P.kp / 4) + k / 4) * 32 + (n % 8) * 4 + (k % 4);
+            hi[at] = h;
+            lo[at] = v - h;
+        }
+}
+
+struct ZMatrixCache {
+    int device = -1;
+    uint32_t nz = 0;
+    float* dev = nullptr; // fwd hi, fwd lo, inv hi, inv lo
+    size_t half = 0;      // floats per half
+    ~ZMatrixCache() {
+        if (dev) cudaFree(dev);
+    }
+    const float* get(uint32_t n, bool inverse, bool lo, cudaStream_t stream) {
+        int d = 0;
+        check(cudaGetDevice(&d), "cudaGetDevice");
+        if (!dev || d != device || n != nz) {
+            if (dev && d == device) cudaFree(dev);
+            dev = nullptr;
+            const std::vector<double> M = z_analysis_matrix(n), S = invert_matrix(M, n);
+            std::vector<float> fh, fl, ih, il;
+            pack_tf32_halves(M, n, fh, fl);
+            pack_tf32_halves(S, n, ih, il);
+            half = fh.size();
+            check(cudaMalloc(&dev, 4 * half * sizeof(float)), "Waltz: cannot allocate Z matrices");
+            std::vector<float> all;
+            for (auto* part : {&fh, &fl, &ih, &il}) all.insert(all.end(), part->begin(), part->end());
+            check(cudaMemcpyAsync(dev, all.data(), all.size() * 4, cudaMemcpyHostToDevice, stream), "Z matrix upload");
+            check(cudaStreamSynchronize(stream), "Z matrix upload");
+            device = d;
+            nz = n;
+        }
+        return dev + (size_t(inverse) * 2 + size_t(lo)) * half;
+    }
+};
+static thread_local ZMatrixCache t_zmat;
+
+// Applies the all-levels Z analysis (or synthesis) matrix to a z-major f32
+// field of nx*ny columns on the tensor cores; `out(col, z, ncols, v)` takes
+// every result. nz <= 64, nx*ny a multiple of 4.
+template <class Out>
+static void zmatrix_apply(const float* x, uint32_t nx, uint32_t ny, uint32_t nz, bool inverse, const Out& out,
+                          uint32_t* status, bool check_finite, cudaStream_t stream) {
+    need(nz >= 1 && nz <= uint32_t(kZmMaxK), "Waltz: matrix form needs 1 <= nz <= 64");
+    const uint64_t ncols = uint64_t(nx) * ny;
+    const ZmPlan P = ZmPlan::make(nz);
+    CUtensorMap map{};
+    need(make_map_3d<float>(&map, x, ncols, nz, 1, ncols, ncols * nz, kZmCols, P.kp, 1),
+         "Waltz: matrix form needs 16-byte aligned planes (nx*ny a multiple of 4)");
+    const float* bhi = t_zmat.get(nz, inverse, false, stream);
+    const float* blo = t_zmat.get(nz, inverse, true, stream);
+    auto kernel = zmatrix_kernel<Out>;
+    const uint32_t smem_max = ZmPlan::make(kZmMaxK).smem();
+    static thread_local int configured_device = -1;
+    int dev = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (configured_device != dev) {
+        check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_max)),
+              "matrix kernel shared memory");
+        configured_device = dev;
+    }
+    const uint64_t tiles = (ncols + kZmCols - 1) / kZmCols;
+    int sms = 0;
+    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+    const unsigned grid = unsigned(std::min<uint64_t>(tiles, uint64_t(sms) * (P.smem() * 2 <= 227u * 1024 ? 2 : 1)));
+    kernel<<<grid, kZmThreads, P.smem(), stream>>>(map, bhi, blo, nz, ncols, out, status, check_finite ? 1u : 0u);
+    note_launch();
+    check(cudaGetLastError(), "matrix kernel launch");
 }
 
 size_t capacity_for(uint64_t n, unsigned width) {
@@ -1172,6 +1332,35 @@ extern "C" int waltz_b200_wzp_encode_noalloc(const uint16_t* d_mag, const uint32
         if (st & ST_CAPACITY) throw Error("WZP output capacity is too small");
         if (st) throw Error("WZP encode failed");
         *written = size_t(host[1]);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// Diagnostic entry of the tensor-core Z transform (declared in include/waltz_b200.h).
+extern "C" int waltz_b200_zmatrix(float* d_data, uint32_t nx, uint32_t ny, uint32_t nz, int inverse, void* stream) {
+    try {
+        need(d_data && nx && ny && nz, "invalid matrix transform arguments");
+        auto s = reinterpret_cast<cudaStream_t>(stream);
+        const uint64_t n = uint64_t(nx) * ny * nz;
+        Carver cv{nullptr};
+        auto plan = [&](Carver& c) {
+            struct P { float* out; uint32_t* status; } p;
+            p.out = c.take<float>(n);
+            p.status = c.take<uint32_t>(1);
+            return p;
+        };
+        plan(cv);
+        Carver real{t_arena.reserve(cv.used)};
+        auto P = plan(real);
+        check(cudaMemsetAsync(P.status, 0, 4, s), "memset");
+        zmatrix_apply(d_data, nx, ny, nz, inverse != 0, ZmStore<float>{P.out}, P.status, false, s);
+        check(cudaMemcpyAsync(d_data, P.out, n * 4, cudaMemcpyDeviceToDevice, s), "copy");
+        uint32_t st = 0;
+        check(cudaMemcpyAsync(&st, P.status, 4, cudaMemcpyDeviceToHost, s), "readback");
+        check(cudaStreamSynchronize(s), "matrix transform");
+        if (st & ST_WAIT_TIMEOUT) throw Error("Waltz: asynchronous copy wait exceeded its bound");
         return 0;
     } catch (const std::exception& e) {
         return fail(e);

@@ -85,7 +85,8 @@ inline EncodeTiledFn encode_tiled() {
 // ordinary loads.
 template <class T>
 inline bool make_map_3d(CUtensorMap* map, const T* base, uint64_t nx, uint64_t ny, uint64_t nz, uint64_t sy,
-                        uint64_t sz, uint32_t bx, uint32_t by, uint32_t bz) {
+                        uint64_t sz, uint32_t bx, uint32_t by, uint32_t bz,
+                        CUtensorMapSwizzle swizzle = CU_TENSOR_MAP_SWIZZLE_NONE) {
     const EncodeTiledFn fn = encode_tiled();
     if (!fn) return false;
     if ((reinterpret_cast<uintptr_t>(base) & 15) || (sy * sizeof(T)) % 16 || (sz * sizeof(T)) % 16) return false;
@@ -95,8 +96,9 @@ inline bool make_map_3d(CUtensorMap* map, const T* base, uint64_t nx, uint64_t n
     const cuuint32_t box[3] = {bx, by, bz};
     const cuuint32_t estr[3] = {1, 1, 1};
     const CUtensorMapDataType type = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    if (swizzle == CU_TENSOR_MAP_SWIZZLE_128B && bx * sizeof(T) > 128) return false;
     return fn(map, type, 3, const_cast<T*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 

@@ -1,0 +1,230 @@
+// Tensor-core Z transform (the precision form's matrix arithmetic).
+//
+// All levels of the CDF 9/7 analysis (or synthesis) along z of a plane
+// schedule form one dense nz x nz matrix Mz: coefficient n of a column is
+// sum_k Mz[n][k] * x[k]. For a field stored z-major (plane z = nx*ny
+// contiguous columns) the whole Z stage is the GEMM  D = X^T * Mz^T  with one
+// row of D per column of the field, computed here on the 5th-generation
+// tensor cores:
+//   * a CTA takes 128 field columns at a time (UMMA M = 128); one TMA box
+//     brings the K = nz planes of those columns, and a shared-memory pass
+//     splits every value into TF32 halves (hi = fp32 truncated to TF32,
+//     lo = x - hi, exact) written transposed into the K-major no-swizzle
+//     operand layout (8-row x 16-byte core matrices);
+//   * Mz's halves are prepared on the host in the same layout and loaded once
+//     per CTA; D = Ahi*Bhi + Ahi*Blo + Alo*Bhi, three tcgen05.mma kind::tf32
+//     per 8-deep K step, FP32 accumulation in tensor memory;
+//   * the epilogue reads D from tensor memory (lane = field column, column =
+//     coefficient) and writes it back z-major, or hands it to an emitter.
+// One thread issues the MMAs and commits them to an mbarrier; every wait is
+// bounded and a block that gives up records ST_WAIT_TIMEOUT, frees its tensor
+// memory and returns. Nothing here multicasts.
+#pragma once
+#include "common.cuh"
+#include "tma.cuh"
+
+namespace wb {
+
+constexpr int kZmCols = 128;   // field columns per tile (UMMA M)
+constexpr int kZmMaxK = 64;    // largest nz handled (operands stay in shared memory)
+constexpr int kZmThreads = 128;
+
+// Instruction descriptor of tcgen05.mma kind::tf32: D f32, A and B tf32,
+// both K-major, M = 128, N = np (bit layout of the UMMA instruction
+// descriptor: c_format [4,6), a_format [7,10), b_format [10,13), a_major 15,
+// b_major 16, N >> 3 at [17,23), M >> 4 at [24,29)).
+__host__ __device__ constexpr uint32_t zm_idesc(uint32_t np) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((np >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+// Shared-memory matrix descriptor: start >> 4 at [0,14), LBO >> 4 at
+// [16,30), SBO >> 4 at [32,46), version 1 at [46,48), layout at [61,64).
+__device__ __forceinline__ uint64_t zm_sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo, uint32_t layout) {
+    return uint64_t((saddr >> 4) & 0x3fffu) | (uint64_t((lbo >> 4) & 0x3fffu) << 16) |
+           (uint64_t((sbo >> 4) & 0x3fffu) << 32) | (uint64_t(1) << 46) | (uint64_t(layout) << 61);
+}
+
+__device__ __forceinline__ void zm_mma(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accumulate) {
+    const uint32_t mask = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(dtmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(mask), "r"(mask), "r"(mask), "r"(mask));
+}
+
+__device__ __forceinline__ void zm_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+
+// Shared-memory plan of one CTA (bytes from a 1024-byte aligned base): the
+// staged planes X (kp rows x 128 columns), the A halves (128 x kp each) and
+// the B halves (np x kp each), all fp32.
+struct ZmPlan {
+    uint32_t kp, np;          // padded K (multiple of 8) and N (multiple of 16)
+    uint32_t a_bytes;         // X, or one A half: 128 x kp x 4 B
+    uint32_t b_bytes;         // one B half: np x kp x 4 B
+    __host__ __device__ static ZmPlan make(uint32_t nz) {
+        ZmPlan p;
+        p.kp = (nz + 7) / 8 * 8;
+        p.np = (nz + 15) / 16 * 16;
+        p.a_bytes = 128 * p.kp * 4;
+        p.b_bytes = p.np * p.kp * 4;
+        return p;
+    }
+    __host__ __device__ uint32_t smem() const { return 1024 + 3 * a_bytes + 2 * b_bytes + 64; }
+};
+
+// Destination of the Z stage: z-major store, or a per-sample emitter.
+template <class T> struct ZmStore {
+    T* dst;       // z-major: dst[z * ncols + col]
+    __device__ __forceinline__ void operator()(uint32_t col, uint32_t z, size_t ncols, T v) const {
+        dst[size_t(z) * ncols + col] = v;
+    }
+};
+template <class Final> struct ZmEmit {
+    Final fin;
+    uint32_t nx;
+    __device__ __forceinline__ void operator()(uint32_t col, uint32_t z, size_t, float v) const {
+        fin(col % nx, col / nx, z, v);
+    }
+};
+
+// B halves: device arrays of np * kp floats each in the K-major no-swizzle
+// core layout (core (n/8, k/4) at ((n/8) * kp/4 + k/4) * 128 B, element
+// (n%8, k%4) at (n%8) * 16 + (k%4) * 4 inside it).
+template <class Out>
+__global__ void __launch_bounds__(kZmThreads, 1)
+    zmatrix_kernel(const __grid_constant__ CUtensorMap xmap, const float* bhi, const float* blo, uint32_t nz,
+                   uint64_t ncols, Out out, uint32_t* status, uint32_t check_finite) {
+    extern __shared__ __align__(1024) unsigned char zm_smem[];
+    const ZmPlan P = ZmPlan::make(nz);
+    unsigned char* base = zm_smem + ((1024 - (smem_u32(zm_smem) & 1023)) & 1023);
+    unsigned char* Xs = base;                  // TMA destination: kp rows of 128 columns
+    unsigned char* Ahi = Xs + P.a_bytes;
+    unsigned char* Alo = Ahi + P.a_bytes;
+    unsigned char* Bhi = Alo + P.a_bytes;
+    unsigned char* Blo = Bhi + P.b_bytes;
+    uint64_t* tma_bar = reinterpret_cast<uint64_t*>(Blo + P.b_bytes);
+    uint64_t* mma_bar = tma_bar + 1;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_bar + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint64_t tiles = (ncols + kZmCols - 1) / kZmCols;
+    const uint32_t ncols_alloc = P.np <= 32 ? 32 : (P.np <= 64 ? 64 : 128);
+
+    // tensor memory for D (128 lanes x np fp32 columns), barriers, operands B
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(ncols_alloc));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        mbar_init(tma_bar, 1);
+        mbar_init(mma_bar, 1);
+        fence_barrier_init();
+    }
+    for (uint32_t i = tid; i < P.b_bytes / 16; i += kZmThreads) {
+        reinterpret_cast<uint4*>(Bhi)[i] = reinterpret_cast<const uint4*>(bhi)[i];
+        reinterpret_cast<uint4*>(Blo)[i] = reinterpret_cast<const uint4*>(blo)[i];
+    }
+    fence_proxy_async();
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t idesc = zm_idesc(P.np);
+    const uint32_t sbo = (P.kp / 4) * 128; // 8-row groups of the K-major operands
+
+    auto issue = [&](uint64_t tile) {
+        mbar_expect_tx(tma_bar, P.a_bytes);
+        tma_load_3d(Xs, &xmap, int(tile * kZmCols), 0, 0, tma_bar);
+    };
+    uint64_t tile = blockIdx.x;
+    if (tid == 0 && tile < tiles) issue(tile);
+    uint32_t phase = 0;
+    bool bad = false;
+    for (; tile < tiles; tile += gridDim.x) {
+        if (!__syncthreads_and(warp != 0 || mbar_wait(tma_bar, phase, kWaitBound))) {
+            if (tid == 0) atomicOr(status, ST_WAIT_TIMEOUT);
+            break;
+        }
+        // split and transpose: thread c takes field column c; element (c, k)
+        // goes to core (c/8, k/4) at ((c/8) * kp/4 + k/4) * 128 B, row c%8
+        {
+            const int c = tid;
+            const float* xcol = reinterpret_cast<const float*>(Xs) + c;
+            unsigned char* hrow = Ahi + (c / 8) * sbo + (c % 8) * 16;
+            unsigned char* lrow = Alo + (c / 8) * sbo + (c % 8) * 16;
+            for (uint32_t k = 0; k < P.kp; k += 4) {
+                uint32_t h[4], l[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const float x = xcol[(k + j) * kZmCols];
+                    if (check_finite) bad |= !finite_bits(x);
+                    h[j] = __float_as_uint(x) & 0xffffe000u;
+                    l[j] = __float_as_uint(__fsub_rn(x, __uint_as_float(h[j])));
+                }
+                *reinterpret_cast<uint4*>(hrow + (k / 4) * 128) = make_uint4(h[0], h[1], h[2], h[3]);
+                *reinterpret_cast<uint4*>(lrow + (k / 4) * 128) = make_uint4(l[0], l[1], l[2], l[3]);
+            }
+        }
+        fence_proxy_async();
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        // X is consumed: bring the next tile while this one is multiplied
+        if (tid == 0 && tile + gridDim.x < tiles) issue(tile + gridDim.x);
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            // A and B: K-major, no swizzle; cores 128 B apart along K (LBO),
+            // 8-row groups kp/4 cores apart (SBO); a K step of 8 is two cores
+            const uint32_t a0 = smem_u32(Ahi), a1 = smem_u32(Alo), b0 = smem_u32(Bhi), b1 = smem_u32(Blo);
+            for (uint32_t s = 0; s < P.kp / 8; ++s) {
+                const uint64_t dah = zm_sdesc(a0 + s * 256, 128, sbo, 0);
+                const uint64_t dal = zm_sdesc(a1 + s * 256, 128, sbo, 0);
+                const uint64_t dbh = zm_sdesc(b0 + s * 256, 128, sbo, 0);
+                const uint64_t dbl = zm_sdesc(b1 + s * 256, 128, sbo, 0);
+                zm_mma(tmem, dah, dbh, idesc, s > 0);
+                zm_mma(tmem, dah, dbl, idesc, 1);
+                zm_mma(tmem, dal, dbh, idesc, 1);
+            }
+            zm_commit(mma_bar);
+        }
+        if (!__syncthreads_and(warp != 0 || mbar_wait(mma_bar, phase, kWaitBound))) {
+            if (tid == 0) atomicOr(status, ST_WAIT_TIMEOUT);
+            break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        // epilogue: lane = field column, 16 coefficients per load
+        const uint64_t col = tile * kZmCols + 32 * warp + lane;
+        for (uint32_t c0 = 0; c0 < P.np; c0 += 16) {
+            uint32_t r[16];
+            tmem_ld16(tmem + (uint32_t(32 * warp) << 16) + c0, r);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (col < ncols) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                    if (c0 + j < nz) out(uint32_t(col), c0 + j, ncols, __uint_as_float(r[j]));
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        phase ^= 1;
+    }
+    if (check_finite && __syncthreads_or(bad) && tid == 0) atomicOr(status, ST_NONFINITE_INPUT);
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols_alloc));
+    }
+}
+
+} // namespace wb
