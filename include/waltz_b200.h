@@ -34,8 +34,23 @@ int waltz_b200_compress(const void* d_input, int width, uint32_t nx, uint32_t ny
                         double abs_error, void* d_archive, size_t capacity, size_t* written,
                         void* stream);
 
+/* Transform forms. PLAIN is the default profile (lifting, archives
+ * byte-identical to the reference CPU codec). MATRIX is the precision form:
+ * the plane schedule's Z stage (all Z levels) runs as one nz x nz matrix on
+ * the tensor cores (TF32 hi/lo halves, FP32 accumulation) and the repair pass
+ * restores the bound; such archives set header flag bit 6, which the
+ * reference's decoders reject. MATRIX needs float data in the plane schedule
+ * (Z levels differ from XY levels) with 1 <= nz <= 64 and nx*ny a multiple of
+ * 4. New surface: the reference has no counterpart (its header reserves the
+ * bit, include/utils/Blob.hpp:46-53). */
+#define WALTZ_B200_FORM_PLAIN 0
+#define WALTZ_B200_FORM_MATRIX 1
+int waltz_b200_compress_form(const void* d_input, int width, uint32_t nx, uint32_t ny, uint32_t nz,
+                             double abs_error, int form, void* d_archive, size_t capacity, size_t* written,
+                             void* stream);
+
 /* Decode an archive of `bytes` bytes into nx*ny*nz samples (the archive does
- * not store its dimensions). */
+ * not store its dimensions); either form. */
 int waltz_b200_decompress(const void* d_archive, size_t bytes, int width, uint32_t nx, uint32_t ny,
                           uint32_t nz, void* d_output, size_t output_bytes, void* stream);
 

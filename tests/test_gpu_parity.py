@@ -300,3 +300,40 @@ def test_tensor_core_z_transform_matches_float64(nxyz):
         scale = np.abs(m).sum(axis=1).max() * np.abs(a).max()
         err = np.abs(got - expect).max()
         assert err <= 4e-6 * scale, (inverse, err, scale)
+
+
+@pytest.mark.parametrize("rel", [1e-3, 1e-5])
+@pytest.mark.parametrize("shape", [(64, 128, 128), (24, 96, 64), (33, 24, 40)])
+def test_matrix_form_round_trip(shape, rel):
+    """Precision form (tensor-core Z stage): the archive carries header bit 6,
+    the reference decoder (the oracle) rejects it, the GPU decoder restores
+    every sample within the bound, twice identically, and the archive stays
+    close to the plain form's size. The field: k^-11/3 random field with 1 %
+    salt spikes of magnitude 50, the shape of the tensor-core configuration."""
+    import waltz_b200
+    from waltz_b200 import synthetic as S
+    a = S.power_law_field(shape, 3)
+    rng = np.random.default_rng(3)
+    spikes = rng.random(a.shape) < 0.01
+    a[spikes] = np.where(rng.random(int(spikes.sum())) < 0.5, -50.0, 50.0)
+    eb = float(rel * (a.max() - a.min()))
+    plain = waltz_b200.compress(a, abs_error=eb)
+    matrix = waltz_b200.compress(a, abs_error=eb, form="matrix")
+    assert matrix[0] == plain[0] | 0x40
+    with pytest.raises(Exception):
+        O.decompress(matrix, a.shape, np.float32)
+    out1 = waltz_b200.decompress(matrix, shape=a.shape, dtype=np.float32)
+    out2 = waltz_b200.decompress(matrix, shape=a.shape, dtype=np.float32)
+    assert out1.tobytes() == out2.tobytes()
+    err = np.abs(out1.astype(np.longdouble) - a.astype(np.longdouble)).max()
+    assert err <= np.longdouble(eb)
+    assert abs(len(matrix) - len(plain)) <= 0.05 * len(plain) + 256
+
+
+def test_matrix_form_rejects_unsuited_fields():
+    import waltz_b200
+    cube = np.zeros((64, 64, 64), np.float32)  # dyadic schedule: no separate Z stage
+    with pytest.raises(waltz_b200.WaltzError, match="matrix form"):
+        waltz_b200.compress(cube, abs_error=1e-3, form="matrix")
+    with pytest.raises(waltz_b200.WaltzError, match="matrix form"):
+        waltz_b200.compress(np.zeros((64, 16, 16)), abs_error=1e-3, form="matrix")  # float64

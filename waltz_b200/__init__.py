@@ -56,19 +56,28 @@ def _stream(torch, stream):
     return C.c_void_p(s.cuda_stream)
 
 
-def compress_tensor(field, abs_error: float, *, stream=None):
+FORMS = {"plain": 0, "matrix": 1}
+
+
+def compress_tensor(field, abs_error: float, *, form: str = "plain", stream=None):
     """Compress a contiguous float32/float64 CUDA tensor of shape (z,y,x) or
-    (y,x). Returns a uint8 CUDA tensor holding the archive."""
+    (y,x). Returns a uint8 CUDA tensor holding the archive.
+
+    form="plain" is the default profile (byte-identical to the reference CPU
+    codec); form="matrix" is the precision form, whose Z stage runs as one
+    matrix on the tensor cores (float, plane schedule, nz <= 64)."""
     torch = _torch()
     if not field.is_cuda or not field.is_contiguous():
         raise ValueError("expected a contiguous CUDA tensor")
+    if form not in FORMS:
+        raise ValueError(f"form must be one of {sorted(FORMS)}")
     nx, ny, nz = _geometry(field.shape, field.element_size())
     cap = compressed_capacity(field.numel(), field.element_size())
     out = torch.empty(cap, dtype=torch.uint8, device=field.device)
     written = C.c_size_t()
-    checked(lib().waltz_b200_compress(C.c_void_p(field.data_ptr()), field.element_size(), nx, ny, nz,
-                                      _bound(abs_error), C.c_void_p(out.data_ptr()), cap, C.byref(written),
-                                      _stream(torch, stream)))
+    checked(lib().waltz_b200_compress_form(C.c_void_p(field.data_ptr()), field.element_size(), nx, ny, nz,
+                                           _bound(abs_error), FORMS[form], C.c_void_p(out.data_ptr()), cap,
+                                           C.byref(written), _stream(torch, stream)))
     return out[:written.value]
 
 
@@ -105,15 +114,16 @@ def rel_to_abs_bound(field, rel: float, *, stream=None) -> float:
     return float(rel) * (hi - lo)
 
 
-def compress(array, *, abs_error):
-    """Return canonical archive bytes of a float32/float64 (z,y,x) or (y,x)
-    numpy array, computed on the current CUDA device."""
+def compress(array, *, abs_error, form="plain"):
+    """Return archive bytes of a float32/float64 (z,y,x) or (y,x) numpy array,
+    computed on the current CUDA device: canonical (reference-identical) in
+    the default plain form, tensor-core Z stage with form="matrix"."""
     torch = _torch()
     a = np.ascontiguousarray(np.asarray(array))
     if a.dtype not in (np.float32, np.float64):
         raise TypeError("Waltz requires native float32 or float64")
     dev = torch.from_numpy(a).cuda()
-    return bytes(compress_tensor(dev, abs_error).cpu().numpy().tobytes())
+    return bytes(compress_tensor(dev, abs_error, form=form).cpu().numpy().tobytes())
 
 
 def decompress(archive, *, shape, dtype):

@@ -367,10 +367,16 @@ static TransformScratch scratch_need(const Geometry& g) {
     return s;
 }
 
-// Forward all-level transform of `in` into the coefficient array C.
+template <class Out>
+static void zmatrix_apply(const float* x, uint32_t nx, uint32_t ny, uint32_t nz, bool inverse, const Out& out,
+                          uint32_t* status, bool check_finite, cudaStream_t stream);
+
+// Forward all-level transform of `in` into the coefficient array C. With
+// `matrix` (the precision form; plane schedule, float) the Z stage is the
+// tensor-core matrix transform instead of Z lifting.
 template <class T>
 static void forward(const Geometry& g, const T* in, T* C, T* lowA, T* lowB, T* inter, uint32_t* status,
-                    cudaStream_t stream) {
+                    cudaStream_t stream, bool matrix = false) {
     const size_t sy = g.nx, sz = size_t(g.nx) * g.ny;
     T* lows[2] = {lowA, lowB};
     if (g.lxy == 0 && g.lz == 0) {
@@ -394,7 +400,13 @@ static void forward(const Geometry& g, const T* in, T* C, T* lowA, T* lowB, T* i
     }
     FwdSrc<T> src{in, sy, sz, status};
     T* zdst = g.lxy ? inter : C;
-    for (unsigned l = 0; l < g.lz; ++l) {
+    if constexpr (std::is_same_v<T, float>) {
+        if (matrix) {
+            zmatrix_apply(in, g.nx, g.ny, g.nz, false, ZmStore<float>{zdst}, status, true, stream);
+            clock.mark("fwd_z_matrix", stream);
+        }
+    }
+    for (unsigned l = 0; l < (matrix ? 0u : g.lz); ++l) {
         const Dims a = g.zl[l], lo = halve(a, AZ);
         const bool last = l + 1 == g.lz;
         FwdOut<T> out{zdst, sy, sz, last ? nullptr : lows[l & 1], lo, a, AZ};
@@ -432,7 +444,7 @@ static uint64_t inverse_low_need(const Geometry& g) {
 // hands every sample to `fin`.
 template <class T, class Final>
 static void inverse(const Geometry& g, T* C, T* bank1, T* bank2, const Final& fin, uint32_t* status,
-                    cudaStream_t stream, const char* final_stage = "inv_l0") {
+                    cudaStream_t stream, const char* final_stage = "inv_l0", bool matrix = false) {
     StageClock& clock = stage_clock();
     const size_t sy = g.nx, sz = size_t(g.nx) * g.ny;
     const uint64_t half_off = ((g.n + 1) / 2 + 63) & ~uint64_t(63);
@@ -481,6 +493,13 @@ static void inverse(const Geometry& g, T* C, T* bank1, T* bank2, const Final& fi
             }
         }
         clock.mark("inv_xy", stream);
+    }
+    if constexpr (std::is_same_v<T, float>) {
+        if (matrix && g.lz) {
+            zmatrix_apply(zbase, g.nx, g.ny, g.nz, true, ZmEmit<Final>{fin, g.nx}, status, false, stream);
+            clock.mark("inv_z_matrix", stream);
+            return;
+        }
     }
     if (g.lz) {
         const T* low = nullptr;
@@ -675,7 +694,19 @@ static uint64_t* pinned() {
 struct EncodeOptions {
     uint32_t spin_cap = 1u << 22;
     uint32_t skip_publish = 0xffffffffu;
+    bool matrix = false; // precision form: tensor-core Z transform, header flag bit 6
 };
+
+// Header flag bit 6: the archive's Z stage is the tensor-core matrix form
+// (a reserved bit of the reference header, include/utils/Blob.hpp:46-53, so
+// the reference decoders reject such archives and the default bytes stay).
+constexpr uint8_t kMatrixFlag = 0x40;
+
+// Fields the matrix form serves: float, plane schedule with Z levels,
+// 1 <= nz <= 64 and nx*ny a multiple of 4 (16-byte planes).
+static bool matrix_form_ok(const Geometry& g, size_t width) {
+    return width == 4 && !g.dyadic && g.lz >= 1 && g.nz <= uint32_t(kZmMaxK) && (uint64_t(g.nx) * g.ny) % 4 == 0;
+}
 
 // ------------------------------------------------------------------ encode
 template <class T>
@@ -746,7 +777,9 @@ static size_t compress(const T* d_in, uint32_t nx, uint32_t ny, uint32_t nz, dou
     StageClock& clock = stage_clock();
     clock.begin(stream);
     // 1. forward transform
-    forward<T>(g, d_in, P.C, P.lowA, P.lowB, P.inter, P.status, stream);
+    need(!opt.matrix || matrix_form_ok(g, sizeof(T)),
+         "Waltz: the matrix form needs float data in the plane schedule with 1 <= nz <= 64 and nx*ny a multiple of 4");
+    forward<T>(g, d_in, P.C, P.lowA, P.lowB, P.inter, P.status, stream, opt.matrix);
     // 2. quantisation + Morton reorder
     // A field made of whole bricks (2^k samples each) is quantised inside the
     // WZP encoder, chunk by chunk; otherwise a separate pass writes the
@@ -785,14 +818,15 @@ static size_t compress(const T* d_in, uint32_t nx, uint32_t ny, uint32_t nz, dou
         T safe = T(eb * (1.0 - std::ldexp(1.0, -21)));
         if (double(safe) > eb * (1.0 - std::ldexp(1.0, -21))) safe = std::nextafter(safe, T(0));
         RepairOut<T> fin{d_in, nx, size_t(nx) * ny, eb, T(eb), P.pbits, P.perr, P.status, safe};
-        inverse<T>(g, P.C, P.inter, P.bank2, fin, P.status, stream, "inv_l0_repair");
+        inverse<T>(g, P.C, P.inter, P.bank2, fin, P.status, stream, "inv_l0_repair", opt.matrix);
     }
     // 5. ordered side records
     compact_count_kernel<<<unsigned(cblocks), kCompactThreads, 0, stream>>>(P.pbits, words, P.counts_p); note_launch();
     compact_count_kernel<<<unsigned(cblocks), kCompactThreads, 0, stream>>>(P.qbits, words, P.counts_q); note_launch();
     compact_scan_kernel<<<1, kCompactThreads, 0, stream>>>(P.counts_p, uint32_t(cblocks), P.np); note_launch();
     compact_scan_kernel<<<1, kCompactThreads, 0, stream>>>(P.counts_q, uint32_t(cblocks), P.nq); note_launch();
-    layout_kernel<<<1, 32, 0, stream>>>(d_out, capacity, P.wzp_total, P.np, P.nq, sizeof(T), g.flags(sizeof(T)),
+    layout_kernel<<<1, 32, 0, stream>>>(d_out, capacity, P.wzp_total, P.np, P.nq, sizeof(T),
+                                        uint8_t(g.flags(sizeof(T)) | (opt.matrix ? kMatrixFlag : 0)),
                                         uint8_t(g.lxy), uint8_t(g.lz), uint8_t(g.bz), quantum, P.layout); note_launch();
     compact_write_kernel<T><<<unsigned(cblocks), kCompactThreads, 0, stream>>>(P.pbits, words, P.counts_p, P.perr,
                                                                                d_out, P.layout, 0, 1, n); note_launch();
@@ -847,7 +881,8 @@ template <class T>
 static Layout validate_header(const Header& h, const Geometry& g, size_t bytes, bool canonical) {
     const uint64_t n = g.n;
     need(bytes >= 32, "invalid Waltz archive header");
-    need(!(h.flags & 0xe0) && (h.flags & 0x18) && ((h.flags & 4) ? 8u : 4u) == sizeof(T), "invalid Waltz archive header");
+    need(!(h.flags & 0xa0) && (h.flags & 0x18) && ((h.flags & 4) ? 8u : 4u) == sizeof(T), "invalid Waltz archive header");
+    need(!(h.flags & kMatrixFlag) || matrix_form_ok(g, sizeof(T)), "invalid Waltz archive header");
     need(((h.flags >> 3) & 3) == 3, "unsupported Waltz synthesis mode");
     need(!(h.flags & 2), "compact repair archives are not supported by this decoder");
     const bool dyadic = h.flags & 1;
@@ -976,7 +1011,7 @@ static void decode_launch(const uint8_t* d_in, const Header& h, const Layout& L,
         qpatch_kernel<T><<<(h.nq + 255) / 256, 256, 0, stream>>>(d_in + L.qi, d_in + L.qv, h.nq, g.n, T(h.q), C,
                                                                  status); note_launch();
     clock.mark("qpatch", stream);
-    inverse<T>(g, C, bank1, bank2, fin, status, stream);
+    inverse<T>(g, C, bank1, bank2, fin, status, stream, "inv_l0", (h.flags & kMatrixFlag) != 0);
     if (h.np)
         rpatch_kernel<T, Patch><<<(h.np + 255) / 256, 256, 0, stream>>>(d_in + L.pi, d_in + L.pv, h.np, g.n, patch,
                                                                         status); note_launch();
@@ -1121,6 +1156,28 @@ int waltz_b200_compress(const void* d_input, int width, uint32_t nx, uint32_t ny
         auto* out = static_cast<uint8_t*>(d_archive);
         *written = width == 4 ? compress(static_cast<const float*>(d_input), nx, ny, nz, abs_error, out, capacity, s)
                               : compress(static_cast<const double*>(d_input), nx, ny, nz, abs_error, out, capacity, s);
+        t_error[0] = 0;
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+int waltz_b200_compress_form(const void* d_input, int width, uint32_t nx, uint32_t ny, uint32_t nz,
+                             double abs_error, int form, void* d_archive, size_t capacity, size_t* written,
+                             void* stream) {
+    try {
+        need(written != nullptr, "null argument");
+        *written = 0;
+        need(width == 4 || width == 8, "type must be FP32 or FP64");
+        need(form == WALTZ_B200_FORM_PLAIN || form == WALTZ_B200_FORM_MATRIX, "unknown transform form");
+        EncodeOptions opt;
+        opt.matrix = form == WALTZ_B200_FORM_MATRIX;
+        auto s = reinterpret_cast<cudaStream_t>(stream);
+        auto* out = static_cast<uint8_t*>(d_archive);
+        *written = width == 4
+                       ? compress(static_cast<const float*>(d_input), nx, ny, nz, abs_error, out, capacity, s, opt)
+                       : compress(static_cast<const double*>(d_input), nx, ny, nz, abs_error, out, capacity, s, opt);
         t_error[0] = 0;
         return 0;
     } catch (const std::exception& e) {
