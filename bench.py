@@ -259,7 +259,94 @@ def gpu_arm(args, rank, world, local_rank):
             result["roofline"]["traffic"] = t
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(field.cpu().numpy(), eb)
+    if not args.no_tc_form and world == 1:
+        del field, out, archive, host_in, host_arch, host_out
+        torch.cuda.empty_cache()
+        result["tc_form"] = tc_form_comparison(dev, lib, args.steps)
     return result
+
+
+def tc_form_comparison(dev, lib, steps):
+    """Plain lifting against the precision form (tensor-core Z stage) on the
+    tensor-core configuration: float32 1024x1024x64 (z=64) k^-11/3 random field
+    (seed 3) with 1 % salt spikes of magnitude 50, REL 1e-3 and 1e-5; device
+    resident, CUDA events, median of `steps` after one warm-up. Also the Z-stage
+    coefficient error of the tensor-core matrix against the float64 lifting
+    transform on 16384 columns of the field."""
+    import torch
+    import waltz_b200
+    from waltz_b200 import _lib
+    from waltz_b200.synthetic import power_law_field_device
+    shape = (64, 1024, 1024)
+    nz, ny, nx = shape
+    f = power_law_field_device(shape, 3, device=dev)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(3)
+    spikes = torch.rand(shape, device=dev, generator=gen) < 0.01
+    signs = torch.where(torch.rand(shape, device=dev, generator=gen) < 0.5, -50.0, 50.0)
+    f = torch.where(spikes, signs, f).to(torch.float32).contiguous()
+    n = f.numel()
+    nbytes = n * 4
+    cap = waltz_b200.compressed_capacity(n, 4)
+    arch = torch.empty(cap, dtype=torch.uint8, device=dev)
+    out = torch.empty_like(f)
+    sp = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    written = C.c_size_t()
+    lo, hi = waltz_b200.extrema(f)
+    report = {"workload": "f32 64x1024x1024 (z,y,x) k^-11/3 GRF seed 3 + 1% spikes of 50, plane schedule 5/3"}
+    for rel in (1e-3, 1e-5):
+        eb = rel * (hi - lo)
+        entry = {}
+        for form, code in (("plain", 0), ("matrix", 1)):
+            def comp():
+                _lib.checked(lib.waltz_b200_compress_form(C.c_void_p(f.data_ptr()), 4, nx, ny, nz, eb, code,
+                                                          C.c_void_p(arch.data_ptr()), cap, C.byref(written), sp))
+                return written.value
+
+            def dec(size):
+                _lib.checked(lib.waltz_b200_decompress(C.c_void_p(arch.data_ptr()), size, 4, nx, ny, nz,
+                                                       C.c_void_p(out.data_ptr()), nbytes, sp))
+            size = comp()
+            dec(size)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            tc, td = [], []
+            for _ in range(max(1, steps)):
+                ev[0].record()
+                size = comp()
+                ev[1].record()
+                dec(size)
+                ev[2].record()
+                torch.cuda.synchronize()
+                tc.append(ev[0].elapsed_time(ev[1]))
+                td.append(ev[1].elapsed_time(ev[2]))
+            header = arch[:32].cpu().numpy().tobytes()
+            err = float((out.double() - f.double()).abs().max())
+            assert err <= eb, f"{form} form violates the bound: {err} > {eb}"
+            entry[form] = {"compress_gbs": round(nbytes / (statistics.median(tc) / 1e3) / 1e9, 3),
+                           "decompress_gbs": round(nbytes / (statistics.median(td) / 1e3) / 1e9, 3),
+                           "compression_ratio": round(nbytes / size, 4),
+                           "repair_records": int.from_bytes(header[24:28], "little"),
+                           "max_abs_error": err, "abs_bound": eb}
+        entry["ratio_change"] = round(entry["matrix"]["compression_ratio"] / entry["plain"]["compression_ratio"] - 1, 5)
+        report[f"rel_{rel:g}"] = entry
+    # coefficient error of the tensor-core Z stage against the float64 lifting
+    cols = 16384
+    x = f.reshape(nz, -1)[:, :cols].contiguous()
+    eye = torch.eye(nz, dtype=torch.float64, device=dev).reshape(nz, nz, 1, 1)
+    m = torch.empty(nz, nz, dtype=torch.float64, device=dev)
+    for k in range(nz):
+        e = eye[:, k].contiguous()
+        _lib.checked(lib.waltz_b200_transform(C.c_void_p(e.data_ptr()), 8, 1, 1, nz, 0, sp))
+        m[:, k] = e.reshape(nz)
+    ref = m @ x.double()
+    tcx = x.clone()
+    _lib.checked(lib.waltz_b200_zmatrix(C.c_void_p(tcx.data_ptr()), cols, 1, nz, 0, sp))
+    diff = (tcx.double() - ref).abs()
+    report["z_coefficient_error_vs_float64"] = {"max_abs": float(diff.max()),
+                                                "max_rel_to_column_max": float((diff.max(0).values /
+                                                                                ref.abs().max(0).values.clamp_min(1e-30)).max()),
+                                                "columns": cols}
+    return report
 
 
 def algorithmic_bytes(n, s, a, fused=True):
@@ -385,6 +472,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tc-form", action="store_true", help="skip the plain vs tensor-core form comparison")
     ap.add_argument("--shape", type=int, nargs=3, default=list(SHAPE), metavar=("NZ", "NY", "NX"),
                     help="field shape (z y x); smaller shapes serve profiler captures")
     args = ap.parse_args()
