@@ -653,9 +653,6 @@ static void zmatrix_apply(const float* x, uint32_t nx, uint32_t ny, uint32_t nz,
     need(nz >= 1 && nz <= uint32_t(kZmMaxK), "Waltz: matrix form needs 1 <= nz <= 64");
     const uint64_t ncols = uint64_t(nx) * ny;
     const ZmPlan P = ZmPlan::make(nz);
-    CUtensorMap map{};
-    need(make_map_3d<float>(&map, x, ncols, nz, 1, ncols, ncols * nz, kZmCols, P.kp, 1),
-         "Waltz: matrix form needs 16-byte aligned planes (nx*ny a multiple of 4)");
     const float* bhi = t_zmat.get(nz, inverse, false, stream);
     const float* blo = t_zmat.get(nz, inverse, true, stream);
     auto kernel = zmatrix_kernel<Out>;
@@ -671,8 +668,8 @@ static void zmatrix_apply(const float* x, uint32_t nx, uint32_t ny, uint32_t nz,
     const uint64_t tiles = (ncols + kZmCols - 1) / kZmCols;
     int sms = 0;
     check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
-    const unsigned grid = unsigned(std::min<uint64_t>(tiles, uint64_t(sms) * (P.smem() * 2 <= 227u * 1024 ? 2 : 1)));
-    kernel<<<grid, kZmThreads, P.smem(), stream>>>(map, bhi, blo, nz, ncols, out, status, check_finite ? 1u : 0u);
+    const unsigned grid = unsigned(std::min<uint64_t>(tiles, resident_slots(kernel, P.smem())));
+    kernel<<<grid, kZmThreads, P.smem(), stream>>>(x, bhi, blo, nz, ncols, out, status, check_finite ? 1u : 0u);
     note_launch();
     check(cudaGetLastError(), "matrix kernel launch");
 }

@@ -6,9 +6,9 @@
 // contiguous columns) the whole Z stage is the GEMM  D = X^T * Mz^T  with one
 // row of D per column of the field, computed here on the 5th-generation
 // tensor cores:
-//   * a CTA takes 128 field columns at a time (UMMA M = 128); one TMA box
-//     brings the K = nz planes of those columns, and a shared-memory pass
-//     splits every value into TF32 halves (hi = fp32 truncated to TF32,
+//   * a CTA takes 128 field columns at a time (UMMA M = 128): its threads
+//     read the K = nz planes of those columns (coalesced rows of 128) and
+//     split every value into TF32 halves (hi = fp32 truncated to TF32,
 //     lo = x - hi, exact) written transposed into the K-major no-swizzle
 //     operand layout (8-row x 16-byte core matrices);
 //   * Mz's halves are prepared on the host in the same layout and loaded once
@@ -27,7 +27,7 @@ namespace wb {
 
 constexpr int kZmCols = 128;   // field columns per tile (UMMA M)
 constexpr int kZmMaxK = 64;    // largest nz handled (operands stay in shared memory)
-constexpr int kZmThreads = 128;
+constexpr int kZmThreads = 256;
 
 // Instruction descriptor of tcgen05.mma kind::tf32: D f32, A and B tf32,
 // both K-major, M = 128, N = np (bit layout of the UMMA instruction
@@ -68,11 +68,10 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
 }
 
 // Shared-memory plan of one CTA (bytes from a 1024-byte aligned base): the
-// staged planes X (kp rows x 128 columns), the A halves (128 x kp each) and
-// the B halves (np x kp each), all fp32.
+// A halves (128 x kp each) and the B halves (np x kp each), all fp32.
 struct ZmPlan {
     uint32_t kp, np;          // padded K (multiple of 8) and N (multiple of 16)
-    uint32_t a_bytes;         // X, or one A half: 128 x kp x 4 B
+    uint32_t a_bytes;         // one A half: 128 x kp x 4 B
     uint32_t b_bytes;         // one B half: np x kp x 4 B
     __host__ __device__ static ZmPlan make(uint32_t nz) {
         ZmPlan p;
@@ -82,7 +81,7 @@ struct ZmPlan {
         p.b_bytes = p.np * p.kp * 4;
         return p;
     }
-    __host__ __device__ uint32_t smem() const { return 1024 + 3 * a_bytes + 2 * b_bytes + 64; }
+    __host__ __device__ uint32_t smem() const { return 1024 + 2 * a_bytes + 2 * b_bytes + 64; }
 };
 
 // Destination of the Z stage: z-major store, or a per-sample emitter.
@@ -104,32 +103,29 @@ template <class Final> struct ZmEmit {
 // core layout (core (n/8, k/4) at ((n/8) * kp/4 + k/4) * 128 B, element
 // (n%8, k%4) at (n%8) * 16 + (k%4) * 4 inside it).
 template <class Out>
-__global__ void __launch_bounds__(kZmThreads, 1)
-    zmatrix_kernel(const __grid_constant__ CUtensorMap xmap, const float* bhi, const float* blo, uint32_t nz,
-                   uint64_t ncols, Out out, uint32_t* status, uint32_t check_finite) {
+__global__ void __launch_bounds__(kZmThreads, 2)
+    zmatrix_kernel(const float* x, const float* bhi, const float* blo, uint32_t nz, uint64_t ncols, Out out,
+                   uint32_t* status, uint32_t check_finite) {
     extern __shared__ __align__(1024) unsigned char zm_smem[];
     const ZmPlan P = ZmPlan::make(nz);
     unsigned char* base = zm_smem + ((1024 - (smem_u32(zm_smem) & 1023)) & 1023);
-    unsigned char* Xs = base;                  // TMA destination: kp rows of 128 columns
-    unsigned char* Ahi = Xs + P.a_bytes;
+    unsigned char* Ahi = base;
     unsigned char* Alo = Ahi + P.a_bytes;
     unsigned char* Bhi = Alo + P.a_bytes;
     unsigned char* Blo = Bhi + P.b_bytes;
-    uint64_t* tma_bar = reinterpret_cast<uint64_t*>(Blo + P.b_bytes);
-    uint64_t* mma_bar = tma_bar + 1;
+    uint64_t* mma_bar = reinterpret_cast<uint64_t*>(Blo + P.b_bytes);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_bar + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint64_t tiles = (ncols + kZmCols - 1) / kZmCols;
     const uint32_t ncols_alloc = P.np <= 32 ? 32 : (P.np <= 64 ? 64 : 128);
 
-    // tensor memory for D (128 lanes x np fp32 columns), barriers, operands B
+    // tensor memory for D (128 lanes x np fp32 columns), barrier, operands B
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                      "r"(ncols_alloc));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        mbar_init(tma_bar, 1);
         mbar_init(mma_bar, 1);
         fence_barrier_init();
     }
@@ -144,45 +140,46 @@ __global__ void __launch_bounds__(kZmThreads, 1)
     const uint32_t tmem = *tmem_slot;
     const uint32_t idesc = zm_idesc(P.np);
     const uint32_t sbo = (P.kp / 4) * 128; // 8-row groups of the K-major operands
+    const uint32_t kh = P.kp / 2;          // planes per half of the threads
 
-    auto issue = [&](uint64_t tile) {
-        mbar_expect_tx(tma_bar, P.a_bytes);
-        tma_load_3d(Xs, &xmap, int(tile * kZmCols), 0, 0, tma_bar);
-    };
-    uint64_t tile = blockIdx.x;
-    if (tid == 0 && tile < tiles) issue(tile);
     uint32_t phase = 0;
     bool bad = false;
-    for (; tile < tiles; tile += gridDim.x) {
-        if (!__syncthreads_and(warp != 0 || mbar_wait(tma_bar, phase, kWaitBound))) {
-            if (tid == 0) atomicOr(status, ST_WAIT_TIMEOUT);
-            break;
-        }
-        // split and transpose: thread c takes field column c; element (c, k)
-        // goes to core (c/8, k/4) at ((c/8) * kp/4 + k/4) * 128 B, row c%8
+    for (uint64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        // split and transpose: thread t takes field column c = t % 128 and the
+        // t / 128 half of the planes; element (c, k) goes to core (c/8, k/4)
+        // at ((c/8) * kp/4 + k/4) * 128 B, row c%8
         {
-            const int c = tid;
-            const float* xcol = reinterpret_cast<const float*>(Xs) + c;
+            const int c = tid % kZmCols, half = tid / kZmCols;
+            const uint64_t col = tile * kZmCols + c;
+            const bool live = col < ncols;
+            const float* xcol = x + col;
             unsigned char* hrow = Ahi + (c / 8) * sbo + (c % 8) * 16;
             unsigned char* lrow = Alo + (c / 8) * sbo + (c % 8) * 16;
-            for (uint32_t k = 0; k < P.kp; k += 4) {
-                uint32_t h[4], l[4];
+            float v[kZmMaxK / 2];
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const float x = xcol[(k + j) * kZmCols];
-                    if (check_finite) bad |= !finite_bits(x);
-                    h[j] = __float_as_uint(x) & 0xffffe000u;
-                    l[j] = __float_as_uint(__fsub_rn(x, __uint_as_float(h[j])));
+            for (int j = 0; j < kZmMaxK / 2; ++j) {
+                const uint32_t k = half * kh + j;
+                v[j] = (j < int(kh) && k < nz && live) ? xcol[size_t(k) * ncols] : 0.f;
+            }
+#pragma unroll
+            for (int j = 0; j < kZmMaxK / 2; j += 4) {
+                if (j < int(kh)) {
+                    uint32_t h[4], l[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        if (check_finite) bad |= !finite_bits(v[j + q]);
+                        h[q] = __float_as_uint(v[j + q]) & 0xffffe000u;
+                        l[q] = __float_as_uint(__fsub_rn(v[j + q], __uint_as_float(h[q])));
+                    }
+                    const uint32_t kq = (half * kh + j) / 4;
+                    *reinterpret_cast<uint4*>(hrow + kq * 128) = make_uint4(h[0], h[1], h[2], h[3]);
+                    *reinterpret_cast<uint4*>(lrow + kq * 128) = make_uint4(l[0], l[1], l[2], l[3]);
                 }
-                *reinterpret_cast<uint4*>(hrow + (k / 4) * 128) = make_uint4(h[0], h[1], h[2], h[3]);
-                *reinterpret_cast<uint4*>(lrow + (k / 4) * 128) = make_uint4(l[0], l[1], l[2], l[3]);
             }
         }
         fence_proxy_async();
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
-        // X is consumed: bring the next tile while this one is multiplied
-        if (tid == 0 && tile + gridDim.x < tiles) issue(tile + gridDim.x);
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             // A and B: K-major, no swizzle; cores 128 B apart along K (LBO),
@@ -204,11 +201,13 @@ __global__ void __launch_bounds__(kZmThreads, 1)
             break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        // epilogue: lane = field column, 16 coefficients per load
-        const uint64_t col = tile * kZmCols + 32 * warp + lane;
-        for (uint32_t c0 = 0; c0 < P.np; c0 += 16) {
+        // epilogue: warp w reads lanes 32 (w % 4) .. (lane = field column) and
+        // every other 16-coefficient group, starting at group w / 4
+        const uint32_t sub = warp % 4;
+        const uint64_t col = tile * kZmCols + 32 * sub + lane;
+        for (uint32_t c0 = 16 * (warp / 4); c0 < P.np; c0 += 32) {
             uint32_t r[16];
-            tmem_ld16(tmem + (uint32_t(32 * warp) << 16) + c0, r);
+            tmem_ld16(tmem + (uint32_t(32 * sub) << 16) + c0, r);
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             if (col < ncols) {
 #pragma unroll
@@ -217,6 +216,7 @@ __global__ void __launch_bounds__(kZmThreads, 1)
             }
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads(); // tensor memory read out, A free: the next tile may overwrite both
         phase ^= 1;
     }
     if (check_finite && __syncthreads_or(bad) && tid == 0) atomicOr(status, ST_NONFINITE_INPUT);
