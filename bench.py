@@ -253,7 +253,7 @@ def gpu_arm(args, rank, world, local_rank):
         "clocks": sampler.summary(t_wall0, t_wall1),
     }
     traffic = ROOT / "profiles" / "traffic.json"
-    if traffic.exists():
+    if traffic.exists() and shape == SHAPE:
         t = json.loads(traffic.read_text()).get(dom)
         if t:
             result["roofline"]["traffic"] = t
@@ -262,11 +262,11 @@ def gpu_arm(args, rank, world, local_rank):
     if not args.no_tc_form and world == 1:
         del field, out, archive, host_in, host_arch, host_out
         torch.cuda.empty_cache()
-        result["tc_form"] = tc_form_comparison(dev, lib, args.steps)
+        result["tc_form"] = tc_form_comparison(dev, lib, args.steps, tuple(args.tc_shape))
     return result
 
 
-def tc_form_comparison(dev, lib, steps):
+def tc_form_comparison(dev, lib, steps, shape=(64, 1024, 1024)):
     """Plain lifting against the precision form (tensor-core Z stage) on the
     tensor-core configuration: float32 1024x1024x64 (z=64) k^-11/3 random field
     (seed 3) with 1 % salt spikes of magnitude 50, REL 1e-3 and 1e-5; device
@@ -277,7 +277,6 @@ def tc_form_comparison(dev, lib, steps):
     import waltz_b200
     from waltz_b200 import _lib
     from waltz_b200.synthetic import power_law_field_device
-    shape = (64, 1024, 1024)
     nz, ny, nx = shape
     f = power_law_field_device(shape, 3, device=dev)
     gen = torch.Generator(device=dev)
@@ -293,7 +292,7 @@ def tc_form_comparison(dev, lib, steps):
     sp = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     written = C.c_size_t()
     lo, hi = waltz_b200.extrema(f)
-    report = {"workload": "f32 64x1024x1024 (z,y,x) k^-11/3 GRF seed 3 + 1% spikes of 50, plane schedule 5/3"}
+    report = {"workload": "f32 %dx%dx%d (z,y,x) k^-11/3 GRF seed 3 + 1%% spikes of 50, plane schedule" % shape}
     for rel in (1e-3, 1e-5):
         eb = rel * (hi - lo)
         entry = {}
@@ -330,7 +329,7 @@ def tc_form_comparison(dev, lib, steps):
         entry["ratio_change"] = round(entry["matrix"]["compression_ratio"] / entry["plain"]["compression_ratio"] - 1, 5)
         report[f"rel_{rel:g}"] = entry
     # coefficient error of the tensor-core Z stage against the float64 lifting
-    cols = 16384
+    cols = min(16384, nx * ny)
     x = f.reshape(nz, -1)[:, :cols].contiguous()
     eye = torch.eye(nz, dtype=torch.float64, device=dev).reshape(nz, nz, 1, 1)
     m = torch.empty(nz, nz, dtype=torch.float64, device=dev)
@@ -473,6 +472,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tc-form", action="store_true", help="skip the plain vs tensor-core form comparison")
+    ap.add_argument("--tc-shape", type=int, nargs=3, default=[64, 1024, 1024], metavar=("NZ", "NY", "NX"),
+                    help="field of the tensor-core comparison (z y x); smaller shapes serve profiler captures")
     ap.add_argument("--shape", type=int, nargs=3, default=list(SHAPE), metavar=("NZ", "NY", "NX"),
                     help="field shape (z y x); smaller shapes serve profiler captures")
     args = ap.parse_args()
