@@ -49,6 +49,22 @@ int waltz_b200_compress_form(const void* d_input, int width, uint32_t nx, uint32
                              double abs_error, int form, void* d_archive, size_t capacity, size_t* written,
                              void* stream);
 
+/* Batched compress of many independent fields of any shapes (the chunked
+ * datasets of the reference's loaders, one archive per chunk): one call,
+ * one CUDA graph replayed while the batch description stays the same, every
+ * chunk's archive byte-identical to waltz_b200_compress of that chunk.
+ * written[i] receives archive i's size. Fails (naming the item) if any item
+ * fails. New surface: the reference has no batched encoder. */
+typedef struct waltz_b200_chunk {
+    const void* input;  /* device, nx*ny*nz samples of `width` bytes */
+    uint32_t nx, ny, nz;
+    double abs_error;
+    void* archive;      /* device */
+    uint64_t capacity;  /* >= waltz_b200_compressed_capacity(nx*ny*nz, width) */
+} waltz_b200_chunk;
+int waltz_b200_compress_batch(const waltz_b200_chunk* chunks, uint32_t count, int width, uint64_t* written,
+                              void* stream);
+
 /* Decode an archive of `bytes` bytes into nx*ny*nz samples (the archive does
  * not store its dimensions); either form. */
 int waltz_b200_decompress(const void* d_archive, size_t bytes, int width, uint32_t nx, uint32_t ny,

@@ -15,9 +15,9 @@ import operator
 
 import numpy as np
 
-from ._lib import BatchShape, WaltzError, checked, lib
+from ._lib import BatchShape, Chunk, WaltzError, checked, lib
 
-__all__ = ["compress", "decompress", "compress_tensor", "decompress_tensor", "extrema",
+__all__ = ["compress", "decompress", "compress_tensor", "decompress_tensor", "compress_batch", "extrema",
            "compressed_capacity", "rel_to_abs_bound", "WaltzError"]
 
 
@@ -97,6 +97,42 @@ def decompress_tensor(archive, shape, dtype, *, out=None, stream=None):
                                         C.c_void_p(out.data_ptr()), out.numel() * itemsize,
                                         _stream(torch, stream)))
     return out
+
+
+def compress_batch(fields, abs_errors, *, out=None, stream=None):
+    """Compress many contiguous CUDA tensors (one dtype, any shapes) in one
+    call: one CUDA graph, kept and replayed while the fields, bounds and
+    output buffer stay the same. Returns one uint8 archive tensor per field,
+    views into `out` (a uint8 CUDA tensor; allocated when not given — pass the
+    same one again to replay the graph). Every archive equals compress_tensor
+    of its field."""
+    torch = _torch()
+    fields = list(fields)
+    if not fields:
+        return []
+    itemsize = fields[0].element_size()
+    if any(f.element_size() != itemsize or not f.is_cuda or not f.is_contiguous() for f in fields):
+        raise ValueError("expected contiguous CUDA tensors of one dtype")
+    bounds = [abs_errors] * len(fields) if not hasattr(abs_errors, "__len__") else list(abs_errors)
+    if len(bounds) != len(fields):
+        raise ValueError("one bound per field")
+    offsets, total = [], 0
+    for f in fields:
+        total = (total + 15) // 16 * 16
+        offsets.append(total)
+        total += compressed_capacity(f.numel(), itemsize)
+    if out is None:
+        out = torch.empty(total, dtype=torch.uint8, device=fields[0].device)
+    if out.numel() < total or out.dtype != torch.uint8:
+        raise ValueError(f"out must be a uint8 CUDA tensor of at least {total} bytes")
+    items = (Chunk * len(fields))()
+    for k, (f, eb, off) in enumerate(zip(fields, bounds, offsets)):
+        nx, ny, nz = _geometry(f.shape, itemsize)
+        items[k] = Chunk(f.data_ptr(), nx, ny, nz, _bound(eb), out.data_ptr() + off,
+                         compressed_capacity(f.numel(), itemsize))
+    written = (C.c_uint64 * len(fields))()
+    checked(lib().waltz_b200_compress_batch(items, len(fields), itemsize, written, _stream(torch, stream)))
+    return [out[off:off + written[k]] for k, off in enumerate(offsets)]
 
 
 def extrema(field, *, stream=None):

@@ -706,36 +706,54 @@ static bool matrix_form_ok(const Geometry& g, size_t width) {
 }
 
 // ------------------------------------------------------------------ encode
-template <class T>
-static size_t compress(const T* d_in, uint32_t nx, uint32_t ny, uint32_t nz, double eb, uint8_t* d_out,
-                       size_t capacity, cudaStream_t stream, const EncodeOptions& opt = EncodeOptions()) {
-    need(nx && ny && nz, "Waltz: nonzero dimensions required");
-    const uint64_t n = uint64_t(nx) * ny * nz;
-    need(n <= 0xffffffffull / sizeof(T), "Waltz: volume exceeds the archive section limits");
-    need(d_in && d_out, "Waltz: null buffer");
-    const double quantum = 1.5 * eb;
-    const T q = T(quantum), inv = T(1.0 / quantum);
-    need(eb > 0 && std::isfinite(eb) && std::isfinite(quantum) && q > T(0) && std::isfinite(q) && std::isfinite(inv),
-         "Waltz: invalid bound (positive finite, representable quantum required)");
-    {
-        const uintptr_t a = reinterpret_cast<uintptr_t>(d_in), b = reinterpret_cast<uintptr_t>(d_out);
-        need(!(a < b + capacity && b < a + n * sizeof(T)), "Waltz: input and output buffers overlap");
-    }
-    need(capacity >= 32 + wzp_header(uint32_t(n)), "Waltz: archive capacity too small");
-    const Geometry g = Geometry::make(nx, ny, nz);
-    const TransformScratch ts = scratch_need(g);
-    const uint32_t chunks = wzp_chunks(uint32_t(n));
-    const uint64_t words = (n + 31) / 32;
-    const uint64_t cblocks = (words + kCompactWords - 1) / kCompactWords;
+// One compression: validated arguments, its scratch plan, the enqueued
+// kernels and the interpretation of the 9 result words (layout[0..7] and the
+// status word) that the last kernels leave in scratch. Split so that a batch
+// can enqueue many of them (inside one CUDA graph) and read all results once.
+template <class T> struct CompressJob {
+    const T* in;
+    uint32_t nx, ny, nz;
+    double eb;
+    uint8_t* out;
+    size_t capacity;
+    EncodeOptions opt;
+    Geometry g;
+    uint64_t n;
 
-    Carver cv{nullptr};
-    auto plan = [&](Carver& c) {
-        struct P {
-            T *C, *lowA, *lowB, *inter, *bank2, *perr;
-            uint16_t* mag;
-            uint32_t *sign, *qbits, *qval, *pbits, *status, *ticket, *counts_p, *counts_q, *np, *nq;
-            uint64_t *state, *sizes, *wzp_total, *layout;
-        } p;
+    struct Plan {
+        T *C, *lowA, *lowB, *inter, *bank2, *perr;
+        uint16_t* mag;
+        uint32_t *sign, *qbits, *qval, *pbits, *status, *ticket, *counts_p, *counts_q, *np, *nq;
+        uint64_t *state, *sizes, *wzp_total, *layout; // layout[8] = status copy
+    };
+
+    static CompressJob make(const T* d_in, uint32_t nx, uint32_t ny, uint32_t nz, double eb, uint8_t* d_out,
+                            size_t capacity, const EncodeOptions& opt) {
+        need(nx && ny && nz, "Waltz: nonzero dimensions required");
+        const uint64_t n = uint64_t(nx) * ny * nz;
+        need(n <= 0xffffffffull / sizeof(T), "Waltz: volume exceeds the archive section limits");
+        need(d_in && d_out, "Waltz: null buffer");
+        const double quantum = 1.5 * eb;
+        const T q = T(quantum), inv = T(1.0 / quantum);
+        need(eb > 0 && std::isfinite(eb) && std::isfinite(quantum) && q > T(0) && std::isfinite(q) &&
+                 std::isfinite(inv),
+             "Waltz: invalid bound (positive finite, representable quantum required)");
+        {
+            const uintptr_t a = reinterpret_cast<uintptr_t>(d_in), b = reinterpret_cast<uintptr_t>(d_out);
+            need(!(a < b + capacity && b < a + n * sizeof(T)), "Waltz: input and output buffers overlap");
+        }
+        need(capacity >= 32 + wzp_header(uint32_t(n)), "Waltz: archive capacity too small");
+        CompressJob j{d_in, nx, ny, nz, eb, d_out, capacity, opt, Geometry::make(nx, ny, nz), n};
+        need(!opt.matrix || matrix_form_ok(j.g, sizeof(T)),
+             "Waltz: the matrix form needs float data in the plane schedule with 1 <= nz <= 64 and nx*ny a multiple of 4");
+        return j;
+    }
+
+    Plan plan(Carver& c) const {
+        const TransformScratch ts = scratch_need(g);
+        const uint32_t chunks = wzp_chunks(uint32_t(n));
+        const uint64_t words = (n + 31) / 32, cblocks = (words + kCompactWords - 1) / kCompactWords;
+        Plan p;
         p.C = c.take<T>(n);
         p.lowA = c.take<T>(ts.low);
         p.lowB = c.take<T>(ts.low);
@@ -756,97 +774,125 @@ static size_t compress(const T* d_in, uint32_t nx, uint32_t ny, uint32_t nz, dou
         p.state = c.take<uint64_t>(chunks);
         p.sizes = c.take<uint64_t>(chunks);
         p.wzp_total = c.take<uint64_t>(1);
-        p.layout = c.take<uint64_t>(8);
+        p.layout = c.take<uint64_t>(9);
         return p;
-    };
-    plan(cv);
-    Carver real{t_arena.reserve(cv.used)};
-    auto P = plan(real);
-    const uint16_t* rank = t_fwd_tables.get(nx, ny, nz, g.bz, false, stream);
-
-    check(cudaMemsetAsync(P.sign, 0, (words + 1) * 4, stream), "memset");
-    check(cudaMemsetAsync(P.qbits, 0, (words + 1) * 4, stream), "memset");
-    check(cudaMemsetAsync(P.pbits, 0, (words + 1) * 4, stream), "memset");
-    check(cudaMemsetAsync(P.status, 0, 4, stream), "memset");
-    check(cudaMemsetAsync(P.ticket, 0, 4, stream), "memset");
-    check(cudaMemsetAsync(P.state, 0, size_t(chunks) * 8, stream), "memset");
-
-    StageClock& clock = stage_clock();
-    clock.begin(stream);
-    // 1. forward transform
-    need(!opt.matrix || matrix_form_ok(g, sizeof(T)),
-         "Waltz: the matrix form needs float data in the plane schedule with 1 <= nz <= 64 and nx*ny a multiple of 4");
-    forward<T>(g, d_in, P.C, P.lowA, P.lowB, P.inter, P.status, stream, opt.matrix);
-    // 2. quantisation + Morton reorder
-    // A field made of whole bricks (2^k samples each) is quantised inside the
-    // WZP encoder, chunk by chunk; otherwise a separate pass writes the
-    // Morton-packed magnitudes and signs first.
-    const uint32_t bsz = 256 * g.bz;
-    const bool fused = nx % 16 == 0 && ny % 16 == 0 && nz % g.bz == 0 && (bsz & (bsz - 1)) == 0 && bsz <= kChunk;
-    if (!fused) {
-        QuantArgs<T> qa{P.C, Bricks::make(nx, ny, nz, g.bz), rank, q, inv, P.mag, P.sign, P.qbits, P.qval, P.status};
-        const uint64_t bricks = qa.b.count();
-        need(bricks < (1ull << 31), "Waltz: brick grid too large");
-        quantize_kernel<T><<<unsigned(bricks), kQuantThreads, 0, stream>>>(qa); note_launch();
-        check(cudaGetLastError(), "quantize launch");
-        clock.mark("quantize", stream);
     }
-    // 3. WZP encode straight into the archive
-    {
-        WzpEncodeArgs wa{uint32_t(n), d_out + 32, capacity - 32, P.ticket, P.state, P.sizes, P.status, opt.spin_cap,
-                         opt.skip_publish};
-        if (fused) {
-            uint32_t lb = 0;
-            while ((1u << lb) < bsz) ++lb;
-            launch_wzp_encode(wa, QuantBricks<T>{P.C, nx, ny, g.bz, lb, rank, q, inv, P.qbits, P.qval, P.status},
-                              chunks, stream);
-        } else {
-            launch_wzp_encode(wa, MagArrays{P.mag, P.sign}, chunks, stream);
+    size_t scratch_bytes() const {
+        Carver c{nullptr};
+        plan(c);
+        return c.used;
+    }
+
+    // Enqueues every kernel of the compression on `stream` (nothing syncs).
+    void enqueue(char* scratch, const uint16_t* rank, cudaStream_t stream) const {
+        Carver cv{scratch};
+        const Plan P = plan(cv);
+        const double quantum = 1.5 * eb;
+        const T q = T(quantum), inv = T(1.0 / quantum);
+        const uint32_t chunks = wzp_chunks(uint32_t(n));
+        const uint64_t words = (n + 31) / 32, cblocks = (words + kCompactWords - 1) / kCompactWords;
+        check(cudaMemsetAsync(P.sign, 0, (words + 1) * 4, stream), "memset");
+        check(cudaMemsetAsync(P.qbits, 0, (words + 1) * 4, stream), "memset");
+        check(cudaMemsetAsync(P.pbits, 0, (words + 1) * 4, stream), "memset");
+        check(cudaMemsetAsync(P.status, 0, 4, stream), "memset");
+        check(cudaMemsetAsync(P.ticket, 0, 4, stream), "memset");
+        check(cudaMemsetAsync(P.state, 0, size_t(chunks) * 8, stream), "memset");
+
+        StageClock& clock = stage_clock();
+        clock.begin(stream);
+        // 1. forward transform
+        forward<T>(g, in, P.C, P.lowA, P.lowB, P.inter, P.status, stream, opt.matrix);
+        // 2. quantisation + Morton reorder: a field made of whole bricks (2^k
+        // samples each) is quantised inside the WZP encoder, chunk by chunk;
+        // otherwise a separate pass writes the Morton-packed magnitudes and
+        // signs first.
+        const uint32_t bsz = 256 * g.bz;
+        const bool fused = nx % 16 == 0 && ny % 16 == 0 && nz % g.bz == 0 && (bsz & (bsz - 1)) == 0 && bsz <= kChunk;
+        if (!fused) {
+            QuantArgs<T> qa{P.C, Bricks::make(nx, ny, nz, g.bz), rank, q, inv, P.mag, P.sign, P.qbits, P.qval, P.status};
+            const uint64_t bricks = qa.b.count();
+            need(bricks < (1ull << 31), "Waltz: brick grid too large");
+            quantize_kernel<T><<<unsigned(bricks), kQuantThreads, 0, stream>>>(qa); note_launch();
+            check(cudaGetLastError(), "quantize launch");
+            clock.mark("quantize", stream);
         }
-        const uint32_t groups = wzp_groups(uint32_t(n));
-        wzp_directory_kernel<<<(groups + 255) / 256, 256, 0, stream>>>(d_out + 32, uint32_t(n), P.state, P.sizes,
-                                                                       P.wzp_total); note_launch();
-        check(cudaGetLastError(), "wzp directory launch");
+        // 3. WZP encode straight into the archive
+        {
+            WzpEncodeArgs wa{uint32_t(n), out + 32, capacity - 32, P.ticket, P.state, P.sizes, P.status, opt.spin_cap,
+                             opt.skip_publish};
+            if (fused) {
+                uint32_t lb = 0;
+                while ((1u << lb) < bsz) ++lb;
+                launch_wzp_encode(wa, QuantBricks<T>{P.C, nx, ny, g.bz, lb, rank, q, inv, P.qbits, P.qval, P.status},
+                                  chunks, stream);
+            } else {
+                launch_wzp_encode(wa, MagArrays{P.mag, P.sign}, chunks, stream);
+            }
+            const uint32_t groups = wzp_groups(uint32_t(n));
+            wzp_directory_kernel<<<(groups + 255) / 256, 256, 0, stream>>>(out + 32, uint32_t(n), P.state, P.sizes,
+                                                                           P.wzp_total); note_launch();
+            check(cudaGetLastError(), "wzp directory launch");
+        }
+        clock.mark("wzp_encode", stream);
+        // 4. inverse transform + repairs; fast-accept threshold of the repair
+        // check (float): eb * (1 - 2^-21), rounded down
+        {
+            T safe = T(eb * (1.0 - std::ldexp(1.0, -21)));
+            if (double(safe) > eb * (1.0 - std::ldexp(1.0, -21))) safe = std::nextafter(safe, T(0));
+            RepairOut<T> fin{in, nx, size_t(nx) * ny, eb, T(eb), P.pbits, P.perr, P.status, safe};
+            inverse<T>(g, P.C, P.inter, P.bank2, fin, P.status, stream, "inv_l0_repair", opt.matrix);
+        }
+        // 5. ordered side records
+        compact_count_kernel<<<unsigned(cblocks), kCompactThreads, 0, stream>>>(P.pbits, words, P.counts_p); note_launch();
+        compact_count_kernel<<<unsigned(cblocks), kCompactThreads, 0, stream>>>(P.qbits, words, P.counts_q); note_launch();
+        compact_scan_kernel<<<1, kCompactThreads, 0, stream>>>(P.counts_p, uint32_t(cblocks), P.np); note_launch();
+        compact_scan_kernel<<<1, kCompactThreads, 0, stream>>>(P.counts_q, uint32_t(cblocks), P.nq); note_launch();
+        layout_kernel<<<1, 32, 0, stream>>>(out, capacity, P.wzp_total, P.np, P.nq, sizeof(T),
+                                            uint8_t(g.flags(sizeof(T)) | (opt.matrix ? kMatrixFlag : 0)),
+                                            uint8_t(g.lxy), uint8_t(g.lz), uint8_t(g.bz), quantum, P.layout); note_launch();
+        compact_write_kernel<T><<<unsigned(cblocks), kCompactThreads, 0, stream>>>(P.pbits, words, P.counts_p, P.perr,
+                                                                                   out, P.layout, 0, 1, n); note_launch();
+        compact_write_kernel<uint32_t><<<unsigned(cblocks), kCompactThreads, 0, stream>>>(P.qbits, words, P.counts_q,
+                                                                                          P.qval, out, P.layout, 2, 3, n); note_launch();
+        check(cudaGetLastError(), "side record launch");
+        check(cudaMemcpyAsync(P.layout + 8, P.status, 4, cudaMemcpyDeviceToDevice, stream), "status copy");
+        clock.mark("side_records", stream);
     }
-    clock.mark("wzp_encode", stream);
-    // 4. inverse transform + repairs
-    {
-        // fast-accept threshold of the repair check (float): eb * (1 - 2^-21), rounded down
-        T safe = T(eb * (1.0 - std::ldexp(1.0, -21)));
-        if (double(safe) > eb * (1.0 - std::ldexp(1.0, -21))) safe = std::nextafter(safe, T(0));
-        RepairOut<T> fin{d_in, nx, size_t(nx) * ny, eb, T(eb), P.pbits, P.perr, P.status, safe};
-        inverse<T>(g, P.C, P.inter, P.bank2, fin, P.status, stream, "inv_l0_repair", opt.matrix);
+
+    // Device address of the 9 result words inside this job's scratch.
+    uint64_t* result(char* scratch) const {
+        Carver cv{scratch};
+        return plan(cv).layout;
     }
-    // 5. ordered side records
-    compact_count_kernel<<<unsigned(cblocks), kCompactThreads, 0, stream>>>(P.pbits, words, P.counts_p); note_launch();
-    compact_count_kernel<<<unsigned(cblocks), kCompactThreads, 0, stream>>>(P.qbits, words, P.counts_q); note_launch();
-    compact_scan_kernel<<<1, kCompactThreads, 0, stream>>>(P.counts_p, uint32_t(cblocks), P.np); note_launch();
-    compact_scan_kernel<<<1, kCompactThreads, 0, stream>>>(P.counts_q, uint32_t(cblocks), P.nq); note_launch();
-    layout_kernel<<<1, 32, 0, stream>>>(d_out, capacity, P.wzp_total, P.np, P.nq, sizeof(T),
-                                        uint8_t(g.flags(sizeof(T)) | (opt.matrix ? kMatrixFlag : 0)),
-                                        uint8_t(g.lxy), uint8_t(g.lz), uint8_t(g.bz), quantum, P.layout); note_launch();
-    compact_write_kernel<T><<<unsigned(cblocks), kCompactThreads, 0, stream>>>(P.pbits, words, P.counts_p, P.perr,
-                                                                               d_out, P.layout, 0, 1, n); note_launch();
-    compact_write_kernel<uint32_t><<<unsigned(cblocks), kCompactThreads, 0, stream>>>(P.qbits, words, P.counts_q,
-                                                                                      P.qval, d_out, P.layout, 2, 3, n); note_launch();
-    check(cudaGetLastError(), "side record launch");
-    clock.mark("side_records", stream);
+
+    // Interprets the 9 result words; returns the archive size or throws.
+    size_t finish(const uint64_t* h) const {
+        const uint32_t status = uint32_t(h[8]);
+        const uint64_t np = h[5], nq = h[6];
+        if (status & ST_NONFINITE_INPUT) throw Error("nonfinite input is unsupported");
+        if (status & ST_QUANT_DOMAIN) throw Error("coefficient exceeds portable integer conversion domain");
+        if (status & ST_BOUND) throw Error("native repair cannot meet strict bound or nonfinite reconstruction");
+        if (status & ST_LOOKBACK_TIMEOUT) throw Error("Waltz: WZP lookback wait exceeded its bound");
+        if (status & ST_WAIT_TIMEOUT) throw Error("Waltz: asynchronous copy wait exceeded its bound");
+        if (status & ST_CAPACITY) throw Error("archive capacity too small");
+        if ((n > (1u << 20) && nq >= (1u << 20)) || (n > (1u << 22) && np >= (1u << 22)))
+            throw Error("portable GPU side-channel capacity reached");
+        if (h[7]) throw Error("archive capacity too small");
+        return size_t(h[4]);
+    }
+};
+
+template <class T>
+static size_t compress(const T* d_in, uint32_t nx, uint32_t ny, uint32_t nz, double eb, uint8_t* d_out,
+                       size_t capacity, cudaStream_t stream, const EncodeOptions& opt = EncodeOptions()) {
+    const CompressJob<T> job = CompressJob<T>::make(d_in, nx, ny, nz, eb, d_out, capacity, opt);
+    char* scratch = t_arena.reserve(job.scratch_bytes());
+    const uint16_t* rank = t_fwd_tables.get(nx, ny, nz, job.g.bz, false, stream);
+    job.enqueue(scratch, rank, stream);
     uint64_t* h = pinned();
-    check(cudaMemcpyAsync(h, P.layout, 8 * 8, cudaMemcpyDeviceToHost, stream), "readback");
-    check(cudaMemcpyAsync(h + 8, P.status, 4, cudaMemcpyDeviceToHost, stream), "readback");
+    check(cudaMemcpyAsync(h, job.result(scratch), 9 * 8, cudaMemcpyDeviceToHost, stream), "readback");
     check(cudaStreamSynchronize(stream), "compress");
-    const uint32_t status = uint32_t(h[8]);
-    const uint64_t np = h[5], nq = h[6];
-    if (status & ST_NONFINITE_INPUT) throw Error("nonfinite input is unsupported");
-    if (status & ST_QUANT_DOMAIN) throw Error("coefficient exceeds portable integer conversion domain");
-    if (status & ST_BOUND) throw Error("native repair cannot meet strict bound or nonfinite reconstruction");
-    if (status & ST_LOOKBACK_TIMEOUT) throw Error("Waltz: WZP lookback wait exceeded its bound");
-    if (status & ST_WAIT_TIMEOUT) throw Error("Waltz: asynchronous copy wait exceeded its bound");
-    if (status & ST_CAPACITY) throw Error("archive capacity too small");
-    if ((n > (1u << 20) && nq >= (1u << 20)) || (n > (1u << 22) && np >= (1u << 22)))
-        throw Error("portable GPU side-channel capacity reached");
-    if (h[7]) throw Error("archive capacity too small");
-    return size_t(h[4]);
+    return job.finish(h);
 }
 
 // ------------------------------------------------------------------ decode
@@ -1124,6 +1170,161 @@ static void extrema(const T* d_in, uint64_t n, double* mn, double* mx, cudaStrea
     *mx = value(pin[3]);
 }
 
+// ------------------------------------------------------------ batched compress
+// Many independent fields (uneven shapes) compressed by one CUDA graph: each
+// field's kernel chain is captured on one of kBatchStreams parallel branches,
+// so fields run concurrently and one graph launch replaces thousands of
+// kernel launches. The instantiated graph is kept and replayed while the
+// batch description (pointers, shapes, bounds) stays the same; all results
+// come back in one copy.
+constexpr int kBatchStreams = 16;
+
+struct BatchTables {
+    struct Entry {
+        uint32_t nx, ny, nz, bz;
+        uint16_t* ptr;
+    };
+    int device = -1;
+    std::vector<Entry> entries;
+    ~BatchTables() {
+        for (auto& e : entries) cudaFree(e.ptr);
+    }
+    const uint16_t* get(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t bz, cudaStream_t stream) {
+        int dev = 0;
+        check(cudaGetDevice(&dev), "cudaGetDevice");
+        if (dev != device) {
+            entries.clear(); // tables of another device's context stay allocated there
+            device = dev;
+        }
+        for (auto& e : entries)
+            if (e.nx == nx && e.ny == ny && e.nz == nz && e.bz == bz) return e.ptr;
+        const auto host = morton_tables(nx, ny, nz, bz, false);
+        uint16_t* p = nullptr;
+        check(cudaMalloc(&p, host.size() * 2), "Waltz: cannot allocate Morton table");
+        check(cudaMemcpyAsync(p, host.data(), host.size() * 2, cudaMemcpyHostToDevice, stream), "table upload");
+        check(cudaStreamSynchronize(stream), "table upload");
+        entries.push_back({nx, ny, nz, bz, p});
+        return p;
+    }
+};
+
+struct BatchCompressState {
+    int device = -1;
+    std::vector<unsigned char> key;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t cap = nullptr;
+    cudaStream_t work[kBatchStreams] = {};
+    cudaEvent_t fork = nullptr, join[kBatchStreams] = {};
+    Arena scratch;
+    uint64_t* host_results = nullptr;
+    size_t host_cap = 0;
+    BatchTables tables;
+    void ensure_streams() {
+        int dev = 0;
+        check(cudaGetDevice(&dev), "cudaGetDevice");
+        if (cap && dev == device) return;
+        check(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "stream");
+        for (auto& w : work) check(cudaStreamCreateWithFlags(&w, cudaStreamNonBlocking), "stream");
+        check(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "event");
+        for (auto& e : join) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+        if (exec) exec = nullptr; // belonged to the previous device
+        key.clear();
+        device = dev;
+    }
+};
+static thread_local BatchCompressState t_bc;
+
+template <class T>
+static void compress_batch(const waltz_b200_chunk* items, uint32_t count, uint64_t* written, cudaStream_t stream) {
+    need(count > 0 && items && written, "invalid batch arguments");
+    std::vector<CompressJob<T>> jobs;
+    jobs.reserve(count);
+    std::vector<size_t> offset(count);
+    size_t total = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        const waltz_b200_chunk& c = items[i];
+        try {
+            jobs.push_back(CompressJob<T>::make(static_cast<const T*>(c.input), c.nx, c.ny, c.nz, c.abs_error,
+                                                static_cast<uint8_t*>(c.archive), c.capacity, EncodeOptions()));
+        } catch (const std::exception& e) {
+            throw Error("batch item " + std::to_string(i) + ": " + e.what());
+        }
+        total = (total + 255) & ~size_t(255);
+        offset[i] = total;
+        total += jobs.back().scratch_bytes();
+    }
+    total = (total + 255) & ~size_t(255);
+    const size_t results_at = total;
+    total += size_t(count) * 9 * 8;
+
+    BatchCompressState& st = t_bc;
+    st.ensure_streams();
+    std::vector<unsigned char> key(reinterpret_cast<const unsigned char*>(items),
+                                   reinterpret_cast<const unsigned char*>(items + count));
+    key.push_back(uint8_t(sizeof(T)));
+    char* base = st.scratch.reserve(total);
+    {
+        // the scratch must not have moved since the graph was captured
+        const uintptr_t b = reinterpret_cast<uintptr_t>(base);
+        key.insert(key.end(), reinterpret_cast<const unsigned char*>(&b), reinterpret_cast<const unsigned char*>(&b) + 8);
+    }
+    uint64_t* results = reinterpret_cast<uint64_t*>(base + results_at);
+    if (!st.exec || key != st.key) {
+        std::vector<const uint16_t*> rank(count);
+        for (uint32_t i = 0; i < count; ++i)
+            rank[i] = st.tables.get(jobs[i].nx, jobs[i].ny, jobs[i].nz, jobs[i].g.bz, st.cap);
+        StageClock& clock = stage_clock();
+        const bool profiling = clock.enabled;
+        clock.enabled = false;
+        cudaGraph_t graph = nullptr;
+        check(cudaStreamBeginCapture(st.cap, cudaStreamCaptureModeThreadLocal), "begin capture");
+        try {
+            check(cudaEventRecord(st.fork, st.cap), "fork");
+            for (auto& w : st.work) check(cudaStreamWaitEvent(w, st.fork, 0), "fork wait");
+            for (uint32_t i = 0; i < count; ++i) {
+                cudaStream_t w = st.work[i % kBatchStreams];
+                jobs[i].enqueue(base + offset[i], rank[i], w);
+                check(cudaMemcpyAsync(results + 9 * size_t(i), jobs[i].result(base + offset[i]), 9 * 8,
+                                      cudaMemcpyDeviceToDevice, w), "result copy");
+            }
+            for (int k = 0; k < kBatchStreams; ++k) {
+                check(cudaEventRecord(st.join[k], st.work[k]), "join");
+                check(cudaStreamWaitEvent(st.cap, st.join[k], 0), "join wait");
+            }
+        } catch (...) {
+            cudaStreamEndCapture(st.cap, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            clock.enabled = profiling;
+            throw;
+        }
+        clock.enabled = profiling;
+        check(cudaStreamEndCapture(st.cap, &graph), "end capture");
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        check(ie, "graph instantiate");
+        if (st.exec) cudaGraphExecDestroy(st.exec);
+        st.exec = exec;
+        st.key = std::move(key);
+    }
+    check(cudaGraphLaunch(st.exec, stream), "graph launch");
+    if (st.host_cap < size_t(count) * 9) {
+        if (st.host_results) cudaFreeHost(st.host_results);
+        st.host_results = nullptr;
+        check(cudaMallocHost(&st.host_results, size_t(count) * 9 * 8), "pinned results");
+        st.host_cap = size_t(count) * 9;
+    }
+    check(cudaMemcpyAsync(st.host_results, results, size_t(count) * 9 * 8, cudaMemcpyDeviceToHost, stream), "readback");
+    check(cudaStreamSynchronize(stream), "batch compress");
+    for (uint32_t i = 0; i < count; ++i) {
+        try {
+            written[i] = jobs[i].finish(st.host_results + 9 * size_t(i));
+        } catch (const std::exception& e) {
+            throw Error("batch item " + std::to_string(i) + ": " + e.what());
+        }
+    }
+}
+
 static thread_local char t_error[256];
 static int fail(const std::exception& e) {
     std::snprintf(t_error, sizeof(t_error), "%s", e.what());
@@ -1175,6 +1376,22 @@ int waltz_b200_compress_form(const void* d_input, int width, uint32_t nx, uint32
         *written = width == 4
                        ? compress(static_cast<const float*>(d_input), nx, ny, nz, abs_error, out, capacity, s, opt)
                        : compress(static_cast<const double*>(d_input), nx, ny, nz, abs_error, out, capacity, s, opt);
+        t_error[0] = 0;
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+int waltz_b200_compress_batch(const waltz_b200_chunk* chunks, uint32_t count, int width, uint64_t* written,
+                              void* stream) {
+    try {
+        need(width == 4 || width == 8, "type must be FP32 or FP64");
+        if (written)
+            for (uint32_t i = 0; i < count; ++i) written[i] = 0;
+        auto s = reinterpret_cast<cudaStream_t>(stream);
+        if (width == 4) compress_batch<float>(chunks, count, written, s);
+        else compress_batch<double>(chunks, count, written, s);
         t_error[0] = 0;
         return 0;
     } catch (const std::exception& e) {
