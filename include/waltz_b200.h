@@ -65,6 +65,26 @@ typedef struct waltz_b200_chunk {
 int waltz_b200_compress_batch(const waltz_b200_chunk* chunks, uint32_t count, int width, uint64_t* written,
                               void* stream);
 
+/* Batched decode of many archives of any shapes and either form into caller
+ * buffers (e.g. views of one preallocated tensor): one call, one CUDA graph.
+ * Archive locations and headers are passed to the graph through a device
+ * table, so the graph is captured once per description (count, shapes, forms,
+ * outputs) and replayed for later batches of other archives with the same
+ * description. `header` optionally points to a host copy of an archive's
+ * first 32 bytes (NULL: read from the device). Every output equals
+ * waltz_b200_decompress of that archive. Fails (naming the item) if any item
+ * fails. New surface: the reference batch decoder needs one tile shape for
+ * the whole batch (waltz_gpu_decode_batch, src/batch_decode.cuh:74-186). */
+typedef struct waltz_b200_archive {
+    const void* archive;  /* device */
+    uint64_t bytes;
+    const void* header;   /* optional host copy of the 32-byte header */
+    uint32_t nx, ny, nz;
+    void* output;         /* device, nx*ny*nz samples of `width` bytes */
+    uint64_t output_bytes;
+} waltz_b200_archive;
+int waltz_b200_decompress_batch(const waltz_b200_archive* archives, uint32_t count, int width, void* stream);
+
 /* Decode an archive of `bytes` bytes into nx*ny*nz samples (the archive does
  * not store its dimensions); either form. */
 int waltz_b200_decompress(const void* d_archive, size_t bytes, int width, uint32_t nx, uint32_t ny,

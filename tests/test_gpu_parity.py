@@ -365,3 +365,74 @@ def test_batch_compress_equals_single_calls():
     bad = fields[:3] + [torch.full((8, 8, 8), float("nan"), device="cuda")]
     with pytest.raises(waltz_b200.WaltzError, match="batch item 3"):
         waltz_b200.compress_batch(bad, 1e-3)
+
+
+def _uneven_batch(torch, seed, count, sides=(16, 17, 32, 48, 64)):
+    from waltz_b200 import synthetic as S
+    rng = np.random.default_rng(seed)
+    fields, bounds = [], []
+    for k in range(count):
+        shape = tuple(int(rng.choice(sides)) for _ in range(3))
+        a = S.power_law_field(shape, seed * 100 + k) * float(10 ** rng.uniform(-2, 3))
+        fields.append(torch.from_numpy(a).cuda())
+        bounds.append(1e-3 * float(a.max() - a.min()))
+    return fields, bounds
+
+
+def test_batch_decompress_equals_single_calls():
+    """Batched decode of uneven archives of both forms into one preallocated
+    tensor: bit-identical to the single-call decode; a second batch of other
+    archives with the same shapes replays the graph; host header copies and a
+    list of output tensors give the same result."""
+    torch = _torch()
+    import waltz_b200
+    from waltz_b200 import synthetic as S
+    fields, bounds = _uneven_batch(torch, 5, 12)
+    # two precision-form archives (plane schedule, nz <= 64)
+    for shape in [(24, 96, 64), (33, 24, 40)]:
+        fields.append(torch.from_numpy(S.power_law_field(shape, 9)).cuda())
+        bounds.append(1e-3)
+    forms = ["plain"] * 12 + ["matrix"] * 2
+    shapes = [tuple(f.shape) for f in fields]
+    total = sum(f.numel() for f in fields)
+    out = torch.full((total,), float("nan"), dtype=torch.float32, device="cuda")
+    for rnd in range(2):
+        if rnd:  # other archives, same shapes and forms: the graph is replayed
+            fields = [f * 1.5 + 0.25 for f in fields]
+        archives = [waltz_b200.compress_tensor(f, eb, form=fm) for f, eb, fm in zip(fields, bounds, forms)]
+        # archives in one staging buffer, like a loader's packed upload
+        staging = torch.cat(archives)
+        views, at = [], 0
+        for a in archives:
+            views.append(staging[at:at + a.numel()])
+            at += a.numel()
+        got = waltz_b200.decompress_batch(views, shapes, torch.float32, out=out)
+        for a, s, g, f, eb in zip(archives, shapes, got, fields, bounds):
+            single = waltz_b200.decompress_tensor(a, s, torch.float32)
+            assert torch.equal(g, single)
+            assert float((g.double() - f.double()).abs().max()) <= eb
+    hdrs = [bytes(a[:32].cpu().numpy()) for a in archives]
+    outs = [torch.empty(s, dtype=torch.float32, device="cuda") for s in shapes]
+    got = waltz_b200.decompress_batch(archives, shapes, torch.float32, out=outs, headers=hdrs)
+    for a, s, g in zip(archives, shapes, got):
+        assert torch.equal(g, waltz_b200.decompress_tensor(a, s, torch.float32))
+
+
+def test_batch_decompress_f64_and_errors():
+    torch = _torch()
+    import waltz_b200
+    from waltz_b200 import synthetic as S
+    fields = [torch.from_numpy(S.power_law_field(s, 11).astype(np.float64)).cuda()
+              for s in [(16, 16, 16), (20, 33, 18), (40, 24, 32)]]
+    archives = [waltz_b200.compress_tensor(f, 1e-6) for f in fields]
+    shapes = [tuple(f.shape) for f in fields]
+    got = waltz_b200.decompress_batch(archives, shapes, torch.float64)
+    for a, s, g in zip(archives, shapes, got):
+        assert torch.equal(g, waltz_b200.decompress_tensor(a, s, torch.float64))
+    # a truncated archive is reported with its index
+    bad = archives[:2] + [archives[2][:-8]]
+    with pytest.raises(waltz_b200.WaltzError, match="batch item 2"):
+        waltz_b200.decompress_batch(bad, shapes, torch.float64)
+    # a shape that does not match the archive's levels
+    with pytest.raises(waltz_b200.WaltzError, match="batch item 1"):
+        waltz_b200.decompress_batch(archives, [shapes[0], (64, 64, 64), shapes[2]], torch.float64)

@@ -15,9 +15,9 @@ import operator
 
 import numpy as np
 
-from ._lib import BatchShape, Chunk, WaltzError, checked, lib
+from ._lib import Archive, BatchShape, Chunk, WaltzError, checked, lib
 
-__all__ = ["compress", "decompress", "compress_tensor", "decompress_tensor", "compress_batch", "extrema",
+__all__ = ["compress", "decompress", "compress_tensor", "decompress_tensor", "compress_batch", "decompress_batch", "extrema",
            "compressed_capacity", "rel_to_abs_bound", "WaltzError"]
 
 
@@ -133,6 +133,57 @@ def compress_batch(fields, abs_errors, *, out=None, stream=None):
     written = (C.c_uint64 * len(fields))()
     checked(lib().waltz_b200_compress_batch(items, len(fields), itemsize, written, _stream(torch, stream)))
     return [out[off:off + written[k]] for k, off in enumerate(offsets)]
+
+
+def decompress_batch(archives, shapes, dtype, *, out=None, headers=None, stream=None):
+    """Decode many archives (uint8 CUDA tensors, e.g. views of one staging
+    buffer) of any shapes in one call, through one CUDA graph that is replayed
+    while the shapes, forms and outputs stay the same. `out` is either one
+    preallocated CUDA tensor of `dtype` holding at least the total sample count
+    (each result is a (z,y,x) view of it, packed back to back) or a list of
+    contiguous CUDA tensors, one per archive. `headers` optionally gives host
+    copies (bytes-like, >= 32 bytes each) of the archives' headers. Returns the
+    list of decoded (z,y,x) tensors."""
+    torch = _torch()
+    dtype = {np.float32: torch.float32, np.float64: torch.float64}.get(dtype, dtype)
+    if dtype not in (torch.float32, torch.float64):
+        raise TypeError("Waltz requires float32 or float64")
+    itemsize = 4 if dtype == torch.float32 else 8
+    archives, shapes = list(archives), [tuple(s) for s in shapes]
+    if len(archives) != len(shapes):
+        raise ValueError("one shape per archive")
+    if not archives:
+        return []
+    if any(not a.is_cuda or not a.is_contiguous() or a.dtype != torch.uint8 for a in archives):
+        raise ValueError("expected contiguous uint8 CUDA archive tensors")
+    sizes = [math.prod(s) for s in shapes]
+    if out is None:
+        out = torch.empty(sum(sizes), dtype=dtype, device=archives[0].device)
+    if isinstance(out, (list, tuple)):
+        views = list(out)
+        if len(views) != len(archives) or any(v.dtype != dtype or not v.is_contiguous() or v.numel() < k
+                                              for v, k in zip(views, sizes)):
+            raise ValueError("one contiguous output tensor of the batch dtype per archive")
+        views = [v.view(-1)[:k].view(s) for v, k, s in zip(views, sizes, shapes)]
+    else:
+        if out.dtype != dtype or not out.is_contiguous() or out.numel() < sum(sizes):
+            raise ValueError(f"out must be a contiguous {dtype} tensor of at least {sum(sizes)} samples")
+        flat, views, at = out.view(-1), [], 0
+        for k, s in zip(sizes, shapes):
+            views.append(flat[at:at + k].view(s))
+            at += k
+    keep = []
+    items = (Archive * len(archives))()
+    for k, (a, s, v) in enumerate(zip(archives, shapes, views)):
+        nx, ny, nz = _geometry(s, itemsize)
+        hdr = None
+        if headers is not None:
+            buf = C.create_string_buffer(bytes(headers[k][:32]), 32)
+            keep.append(buf)
+            hdr = C.cast(buf, C.c_void_p)
+        items[k] = Archive(a.data_ptr(), a.numel(), hdr, nx, ny, nz, v.data_ptr(), v.numel() * itemsize)
+    checked(lib().waltz_b200_decompress_batch(items, len(archives), itemsize, _stream(torch, stream)))
+    return views
 
 
 def extrema(field, *, stream=None):

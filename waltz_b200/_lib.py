@@ -26,6 +26,7 @@ SIGNATURES = {
     "waltz_b200_compress_form": (C.c_int, [C.c_void_p, C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_double,
                                            C.c_int, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t), C.c_void_p]),
     "waltz_b200_compress_batch": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int, C.POINTER(C.c_uint64), C.c_void_p]),
+    "waltz_b200_decompress_batch": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int, C.c_void_p]),
     "waltz_b200_decompress": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_uint32, C.c_uint32, C.c_uint32,
                                         C.c_void_p, C.c_size_t, C.c_void_p]),
     "waltz_b200_extrema": (C.c_int, [C.c_void_p, C.c_int, C.c_uint64, C.POINTER(C.c_double),
@@ -56,6 +57,12 @@ class Chunk(C.Structure):
     """waltz_b200_chunk (include/waltz_b200.h)."""
     _fields_ = [("input", C.c_void_p), ("nx", C.c_uint32), ("ny", C.c_uint32), ("nz", C.c_uint32),
                 ("abs_error", C.c_double), ("archive", C.c_void_p), ("capacity", C.c_uint64)]
+
+
+class Archive(C.Structure):
+    """waltz_b200_archive (include/waltz_b200.h)."""
+    _fields_ = [("archive", C.c_void_p), ("bytes", C.c_uint64), ("header", C.c_void_p), ("nx", C.c_uint32),
+                ("ny", C.c_uint32), ("nz", C.c_uint32), ("output", C.c_void_p), ("output_bytes", C.c_uint64)]
 
 
 class WaltzError(RuntimeError):

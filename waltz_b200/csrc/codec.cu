@@ -612,34 +612,45 @@ static void pack_tf32_halves(const std::vector<double>& m, uint32_t nz, std::vec
         }
 }
 
+// Device copies of the Z matrices per column length, kept until exit: a
+// captured graph may hold their addresses.
 struct ZMatrixCache {
+    struct Entry {
+        uint32_t nz;
+        float* dev; // fwd hi, fwd lo, inv hi, inv lo
+        size_t half; // floats per half
+    };
     int device = -1;
-    uint32_t nz = 0;
-    float* dev = nullptr; // fwd hi, fwd lo, inv hi, inv lo
-    size_t half = 0;      // floats per half
+    std::vector<Entry> entries;
     ~ZMatrixCache() {
-        if (dev) cudaFree(dev);
+        for (auto& e : entries) cudaFree(e.dev);
     }
     const float* get(uint32_t n, bool inverse, bool lo, cudaStream_t stream) {
         int d = 0;
         check(cudaGetDevice(&d), "cudaGetDevice");
-        if (!dev || d != device || n != nz) {
-            if (dev && d == device) cudaFree(dev);
-            dev = nullptr;
+        if (d != device) {
+            entries.clear(); // matrices of another device's context stay allocated there
+            device = d;
+        }
+        const Entry* hit = nullptr;
+        for (auto& e : entries)
+            if (e.nz == n) hit = &e;
+        if (!hit) {
             const std::vector<double> M = z_analysis_matrix(n), S = invert_matrix(M, n);
             std::vector<float> fh, fl, ih, il;
             pack_tf32_halves(M, n, fh, fl);
             pack_tf32_halves(S, n, ih, il);
-            half = fh.size();
-            check(cudaMalloc(&dev, 4 * half * sizeof(float)), "Waltz: cannot allocate Z matrices");
+            Entry e{n, nullptr, fh.size()};
+            check(cudaMalloc(&e.dev, 4 * e.half * sizeof(float)), "Waltz: cannot allocate Z matrices");
             std::vector<float> all;
             for (auto* part : {&fh, &fl, &ih, &il}) all.insert(all.end(), part->begin(), part->end());
-            check(cudaMemcpyAsync(dev, all.data(), all.size() * 4, cudaMemcpyHostToDevice, stream), "Z matrix upload");
+            check(cudaMemcpyAsync(e.dev, all.data(), all.size() * 4, cudaMemcpyHostToDevice, stream),
+                  "Z matrix upload");
             check(cudaStreamSynchronize(stream), "Z matrix upload");
-            device = d;
-            nz = n;
+            entries.push_back(e);
+            hit = &entries.back();
         }
-        return dev + (size_t(inverse) * 2 + size_t(lo)) * half;
+        return hit->dev + (size_t(inverse) * 2 + size_t(lo)) * hit->half;
     }
 };
 static thread_local ZMatrixCache t_zmat;
@@ -955,8 +966,11 @@ static Layout validate_header(const Header& h, const Geometry& g, size_t bytes, 
 // Directory check: group spans must tile the payload exactly. The fast path
 // verifies canonical (increasing) order on the device; anything else is
 // checked on the host like cpu/src/wzp_cpu.cpp:720-761.
-__global__ void directory_check_kernel(const uint8_t* in, uint32_t n, uint64_t payload, uint32_t* status) {
+__global__ void directory_check_kernel(JobRef job, uint32_t n, uint32_t* status) {
     __shared__ uint32_t tmp[40];
+    const DecodeJob J = job.get();
+    const uint8_t* in = J.base + 32;
+    const uint64_t payload = J.wzp - wzp_header(n);
     const uint32_t chunks = wzp_chunks(n), groups = wzp_groups(n);
     const uint8_t* meta = in + size_t(groups) * 4;
     uint64_t carry = 0;
@@ -1015,18 +1029,21 @@ static void host_directory_check(const uint8_t* in, uint32_t n, uint64_t payload
     need(cursor == payload, "WZP trailing or missing payload bytes");
 }
 
+static DecodeJob decode_job(const uint8_t* d_in, const Header& h, const Layout& L) {
+    return DecodeJob{d_in, h.wzp, L.pi, L.pv, L.qi, L.qv, h.q, h.np, h.nq};
+}
+
 // Decoder kernels of one archive, launched without synchronising. Scratch:
-// C, bank1, bank2 of n samples each and the inverse Morton table.
+// C, bank1, bank2 of n samples each and the inverse Morton table. With
+// `job.ptr` set (graph capture) the side-record kernels are always launched
+// on a fixed grid, as the counts are only known on the device.
 template <class T, class Final, class Patch>
-static void decode_launch(const uint8_t* d_in, const Header& h, const Layout& L, const Geometry& g,
-                          const uint16_t* irank, T* C, T* bank1, T* bank2, const Final& fin, const Patch& patch,
-                          uint32_t* status, cudaStream_t stream) {
+static void decode_launch(const JobRef& job, bool matrix, const Geometry& g, const uint16_t* irank, T* C, T* bank1,
+                          T* bank2, const Final& fin, const Patch& patch, uint32_t* status, cudaStream_t stream) {
     const uint32_t n = uint32_t(g.n);
-    const uint8_t* wzp = d_in + 32;
-    const uint64_t header = wzp_header(n);
     StageClock& clock = stage_clock();
     clock.begin(stream);
-    directory_check_kernel<<<1, 256, 0, stream>>>(wzp, n, h.wzp - header, status); note_launch();
+    directory_check_kernel<<<1, 256, 0, stream>>>(job, n, status); note_launch();
     {
         static thread_local int cfg_dev = -1;
         int dev = 0;
@@ -1045,19 +1062,23 @@ static void decode_launch(const uint8_t* d_in, const Header& h, const Layout& L,
             map.fast = true;
             while ((1u << map.lb) < bsz) ++map.lb;
         }
-        WzpDecodeArgs<T> da{wzp, h.wzp, n, map, T(h.q), C, status};
+        WzpDecodeArgs<T> da{job, n, map, C, status};
         wzp_decode_kernel<T><<<wzp_chunks(n), kWzpThreads, sizeof(WzpDecodeSmem), stream>>>(da); note_launch();
         check(cudaGetLastError(), "wzp decode launch");
     }
     clock.mark("wzp_decode", stream);
-    if (h.nq)
-        qpatch_kernel<T><<<(h.nq + 255) / 256, 256, 0, stream>>>(d_in + L.qi, d_in + L.qv, h.nq, g.n, T(h.q), C,
-                                                                 status); note_launch();
+    const unsigned fixed = unsigned(std::min<uint64_t>((g.n + 255) / 256, 32));
+    if (job.ptr || job.val.nq) {
+        qpatch_kernel<T><<<job.ptr ? fixed : (job.val.nq + 255) / 256, 256, 0, stream>>>(job, g.n, C, status);
+        note_launch();
+    }
     clock.mark("qpatch", stream);
-    inverse<T>(g, C, bank1, bank2, fin, status, stream, "inv_l0", (h.flags & kMatrixFlag) != 0);
-    if (h.np)
-        rpatch_kernel<T, Patch><<<(h.np + 255) / 256, 256, 0, stream>>>(d_in + L.pi, d_in + L.pv, h.np, g.n, patch,
-                                                                        status); note_launch();
+    inverse<T>(g, C, bank1, bank2, fin, status, stream, "inv_l0", matrix);
+    if (job.ptr || job.val.np) {
+        rpatch_kernel<T, Patch><<<job.ptr ? fixed : (job.val.np + 255) / 256, 256, 0, stream>>>(job, g.n, patch,
+                                                                                                 status);
+        note_launch();
+    }
     check(cudaGetLastError(), "decode launch");
     clock.mark("rpatch", stream);
 }
@@ -1141,7 +1162,8 @@ static void decompress(const uint8_t* d_in, size_t bytes, uint32_t nx, uint32_t 
     const uint16_t* irank = t_inv_tables.get(nx, ny, nz, g.bz, true, stream);
     check(cudaMemsetAsync(P.status, 0, 4, stream), "memset");
     FinalOut<T> fin{d_out, nx, size_t(nx) * ny, P.status};
-    decode_launch<T>(d_in, h, L, g, irank, P.C, P.bank1, P.bank2, fin, RowPatch<T>{d_out}, P.status, stream);
+    decode_launch<T>(JobRef{nullptr, decode_job(d_in, h, L)}, (h.flags & kMatrixFlag) != 0, g, irank, P.C, P.bank1,
+                     P.bank2, fin, RowPatch<T>{d_out}, P.status, stream);
     check(cudaMemcpyAsync(pin + 8, P.status, 4, cudaMemcpyDeviceToHost, stream), "readback");
     check(cudaStreamSynchronize(stream), "decompress");
     decode_finish<T>(uint32_t(pin[8]), d_in, h, L, g, P.status, P.seen, stream);
@@ -1182,6 +1204,7 @@ constexpr int kBatchStreams = 16;
 struct BatchTables {
     struct Entry {
         uint32_t nx, ny, nz, bz;
+        bool inverse;
         uint16_t* ptr;
     };
     int device = -1;
@@ -1189,7 +1212,7 @@ struct BatchTables {
     ~BatchTables() {
         for (auto& e : entries) cudaFree(e.ptr);
     }
-    const uint16_t* get(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t bz, cudaStream_t stream) {
+    const uint16_t* get(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t bz, bool inverse, cudaStream_t stream) {
         int dev = 0;
         check(cudaGetDevice(&dev), "cudaGetDevice");
         if (dev != device) {
@@ -1197,29 +1220,24 @@ struct BatchTables {
             device = dev;
         }
         for (auto& e : entries)
-            if (e.nx == nx && e.ny == ny && e.nz == nz && e.bz == bz) return e.ptr;
-        const auto host = morton_tables(nx, ny, nz, bz, false);
+            if (e.nx == nx && e.ny == ny && e.nz == nz && e.bz == bz && e.inverse == inverse) return e.ptr;
+        const auto host = morton_tables(nx, ny, nz, bz, inverse);
         uint16_t* p = nullptr;
         check(cudaMalloc(&p, host.size() * 2), "Waltz: cannot allocate Morton table");
         check(cudaMemcpyAsync(p, host.data(), host.size() * 2, cudaMemcpyHostToDevice, stream), "table upload");
         check(cudaStreamSynchronize(stream), "table upload");
-        entries.push_back({nx, ny, nz, bz, p});
+        entries.push_back({nx, ny, nz, bz, inverse, p});
         return p;
     }
 };
 
-struct BatchCompressState {
+// The capture stream, the parallel branches and their fork/join events.
+struct BatchStreams {
     int device = -1;
-    std::vector<unsigned char> key;
-    cudaGraphExec_t exec = nullptr;
     cudaStream_t cap = nullptr;
     cudaStream_t work[kBatchStreams] = {};
     cudaEvent_t fork = nullptr, join[kBatchStreams] = {};
-    Arena scratch;
-    uint64_t* host_results = nullptr;
-    size_t host_cap = 0;
-    BatchTables tables;
-    void ensure_streams() {
+    void ensure() {
         int dev = 0;
         check(cudaGetDevice(&dev), "cudaGetDevice");
         if (cap && dev == device) return;
@@ -1227,10 +1245,88 @@ struct BatchCompressState {
         for (auto& w : work) check(cudaStreamCreateWithFlags(&w, cudaStreamNonBlocking), "stream");
         check(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "event");
         for (auto& e : join) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
-        if (exec) exec = nullptr; // belonged to the previous device
-        key.clear();
         device = dev;
     }
+};
+static thread_local BatchStreams t_batch_streams;
+
+// One instantiated batch graph and the description it was captured for.
+struct CachedGraph {
+    int device = -1;
+    std::vector<unsigned char> key;
+    cudaGraphExec_t exec = nullptr;
+    bool valid(const std::vector<unsigned char>& k) const {
+        int dev = 0;
+        return exec && cudaGetDevice(&dev) == cudaSuccess && dev == device && k == key;
+    }
+};
+
+// Captures `body(work streams)` between a fork and a join on the capture
+// stream and replaces the cached graph with its instantiation.
+template <class Body>
+static void capture_batch(BatchStreams& bs, CachedGraph& cg, std::vector<unsigned char>&& key, Body body) {
+    StageClock& clock = stage_clock();
+    const bool profiling = clock.enabled;
+    clock.enabled = false;
+    cudaGraph_t graph = nullptr;
+    check(cudaStreamBeginCapture(bs.cap, cudaStreamCaptureModeThreadLocal), "begin capture");
+    try {
+        check(cudaEventRecord(bs.fork, bs.cap), "fork");
+        for (auto& w : bs.work) check(cudaStreamWaitEvent(w, bs.fork, 0), "fork wait");
+        body(bs.work);
+        for (int k = 0; k < kBatchStreams; ++k) {
+            check(cudaEventRecord(bs.join[k], bs.work[k]), "join");
+            check(cudaStreamWaitEvent(bs.cap, bs.join[k], 0), "join wait");
+        }
+    } catch (...) {
+        cudaStreamEndCapture(bs.cap, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        clock.enabled = profiling;
+        throw;
+    }
+    clock.enabled = profiling;
+    check(cudaStreamEndCapture(bs.cap, &graph), "end capture");
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    check(ie, "graph instantiate");
+    int dev = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (cg.exec && cg.device == dev) cudaGraphExecDestroy(cg.exec);
+    cg.exec = exec;
+    cg.device = dev;
+    cg.key = std::move(key);
+}
+
+// Pinned host staging that grows on demand.
+struct PinnedBuffer {
+    void* ptr = nullptr;
+    size_t cap = 0;
+    ~PinnedBuffer() {
+        if (ptr) cudaFreeHost(ptr);
+    }
+    template <class V> V* get(size_t count) {
+        if (cap < count * sizeof(V)) {
+            if (ptr) cudaFreeHost(ptr);
+            ptr = nullptr;
+            cap = 0;
+            check(cudaMallocHost(&ptr, count * sizeof(V)), "pinned staging");
+            cap = count * sizeof(V);
+        }
+        return static_cast<V*>(ptr);
+    }
+};
+
+template <class V> static void append_key(std::vector<unsigned char>& key, const V& v) {
+    const unsigned char* p = reinterpret_cast<const unsigned char*>(&v);
+    key.insert(key.end(), p, p + sizeof(V));
+}
+
+struct BatchCompressState {
+    CachedGraph graph;
+    Arena scratch;
+    PinnedBuffer results;
+    BatchTables tables;
 };
 static thread_local BatchCompressState t_bc;
 
@@ -1258,69 +1354,202 @@ static void compress_batch(const waltz_b200_chunk* items, uint32_t count, uint64
     total += size_t(count) * 9 * 8;
 
     BatchCompressState& st = t_bc;
-    st.ensure_streams();
+    BatchStreams& bs = t_batch_streams;
+    bs.ensure();
     std::vector<unsigned char> key(reinterpret_cast<const unsigned char*>(items),
                                    reinterpret_cast<const unsigned char*>(items + count));
     key.push_back(uint8_t(sizeof(T)));
     char* base = st.scratch.reserve(total);
-    {
-        // the scratch must not have moved since the graph was captured
-        const uintptr_t b = reinterpret_cast<uintptr_t>(base);
-        key.insert(key.end(), reinterpret_cast<const unsigned char*>(&b), reinterpret_cast<const unsigned char*>(&b) + 8);
-    }
+    append_key(key, base); // the scratch must not have moved since the graph was captured
     uint64_t* results = reinterpret_cast<uint64_t*>(base + results_at);
-    if (!st.exec || key != st.key) {
+    if (!st.graph.valid(key)) {
         std::vector<const uint16_t*> rank(count);
         for (uint32_t i = 0; i < count; ++i)
-            rank[i] = st.tables.get(jobs[i].nx, jobs[i].ny, jobs[i].nz, jobs[i].g.bz, st.cap);
-        StageClock& clock = stage_clock();
-        const bool profiling = clock.enabled;
-        clock.enabled = false;
-        cudaGraph_t graph = nullptr;
-        check(cudaStreamBeginCapture(st.cap, cudaStreamCaptureModeThreadLocal), "begin capture");
-        try {
-            check(cudaEventRecord(st.fork, st.cap), "fork");
-            for (auto& w : st.work) check(cudaStreamWaitEvent(w, st.fork, 0), "fork wait");
+            rank[i] = st.tables.get(jobs[i].nx, jobs[i].ny, jobs[i].nz, jobs[i].g.bz, false, bs.cap);
+        capture_batch(bs, st.graph, std::move(key), [&](cudaStream_t* work) {
             for (uint32_t i = 0; i < count; ++i) {
-                cudaStream_t w = st.work[i % kBatchStreams];
+                cudaStream_t w = work[i % kBatchStreams];
                 jobs[i].enqueue(base + offset[i], rank[i], w);
                 check(cudaMemcpyAsync(results + 9 * size_t(i), jobs[i].result(base + offset[i]), 9 * 8,
                                       cudaMemcpyDeviceToDevice, w), "result copy");
             }
-            for (int k = 0; k < kBatchStreams; ++k) {
-                check(cudaEventRecord(st.join[k], st.work[k]), "join");
-                check(cudaStreamWaitEvent(st.cap, st.join[k], 0), "join wait");
-            }
-        } catch (...) {
-            cudaStreamEndCapture(st.cap, &graph);
-            if (graph) cudaGraphDestroy(graph);
-            clock.enabled = profiling;
-            throw;
-        }
-        clock.enabled = profiling;
-        check(cudaStreamEndCapture(st.cap, &graph), "end capture");
-        cudaGraphExec_t exec = nullptr;
-        const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
-        cudaGraphDestroy(graph);
-        check(ie, "graph instantiate");
-        if (st.exec) cudaGraphExecDestroy(st.exec);
-        st.exec = exec;
-        st.key = std::move(key);
+        });
     }
-    check(cudaGraphLaunch(st.exec, stream), "graph launch");
-    if (st.host_cap < size_t(count) * 9) {
-        if (st.host_results) cudaFreeHost(st.host_results);
-        st.host_results = nullptr;
-        check(cudaMallocHost(&st.host_results, size_t(count) * 9 * 8), "pinned results");
-        st.host_cap = size_t(count) * 9;
-    }
-    check(cudaMemcpyAsync(st.host_results, results, size_t(count) * 9 * 8, cudaMemcpyDeviceToHost, stream), "readback");
+    check(cudaGraphLaunch(st.graph.exec, stream), "graph launch");
+    uint64_t* host = st.results.get<uint64_t>(size_t(count) * 9);
+    check(cudaMemcpyAsync(host, results, size_t(count) * 9 * 8, cudaMemcpyDeviceToHost, stream), "readback");
     check(cudaStreamSynchronize(stream), "batch compress");
     for (uint32_t i = 0; i < count; ++i) {
         try {
-            written[i] = jobs[i].finish(st.host_results + 9 * size_t(i));
+            written[i] = jobs[i].finish(host + 9 * size_t(i));
         } catch (const std::exception& e) {
             throw Error("batch item " + std::to_string(i) + ": " + e.what());
+        }
+    }
+}
+
+// ---------------------------------------------------------- batched decode
+// Many archives (uneven shapes, either form) decoded by one CUDA graph into
+// caller buffers, e.g. views of one preallocated tensor. Archive parameters
+// live in a device job table rewritten before every launch, so the graph is
+// captured once per (shapes, forms, output buffers) and replayed for every
+// later batch of other archives with that description — the data-loader
+// pattern, where a staging buffer and an output tensor are reused.
+__global__ void gather_headers_kernel(const uint8_t* const* archives, uint8_t* headers) {
+    headers[size_t(blockIdx.x) * 32 + threadIdx.x] = archives[blockIdx.x][threadIdx.x];
+}
+
+struct BatchDecodeState {
+    CachedGraph graph;
+    Arena scratch;
+    PinnedBuffer stage; // job table, then archive pointers / headers / status words
+    BatchTables tables;
+};
+static thread_local BatchDecodeState t_bd;
+
+template <class T>
+static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cudaStream_t stream) {
+    need(count > 0 && items, "invalid batch arguments");
+    struct Item {
+        Geometry g;
+        Header h;
+        Layout L;
+    };
+    std::vector<Item> list(count);
+    auto item_error = [](uint32_t i, const char* what) {
+        return Error("batch item " + std::to_string(i) + ": " + what);
+    };
+    uint64_t max_n = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        const waltz_b200_archive& a = items[i];
+        try {
+            need(a.nx && a.ny && a.nz, "Waltz: nonzero dimensions required");
+            const uint64_t n = uint64_t(a.nx) * a.ny * a.nz;
+            need(n <= 0xffffffffull / sizeof(T), "Waltz: volume exceeds the archive section limits");
+            need(a.archive && a.output, "Waltz: null buffer");
+            need(a.output_bytes >= n * sizeof(T), "output capacity too small");
+            need(a.bytes >= 32, "invalid Waltz archive header");
+            const uintptr_t p = reinterpret_cast<uintptr_t>(a.archive), q = reinterpret_cast<uintptr_t>(a.output);
+            need(!(p < q + n * sizeof(T) && q < p + a.bytes), "Waltz: input and output buffers overlap");
+            need(!(q % sizeof(T)), "Waltz: misaligned output");
+            list[i].g = Geometry::make(a.nx, a.ny, a.nz);
+            max_n = std::max(max_n, n);
+        } catch (const std::exception& e) {
+            throw item_error(i, e.what());
+        }
+    }
+    // Scratch: job table, status words, archive pointers, gathered headers,
+    // the duplicate-check bitmap, then C / bank1 / bank2 per branch, sized by
+    // the largest field on that branch.
+    uint64_t branch_n[kBatchStreams] = {};
+    for (uint32_t i = 0; i < count; ++i)
+        branch_n[i % kBatchStreams] = std::max<uint64_t>(branch_n[i % kBatchStreams], list[i].g.n);
+    Carver plan{nullptr};
+    auto carve = [&](Carver& c) {
+        struct P {
+            DecodeJob* jobs;
+            uint32_t* status;
+            const uint8_t** ptrs;
+            uint8_t* headers;
+            uint32_t* seen;
+            T *C[kBatchStreams], *b1[kBatchStreams], *b2[kBatchStreams];
+        } p;
+        p.jobs = c.take<DecodeJob>(count);
+        p.status = c.take<uint32_t>(count);
+        p.ptrs = c.take<const uint8_t*>(count);
+        p.headers = c.take<uint8_t>(size_t(count) * 32);
+        p.seen = c.take<uint32_t>((max_n + 31) / 32 + 1);
+        for (int k = 0; k < kBatchStreams; ++k) {
+            p.C[k] = c.take<T>(branch_n[k]);
+            p.b1[k] = c.take<T>(branch_n[k]);
+            p.b2[k] = c.take<T>(branch_n[k]);
+        }
+        return p;
+    };
+    carve(plan);
+    BatchDecodeState& st = t_bd;
+    BatchStreams& bs = t_batch_streams;
+    bs.ensure();
+    Carver real{st.scratch.reserve(plan.used)};
+    auto P = carve(real);
+    // Pinned words: job table (8 per archive), archive pointers (1), gathered
+    // headers (4), status words (1/2).
+    uint64_t* pin = st.stage.get<uint64_t>(size_t(count) * 14 + 1);
+    DecodeJob* jobs = reinterpret_cast<DecodeJob*>(pin);
+    uint64_t* ptrs = pin + size_t(count) * 8;
+    uint8_t* gathered = reinterpret_cast<uint8_t*>(pin + size_t(count) * 9);
+    uint32_t* status = reinterpret_cast<uint32_t*>(pin + size_t(count) * 13);
+
+    // Headers: from the caller's host copies, else gathered on the device.
+    std::vector<const uint8_t*> hdr(count, nullptr);
+    bool gather = false;
+    for (uint32_t i = 0; i < count; ++i) {
+        hdr[i] = static_cast<const uint8_t*>(items[i].header);
+        gather |= !hdr[i];
+    }
+    if (gather) {
+        for (uint32_t i = 0; i < count; ++i) ptrs[i] = reinterpret_cast<uint64_t>(items[i].archive);
+        check(cudaMemcpyAsync(P.ptrs, ptrs, size_t(count) * 8, cudaMemcpyHostToDevice, stream), "pointer upload");
+        gather_headers_kernel<<<count, 32, 0, stream>>>(P.ptrs, P.headers); note_launch();
+        check(cudaGetLastError(), "header gather");
+        check(cudaMemcpyAsync(gathered, P.headers, size_t(count) * 32, cudaMemcpyDeviceToHost, stream),
+              "header readback");
+        check(cudaStreamSynchronize(stream), "header readback");
+    }
+    for (uint32_t i = 0; i < count; ++i) {
+        Item& it = list[i];
+        it.h = Header::parse(hdr[i] ? hdr[i] : gathered + size_t(i) * 32);
+        try {
+            it.L = validate_header<T>(it.h, it.g, items[i].bytes, false);
+        } catch (const std::exception& e) {
+            throw item_error(i, e.what());
+        }
+    }
+    for (uint32_t i = 0; i < count; ++i)
+        jobs[i] = decode_job(static_cast<const uint8_t*>(items[i].archive), list[i].h, list[i].L);
+    check(cudaMemcpyAsync(P.jobs, jobs, size_t(count) * sizeof(DecodeJob), cudaMemcpyHostToDevice, stream),
+          "job table upload");
+    check(cudaMemsetAsync(P.status, 0, size_t(count) * 4, stream), "memset");
+
+    std::vector<unsigned char> key;
+    key.push_back(uint8_t(sizeof(T)));
+    append_key(key, count);
+    append_key(key, static_cast<const void*>(P.jobs));
+    for (uint32_t i = 0; i < count; ++i) {
+        append_key(key, items[i].nx);
+        append_key(key, items[i].ny);
+        append_key(key, items[i].nz);
+        append_key(key, items[i].output);
+        key.push_back(list[i].h.flags & kMatrixFlag);
+    }
+    if (!st.graph.valid(key)) {
+        std::vector<const uint16_t*> irank(count);
+        for (uint32_t i = 0; i < count; ++i) {
+            const Geometry& g = list[i].g;
+            irank[i] = st.tables.get(g.nx, g.ny, g.nz, g.bz, true, bs.cap);
+            if (list[i].h.flags & kMatrixFlag) t_zmat.get(g.nz, true, false, bs.cap); // upload before capture
+        }
+        capture_batch(bs, st.graph, std::move(key), [&](cudaStream_t* work) {
+            for (uint32_t i = 0; i < count; ++i) {
+                const int k = int(i % kBatchStreams);
+                const Geometry& g = list[i].g;
+                T* out = static_cast<T*>(items[i].output);
+                FinalOut<T> fin{out, g.nx, size_t(g.nx) * g.ny, P.status + i};
+                decode_launch<T>(JobRef{P.jobs + i, {}}, (list[i].h.flags & kMatrixFlag) != 0, g, irank[i], P.C[k],
+                                 P.b1[k], P.b2[k], fin, RowPatch<T>{out}, P.status + i, work[k]);
+            }
+        });
+    }
+    check(cudaGraphLaunch(st.graph.exec, stream), "graph launch");
+    check(cudaMemcpyAsync(status, P.status, size_t(count) * 4, cudaMemcpyDeviceToHost, stream), "readback");
+    check(cudaStreamSynchronize(stream), "batch decompress");
+    for (uint32_t i = 0; i < count; ++i) {
+        if (!status[i]) continue;
+        try {
+            decode_finish<T>(status[i], static_cast<const uint8_t*>(items[i].archive), list[i].h, list[i].L,
+                             list[i].g, P.status + i, P.seen, stream);
+        } catch (const std::exception& e) {
+            throw item_error(i, e.what());
         }
     }
 }
@@ -1393,6 +1622,18 @@ int waltz_b200_compress_batch(const waltz_b200_chunk* chunks, uint32_t count, in
         if (width == 4) compress_batch<float>(chunks, count, written, s);
         else compress_batch<double>(chunks, count, written, s);
         t_error[0] = 0;
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+int waltz_b200_decompress_batch(const waltz_b200_archive* archives, uint32_t count, int width, void* stream) {
+    using namespace wb;
+    try {
+        need(width == 4 || width == 8, "Waltz: width must be 4 or 8");
+        if (width == 4) decompress_batch<float>(archives, count, reinterpret_cast<cudaStream_t>(stream));
+        else decompress_batch<double>(archives, count, reinterpret_cast<cudaStream_t>(stream));
         return 0;
     } catch (const std::exception& e) {
         return fail(e);

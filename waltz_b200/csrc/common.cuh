@@ -245,4 +245,23 @@ __host__ __device__ inline size_t wzp_max_bytes(uint32_t n) {
     return wzp_header(n) + size_t(n) * 2 + (size_t(n) + 7) / 8;
 }
 
+// Where one archive's sections lie, as the host validated them from its
+// 32-byte header: base, WZP stream length, section offsets from the base,
+// quantum and side-record counts.
+struct DecodeJob {
+    const uint8_t* base;
+    uint64_t wzp, pi, pv, qi, qv;
+    double q;
+    uint32_t np, nq;
+};
+
+// A decode kernel's archive parameters: by value (one archive decoded by
+// direct launches), or in device memory (a captured decode graph replayed
+// over other archives of the same shapes, parameters rewritten each time).
+struct JobRef {
+    const DecodeJob* ptr;
+    DecodeJob val;
+    __device__ __forceinline__ DecodeJob get() const { return ptr ? *ptr : val; }
+};
+
 } // namespace wb

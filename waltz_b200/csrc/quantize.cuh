@@ -342,21 +342,24 @@ __global__ void layout_kernel(uint8_t* archive, size_t capacity, const uint64_t*
 // ------------------------------------------------------------ decode patches
 // Validates ascending/in-range indices (flags unordered lists for an exact
 // duplicate check) and patches q-outliers: coeff = +-T(v) * q with the sign of
-// the clamped value already in place.
+// the clamped value already in place. Grid-stride over the archive's count,
+// which a graph-replayed launch reads from device memory.
 template <class T>
-__global__ void qpatch_kernel(const uint8_t* qi, const uint8_t* qv, uint32_t nq, uint64_t n, T q, T* coeff,
-                              uint32_t* status) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nq) return;
-    uint32_t at, v, prev = 0;
-    memcpy(&at, qi + 4 * uint64_t(i), 4);
-    memcpy(&v, qv + 4 * uint64_t(i), 4);
-    if (i) memcpy(&prev, qi + 4 * uint64_t(i - 1), 4);
-    if (at >= n) { atomicOr(status, ST_BAD_INDEX); return; }
-    if (i && prev >= at) atomicOr(status, ST_UNORDERED);
-    if (v <= 65535u || v > 0x7fffffffu) { atomicOr(status, ST_BAD_QOUT); return; }
-    const T x = Lift<T>::mul(T(v), q);
-    coeff[at] = coeff[at] < T(0) ? -x : x;
+__global__ void qpatch_kernel(JobRef job, uint64_t n, T* coeff, uint32_t* status) {
+    const DecodeJob J = job.get();
+    const uint8_t *qi = J.base + J.qi, *qv = J.base + J.qv;
+    const T q = T(J.q);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < J.nq; i += gridDim.x * blockDim.x) {
+        uint32_t at, v, prev = 0;
+        memcpy(&at, qi + 4 * uint64_t(i), 4);
+        memcpy(&v, qv + 4 * uint64_t(i), 4);
+        if (i) memcpy(&prev, qi + 4 * uint64_t(i - 1), 4);
+        if (at >= n) { atomicOr(status, ST_BAD_INDEX); continue; }
+        if (i && prev >= at) atomicOr(status, ST_UNORDERED);
+        if (v <= 65535u || v > 0x7fffffffu) { atomicOr(status, ST_BAD_QOUT); continue; }
+        const T x = Lift<T>::mul(T(v), q);
+        coeff[at] = coeff[at] < T(0) ? -x : x;
+    }
 }
 
 // Repair patch targets: a row-major output, or a tile clipped into a frame.
@@ -367,23 +370,24 @@ template <class T> struct RowPatch {
 
 // Repair records: validate, then out[i] -= err (after synthesis).
 template <class T, class Patch>
-__global__ void rpatch_kernel(const uint8_t* pi, const uint8_t* pv, uint32_t np, uint64_t n, Patch patch,
-                              uint32_t* status) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= np) return;
-    uint32_t at, prev = 0;
-    T err;
-    memcpy(&at, pi + 4 * uint64_t(i), 4);
-    memcpy(&err, pv + sizeof(T) * uint64_t(i), sizeof(T));
-    if (i) memcpy(&prev, pi + 4 * uint64_t(i - 1), 4);
-    if (at >= n) { atomicOr(status, ST_BAD_INDEX); return; }
-    if (i && prev >= at) atomicOr(status, ST_UNORDERED);
-    if (!finite_bits(err)) { atomicOr(status, ST_BAD_REPAIR); return; }
-    T* p = patch.at(at);
-    if (!p) return;
-    const T r = Lift<T>::sub(*p, err);
-    *p = r;
-    if (!finite_bits(r)) atomicOr(status, ST_NONFINITE_INPUT);
+__global__ void rpatch_kernel(JobRef job, uint64_t n, Patch patch, uint32_t* status) {
+    const DecodeJob J = job.get();
+    const uint8_t *pi = J.base + J.pi, *pv = J.base + J.pv;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < J.np; i += gridDim.x * blockDim.x) {
+        uint32_t at, prev = 0;
+        T err;
+        memcpy(&at, pi + 4 * uint64_t(i), 4);
+        memcpy(&err, pv + sizeof(T) * uint64_t(i), sizeof(T));
+        if (i) memcpy(&prev, pi + 4 * uint64_t(i - 1), 4);
+        if (at >= n) { atomicOr(status, ST_BAD_INDEX); continue; }
+        if (i && prev >= at) atomicOr(status, ST_UNORDERED);
+        if (!finite_bits(err)) { atomicOr(status, ST_BAD_REPAIR); continue; }
+        T* p = patch.at(at);
+        if (!p) continue;
+        const T r = Lift<T>::sub(*p, err);
+        *p = r;
+        if (!finite_bits(r)) atomicOr(status, ST_NONFINITE_INPUT);
+    }
 }
 
 // Exact duplicate test of an unordered index list (test-and-set bitmap).

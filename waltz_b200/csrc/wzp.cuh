@@ -523,11 +523,9 @@ __device__ __forceinline__ uint32_t stage_bytes(uint8_t* dst, const uint8_t* src
 }
 
 template <class T> struct WzpDecodeArgs {
-    const uint8_t* in;  // start of the WZP stream
-    size_t bytes;       // stream length (header + payload)
+    JobRef job;         // archive base, WZP stream length, quantum
     uint32_t n;
     BrickMap map;
-    T q;
     T* coeff;           // row-major dequantised coefficients (output)
     uint32_t* status;
 };
@@ -542,9 +540,12 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_decode_kernel(WzpDecodeArgs<T
     const uint32_t c = blockIdx.x;
     const uint32_t first = c * kChunk, count = min(kChunk, A.n - first);
     const size_t header = size_t(groups) * 4 + size_t(chunks) * 3;
-    const uint8_t* meta = A.in + size_t(groups) * 4;
-    const uint8_t* payload = A.in + header;
-    const size_t payload_bytes = A.bytes - header;
+    const DecodeJob J = A.job.get();
+    const uint8_t* in = J.base + 32;
+    const T q = T(J.q);
+    const uint8_t* meta = in + size_t(groups) * 4;
+    const uint8_t* payload = in + header;
+    const size_t payload_bytes = J.wzp - header;
 
     if (warp == 0) {
         // Lane k reads the metadata of the group's chunk k; the chunk's payload
@@ -560,7 +561,7 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_decode_kernel(WzpDecodeArgs<T
         const uint32_t sb = __shfl_sync(0xffffffffu, ci.sbytes, me);
         const bool raw = __shfl_sync(0xffffffffu, ci.raw ? 1u : 0u, me) != 0;
         if (lane == 0) {
-            const uint64_t off = uint64_t(load_u32(A.in + size_t(g) * 4)) + before;
+            const uint64_t off = uint64_t(load_u32(in + size_t(g) * 4)) + before;
             const bool ok = ok_all && off + mb + sb <= payload_bytes;
             S.off = uint32_t(off);
             S.mbytes = mb;
@@ -768,7 +769,7 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_decode_kernel(WzpDecodeArgs<T
             if (rank < 8 * sbytes) neg = (sgn[rank >> 3] >> (rank & 7)) & 1u;
         }
         if (uint32_t(e) < count) {
-            const T mag = Lift<T>::mul(T(v), A.q);
+            const T mag = Lift<T>::mul(T(v), q);
             const uint32_t at = A.map.fast ? A.map.in_full_brick(S.bbase[uint32_t(e) >> A.map.lb],
                                                                  uint32_t(e) & ((1u << A.map.lb) - 1u))
                                            : A.map.rowmajor(first + uint32_t(e));

@@ -48,7 +48,7 @@ def power_law_field(shape, seed, slope=-11.0 / 3.0, dtype=np.float32):
     rng = np.random.Generator(np.random.PCG64(seed))
     white = rng.standard_normal(shape)
     spec = np.fft.rfftn(white) * _spectral_amplitude(shape, slope)
-    field = np.fft.irfftn(spec, s=shape)
+    field = np.fft.irfftn(spec, s=shape, axes=tuple(range(len(shape))))
     field -= field.mean()
     field /= field.std()
     return field.astype(dtype)
