@@ -263,6 +263,9 @@ def gpu_arm(args, rank, world, local_rank):
         del field, out, archive, host_in, host_arch, host_out
         torch.cuda.empty_cache()
         result["tc_form"] = tc_form_comparison(dev, lib, args.steps, tuple(args.tc_shape))
+    if not args.no_batch and world == 1:
+        torch.cuda.empty_cache()
+        result["batched_form"] = batch_comparison(dev, lib, args.steps)
     return result
 
 
@@ -345,6 +348,119 @@ def tc_form_comparison(dev, lib, steps, shape=(64, 1024, 1024)):
                                                 "max_rel_to_column_max": float((diff.max(0).values /
                                                                                 ref.abs().max(0).values.clamp_min(1e-30)).max()),
                                                 "columns": cols}
+    return report
+
+
+def batch_comparison(dev, lib, steps, count=512):
+    """Batched form against one call per chunk on the uneven-chunk workload:
+    512 float32 chunks, per-axis sides drawn from {32,48,64,96,128} (seed 4),
+    k^-11/3 fields each rescaled to a range drawn log-uniformly in [1e-2,1e3],
+    REL 1e-3 per chunk. Batched: waltz_b200_compress_batch (one graph) and
+    waltz_b200_decompress_batch into one preallocated tensor (one graph,
+    archives read from one staging buffer). Per-chunk: waltz_b200_compress /
+    waltz_b200_decompress once per chunk. Device-resident; CUDA events per
+    batch; latency percentiles over the timed batches after warm-up (the
+    first batched call captures the graphs)."""
+    import torch
+    import waltz_b200
+    from waltz_b200 import _lib
+    from waltz_b200.synthetic import uneven_chunks_device
+    fields = uneven_chunks_device(count, 4, device=dev)
+    sp = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    sizes = [f.numel() for f in fields]
+    nbytes = 4 * sum(sizes)
+    bounds = []
+    for f in fields:
+        lo, hi = waltz_b200.extrema(f)
+        bounds.append(REL * (hi - lo))
+    caps = [waltz_b200.compressed_capacity(k, 4) for k in sizes]
+    offs = [0]
+    for c in caps:
+        offs.append(offs[-1] + (c + 255) // 256 * 256)
+    arch = torch.empty(offs[-1], dtype=torch.uint8, device=dev)
+    items = (_lib.Chunk * count)()
+    for i, f in enumerate(fields):
+        nz, ny, nx = f.shape
+        items[i] = _lib.Chunk(f.data_ptr(), nx, ny, nz, bounds[i], arch.data_ptr() + offs[i], caps[i])
+    written = (C.c_uint64 * count)()
+    out = torch.empty(sum(sizes), dtype=torch.float32, device=dev)
+    outs, at = [], 0
+    for k in sizes:
+        outs.append(out[at:at + k])
+        at += k
+
+    def comp_batch():
+        _lib.checked(lib.waltz_b200_compress_batch(items, count, 4, written, sp))
+
+    dec_items = (_lib.Archive * count)()
+
+    def dec_batch():
+        _lib.checked(lib.waltz_b200_decompress_batch(dec_items, count, 4, sp))
+
+    one = C.c_size_t()
+
+    def comp_each():
+        for i, f in enumerate(fields):
+            nz, ny, nx = f.shape
+            _lib.checked(lib.waltz_b200_compress(C.c_void_p(f.data_ptr()), 4, nx, ny, nz, bounds[i],
+                                                 C.c_void_p(arch.data_ptr() + offs[i]), caps[i], C.byref(one), sp))
+
+    def dec_each():
+        for i, f in enumerate(fields):
+            nz, ny, nx = f.shape
+            _lib.checked(lib.waltz_b200_decompress(C.c_void_p(arch.data_ptr() + offs[i]), written[i], 4, nx, ny, nz,
+                                                   C.c_void_p(outs[i].data_ptr()), 4 * sizes[i], sp))
+
+    def timed(fn, reps):
+        ms = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return ms
+
+    comp_batch()
+    first = [bytes(arch[offs[i]:offs[i] + written[i]].cpu().numpy()) for i in range(0, count, 37)]
+    for i, f in enumerate(fields):
+        nz, ny, nx = f.shape
+        dec_items[i] = _lib.Archive(arch.data_ptr() + offs[i], written[i], None, nx, ny, nz, outs[i].data_ptr(),
+                                    4 * sizes[i])
+    dec_batch()
+    worst = max(float((o.view(f.shape).double() - f.double()).abs().max()) / eb
+                for o, f, eb in zip(outs, fields, bounds))
+    assert worst <= 1.0, f"bound violated in the batch: {worst}"
+    archive_bytes = sum(written)
+    reps = max(steps, 20)
+    for _ in range(3):
+        comp_batch()
+        dec_batch()
+    cb = timed(comp_batch, reps)
+    db = timed(dec_batch, reps)
+    ce = timed(comp_each, max(3, steps // 4))
+    de = timed(dec_each, max(3, steps // 4))
+    # per-chunk archives equal the batched ones
+    for j, i in enumerate(range(0, count, 37)):
+        assert bytes(arch[offs[i]:offs[i] + written[i]].cpu().numpy()) == first[j], "batched archive differs"
+
+    def stats(ms):
+        ms = sorted(ms)
+        med = statistics.median(ms)
+        return {"chunks_per_s": round(count / (med / 1e3), 1), "gbs": round(nbytes / (med / 1e3) / 1e9, 3),
+                "p50_ms": round(med, 4), "p99_ms": round(ms[min(len(ms) - 1, int(0.99 * len(ms)))], 4),
+                "batches": len(ms)}
+    report = {
+        "workload": f"{count} f32 chunks, sides per axis from {{32,48,64,96,128}} (seed 4), k^-11/3 fields, "
+                    "ranges log-uniform in [1e-2,1e3], REL 1e-3 per chunk",
+        "samples": sum(sizes), "bytes": nbytes, "archive_bytes": archive_bytes,
+        "compression_ratio": round(nbytes / archive_bytes, 4), "max_err_over_bound": round(worst, 6),
+        "compress": {"batched": stats(cb), "per_chunk": stats(ce)},
+        "decompress": {"batched": stats(db), "per_chunk": stats(de)},
+    }
+    for k in ("compress", "decompress"):
+        report[k]["speedup"] = round(report[k]["batched"]["gbs"] / report[k]["per_chunk"]["gbs"], 3)
     return report
 
 
@@ -472,6 +588,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tc-form", action="store_true", help="skip the plain vs tensor-core form comparison")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched vs per-chunk comparison")
     ap.add_argument("--tc-shape", type=int, nargs=3, default=[64, 1024, 1024], metavar=("NZ", "NY", "NX"),
                     help="field of the tensor-core comparison (z y x); smaller shapes serve profiler captures")
     ap.add_argument("--shape", type=int, nargs=3, default=list(SHAPE), metavar=("NZ", "NY", "NX"),

@@ -110,6 +110,22 @@ def uneven_chunks(count=512, seed=4, sides=(32, 48, 64, 96, 128), dtype=np.float
     return out
 
 
+def uneven_chunks_device(count=512, seed=4, sides=(32, 48, 64, 96, 128), device="cuda"):
+    """uneven_chunks built with torch on a GPU: the same shape and value-range
+    draws (numpy PCG64 stream of `seed`), device-generated k^-11/3 fields.
+    Returns float32 CUDA tensors."""
+    import torch
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for i in range(count):
+        shape = tuple(int(s) for s in rng.choice(sides, 3))
+        f = power_law_field_device(shape, seed * 100003 + i, dtype=torch.float64, device=device)
+        span = 10 ** rng.uniform(-2, 3)
+        lo, hi = f.min(), f.max()
+        out.append(((f - lo) / (hi - lo) * span).to(torch.float32).contiguous())
+    return out
+
+
 def rel_to_abs(field, rel: float) -> float:
     """REL bound -> absolute bound: rel * (max - min) evaluated in double."""
     lo = float(field.min())
