@@ -66,12 +66,13 @@ int waltz_b200_compress_batch(const waltz_b200_chunk* chunks, uint32_t count, in
                               void* stream);
 
 /* Batched decode of many archives of any shapes and either form into caller
- * buffers (e.g. views of one preallocated tensor): one call, one CUDA graph.
- * Archive locations and headers are passed to the graph through a device
- * table, so the graph is captured once per description (count, shapes, forms,
- * outputs) and replayed for later batches of other archives with the same
- * description. `header` optionally points to a host copy of an archive's
- * first 32 bytes (NULL: read from the device). Every output equals
+ * buffers (views of one preallocated tensor, or boxes inside a larger frame
+ * through the output strides): one call, one CUDA graph. Archive and output
+ * addresses and headers reach the graph through a device table, so the graph
+ * is captured once per description (count, shapes, forms, output strides)
+ * and replayed for later batches of other archives and other outputs with
+ * the same description. `header` optionally points to a host copy of an
+ * archive's first 32 bytes (NULL: read from the device). Every output equals
  * waltz_b200_decompress of that archive. Fails (naming the item) if any item
  * fails. New surface: the reference batch decoder needs one tile shape for
  * the whole batch (waltz_gpu_decode_batch, src/batch_decode.cuh:74-186). */
@@ -80,10 +81,18 @@ typedef struct waltz_b200_archive {
     uint64_t bytes;
     const void* header;   /* optional host copy of the 32-byte header */
     uint32_t nx, ny, nz;
-    void* output;         /* device, nx*ny*nz samples of `width` bytes */
-    uint64_t output_bytes;
+    void* output;         /* device; sample (x,y,z) at output[z*stride_z + y*stride_y + x] */
+    uint64_t output_bytes;/* bytes from `output` to the end of the chunk's box */
+    uint64_t stride_y;    /* elements between rows; 0 = nx */
+    uint64_t stride_z;    /* elements between planes; 0 = stride_y*ny */
 } waltz_b200_archive;
 int waltz_b200_decompress_batch(const waltz_b200_archive* archives, uint32_t count, int width, void* stream);
+
+/* Parallel branches (1..64, default 16) of the batch graphs that the calling
+ * thread captures next: chunk i runs on branch i mod branches. Returns the
+ * previous value; out-of-range values only query it. Performance knob only:
+ * results do not depend on it. */
+int waltz_b200_batch_branches(int branches);
 
 /* Decode an archive of `bytes` bytes into nx*ny*nz samples (the archive does
  * not store its dimensions); either form. */
@@ -142,6 +151,8 @@ int waltz_b200_test_lookback_timeout(const void* d_input, int width, uint32_t nx
  * returns how many stages were timed (the reference's per-stage GPUTimer
  * report, include/utils/Timer.hpp:5-63). */
 unsigned long long waltz_b200_launch_count(void);
+/* Batch graphs captured since load (replays do not count). */
+unsigned long long waltz_b200_graph_count(void);
 void waltz_b200_profile(int enable);
 int waltz_b200_stage_times(double* ms, const char** names, int cap);
 

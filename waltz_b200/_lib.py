@@ -26,6 +26,7 @@ SIGNATURES = {
     "waltz_b200_compress_form": (C.c_int, [C.c_void_p, C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_double,
                                            C.c_int, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t), C.c_void_p]),
     "waltz_b200_compress_batch": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int, C.POINTER(C.c_uint64), C.c_void_p]),
+    "waltz_b200_batch_branches": (C.c_int, [C.c_int]),
     "waltz_b200_decompress_batch": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int, C.c_void_p]),
     "waltz_b200_decompress": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_uint32, C.c_uint32, C.c_uint32,
                                         C.c_void_p, C.c_size_t, C.c_void_p]),
@@ -43,6 +44,7 @@ SIGNATURES = {
                                                    C.c_double, C.c_void_p, C.c_size_t, C.c_uint32, C.c_uint32,
                                                    C.c_void_p]),
     "waltz_b200_launch_count": (C.c_ulonglong, []),
+    "waltz_b200_graph_count": (C.c_ulonglong, []),
     "waltz_b200_profile": (None, [C.c_int]),
     "waltz_b200_stage_times": (C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_char_p), C.c_int]),
     "waltz_cuda_decode_chunk": (C.c_char_p, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_void_p,
@@ -62,7 +64,8 @@ class Chunk(C.Structure):
 class Archive(C.Structure):
     """waltz_b200_archive (include/waltz_b200.h)."""
     _fields_ = [("archive", C.c_void_p), ("bytes", C.c_uint64), ("header", C.c_void_p), ("nx", C.c_uint32),
-                ("ny", C.c_uint32), ("nz", C.c_uint32), ("output", C.c_void_p), ("output_bytes", C.c_uint64)]
+                ("ny", C.c_uint32), ("nz", C.c_uint32), ("output", C.c_void_p), ("output_bytes", C.c_uint64),
+                ("stride_y", C.c_uint64), ("stride_z", C.c_uint64)]
 
 
 class WaltzError(RuntimeError):

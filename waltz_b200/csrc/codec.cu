@@ -12,6 +12,7 @@
 #include "common.cuh"
 #include "inverse.cuh"
 #include "quantize.cuh"
+#include "stage.cuh"
 #include "stream.cuh"
 #include "transform.cuh"
 #include "wzp.cuh"
@@ -347,6 +348,86 @@ static unsigned grid_for(uint64_t n, unsigned threads = 256) {
     return unsigned(std::min<uint64_t>(std::max<uint64_t>(b, 1), 148ull * 64));
 }
 
+// ------------------------------------------------ whole-stage plane kernels
+static StageLevels z_levels(const Geometry& g) {
+    StageLevels lv{};
+    lv.count = g.lz;
+    for (unsigned l = 0; l < g.lz; ++l) lv.z[l] = g.zl[l].z;
+    return lv;
+}
+static StageLevels xy_levels(const Geometry& g) {
+    StageLevels lv{};
+    lv.count = g.lxy;
+    for (unsigned l = 0; l < g.lxy; ++l) {
+        lv.x[l] = g.xyl[l].x;
+        lv.y[l] = g.xyl[l].y;
+    }
+    return lv;
+}
+template <class T> static bool zstage_ok(const Geometry& g) { return g.lz && zstage_smem<T>(g.nz) <= kStageSmemCap; }
+template <class T> static bool xystage_ok(const Geometry& g) {
+    return g.lxy && xystage_smem<T>(g.nx, g.ny) <= kStageSmemCap;
+}
+
+// Opts a kernel into the stage kernels' shared-memory size once per device.
+template <class K> static void stage_smem_attr(K kernel, int& configured) {
+    int dev = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (configured != dev) {
+        check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kStageSmemCap)),
+              "stage kernel shared memory");
+        configured = dev;
+    }
+}
+
+static unsigned zstage_grid(const Geometry& g, int cx, int cy) {
+    return unsigned(((g.nx + cx - 1) / cx) * uint64_t((g.ny + cy - 1) / cy));
+}
+
+template <class T>
+static void zstage_forward(const T* in, size_t sy, size_t sz, const Geometry& g, T* dst, uint32_t* status,
+                           cudaStream_t stream) {
+    static thread_local int configured = -1;
+    stage_smem_attr(zstage_fwd_kernel<T>, configured);
+    zstage_fwd_kernel<T><<<zstage_grid(g, ZCols<T>::CX, ZCols<T>::CY), kZStageThreads, zstage_smem<T>(g.nz),
+                           stream>>>(in, sy, sz, g.nx, g.ny, g.nz, z_levels(g), dst, status);
+    note_launch();
+    check(cudaGetLastError(), "z stage launch");
+}
+
+template <class T, class Out>
+static void zstage_inverse(const T* coef, size_t sy, size_t sz, const Geometry& g, const Out& out,
+                           cudaStream_t stream) {
+    static thread_local int configured = -1;
+    stage_smem_attr(zstage_inv_kernel<T, Out>, configured);
+    zstage_inv_kernel<T, Out><<<zstage_grid(g, ZCols<T>::CX, ZCols<T>::CY), kZStageThreads, zstage_smem<T>(g.nz),
+                                stream>>>(coef, sy, sz, g.nx, g.ny, g.nz, z_levels(g), out);
+    note_launch();
+    check(cudaGetLastError(), "z stage launch");
+}
+
+template <class T>
+static void xystage_forward(const T* in, size_t sy, size_t sz, const Geometry& g, T* dst, size_t dsy, size_t dsz,
+                            uint32_t* status, cudaStream_t stream) {
+    static thread_local int configured = -1;
+    stage_smem_attr(xystage_fwd_kernel<T>, configured);
+    xystage_fwd_kernel<T><<<g.nz, kXYStageThreads, xystage_smem<T>(g.nx, g.ny), stream>>>(
+        in, sy, sz, g.nx, g.ny, xy_levels(g), dst, dsy, dsz, status);
+    note_launch();
+    check(cudaGetLastError(), "xy stage launch");
+}
+
+template <class T, class Out>
+static void xystage_inverse(const T* coef, size_t sy, size_t sz, const Geometry& g, const Out& out,
+                            cudaStream_t stream) {
+    static thread_local int configured = -1;
+    stage_smem_attr(xystage_inv_kernel<T, Out>, configured);
+    xystage_inv_kernel<T, Out><<<g.nz, kXYStageThreads, xystage_smem<T>(g.nx, g.ny), stream>>>(
+        coef, sy, sz, g.nx, g.ny, xy_levels(g), out);
+    note_launch();
+    check(cudaGetLastError(), "xy stage launch");
+}
+
 // Scratch element counts for the forward and inverse transforms.
 struct TransformScratch {
     uint64_t low;   // each of two compact ping-pong buffers
@@ -406,7 +487,9 @@ static void forward(const Geometry& g, const T* in, T* C, T* lowA, T* lowB, T* i
             clock.mark("fwd_z_matrix", stream);
         }
     }
-    for (unsigned l = 0; l < (matrix ? 0u : g.lz); ++l) {
+    const bool zstage = !matrix && zstage_ok<T>(g);
+    if (zstage) zstage_forward<T>(in, sy, sz, g, zdst, status, stream);
+    for (unsigned l = 0; l < (matrix || zstage ? 0u : g.lz); ++l) {
         const Dims a = g.zl[l], lo = halve(a, AZ);
         const bool last = l + 1 == g.lz;
         FwdOut<T> out{zdst, sy, sz, last ? nullptr : lows[l & 1], lo, a, AZ};
@@ -415,6 +498,11 @@ static void forward(const Geometry& g, const T* in, T* C, T* lowA, T* lowB, T* i
     }
     if (g.lz) clock.mark("fwd_z", stream);
     if (g.lz) src = FwdSrc<T>{inter, sy, sz};
+    if (xystage_ok<T>(g)) {
+        xystage_forward<T>(src.p, sy, sz, g, C, sy, sz, g.lz ? nullptr : status, stream);
+        clock.mark("fwd_xy", stream);
+        return;
+    }
     for (unsigned l = 0; l < g.lxy; ++l) {
         const Dims a = g.xyl[l], lo = halve(a, AX | AY);
         const bool last = l + 1 == g.lxy;
@@ -475,7 +563,16 @@ static void inverse(const Geometry& g, T* C, T* bank1, T* bank2, const Final& fi
     }
     const T* zbase = C;
     T* zping[2] = {bank2, bank1};
-    if (g.lxy) {
+    if (xystage_ok<T>(g)) {
+        if (g.lz) {
+            xystage_inverse<T>(C, sy, sz, g, StoreOut<T>{bank1, sy, sz}, stream);
+            zbase = bank1;
+            zping[1] = C;
+        } else {
+            xystage_inverse<T>(C, sy, sz, g, fin, stream);
+        }
+        clock.mark("inv_xy", stream);
+    } else if (g.lxy) {
         const T* low = nullptr;
         for (int l = int(g.lxy) - 1; l >= 0; --l) {
             const Dims a = g.xyl[l];
@@ -501,7 +598,10 @@ static void inverse(const Geometry& g, T* C, T* bank1, T* bank2, const Final& fi
             return;
         }
     }
-    if (g.lz) {
+    if (zstage_ok<T>(g)) {
+        zstage_inverse<T>(zbase, sy, sz, g, fin, stream);
+        clock.mark("inv_z", stream);
+    } else if (g.lz) {
         const T* low = nullptr;
         for (int l = int(g.lz) - 1; l >= 0; --l) {
             const Dims a = g.zl[l];
@@ -734,7 +834,7 @@ template <class T> struct CompressJob {
     struct Plan {
         T *C, *lowA, *lowB, *inter, *bank2, *perr;
         uint16_t* mag;
-        uint32_t *sign, *qbits, *qval, *pbits, *status, *ticket, *counts_p, *counts_q, *np, *nq;
+        uint32_t *sign, *qbits, *qval, *pbits, *status, *ticket, *counts_p, *counts_q;
         uint64_t *state, *sizes, *wzp_total, *layout; // layout[8] = status copy
     };
 
@@ -772,17 +872,16 @@ template <class T> struct CompressJob {
         p.bank2 = c.take<T>(n);
         p.perr = c.take<T>(n);
         p.mag = c.take<uint16_t>(n + 8);
+        p.qval = c.take<uint32_t>(n);
+        // zero-initialised block (one memset): bitmaps, status, ticket, lookback states
         p.sign = c.take<uint32_t>(words + 1);
         p.qbits = c.take<uint32_t>(words + 1);
-        p.qval = c.take<uint32_t>(n);
         p.pbits = c.take<uint32_t>(words + 1);
         p.status = c.take<uint32_t>(1);
         p.ticket = c.take<uint32_t>(1);
+        p.state = c.take<uint64_t>(chunks);
         p.counts_p = c.take<uint32_t>(cblocks);
         p.counts_q = c.take<uint32_t>(cblocks);
-        p.np = c.take<uint32_t>(1);
-        p.nq = c.take<uint32_t>(1);
-        p.state = c.take<uint64_t>(chunks);
         p.sizes = c.take<uint64_t>(chunks);
         p.wzp_total = c.take<uint64_t>(1);
         p.layout = c.take<uint64_t>(9);
@@ -802,12 +901,8 @@ template <class T> struct CompressJob {
         const T q = T(quantum), inv = T(1.0 / quantum);
         const uint32_t chunks = wzp_chunks(uint32_t(n));
         const uint64_t words = (n + 31) / 32, cblocks = (words + kCompactWords - 1) / kCompactWords;
-        check(cudaMemsetAsync(P.sign, 0, (words + 1) * 4, stream), "memset");
-        check(cudaMemsetAsync(P.qbits, 0, (words + 1) * 4, stream), "memset");
-        check(cudaMemsetAsync(P.pbits, 0, (words + 1) * 4, stream), "memset");
-        check(cudaMemsetAsync(P.status, 0, 4, stream), "memset");
-        check(cudaMemsetAsync(P.ticket, 0, 4, stream), "memset");
-        check(cudaMemsetAsync(P.state, 0, size_t(chunks) * 8, stream), "memset");
+        check(cudaMemsetAsync(P.sign, 0, reinterpret_cast<char*>(P.state + chunks) - reinterpret_cast<char*>(P.sign),
+                              stream), "memset");
 
         StageClock& clock = stage_clock();
         clock.begin(stream);
@@ -854,19 +949,18 @@ template <class T> struct CompressJob {
             inverse<T>(g, P.C, P.inter, P.bank2, fin, P.status, stream, "inv_l0_repair", opt.matrix);
         }
         // 5. ordered side records
-        compact_count_kernel<<<unsigned(cblocks), kCompactThreads, 0, stream>>>(P.pbits, words, P.counts_p); note_launch();
-        compact_count_kernel<<<unsigned(cblocks), kCompactThreads, 0, stream>>>(P.qbits, words, P.counts_q); note_launch();
-        compact_scan_kernel<<<1, kCompactThreads, 0, stream>>>(P.counts_p, uint32_t(cblocks), P.np); note_launch();
-        compact_scan_kernel<<<1, kCompactThreads, 0, stream>>>(P.counts_q, uint32_t(cblocks), P.nq); note_launch();
-        layout_kernel<<<1, 32, 0, stream>>>(out, capacity, P.wzp_total, P.np, P.nq, sizeof(T),
-                                            uint8_t(g.flags(sizeof(T)) | (opt.matrix ? kMatrixFlag : 0)),
-                                            uint8_t(g.lxy), uint8_t(g.lz), uint8_t(g.bz), quantum, P.layout); note_launch();
-        compact_write_kernel<T><<<unsigned(cblocks), kCompactThreads, 0, stream>>>(P.pbits, words, P.counts_p, P.perr,
-                                                                                   out, P.layout, 0, 1, n); note_launch();
-        compact_write_kernel<uint32_t><<<unsigned(cblocks), kCompactThreads, 0, stream>>>(P.qbits, words, P.counts_q,
-                                                                                          P.qval, out, P.layout, 2, 3, n); note_launch();
+        const dim3 both(unsigned(cblocks), 2);
+        compact_count_kernel<<<both, kCompactThreads, 0, stream>>>(P.pbits, P.qbits, words, P.counts_p, P.counts_q);
+        note_launch();
+        compact_scan_layout_kernel<<<1, kCompactThreads, 0, stream>>>(
+            P.counts_p, P.counts_q, uint32_t(cblocks), P.wzp_total, P.status, out, capacity, sizeof(T),
+            uint8_t(g.flags(sizeof(T)) | (opt.matrix ? kMatrixFlag : 0)), uint8_t(g.lxy), uint8_t(g.lz),
+            uint8_t(g.bz), quantum, P.layout);
+        note_launch();
+        compact_write_kernel<T><<<both, kCompactThreads, 0, stream>>>(P.pbits, P.qbits, words, P.counts_p, P.counts_q,
+                                                                      P.perr, P.qval, out, P.layout, n);
+        note_launch();
         check(cudaGetLastError(), "side record launch");
-        check(cudaMemcpyAsync(P.layout + 8, P.status, 4, cudaMemcpyDeviceToDevice, stream), "status copy");
         clock.mark("side_records", stream);
     }
 
@@ -1029,8 +1123,8 @@ static void host_directory_check(const uint8_t* in, uint32_t n, uint64_t payload
     need(cursor == payload, "WZP trailing or missing payload bytes");
 }
 
-static DecodeJob decode_job(const uint8_t* d_in, const Header& h, const Layout& L) {
-    return DecodeJob{d_in, h.wzp, L.pi, L.pv, L.qi, L.qv, h.q, h.np, h.nq};
+static DecodeJob decode_job(const uint8_t* d_in, const Header& h, const Layout& L, void* out = nullptr) {
+    return DecodeJob{d_in, h.wzp, L.pi, L.pv, L.qi, L.qv, h.q, h.np, h.nq, out};
 }
 
 // Decoder kernels of one archive, launched without synchronising. Scratch:
@@ -1194,12 +1288,13 @@ static void extrema(const T* d_in, uint64_t n, double* mn, double* mx, cudaStrea
 
 // ------------------------------------------------------------ batched compress
 // Many independent fields (uneven shapes) compressed by one CUDA graph: each
-// field's kernel chain is captured on one of kBatchStreams parallel branches,
+// field's kernel chain is captured on one of several parallel branches,
 // so fields run concurrently and one graph launch replaces thousands of
 // kernel launches. The instantiated graph is kept and replayed while the
 // batch description (pointers, shapes, bounds) stays the same; all results
 // come back in one copy.
-constexpr int kBatchStreams = 16;
+constexpr int kMaxBranches = 64;
+static thread_local int t_branches = 16; // parallel branches of the next captured batch graph
 
 struct BatchTables {
     struct Entry {
@@ -1235,8 +1330,8 @@ struct BatchTables {
 struct BatchStreams {
     int device = -1;
     cudaStream_t cap = nullptr;
-    cudaStream_t work[kBatchStreams] = {};
-    cudaEvent_t fork = nullptr, join[kBatchStreams] = {};
+    cudaStream_t work[kMaxBranches] = {};
+    cudaEvent_t fork = nullptr, join[kMaxBranches] = {};
     void ensure() {
         int dev = 0;
         check(cudaGetDevice(&dev), "cudaGetDevice");
@@ -1261,10 +1356,11 @@ struct CachedGraph {
     }
 };
 
-// Captures `body(work streams)` between a fork and a join on the capture
-// stream and replaces the cached graph with its instantiation.
+// Captures `body(work streams)` between a fork and a join of `branches`
+// parallel streams and replaces the cached graph with its instantiation.
 template <class Body>
-static void capture_batch(BatchStreams& bs, CachedGraph& cg, std::vector<unsigned char>&& key, Body body) {
+static void capture_batch(BatchStreams& bs, int branches, CachedGraph& cg, std::vector<unsigned char>&& key,
+                          Body body) {
     StageClock& clock = stage_clock();
     const bool profiling = clock.enabled;
     clock.enabled = false;
@@ -1272,9 +1368,9 @@ static void capture_batch(BatchStreams& bs, CachedGraph& cg, std::vector<unsigne
     check(cudaStreamBeginCapture(bs.cap, cudaStreamCaptureModeThreadLocal), "begin capture");
     try {
         check(cudaEventRecord(bs.fork, bs.cap), "fork");
-        for (auto& w : bs.work) check(cudaStreamWaitEvent(w, bs.fork, 0), "fork wait");
+        for (int k = 0; k < branches; ++k) check(cudaStreamWaitEvent(bs.work[k], bs.fork, 0), "fork wait");
         body(bs.work);
-        for (int k = 0; k < kBatchStreams; ++k) {
+        for (int k = 0; k < branches; ++k) {
             check(cudaEventRecord(bs.join[k], bs.work[k]), "join");
             check(cudaStreamWaitEvent(bs.cap, bs.join[k], 0), "join wait");
         }
@@ -1290,6 +1386,7 @@ static void capture_batch(BatchStreams& bs, CachedGraph& cg, std::vector<unsigne
     const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
     cudaGraphDestroy(graph);
     check(ie, "graph instantiate");
+    graph_counter().fetch_add(1, std::memory_order_relaxed);
     int dev = 0;
     check(cudaGetDevice(&dev), "cudaGetDevice");
     if (cg.exec && cg.device == dev) cudaGraphExecDestroy(cg.exec);
@@ -1359,6 +1456,8 @@ static void compress_batch(const waltz_b200_chunk* items, uint32_t count, uint64
     std::vector<unsigned char> key(reinterpret_cast<const unsigned char*>(items),
                                    reinterpret_cast<const unsigned char*>(items + count));
     key.push_back(uint8_t(sizeof(T)));
+    const int branches = t_branches;
+    append_key(key, branches);
     char* base = st.scratch.reserve(total);
     append_key(key, base); // the scratch must not have moved since the graph was captured
     uint64_t* results = reinterpret_cast<uint64_t*>(base + results_at);
@@ -1366,9 +1465,9 @@ static void compress_batch(const waltz_b200_chunk* items, uint32_t count, uint64
         std::vector<const uint16_t*> rank(count);
         for (uint32_t i = 0; i < count; ++i)
             rank[i] = st.tables.get(jobs[i].nx, jobs[i].ny, jobs[i].nz, jobs[i].g.bz, false, bs.cap);
-        capture_batch(bs, st.graph, std::move(key), [&](cudaStream_t* work) {
+        capture_batch(bs, branches, st.graph, std::move(key), [&](cudaStream_t* work) {
             for (uint32_t i = 0; i < count; ++i) {
-                cudaStream_t w = work[i % kBatchStreams];
+                cudaStream_t w = work[i % branches];
                 jobs[i].enqueue(base + offset[i], rank[i], w);
                 check(cudaMemcpyAsync(results + 9 * size_t(i), jobs[i].result(base + offset[i]), 9 * 8,
                                       cudaMemcpyDeviceToDevice, w), "result copy");
@@ -1390,11 +1489,12 @@ static void compress_batch(const waltz_b200_chunk* items, uint32_t count, uint64
 
 // ---------------------------------------------------------- batched decode
 // Many archives (uneven shapes, either form) decoded by one CUDA graph into
-// caller buffers, e.g. views of one preallocated tensor. Archive parameters
-// live in a device job table rewritten before every launch, so the graph is
-// captured once per (shapes, forms, output buffers) and replayed for every
-// later batch of other archives with that description — the data-loader
-// pattern, where a staging buffer and an output tensor are reused.
+// caller buffers: views of one preallocated tensor, or boxes of a larger
+// frame (output strides). Archive and output addresses live in a device job
+// table rewritten before every launch, so the graph is captured once per
+// (shapes, forms, output strides) and replayed for every later batch with
+// that description — the data-loader pattern, where every batch brings other
+// archives and a fresh output tensor.
 __global__ void gather_headers_kernel(const uint8_t* const* archives, uint8_t* headers) {
     headers[size_t(blockIdx.x) * 32 + threadIdx.x] = archives[blockIdx.x][threadIdx.x];
 }
@@ -1414,6 +1514,7 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
         Geometry g;
         Header h;
         Layout L;
+        uint64_t sy, sz; // output strides (elements)
     };
     std::vector<Item> list(count);
     auto item_error = [](uint32_t i, const char* what) {
@@ -1427,11 +1528,16 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
             const uint64_t n = uint64_t(a.nx) * a.ny * a.nz;
             need(n <= 0xffffffffull / sizeof(T), "Waltz: volume exceeds the archive section limits");
             need(a.archive && a.output, "Waltz: null buffer");
-            need(a.output_bytes >= n * sizeof(T), "output capacity too small");
+            const uint64_t sy = a.stride_y ? a.stride_y : a.nx, sz = a.stride_z ? a.stride_z : sy * a.ny;
+            need(sy >= a.nx && sz >= sy * a.ny, "Waltz: output strides smaller than the chunk");
+            const uint64_t extent = ((a.nz - 1) * sz + (a.ny - 1) * sy + a.nx) * sizeof(T);
+            need(a.output_bytes >= extent, "output capacity too small");
             need(a.bytes >= 32, "invalid Waltz archive header");
             const uintptr_t p = reinterpret_cast<uintptr_t>(a.archive), q = reinterpret_cast<uintptr_t>(a.output);
-            need(!(p < q + n * sizeof(T) && q < p + a.bytes), "Waltz: input and output buffers overlap");
+            need(!(p < q + extent && q < p + a.bytes), "Waltz: input and output buffers overlap");
             need(!(q % sizeof(T)), "Waltz: misaligned output");
+            list[i].sy = sy;
+            list[i].sz = sz;
             list[i].g = Geometry::make(a.nx, a.ny, a.nz);
             max_n = std::max(max_n, n);
         } catch (const std::exception& e) {
@@ -1441,9 +1547,10 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
     // Scratch: job table, status words, archive pointers, gathered headers,
     // the duplicate-check bitmap, then C / bank1 / bank2 per branch, sized by
     // the largest field on that branch.
-    uint64_t branch_n[kBatchStreams] = {};
+    const int branches = t_branches;
+    uint64_t branch_n[kMaxBranches] = {};
     for (uint32_t i = 0; i < count; ++i)
-        branch_n[i % kBatchStreams] = std::max<uint64_t>(branch_n[i % kBatchStreams], list[i].g.n);
+        branch_n[i % branches] = std::max<uint64_t>(branch_n[i % branches], list[i].g.n);
     Carver plan{nullptr};
     auto carve = [&](Carver& c) {
         struct P {
@@ -1452,14 +1559,14 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
             const uint8_t** ptrs;
             uint8_t* headers;
             uint32_t* seen;
-            T *C[kBatchStreams], *b1[kBatchStreams], *b2[kBatchStreams];
+            T *C[kMaxBranches], *b1[kMaxBranches], *b2[kMaxBranches];
         } p;
         p.jobs = c.take<DecodeJob>(count);
         p.status = c.take<uint32_t>(count);
         p.ptrs = c.take<const uint8_t*>(count);
         p.headers = c.take<uint8_t>(size_t(count) * 32);
         p.seen = c.take<uint32_t>((max_n + 31) / 32 + 1);
-        for (int k = 0; k < kBatchStreams; ++k) {
+        for (int k = 0; k < branches; ++k) {
             p.C[k] = c.take<T>(branch_n[k]);
             p.b1[k] = c.take<T>(branch_n[k]);
             p.b2[k] = c.take<T>(branch_n[k]);
@@ -1506,20 +1613,22 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
         }
     }
     for (uint32_t i = 0; i < count; ++i)
-        jobs[i] = decode_job(static_cast<const uint8_t*>(items[i].archive), list[i].h, list[i].L);
+        jobs[i] = decode_job(static_cast<const uint8_t*>(items[i].archive), list[i].h, list[i].L, items[i].output);
     check(cudaMemcpyAsync(P.jobs, jobs, size_t(count) * sizeof(DecodeJob), cudaMemcpyHostToDevice, stream),
           "job table upload");
     check(cudaMemsetAsync(P.status, 0, size_t(count) * 4, stream), "memset");
 
     std::vector<unsigned char> key;
     key.push_back(uint8_t(sizeof(T)));
+    append_key(key, branches);
     append_key(key, count);
     append_key(key, static_cast<const void*>(P.jobs));
     for (uint32_t i = 0; i < count; ++i) {
         append_key(key, items[i].nx);
         append_key(key, items[i].ny);
         append_key(key, items[i].nz);
-        append_key(key, items[i].output);
+        append_key(key, list[i].sy);
+        append_key(key, list[i].sz);
         key.push_back(list[i].h.flags & kMatrixFlag);
     }
     if (!st.graph.valid(key)) {
@@ -1529,14 +1638,15 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
             irank[i] = st.tables.get(g.nx, g.ny, g.nz, g.bz, true, bs.cap);
             if (list[i].h.flags & kMatrixFlag) t_zmat.get(g.nz, true, false, bs.cap); // upload before capture
         }
-        capture_batch(bs, st.graph, std::move(key), [&](cudaStream_t* work) {
+        capture_batch(bs, branches, st.graph, std::move(key), [&](cudaStream_t* work) {
             for (uint32_t i = 0; i < count; ++i) {
-                const int k = int(i % kBatchStreams);
+                const int k = int(i % branches);
                 const Geometry& g = list[i].g;
-                T* out = static_cast<T*>(items[i].output);
-                FinalOut<T> fin{out, g.nx, size_t(g.nx) * g.ny, P.status + i};
-                decode_launch<T>(JobRef{P.jobs + i, {}}, (list[i].h.flags & kMatrixFlag) != 0, g, irank[i], P.C[k],
-                                 P.b1[k], P.b2[k], fin, RowPatch<T>{out}, P.status + i, work[k]);
+                const DecodeJob* job = P.jobs + i;
+                JobOut<T> fin{job, list[i].sy, list[i].sz, P.status + i};
+                JobPatch<T> patch{job, g.nx, g.ny, list[i].sy, list[i].sz};
+                decode_launch<T>(JobRef{job, {}}, (list[i].h.flags & kMatrixFlag) != 0, g, irank[i], P.C[k], P.b1[k],
+                                 P.b2[k], fin, patch, P.status + i, work[k]);
             }
         });
     }
@@ -1626,6 +1736,13 @@ int waltz_b200_compress_batch(const waltz_b200_chunk* chunks, uint32_t count, in
     } catch (const std::exception& e) {
         return fail(e);
     }
+}
+
+int waltz_b200_batch_branches(int branches) {
+    using namespace wb;
+    const int prev = t_branches;
+    if (branches >= 1 && branches <= kMaxBranches) t_branches = branches;
+    return prev;
 }
 
 int waltz_b200_decompress_batch(const waltz_b200_archive* archives, uint32_t count, int width, void* stream) {
@@ -1880,6 +1997,8 @@ extern "C" int waltz_b200_zmatrix(float* d_data, uint32_t nx, uint32_t ny, uint3
 }
 
 extern "C" unsigned long long waltz_b200_launch_count(void) { return launch_counter().load(); }
+
+extern "C" unsigned long long waltz_b200_graph_count(void) { return graph_counter().load(); }
 
 extern "C" void waltz_b200_profile(int enable) { stage_clock().enabled = enable != 0; }
 

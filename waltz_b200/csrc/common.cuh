@@ -25,6 +25,11 @@ inline std::atomic<unsigned long long>& launch_counter() {
     return c;
 }
 inline void note_launch() { launch_counter().fetch_add(1, std::memory_order_relaxed); }
+// Batch graphs captured and instantiated (a replayed graph does not count).
+inline std::atomic<unsigned long long>& graph_counter() {
+    static std::atomic<unsigned long long> c{0};
+    return c;
+}
 
 struct StageClock {
     static constexpr int kMax = 16;
@@ -253,6 +258,7 @@ struct DecodeJob {
     uint64_t wzp, pi, pv, qi, qv;
     double q;
     uint32_t np, nq;
+    void* out; // where the samples go (read by JobOut / JobPatch)
 };
 
 // A decode kernel's archive parameters: by value (one archive decoded by

@@ -228,45 +228,48 @@ template <class T> struct FinalOut {
     }
 };
 
+// Output into a strided box whose base address is read from the device job
+// table at each store, so a replayed decode graph writes wherever the job
+// table says (a fresh tensor per batch).
+template <class T> struct JobOut {
+    static constexpr bool kPrefetch = false;
+    const DecodeJob* job;
+    size_t sy, sz;
+    uint32_t* status;
+    __device__ __forceinline__ void operator()(uint32_t x, uint32_t y, uint32_t z, T v) const {
+        T* dst = reinterpret_cast<T*>(__ldg(reinterpret_cast<const unsigned long long*>(&job->out)));
+        dst[size_t(z) * sz + size_t(y) * sy + x] = v;
+        if (!finite_bits(v)) atomicOr(status, ST_NONFINITE_INPUT);
+    }
+};
+
 // ----------------------------------------------- ordered bitmap compaction
 // Set bits of a row-major bitmap, in ascending index order, become
 // (index, value) records: pass 1 counts per block, pass 2 scans the block
-// counts (single CTA), pass 3 writes. Ordered by construction, no sort.
+// counts (single CTA) and lays out the archive, pass 3 writes. Ordered by
+// construction, no sort. Both record lists (repair records, q-outliers) go
+// through each pass together: blockIdx.y selects the list.
 constexpr int kCompactThreads = 256;
 constexpr int kCompactWords = kCompactThreads * 4; // bitmap words per block
 
-__global__ void compact_count_kernel(const uint32_t* bits, uint64_t words, uint32_t* counts) {
+__global__ void compact_count_kernel(const uint32_t* pbits, const uint32_t* qbits, uint64_t words, uint32_t* counts_p,
+                                     uint32_t* counts_q) {
     __shared__ uint32_t tmp[40];
+    const uint32_t* bits = blockIdx.y ? qbits : pbits;
     const uint64_t w0 = uint64_t(blockIdx.x) * kCompactWords + threadIdx.x * 4;
     uint32_t c = 0;
     for (int k = 0; k < 4; ++k)
         if (w0 + k < words) c += __popc(bits[w0 + k]);
     const uint32_t total = block_sum<kCompactThreads>(c, tmp);
-    if (threadIdx.x == 0) counts[blockIdx.x] = total;
+    if (threadIdx.x == 0) (blockIdx.y ? counts_q : counts_p)[blockIdx.x] = total;
 }
 
-// Exclusive scan of `count` block counts in place; writes the grand total.
-__global__ void compact_scan_kernel(uint32_t* counts, uint32_t count, uint32_t* total) {
-    __shared__ uint32_t tmp[40];
-    uint32_t carry = 0;
-    for (uint32_t base = 0; base < count; base += kCompactThreads) {
-        const uint32_t i = base + threadIdx.x;
-        const uint32_t v = i < count ? counts[i] : 0;
-        uint32_t sum;
-        const uint32_t ex = block_excl_scan<kCompactThreads>(v, tmp, sum);
-        if (i < count) counts[i] = carry + ex;
-        carry += sum;
-    }
-    if (threadIdx.x == 0) *total = carry;
-}
-
-// Record sink: indices as u32 LE, values of `VB` bytes, both at device-side
-// offsets inside the archive (given by `layout`).
+// Record sink: indices as u32 LE, values of sizeof(V) bytes, both at
+// device-side offsets inside the archive (given by `layout`).
 template <class V>
-__global__ void compact_write_kernel(const uint32_t* bits, uint64_t words, const uint32_t* offsets,
-                                     const V* values, uint8_t* archive, const uint64_t* layout, int idx_slot,
-                                     int val_slot, uint64_t cap_records) {
-    __shared__ uint32_t tmp[40];
+__device__ __forceinline__ void compact_write_block(const uint32_t* bits, uint64_t words, const uint32_t* offsets,
+                                                    const V* values, uint8_t* archive, const uint64_t* layout,
+                                                    int idx_slot, int val_slot, uint64_t cap_records, uint32_t* tmp) {
     const uint64_t w0 = uint64_t(blockIdx.x) * kCompactWords + threadIdx.x * 4;
     uint32_t wv[4];
     uint32_t c = 0;
@@ -296,15 +299,44 @@ __global__ void compact_write_kernel(const uint32_t* bits, uint64_t words, const
         }
 }
 
-// Archive layout from device-side counts. layout[]: 0 pi, 1 pv, 2 qi, 3 qv,
-// 4 end, 5 np, 6 nq, 7 overflow flag. Also writes the 32-byte header and
-// zeroes every padding byte between sections.
-__global__ void layout_kernel(uint8_t* archive, size_t capacity, const uint64_t* wzp_total, const uint32_t* np_p,
-                              const uint32_t* nq_p, uint32_t width, uint8_t flags, uint8_t lxy, uint8_t lz,
-                              uint8_t bz, double quantum, uint64_t* layout) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+template <class T>
+__global__ void compact_write_kernel(const uint32_t* pbits, const uint32_t* qbits, uint64_t words,
+                                     const uint32_t* offsets_p, const uint32_t* offsets_q, const T* perr,
+                                     const uint32_t* qval, uint8_t* archive, const uint64_t* layout,
+                                     uint64_t cap_records) {
+    __shared__ uint32_t tmp[40];
+    if (blockIdx.y == 0)
+        compact_write_block<T>(pbits, words, offsets_p, perr, archive, layout, 0, 1, cap_records, tmp);
+    else
+        compact_write_block<uint32_t>(qbits, words, offsets_q, qval, archive, layout, 2, 3, cap_records, tmp);
+}
+
+// Exclusive scan of both lists' block counts in place, then the archive
+// layout from the totals. layout[]: 0 pi, 1 pv, 2 qi, 3 qv, 4 end, 5 np,
+// 6 nq, 7 overflow flag, 8 the pipeline's status word. Also writes the
+// 32-byte header and zeroes every padding byte between sections.
+__global__ void compact_scan_layout_kernel(uint32_t* counts_p, uint32_t* counts_q, uint32_t count,
+                                           const uint64_t* wzp_total, const uint32_t* status, uint8_t* archive,
+                                           size_t capacity, uint32_t width, uint8_t flags, uint8_t lxy, uint8_t lz,
+                                           uint8_t bz, double quantum, uint64_t* layout) {
+    __shared__ uint32_t tmp[40];
+    uint32_t totals[2];
+    for (int list = 0; list < 2; ++list) {
+        uint32_t* counts = list ? counts_q : counts_p;
+        uint32_t carry = 0;
+        for (uint32_t base = 0; base < count; base += kCompactThreads) {
+            const uint32_t i = base + threadIdx.x;
+            const uint32_t v = i < count ? counts[i] : 0;
+            uint32_t sum;
+            const uint32_t ex = block_excl_scan<kCompactThreads>(v, tmp, sum);
+            if (i < count) counts[i] = carry + ex;
+            carry += sum;
+        }
+        totals[list] = carry;
+    }
+    if (threadIdx.x != 0) return;
     const uint64_t wb = *wzp_total; // includes the WZP header
-    const uint32_t np = *np_p, nq = *nq_p;
+    const uint32_t np = totals[0], nq = totals[1];
     const uint64_t pi = 32 + pad8(wb);
     const uint64_t pv = pi + pad8(uint64_t(np) * 4);
     const uint64_t qi = pv + pad8(uint64_t(np) * width);
@@ -318,6 +350,7 @@ __global__ void layout_kernel(uint8_t* archive, size_t capacity, const uint64_t*
     layout[5] = np;
     layout[6] = nq;
     layout[7] = end > capacity;
+    layout[8] = *status;
     if (end > capacity) return;
     archive[0] = flags;
     archive[1] = lxy;
@@ -362,10 +395,20 @@ __global__ void qpatch_kernel(JobRef job, uint64_t n, T* coeff, uint32_t* status
     }
 }
 
-// Repair patch targets: a row-major output, or a tile clipped into a frame.
+// Repair patch targets: a row-major output, a strided box at the job
+// table's output address, or a tile clipped into a frame.
 template <class T> struct RowPatch {
     T* out;
     __device__ __forceinline__ T* at(uint32_t i) const { return out + i; }
+};
+template <class T> struct JobPatch {
+    const DecodeJob* job;
+    uint32_t nx, ny;
+    size_t sy, sz;
+    __device__ __forceinline__ T* at(uint32_t i) const {
+        const uint32_t x = i % nx, y = (i / nx) % ny, z = i / (nx * ny);
+        return static_cast<T*>(job->out) + size_t(z) * sz + size_t(y) * sy + x;
+    }
 };
 
 // Repair records: validate, then out[i] -= err (after synthesis).
