@@ -88,11 +88,17 @@ typedef struct waltz_b200_archive {
 } waltz_b200_archive;
 int waltz_b200_decompress_batch(const waltz_b200_archive* archives, uint32_t count, int width, void* stream);
 
-/* Parallel branches (1..64, default 16) of the batch graphs that the calling
- * thread captures next: chunk i runs on branch i mod branches. Returns the
- * previous value; out-of-range values only query it. Performance knob only:
- * results do not depend on it. */
-int waltz_b200_batch_branches(int branches);
+/* Execution form of the batch graphs that the calling thread captures next
+ * (a performance knob: results do not depend on it).
+ * WALTZ_B200_BATCH_STAGES: fields split round-robin into `width` groups; per
+ *   group every pipeline stage is one launch over all its fields' tiles (a
+ *   chunk-tile work list); groups run as parallel graph branches.
+ * WALTZ_B200_BATCH_FIELDS: each field's own launches, fields round-robin on
+ *   `width` parallel graph branches. Default, width 32.
+ * width 1..64. Returns 0, or -1 for an invalid configuration. */
+#define WALTZ_B200_BATCH_STAGES 0
+#define WALTZ_B200_BATCH_FIELDS 1
+int waltz_b200_batch_config(int mode, int width);
 
 /* Decode an archive of `bytes` bytes into nx*ny*nz samples (the archive does
  * not store its dimensions); either form. */

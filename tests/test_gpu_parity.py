@@ -339,7 +339,18 @@ def test_matrix_form_rejects_unsuited_fields():
         waltz_b200.compress(np.zeros((64, 16, 16)), abs_error=1e-3, form="matrix")  # float64
 
 
-def test_batch_compress_equals_single_calls():
+BATCH_FORMS = [(0, 1), (0, 3), (1, 32)]  # (stage-batched | field chains, width)
+
+
+@pytest.fixture(params=BATCH_FORMS, ids=lambda f: f"mode{f[0]}w{f[1]}")
+def batch_form(request):
+    lib = _lib()
+    assert lib.waltz_b200_batch_config(*request.param) == 0
+    yield request.param
+    lib.waltz_b200_batch_config(1, 32)
+
+
+def test_batch_compress_equals_single_calls(batch_form):
     """Batched compress of uneven chunks (one CUDA graph): every archive is
     byte-identical to the single-call archive of its chunk, on the first call
     and on the replay; per-chunk bounds differ."""
@@ -379,7 +390,7 @@ def _uneven_batch(torch, seed, count, sides=(16, 17, 32, 48, 64)):
     return fields, bounds
 
 
-def test_batch_decompress_equals_single_calls():
+def test_batch_decompress_equals_single_calls(batch_form):
     """Batched decode of uneven archives of both forms into one preallocated
     tensor: bit-identical to the single-call decode; a second batch of other
     archives with the same shapes replays the graph; host header copies and a
@@ -418,7 +429,7 @@ def test_batch_decompress_equals_single_calls():
         assert torch.equal(g, waltz_b200.decompress_tensor(a, s, torch.float32))
 
 
-def test_batch_decompress_f64_and_errors():
+def test_batch_decompress_f64_and_errors(batch_form):
     torch = _torch()
     import waltz_b200
     from waltz_b200 import synthetic as S
@@ -436,3 +447,12 @@ def test_batch_decompress_f64_and_errors():
     # a shape that does not match the archive's levels
     with pytest.raises(waltz_b200.WaltzError, match="batch item 1"):
         waltz_b200.decompress_batch(archives, [shapes[0], (64, 64, 64), shapes[2]], torch.float64)
+
+
+def test_batch_config_rejects_invalid_forms():
+    lib = _lib()
+    assert lib.waltz_b200_batch_config(2, 4) == -1
+    assert lib.waltz_b200_batch_config(0, 0) == -1
+    assert lib.waltz_b200_batch_config(1, 65) == -1
+    assert b"invalid batch configuration" in lib.waltz_b200_last_error()
+    assert lib.waltz_b200_batch_config(1, 32) == 0

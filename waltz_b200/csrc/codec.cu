@@ -11,6 +11,8 @@
 // read at the call's single synchronisation point.
 #include "common.cuh"
 #include "inverse.cuh"
+#include "launch.cuh"
+#include "ops.cuh"
 #include "quantize.cuh"
 #include "stage.cuh"
 #include "stream.cuh"
@@ -195,36 +197,27 @@ template <> struct Tiles<double> {
 };
 
 template <class T, bool Inverse, int Mask, int UX, int UY, int UZ, class Src, class Out>
-static void launch_level(const Src& src, Dims a, const Out& out, cudaStream_t stream) {
-    auto kernel = level_kernel<T, Inverse, Mask, UX, UY, UZ, Src, Out>;
+static void launch_level(const Src& src, Dims a, const Out& out, Sink& sink) {
+    using Op = LevelOp<T, Inverse, Mask, UX, UY, UZ, Src, Out>;
     constexpr size_t smem = level_smem<T, Inverse, Mask, UX, UY, UZ>();
-    static thread_local int configured_device = -1;
-    int dev = 0;
-    check(cudaGetDevice(&dev), "cudaGetDevice");
-    if (configured_device != dev) {
-        check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
-              "level kernel shared memory");
-        configured_device = dev;
-    }
     const Dims grid{(a.x + UX - 1) / UX, (a.y + UY - 1) / UY, (a.z + UZ - 1) / UZ};
     const uint64_t blocks = uint64_t(grid.x) * grid.y * grid.z;
     need(blocks < (1ull << 31), "Waltz: level grid too large");
-    kernel<<<unsigned(blocks), 256, smem, stream>>>(src, a, grid, out); note_launch();
-    check(cudaGetLastError(), "level kernel launch");
+    sink.run<Op>(typename Op::Params{src, a, grid, out}, uint32_t(blocks), smem);
 }
 
 template <class T, bool Inverse, int Mask, class Src, class Out>
-static void level(const Src& src, Dims a, const Out& out, cudaStream_t stream) {
+static void level(const Src& src, Dims a, const Out& out, Sink& sink) {
     if constexpr (Mask == (AX | AY | AZ))
-        launch_level<T, Inverse, Mask, Tiles<T>::XYZ[0], Tiles<T>::XYZ[1], Tiles<T>::XYZ[2]>(src, a, out, stream);
+        launch_level<T, Inverse, Mask, Tiles<T>::XYZ[0], Tiles<T>::XYZ[1], Tiles<T>::XYZ[2]>(src, a, out, sink);
     else if constexpr (Mask == (AX | AY))
-        launch_level<T, Inverse, Mask, Tiles<T>::XY[0], Tiles<T>::XY[1], Tiles<T>::XY[2]>(src, a, out, stream);
+        launch_level<T, Inverse, Mask, Tiles<T>::XY[0], Tiles<T>::XY[1], Tiles<T>::XY[2]>(src, a, out, sink);
     else
-        launch_level<T, Inverse, Mask, Tiles<T>::Z[0], Tiles<T>::Z[1], Tiles<T>::Z[2]>(src, a, out, stream);
+        launch_level<T, Inverse, Mask, Tiles<T>::Z[0], Tiles<T>::Z[1], Tiles<T>::Z[2]>(src, a, out, sink);
 }
 
 // Resident CTAs of a kernel per SM times the SM count, cached per device.
-template <class K> static uint64_t resident_slots(K kernel, size_t smem) {
+template <class K> static uint64_t resident_slots(K kernel, size_t smem, int threads = 256) {
     static thread_local int cached_dev = -1;
     static thread_local uint64_t slots = 0;
     int dev = 0;
@@ -232,7 +225,7 @@ template <class K> static uint64_t resident_slots(K kernel, size_t smem) {
     if (cached_dev != dev) {
         int sms = 0, occ = 0;
         check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
-        check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, 256, smem), "occupancy");
+        check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem), "occupancy");
         slots = uint64_t(sms) * uint64_t(occ > 0 ? occ : 1);
         cached_dev = dev;
     }
@@ -240,108 +233,116 @@ template <class K> static uint64_t resident_slots(K kernel, size_t smem) {
 }
 
 // One dyadic forward level as a z-march: XY tiles, and the z axis split into
-// ranges only as far as needed to give every resident CTA slot work. Planes
-// are staged by TMA when the source rows meet the copy engine's alignment.
+// ranges only as far as needed to give every resident CTA slot work (one
+// range per column tile when many fields share the GPU). Planes are staged by
+// TMA when the source rows meet the copy engine's alignment.
 template <class T>
-static void level_fwd_stream(const FwdSrc<T>& src, Dims a, const FwdOut<T>& out, uint32_t* status,
-                             cudaStream_t stream) {
+static void level_fwd_stream(const FwdSrc<T>& src, Dims a, const FwdOut<T>& out, uint32_t* status, Sink& sink) {
     constexpr int UX = StreamTile<T>::UX, UY = StreamTile<T>::UY, Q = StreamTile<T>::Q;
     using S = StreamShape<T, UX, UY, Q>;
-    CUtensorMap map{};
-    const bool tma = make_map_3d<T>(&map, src.p, a.x, a.y, a.z, src.sy, src.sz, S::FX, S::FY, 1);
-    auto kernel = tma ? fwd_stream_kernel<T, UX, UY, Q, true> : fwd_stream_kernel<T, UX, UY, Q, false>;
-    static thread_local int configured_device = -1;
-    int dev = 0;
-    check(cudaGetDevice(&dev), "cudaGetDevice");
-    if (configured_device != dev) {
-        check(cudaFuncSetAttribute(fwd_stream_kernel<T, UX, UY, Q, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   int(S::smem)), "stream kernel shared memory");
-        check(cudaFuncSetAttribute(fwd_stream_kernel<T, UX, UY, Q, false>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(S::smem)),
-              "stream kernel shared memory");
-        configured_device = dev;
-    }
+    using OpT = FwdStreamOp<T, UX, UY, Q, true>;
+    using OpL = FwdStreamOp<T, UX, UY, Q, false>;
+    typename OpT::Params p{};
+    const bool tma = make_map_3d<T>(&p.map, src.p, a.x, a.y, a.z, src.sy, src.sz, S::FX, S::FY, 1);
     const uint32_t tx = (a.x + UX - 1) / UX, ty = (a.y + UY - 1) / UY;
-    const uint64_t tiles = uint64_t(tx) * ty, slots = resident_slots(kernel, S::smem);
-    // z ranges: maximise (filled share of the last wave) x (planes kept out of
-    // the 8-plane halo a range re-reads), over up to 16 ranges of >= 16 planes
+    const uint64_t tiles = uint64_t(tx) * ty;
     uint32_t zrange = a.z + (a.z & 1);
-    double best = -1;
-    for (uint32_t k = 1; k <= 16; ++k) {
-        uint32_t r = (a.z + k - 1) / k;
-        r += r & 1;
-        if (k > 1 && r < 16) break;
-        const uint64_t blocks = tiles * ((a.z + r - 1) / r);
-        const double waves = double((blocks + slots - 1) / slots);
-        const double score = double(blocks) / (waves * double(slots)) * double(r) / double(r + 8);
-        if (score > best + 1e-9) {
-            best = score;
-            zrange = r;
+    if (!sink.many) {
+        // maximise (filled share of the last wave) x (planes kept out of the
+        // 8-plane halo a range re-reads), over up to 16 ranges of >= 16 planes
+        static thread_local int device = -1;
+        static thread_local size_t granted = 0;
+        opt_in_smem(op_kernel_for<OpT>(), S::smem, device, granted);
+        const uint64_t slots = resident_slots(op_kernel_for<OpT>(), S::smem);
+        double best = -1;
+        for (uint32_t k = 1; k <= 16; ++k) {
+            uint32_t r = (a.z + k - 1) / k;
+            r += r & 1;
+            if (k > 1 && r < 16) break;
+            const uint64_t blocks = tiles * ((a.z + r - 1) / r);
+            const double waves = double((blocks + slots - 1) / slots);
+            const double score = double(blocks) / (waves * double(slots)) * double(r) / double(r + 8);
+            if (score > best + 1e-9) {
+                best = score;
+                zrange = r;
+            }
         }
     }
     const uint64_t blocks = tiles * ((a.z + zrange - 1) / zrange);
     need(blocks < (1ull << 31), "Waltz: level grid too large");
-    kernel<<<unsigned(blocks), 256, S::smem, stream>>>(src, map, a, tx, ty, zrange, out, status); note_launch();
-    check(cudaGetLastError(), "stream level launch");
+    p.src = src;
+    p.a = a;
+    p.tiles_x = tx;
+    p.tiles_y = ty;
+    p.zrange = zrange;
+    p.out = out;
+    p.status = status;
+    if (tma) {
+        sink.run<OpT>(p, uint32_t(blocks), S::smem);
+    } else {
+        typename OpL::Params q{};
+        q.src = src;
+        q.a = a;
+        q.tiles_x = tx;
+        q.tiles_y = ty;
+        q.zrange = zrange;
+        q.out = out;
+        q.status = status;
+        sink.run<OpL>(q, uint32_t(blocks), S::smem);
+    }
 }
 
 // One dyadic inverse level from TMA-staged parity boxes when the coefficient
 // rows meet the copy engine's alignment; the generic level kernel otherwise.
 template <class T, class Out>
-static void level_inv(const InvSrc<T>& src, Dims a, const Out& out, uint32_t* status, cudaStream_t stream) {
+static void level_inv(const InvSrc<T>& src, Dims a, const Out& out, uint32_t* status, Sink& sink) {
     constexpr int UX = InvTile<T>::UX, UY = InvTile<T>::UY, UZ = InvTile<T>::UZ;
     using S = InvShape<T, UX, UY, UZ>;
-    CUtensorMap cmap{}, lmap{};
+    using Op = InvTileOp<T, UX, UY, UZ, Out>;
+    typename Op::Params p{};
     bool tma = half_len(a.x) % S::V == 0 &&
-               make_map_3d<T>(&cmap, src.base, a.x, a.y, a.z, src.sy, src.sz, S::BX, S::HY, S::HZ);
+               make_map_3d<T>(&p.cmap, src.base, a.x, a.y, a.z, src.sy, src.sz, S::BX, S::HY, S::HZ);
     if (tma && src.low)
-        tma = make_map_3d<T>(&lmap, src.low, src.lo.x, src.lo.y, src.lo.z, src.lo.x, uint64_t(src.lo.x) * src.lo.y,
+        tma = make_map_3d<T>(&p.lmap, src.low, src.lo.x, src.lo.y, src.lo.z, src.lo.x, uint64_t(src.lo.x) * src.lo.y,
                              S::BX, S::HY, S::HZ);
     if (!tma) {
-        level<T, true, AX | AY | AZ>(src, a, out, stream);
+        level<T, true, AX | AY | AZ>(src, a, out, sink);
         return;
-    }
-    auto kernel = inv_tile_kernel<T, UX, UY, UZ, Out>;
-    static thread_local int configured_device = -1;
-    int dev = 0;
-    check(cudaGetDevice(&dev), "cudaGetDevice");
-    if (configured_device != dev) {
-        check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(S::smem)),
-              "inverse tile shared memory");
-        configured_device = dev;
     }
     const uint32_t tx = (a.x + UX - 1) / UX, ty = (a.y + UY - 1) / UY, tz = (a.z + UZ - 1) / UZ;
     const uint64_t blocks = uint64_t(tx) * ty * tz;
     need(blocks < (1ull << 31), "Waltz: level grid too large");
-    const InvLevel<T> lv{src.base, src.sy, src.sz, src.low, src.lo, a};
-    kernel<<<unsigned(blocks), 256, S::smem, stream>>>(lv, cmap, lmap, tx, ty, out, status); note_launch();
-    check(cudaGetLastError(), "inverse tile launch");
+    p.lv = InvLevel<T>{src.base, src.sy, src.sz, src.low, src.lo, a};
+    p.tiles_x = tx;
+    p.tiles_y = ty;
+    p.out = out;
+    p.status = status;
+    sink.run<Op>(p, uint32_t(blocks), S::smem);
 }
 
-// WZP encoder launch for one magnitude source (shared memory set up once per
-// device and source type).
+// WZP encoder of one magnitude source: one CTA per 8192-sample chunk.
 template <class Src>
-static void launch_wzp_encode(const WzpEncodeArgs& wa, const Src& src, uint32_t chunks, cudaStream_t stream) {
-    static thread_local int cfg_dev = -1;
-    int dev = 0;
-    check(cudaGetDevice(&dev), "cudaGetDevice");
-    if (cfg_dev != dev) {
-        check(cudaFuncSetAttribute(wzp_encode_kernel<Src>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   int(sizeof(WzpEncodeSmem))), "wzp smem");
-        cfg_dev = dev;
-    }
-    wzp_encode_kernel<Src><<<chunks, kWzpThreads, sizeof(WzpEncodeSmem), stream>>>(wa, src); note_launch();
-    check(cudaGetLastError(), "wzp encode launch");
+static void launch_wzp_encode(const WzpEncodeArgs& wa, const Src& src, uint32_t chunks, Sink& sink) {
+    sink.run<WzpEncodeOp<Src>>(typename WzpEncodeOp<Src>::Params{wa, src}, chunks, sizeof(WzpEncodeSmem));
 }
 
-template <class T, class Out>
-__global__ void identity_kernel(const T* in, Dims d, Out out) {
-    const uint64_t n = vol(d);
-    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
-        const uint32_t x = uint32_t(i % d.x), y = uint32_t((i / d.x) % d.y), z = uint32_t(i / (uint64_t(d.x) * d.y));
-        out(x, y, z, in[i]);
+template <class T, class Out> struct IdentityOp {
+    static constexpr int kThreads = 256, kMinBlocks = 0; // no occupancy floor: the compiler picks the register budget
+    struct Params {
+        const T* in;
+        Dims d;
+        Out out;
+    };
+    static __device__ __forceinline__ void run(const Params P, uint32_t block, uint32_t blocks) {
+        const Dims d = P.d;
+        const uint64_t n = vol(d);
+        for (uint64_t i = block * uint64_t(kThreads) + threadIdx.x; i < n; i += uint64_t(blocks) * kThreads) {
+            const uint32_t x = uint32_t(i % d.x), y = uint32_t((i / d.x) % d.y),
+                           z = uint32_t(i / (uint64_t(d.x) * d.y));
+            P.out(x, y, z, P.in[i]);
+        }
     }
-}
+};
 
 static unsigned grid_for(uint64_t n, unsigned threads = 256) {
     uint64_t b = (n + threads - 1) / threads;
@@ -369,63 +370,35 @@ template <class T> static bool xystage_ok(const Geometry& g) {
     return g.lxy && xystage_smem<T>(g.nx, g.ny) <= kStageSmemCap;
 }
 
-// Opts a kernel into the stage kernels' shared-memory size once per device.
-template <class K> static void stage_smem_attr(K kernel, int& configured) {
-    int dev = 0;
-    check(cudaGetDevice(&dev), "cudaGetDevice");
-    if (configured != dev) {
-        check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kStageSmemCap)),
-              "stage kernel shared memory");
-        configured = dev;
-    }
-}
-
 static unsigned zstage_grid(const Geometry& g, int cx, int cy) {
     return unsigned(((g.nx + cx - 1) / cx) * uint64_t((g.ny + cy - 1) / cy));
 }
 
 template <class T>
 static void zstage_forward(const T* in, size_t sy, size_t sz, const Geometry& g, T* dst, uint32_t* status,
-                           cudaStream_t stream) {
-    static thread_local int configured = -1;
-    stage_smem_attr(zstage_fwd_kernel<T>, configured);
-    zstage_fwd_kernel<T><<<zstage_grid(g, ZCols<T>::CX, ZCols<T>::CY), kZStageThreads, zstage_smem<T>(g.nz),
-                           stream>>>(in, sy, sz, g.nx, g.ny, g.nz, z_levels(g), dst, status);
-    note_launch();
-    check(cudaGetLastError(), "z stage launch");
+                           Sink& sink) {
+    sink.run<ZStageFwdOp<T>>(typename ZStageFwdOp<T>::Params{in, sy, sz, g.nx, g.ny, g.nz, z_levels(g), dst, status},
+                             zstage_grid(g, ZCols<T>::CX, ZCols<T>::CY), zstage_smem<T>(g.nz));
 }
 
 template <class T, class Out>
-static void zstage_inverse(const T* coef, size_t sy, size_t sz, const Geometry& g, const Out& out,
-                           cudaStream_t stream) {
-    static thread_local int configured = -1;
-    stage_smem_attr(zstage_inv_kernel<T, Out>, configured);
-    zstage_inv_kernel<T, Out><<<zstage_grid(g, ZCols<T>::CX, ZCols<T>::CY), kZStageThreads, zstage_smem<T>(g.nz),
-                                stream>>>(coef, sy, sz, g.nx, g.ny, g.nz, z_levels(g), out);
-    note_launch();
-    check(cudaGetLastError(), "z stage launch");
+static void zstage_inverse(const T* coef, size_t sy, size_t sz, const Geometry& g, const Out& out, Sink& sink) {
+    sink.run<ZStageInvOp<T, Out>>(typename ZStageInvOp<T, Out>::Params{coef, sy, sz, g.nx, g.ny, g.nz, z_levels(g), out},
+                                  zstage_grid(g, ZCols<T>::CX, ZCols<T>::CY), zstage_smem<T>(g.nz));
 }
 
 template <class T>
 static void xystage_forward(const T* in, size_t sy, size_t sz, const Geometry& g, T* dst, size_t dsy, size_t dsz,
-                            uint32_t* status, cudaStream_t stream) {
-    static thread_local int configured = -1;
-    stage_smem_attr(xystage_fwd_kernel<T>, configured);
-    xystage_fwd_kernel<T><<<g.nz, kXYStageThreads, xystage_smem<T>(g.nx, g.ny), stream>>>(
-        in, sy, sz, g.nx, g.ny, xy_levels(g), dst, dsy, dsz, status);
-    note_launch();
-    check(cudaGetLastError(), "xy stage launch");
+                            uint32_t* status, Sink& sink) {
+    sink.run<XYStageFwdOp<T>>(
+        typename XYStageFwdOp<T>::Params{in, sy, sz, g.nx, g.ny, xy_levels(g), dst, dsy, dsz, status}, g.nz,
+        xystage_smem<T>(g.nx, g.ny));
 }
 
 template <class T, class Out>
-static void xystage_inverse(const T* coef, size_t sy, size_t sz, const Geometry& g, const Out& out,
-                            cudaStream_t stream) {
-    static thread_local int configured = -1;
-    stage_smem_attr(xystage_inv_kernel<T, Out>, configured);
-    xystage_inv_kernel<T, Out><<<g.nz, kXYStageThreads, xystage_smem<T>(g.nx, g.ny), stream>>>(
-        coef, sy, sz, g.nx, g.ny, xy_levels(g), out);
-    note_launch();
-    check(cudaGetLastError(), "xy stage launch");
+static void xystage_inverse(const T* coef, size_t sy, size_t sz, const Geometry& g, const Out& out, Sink& sink) {
+    sink.run<XYStageInvOp<T, Out>>(typename XYStageInvOp<T, Out>::Params{coef, sy, sz, g.nx, g.ny, xy_levels(g), out},
+                                   g.nz, xystage_smem<T>(g.nx, g.ny));
 }
 
 // Scratch element counts for the forward and inverse transforms.
@@ -450,31 +423,29 @@ static TransformScratch scratch_need(const Geometry& g) {
 
 template <class Out>
 static void zmatrix_apply(const float* x, uint32_t nx, uint32_t ny, uint32_t nz, bool inverse, const Out& out,
-                          uint32_t* status, bool check_finite, cudaStream_t stream);
+                          uint32_t* status, bool check_finite, Sink& sink);
 
 // Forward all-level transform of `in` into the coefficient array C. With
 // `matrix` (the precision form; plane schedule, float) the Z stage is the
 // tensor-core matrix transform instead of Z lifting.
 template <class T>
 static void forward(const Geometry& g, const T* in, T* C, T* lowA, T* lowB, T* inter, uint32_t* status,
-                    cudaStream_t stream, bool matrix = false) {
+                    Sink& sink, bool matrix = false) {
     const size_t sy = g.nx, sz = size_t(g.nx) * g.ny;
     T* lows[2] = {lowA, lowB};
     if (g.lxy == 0 && g.lz == 0) {
-        copy_finite_kernel<T><<<grid_for(g.n), 256, 0, stream>>>(in, C, g.n, status); note_launch();
-        check(cudaGetLastError(), "copy launch");
+        sink.run<CopyFiniteOp<T>>(typename CopyFiniteOp<T>::Params{in, C, g.n, status}, grid_for(g.n));
         return;
     }
-    StageClock& clock = stage_clock();
     if (g.dyadic) {
         FwdSrc<T> src{in, sy, sz, status};
         for (unsigned l = 0; l < g.lxy; ++l) {
             const Dims a = g.dyad[l], lo = halve(a, AX | AY | AZ);
             const bool last = l + 1 == g.lxy;
             FwdOut<T> out{C, sy, sz, last ? nullptr : lows[l & 1], lo, a, AX | AY | AZ};
-            level_fwd_stream<T>(src, a, out, status, stream);
+            level_fwd_stream<T>(src, a, out, status, sink);
             static const char* const kFwdNames[5] = {"fwd_l0", "fwd_l1", "fwd_l2", "fwd_l3", "fwd_l4"};
-            clock.mark(kFwdNames[l], stream);
+            sink.mark(kFwdNames[l]);
             src = FwdSrc<T>{lows[l & 1], lo.x, size_t(lo.x) * lo.y};
         }
         return;
@@ -483,34 +454,34 @@ static void forward(const Geometry& g, const T* in, T* C, T* lowA, T* lowB, T* i
     T* zdst = g.lxy ? inter : C;
     if constexpr (std::is_same_v<T, float>) {
         if (matrix) {
-            zmatrix_apply(in, g.nx, g.ny, g.nz, false, ZmStore<float>{zdst}, status, true, stream);
-            clock.mark("fwd_z_matrix", stream);
+            zmatrix_apply(in, g.nx, g.ny, g.nz, false, ZmStore<float>{zdst}, status, true, sink);
+            sink.mark("fwd_z_matrix");
         }
     }
     const bool zstage = !matrix && zstage_ok<T>(g);
-    if (zstage) zstage_forward<T>(in, sy, sz, g, zdst, status, stream);
+    if (zstage) zstage_forward<T>(in, sy, sz, g, zdst, status, sink);
     for (unsigned l = 0; l < (matrix || zstage ? 0u : g.lz); ++l) {
         const Dims a = g.zl[l], lo = halve(a, AZ);
         const bool last = l + 1 == g.lz;
         FwdOut<T> out{zdst, sy, sz, last ? nullptr : lows[l & 1], lo, a, AZ};
-        level<T, false, AZ>(src, a, out, stream);
+        level<T, false, AZ>(src, a, out, sink);
         src = FwdSrc<T>{lows[l & 1], lo.x, size_t(lo.x) * lo.y};
     }
-    if (g.lz) clock.mark("fwd_z", stream);
+    if (g.lz) sink.mark("fwd_z");
     if (g.lz) src = FwdSrc<T>{inter, sy, sz};
     if (xystage_ok<T>(g)) {
-        xystage_forward<T>(src.p, sy, sz, g, C, sy, sz, g.lz ? nullptr : status, stream);
-        clock.mark("fwd_xy", stream);
+        xystage_forward<T>(src.p, sy, sz, g, C, sy, sz, g.lz ? nullptr : status, sink);
+        sink.mark("fwd_xy");
         return;
     }
     for (unsigned l = 0; l < g.lxy; ++l) {
         const Dims a = g.xyl[l], lo = halve(a, AX | AY);
         const bool last = l + 1 == g.lxy;
         FwdOut<T> out{C, sy, sz, last ? nullptr : lows[l & 1], lo, a, AX | AY};
-        level<T, false, AX | AY>(src, a, out, stream);
+        level<T, false, AX | AY>(src, a, out, sink);
         src = FwdSrc<T>{lows[l & 1], lo.x, size_t(lo.x) * lo.y};
     }
-    if (g.lxy) clock.mark("fwd_xy", stream);
+    if (g.lxy) sink.mark("fwd_xy");
 }
 
 // Largest compact low band the inverse keeps between two levels of one stage.
@@ -532,15 +503,14 @@ static uint64_t inverse_low_need(const Geometry& g) {
 // hands every sample to `fin`.
 template <class T, class Final>
 static void inverse(const Geometry& g, T* C, T* bank1, T* bank2, const Final& fin, uint32_t* status,
-                    cudaStream_t stream, const char* final_stage = "inv_l0", bool matrix = false) {
-    StageClock& clock = stage_clock();
+                    Sink& sink, const char* final_stage = "inv_l0", bool matrix = false) {
     const size_t sy = g.nx, sz = size_t(g.nx) * g.ny;
     const uint64_t half_off = ((g.n + 1) / 2 + 63) & ~uint64_t(63);
     need(inverse_low_need(g) <= g.n - std::min(g.n, half_off), "Waltz: inverse scratch layout");
     T* halves[2] = {bank2, bank2 + half_off};
     if (g.lxy == 0 && g.lz == 0) {
-        identity_kernel<T, Final><<<grid_for(g.n), 256, 0, stream>>>(C, Dims{g.nx, g.ny, g.nz}, fin); note_launch();
-        check(cudaGetLastError(), "identity launch");
+        sink.run<IdentityOp<T, Final>>(typename IdentityOp<T, Final>::Params{C, Dims{g.nx, g.ny, g.nz}, fin},
+                                       grid_for(g.n));
         return;
     }
     if (g.dyadic) {
@@ -550,13 +520,13 @@ static void inverse(const Geometry& g, T* C, T* bank1, T* bank2, const Final& fi
             InvSrc<T> src{C, sy, sz, low, halve(a, AX | AY | AZ)};
             if (l > 0) {
                 T* dst = halves[l & 1];
-                level_inv<T>(src, a, StoreOut<T>{dst, a.x, size_t(a.x) * a.y}, status, stream);
+                level_inv<T>(src, a, StoreOut<T>{dst, a.x, size_t(a.x) * a.y}, status, sink);
                 low = dst;
                 static const char* const kInvNames[5] = {"inv_l0", "inv_l1", "inv_l2", "inv_l3", "inv_l4"};
-                clock.mark(kInvNames[l], stream);
+                sink.mark(kInvNames[l]);
             } else {
-                level_inv<T>(src, a, fin, status, stream);
-                clock.mark(final_stage, stream);
+                level_inv<T>(src, a, fin, status, sink);
+                sink.mark(final_stage);
             }
         }
         return;
@@ -565,13 +535,13 @@ static void inverse(const Geometry& g, T* C, T* bank1, T* bank2, const Final& fi
     T* zping[2] = {bank2, bank1};
     if (xystage_ok<T>(g)) {
         if (g.lz) {
-            xystage_inverse<T>(C, sy, sz, g, StoreOut<T>{bank1, sy, sz}, stream);
+            xystage_inverse<T>(C, sy, sz, g, StoreOut<T>{bank1, sy, sz}, sink);
             zbase = bank1;
             zping[1] = C;
         } else {
-            xystage_inverse<T>(C, sy, sz, g, fin, stream);
+            xystage_inverse<T>(C, sy, sz, g, fin, sink);
         }
-        clock.mark("inv_xy", stream);
+        sink.mark("inv_xy");
     } else if (g.lxy) {
         const T* low = nullptr;
         for (int l = int(g.lxy) - 1; l >= 0; --l) {
@@ -579,28 +549,28 @@ static void inverse(const Geometry& g, T* C, T* bank1, T* bank2, const Final& fi
             InvSrc<T> src{C, sy, sz, low, halve(a, AX | AY)};
             if (l > 0) {
                 T* dst = halves[l & 1];
-                level<T, true, AX | AY>(src, a, StoreOut<T>{dst, a.x, size_t(a.x) * a.y}, stream);
+                level<T, true, AX | AY>(src, a, StoreOut<T>{dst, a.x, size_t(a.x) * a.y}, sink);
                 low = dst;
             } else if (g.lz) {
-                level<T, true, AX | AY>(src, a, StoreOut<T>{bank1, sy, sz}, stream);
+                level<T, true, AX | AY>(src, a, StoreOut<T>{bank1, sy, sz}, sink);
                 zbase = bank1;
                 zping[1] = C; // the coefficients are no longer read
             } else {
-                level<T, true, AX | AY>(src, a, fin, stream);
+                level<T, true, AX | AY>(src, a, fin, sink);
             }
         }
-        clock.mark("inv_xy", stream);
+        sink.mark("inv_xy");
     }
     if constexpr (std::is_same_v<T, float>) {
         if (matrix && g.lz) {
-            zmatrix_apply(zbase, g.nx, g.ny, g.nz, true, ZmEmit<Final>{fin, g.nx}, status, false, stream);
-            clock.mark("inv_z_matrix", stream);
+            zmatrix_apply(zbase, g.nx, g.ny, g.nz, true, ZmEmit<Final>{fin, g.nx}, status, false, sink);
+            sink.mark("inv_z_matrix");
             return;
         }
     }
     if (zstage_ok<T>(g)) {
-        zstage_inverse<T>(zbase, sy, sz, g, fin, stream);
-        clock.mark("inv_z", stream);
+        zstage_inverse<T>(zbase, sy, sz, g, fin, sink);
+        sink.mark("inv_z");
     } else if (g.lz) {
         const T* low = nullptr;
         for (int l = int(g.lz) - 1; l >= 0; --l) {
@@ -608,13 +578,13 @@ static void inverse(const Geometry& g, T* C, T* bank1, T* bank2, const Final& fi
             InvSrc<T> src{zbase, sy, sz, low, halve(a, AZ)};
             if (l > 0) {
                 T* dst = zping[l & 1];
-                level<T, true, AZ>(src, a, StoreOut<T>{dst, a.x, size_t(a.x) * a.y}, stream);
+                level<T, true, AZ>(src, a, StoreOut<T>{dst, a.x, size_t(a.x) * a.y}, sink);
                 low = dst;
             } else {
-                level<T, true, AZ>(src, a, fin, stream);
+                level<T, true, AZ>(src, a, fin, sink);
             }
         }
-        clock.mark("inv_z", stream);
+        sink.mark("inv_z");
     }
 }
 
@@ -760,29 +730,30 @@ static thread_local ZMatrixCache t_zmat;
 // every result. nz <= 64, nx*ny a multiple of 4.
 template <class Out>
 static void zmatrix_apply(const float* x, uint32_t nx, uint32_t ny, uint32_t nz, bool inverse, const Out& out,
-                          uint32_t* status, bool check_finite, cudaStream_t stream) {
+                          uint32_t* status, bool check_finite, Sink& sink) {
     need(nz >= 1 && nz <= uint32_t(kZmMaxK), "Waltz: matrix form needs 1 <= nz <= 64");
     const uint64_t ncols = uint64_t(nx) * ny;
     const ZmPlan P = ZmPlan::make(nz);
-    const float* bhi = t_zmat.get(nz, inverse, false, stream);
-    const float* blo = t_zmat.get(nz, inverse, true, stream);
-    auto kernel = zmatrix_kernel<Out>;
-    const uint32_t smem_max = ZmPlan::make(kZmMaxK).smem();
-    static thread_local int configured_device = -1;
-    int dev = 0;
-    check(cudaGetDevice(&dev), "cudaGetDevice");
-    if (configured_device != dev) {
-        check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_max)),
-              "matrix kernel shared memory");
-        configured_device = dev;
-    }
-    const uint64_t tiles = (ncols + kZmCols - 1) / kZmCols;
-    int sms = 0;
-    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
-    const unsigned grid = unsigned(std::min<uint64_t>(tiles, resident_slots(kernel, P.smem())));
-    kernel<<<grid, kZmThreads, P.smem(), stream>>>(x, bhi, blo, nz, ncols, out, status, check_finite ? 1u : 0u);
-    note_launch();
-    check(cudaGetLastError(), "matrix kernel launch");
+    const float* bhi = t_zmat.get(nz, inverse, false, sink.stream);
+    const float* blo = t_zmat.get(nz, inverse, true, sink.stream);
+    // no batched form: every field keeps its own persistent launch
+    sink.direct([=](cudaStream_t stream) {
+        auto kernel = zmatrix_kernel<Out>;
+        const uint32_t smem_max = ZmPlan::make(kZmMaxK).smem();
+        static thread_local int configured_device = -1;
+        int dev = 0;
+        check(cudaGetDevice(&dev), "cudaGetDevice");
+        if (configured_device != dev) {
+            check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_max)),
+                  "matrix kernel shared memory");
+            configured_device = dev;
+        }
+        const uint64_t tiles = (ncols + kZmCols - 1) / kZmCols;
+        const unsigned grid = unsigned(std::min<uint64_t>(tiles, resident_slots(kernel, P.smem())));
+        kernel<<<grid, kZmThreads, P.smem(), stream>>>(x, bhi, blo, nz, ncols, out, status, check_finite ? 1u : 0u);
+        note_launch();
+        check(cudaGetLastError(), "matrix kernel launch");
+    });
 }
 
 size_t capacity_for(uint64_t n, unsigned width) {
@@ -894,20 +865,23 @@ template <class T> struct CompressJob {
     }
 
     // Enqueues every kernel of the compression on `stream` (nothing syncs).
-    void enqueue(char* scratch, const uint16_t* rank, cudaStream_t stream) const {
+    // Enqueues every stage of the compression into `sink` (nothing syncs).
+    // The 9 result words go to `results` (default: inside the scratch).
+    void enqueue(char* scratch, const uint16_t* rank, Sink& sink, uint64_t* results = nullptr) const {
         Carver cv{scratch};
         const Plan P = plan(cv);
+        uint64_t* const layout = results ? results : P.layout;
         const double quantum = 1.5 * eb;
         const T q = T(quantum), inv = T(1.0 / quantum);
         const uint32_t chunks = wzp_chunks(uint32_t(n));
         const uint64_t words = (n + 31) / 32, cblocks = (words + kCompactWords - 1) / kCompactWords;
-        check(cudaMemsetAsync(P.sign, 0, reinterpret_cast<char*>(P.state + chunks) - reinterpret_cast<char*>(P.sign),
-                              stream), "memset");
+        sink.phase(PH_INIT);
+        sink.zero(P.sign, reinterpret_cast<char*>(P.state + chunks) - reinterpret_cast<char*>(P.sign));
 
-        StageClock& clock = stage_clock();
-        clock.begin(stream);
+        if (!sink.rec) stage_clock().begin(sink.stream);
         // 1. forward transform
-        forward<T>(g, in, P.C, P.lowA, P.lowB, P.inter, P.status, stream, opt.matrix);
+        sink.phase(PH_FORWARD);
+        forward<T>(g, in, P.C, P.lowA, P.lowB, P.inter, P.status, sink, opt.matrix);
         // 2. quantisation + Morton reorder: a field made of whole bricks (2^k
         // samples each) is quantised inside the WZP encoder, chunk by chunk;
         // otherwise a separate pass writes the Morton-packed magnitudes and
@@ -915,53 +889,57 @@ template <class T> struct CompressJob {
         const uint32_t bsz = 256 * g.bz;
         const bool fused = nx % 16 == 0 && ny % 16 == 0 && nz % g.bz == 0 && (bsz & (bsz - 1)) == 0 && bsz <= kChunk;
         if (!fused) {
+            sink.phase(PH_QUANT);
             QuantArgs<T> qa{P.C, Bricks::make(nx, ny, nz, g.bz), rank, q, inv, P.mag, P.sign, P.qbits, P.qval, P.status};
             const uint64_t bricks = qa.b.count();
             need(bricks < (1ull << 31), "Waltz: brick grid too large");
-            quantize_kernel<T><<<unsigned(bricks), kQuantThreads, 0, stream>>>(qa); note_launch();
-            check(cudaGetLastError(), "quantize launch");
-            clock.mark("quantize", stream);
+            sink.run<QuantizeOp<T>>(qa, uint32_t(bricks));
+            sink.mark("quantize");
         }
         // 3. WZP encode straight into the archive
         {
+            sink.phase(PH_ENCODE);
             WzpEncodeArgs wa{uint32_t(n), out + 32, capacity - 32, P.ticket, P.state, P.sizes, P.status, opt.spin_cap,
                              opt.skip_publish};
             if (fused) {
                 uint32_t lb = 0;
                 while ((1u << lb) < bsz) ++lb;
                 launch_wzp_encode(wa, QuantBricks<T>{P.C, nx, ny, g.bz, lb, rank, q, inv, P.qbits, P.qval, P.status},
-                                  chunks, stream);
+                                  chunks, sink);
             } else {
-                launch_wzp_encode(wa, MagArrays{P.mag, P.sign}, chunks, stream);
+                launch_wzp_encode(wa, MagArrays{P.mag, P.sign}, chunks, sink);
             }
+            sink.phase(PH_DIRECTORY);
             const uint32_t groups = wzp_groups(uint32_t(n));
-            wzp_directory_kernel<<<(groups + 255) / 256, 256, 0, stream>>>(out + 32, uint32_t(n), P.state, P.sizes,
-                                                                           P.wzp_total); note_launch();
-            check(cudaGetLastError(), "wzp directory launch");
+            sink.run<WzpDirectoryOp>(WzpDirectoryOp::Params{out + 32, uint32_t(n), P.state, P.sizes, P.wzp_total},
+                                     (groups + 255) / 256);
         }
-        clock.mark("wzp_encode", stream);
+        sink.mark("wzp_encode");
         // 4. inverse transform + repairs; fast-accept threshold of the repair
         // check (float): eb * (1 - 2^-21), rounded down
         {
+            sink.phase(PH_INVERSE);
             T safe = T(eb * (1.0 - std::ldexp(1.0, -21)));
             if (double(safe) > eb * (1.0 - std::ldexp(1.0, -21))) safe = std::nextafter(safe, T(0));
             RepairOut<T> fin{in, nx, size_t(nx) * ny, eb, T(eb), P.pbits, P.perr, P.status, safe};
-            inverse<T>(g, P.C, P.inter, P.bank2, fin, P.status, stream, "inv_l0_repair", opt.matrix);
+            inverse<T>(g, P.C, P.inter, P.bank2, fin, P.status, sink, "inv_l0_repair", opt.matrix);
         }
         // 5. ordered side records
-        const dim3 both(unsigned(cblocks), 2);
-        compact_count_kernel<<<both, kCompactThreads, 0, stream>>>(P.pbits, P.qbits, words, P.counts_p, P.counts_q);
-        note_launch();
-        compact_scan_layout_kernel<<<1, kCompactThreads, 0, stream>>>(
-            P.counts_p, P.counts_q, uint32_t(cblocks), P.wzp_total, P.status, out, capacity, sizeof(T),
-            uint8_t(g.flags(sizeof(T)) | (opt.matrix ? kMatrixFlag : 0)), uint8_t(g.lxy), uint8_t(g.lz),
-            uint8_t(g.bz), quantum, P.layout);
-        note_launch();
-        compact_write_kernel<T><<<both, kCompactThreads, 0, stream>>>(P.pbits, P.qbits, words, P.counts_p, P.counts_q,
-                                                                      P.perr, P.qval, out, P.layout, n);
-        note_launch();
-        check(cudaGetLastError(), "side record launch");
-        clock.mark("side_records", stream);
+        sink.phase(PH_SIDE);
+        const uint32_t both = uint32_t(2 * cblocks);
+        sink.run<CompactCountOp>(CompactCountOp::Params{P.pbits, P.qbits, words, P.counts_p, P.counts_q,
+                                                        uint32_t(cblocks)},
+                                 both);
+        sink.run<ScanLayoutOp>(ScanLayoutOp::Params{P.counts_p, P.counts_q, uint32_t(cblocks), P.wzp_total, P.status,
+                                                    out, capacity, uint32_t(sizeof(T)),
+                                                    uint8_t(g.flags(sizeof(T)) | (opt.matrix ? kMatrixFlag : 0)),
+                                                    uint8_t(g.lxy), uint8_t(g.lz), uint8_t(g.bz), quantum, layout},
+                               1);
+        sink.run<CompactWriteOp<T>>(typename CompactWriteOp<T>::Params{P.pbits, P.qbits, words, P.counts_p,
+                                                                       P.counts_q, P.perr, P.qval, out, layout, n,
+                                                                       uint32_t(cblocks)},
+                                    both);
+        sink.mark("side_records");
     }
 
     // Device address of the 9 result words inside this job's scratch.
@@ -993,7 +971,8 @@ static size_t compress(const T* d_in, uint32_t nx, uint32_t ny, uint32_t nz, dou
     const CompressJob<T> job = CompressJob<T>::make(d_in, nx, ny, nz, eb, d_out, capacity, opt);
     char* scratch = t_arena.reserve(job.scratch_bytes());
     const uint16_t* rank = t_fwd_tables.get(nx, ny, nz, job.g.bz, false, stream);
-    job.enqueue(scratch, rank, stream);
+    Sink sink{stream};
+    job.enqueue(scratch, rank, sink);
     uint64_t* h = pinned();
     check(cudaMemcpyAsync(h, job.result(scratch), 9 * 8, cudaMemcpyDeviceToHost, stream), "readback");
     check(cudaStreamSynchronize(stream), "compress");
@@ -1060,7 +1039,20 @@ static Layout validate_header(const Header& h, const Geometry& g, size_t bytes, 
 // Directory check: group spans must tile the payload exactly. The fast path
 // verifies canonical (increasing) order on the device; anything else is
 // checked on the host like cpu/src/wzp_cpu.cpp:720-761.
-__global__ void directory_check_kernel(JobRef job, uint32_t n, uint32_t* status) {
+struct DirectoryCheckOp {
+    static constexpr int kThreads = 256, kMinBlocks = 0; // no occupancy floor: the compiler picks the register budget
+    struct Params {
+        JobRef job;
+        uint32_t n;
+        uint32_t* status;
+    };
+    static __device__ __forceinline__ void run(const Params P, uint32_t, uint32_t);
+};
+
+__device__ __forceinline__ void DirectoryCheckOp::run(const Params P, uint32_t, uint32_t) {
+    const uint32_t n = P.n;
+    uint32_t* const status = P.status;
+    const JobRef& job = P.job;
     __shared__ uint32_t tmp[40];
     const DecodeJob J = job.get();
     const uint8_t* in = J.base + 32;
@@ -1133,22 +1125,13 @@ static DecodeJob decode_job(const uint8_t* d_in, const Header& h, const Layout& 
 // on a fixed grid, as the counts are only known on the device.
 template <class T, class Final, class Patch>
 static void decode_launch(const JobRef& job, bool matrix, const Geometry& g, const uint16_t* irank, T* C, T* bank1,
-                          T* bank2, const Final& fin, const Patch& patch, uint32_t* status, cudaStream_t stream) {
+                          T* bank2, const Final& fin, const Patch& patch, uint32_t* status, Sink& sink) {
     const uint32_t n = uint32_t(g.n);
-    StageClock& clock = stage_clock();
-    clock.begin(stream);
-    directory_check_kernel<<<1, 256, 0, stream>>>(job, n, status); note_launch();
+    if (!sink.rec) stage_clock().begin(sink.stream);
+    sink.phase(PH_DCHECK);
+    sink.run<DirectoryCheckOp>(DirectoryCheckOp::Params{job, n, status}, 1);
     {
-        static thread_local int cfg_dev = -1;
-        int dev = 0;
-        check(cudaGetDevice(&dev), "cudaGetDevice");
-        if (cfg_dev != dev) {
-            check(cudaFuncSetAttribute(wzp_decode_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       int(sizeof(WzpDecodeSmem))), "wzp smem");
-            check(cudaFuncSetAttribute(wzp_decode_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       int(sizeof(WzpDecodeSmem))), "wzp smem");
-            cfg_dev = dev;
-        }
+        sink.phase(PH_DECODE);
         BrickMap map{g.nx, g.ny, g.nz, g.bz, irank, false, 0};
         const uint32_t bsz = 256 * g.bz;
         if (g.nx % 16 == 0 && g.ny % 16 == 0 && g.nz % g.bz == 0 && (bsz & (bsz - 1)) == 0 && bsz <= kChunk &&
@@ -1156,25 +1139,24 @@ static void decode_launch(const JobRef& job, bool matrix, const Geometry& g, con
             map.fast = true;
             while ((1u << map.lb) < bsz) ++map.lb;
         }
-        WzpDecodeArgs<T> da{job, n, map, C, status};
-        wzp_decode_kernel<T><<<wzp_chunks(n), kWzpThreads, sizeof(WzpDecodeSmem), stream>>>(da); note_launch();
-        check(cudaGetLastError(), "wzp decode launch");
+        sink.run<WzpDecodeOp<T>>(WzpDecodeArgs<T>{job, n, map, C, status}, wzp_chunks(n), sizeof(WzpDecodeSmem));
     }
-    clock.mark("wzp_decode", stream);
-    const unsigned fixed = unsigned(std::min<uint64_t>((g.n + 255) / 256, 32));
+    sink.mark("wzp_decode");
+    const uint32_t fixed = uint32_t(std::min<uint64_t>((g.n + 255) / 256, 32));
     if (job.ptr || job.val.nq) {
-        qpatch_kernel<T><<<job.ptr ? fixed : (job.val.nq + 255) / 256, 256, 0, stream>>>(job, g.n, C, status);
-        note_launch();
+        sink.phase(PH_QPATCH);
+        sink.run<QPatchOp<T>>(typename QPatchOp<T>::Params{job, g.n, C, status},
+                              job.ptr ? fixed : (job.val.nq + 255) / 256);
     }
-    clock.mark("qpatch", stream);
-    inverse<T>(g, C, bank1, bank2, fin, status, stream, "inv_l0", matrix);
+    sink.mark("qpatch");
+    sink.phase(PH_DINVERSE);
+    inverse<T>(g, C, bank1, bank2, fin, status, sink, "inv_l0", matrix);
     if (job.ptr || job.val.np) {
-        rpatch_kernel<T, Patch><<<job.ptr ? fixed : (job.val.np + 255) / 256, 256, 0, stream>>>(job, g.n, patch,
-                                                                                                 status);
-        note_launch();
+        sink.phase(PH_RPATCH);
+        sink.run<RPatchOp<T, Patch>>(typename RPatchOp<T, Patch>::Params{job, g.n, patch, status},
+                                     job.ptr ? fixed : (job.val.np + 255) / 256);
     }
-    check(cudaGetLastError(), "decode launch");
-    clock.mark("rpatch", stream);
+    sink.mark("rpatch");
 }
 
 // Status word -> exception, with the exact checks that need the host: a
@@ -1256,8 +1238,9 @@ static void decompress(const uint8_t* d_in, size_t bytes, uint32_t nx, uint32_t 
     const uint16_t* irank = t_inv_tables.get(nx, ny, nz, g.bz, true, stream);
     check(cudaMemsetAsync(P.status, 0, 4, stream), "memset");
     FinalOut<T> fin{d_out, nx, size_t(nx) * ny, P.status};
+    Sink sink{stream};
     decode_launch<T>(JobRef{nullptr, decode_job(d_in, h, L)}, (h.flags & kMatrixFlag) != 0, g, irank, P.C, P.bank1,
-                     P.bank2, fin, RowPatch<T>{d_out}, P.status, stream);
+                     P.bank2, fin, RowPatch<T>{d_out}, P.status, sink);
     check(cudaMemcpyAsync(pin + 8, P.status, 4, cudaMemcpyDeviceToHost, stream), "readback");
     check(cudaStreamSynchronize(stream), "decompress");
     decode_finish<T>(uint32_t(pin[8]), d_in, h, L, g, P.status, P.seen, stream);
@@ -1293,8 +1276,17 @@ static void extrema(const T* d_in, uint64_t n, double* mn, double* mx, cudaStrea
 // kernel launches. The instantiated graph is kept and replayed while the
 // batch description (pointers, shapes, bounds) stays the same; all results
 // come back in one copy.
+// Batch execution of the calling thread's next captured batch graphs:
+// stage-batched (fields split round-robin into `width` groups, each group one
+// graph branch on which every stage is one batched launch per op type over
+// the group's fields), or field chains (each field's own launches, fields
+// round-robin on `width` branches).
 constexpr int kMaxBranches = 64;
-static thread_local int t_branches = 16; // parallel branches of the next captured batch graph
+struct BatchConfig {
+    int mode = WALTZ_B200_BATCH_FIELDS;
+    int width = 32;
+};
+static thread_local BatchConfig t_batch_cfg;
 
 struct BatchTables {
     struct Entry {
@@ -1357,7 +1349,8 @@ struct CachedGraph {
 };
 
 // Captures `body(work streams)` between a fork and a join of `branches`
-// parallel streams and replaces the cached graph with its instantiation.
+// parallel streams (or, with no branches, on the capture stream alone) and
+// replaces the cached graph with its instantiation.
 template <class Body>
 static void capture_batch(BatchStreams& bs, int branches, CachedGraph& cg, std::vector<unsigned char>&& key,
                           Body body) {
@@ -1367,12 +1360,16 @@ static void capture_batch(BatchStreams& bs, int branches, CachedGraph& cg, std::
     cudaGraph_t graph = nullptr;
     check(cudaStreamBeginCapture(bs.cap, cudaStreamCaptureModeThreadLocal), "begin capture");
     try {
-        check(cudaEventRecord(bs.fork, bs.cap), "fork");
-        for (int k = 0; k < branches; ++k) check(cudaStreamWaitEvent(bs.work[k], bs.fork, 0), "fork wait");
-        body(bs.work);
-        for (int k = 0; k < branches; ++k) {
-            check(cudaEventRecord(bs.join[k], bs.work[k]), "join");
-            check(cudaStreamWaitEvent(bs.cap, bs.join[k], 0), "join wait");
+        if (branches == 0) {
+            body(&bs.cap); // one chain on the capture stream
+        } else {
+            check(cudaEventRecord(bs.fork, bs.cap), "fork");
+            for (int k = 0; k < branches; ++k) check(cudaStreamWaitEvent(bs.work[k], bs.fork, 0), "fork wait");
+            body(bs.work);
+            for (int k = 0; k < branches; ++k) {
+                check(cudaEventRecord(bs.join[k], bs.work[k]), "join");
+                check(cudaStreamWaitEvent(bs.cap, bs.join[k], 0), "join wait");
+            }
         }
     } catch (...) {
         cudaStreamEndCapture(bs.cap, &graph);
@@ -1421,10 +1418,40 @@ template <class V> static void append_key(std::vector<unsigned char>& key, const
 
 struct BatchCompressState {
     CachedGraph graph;
-    Arena scratch;
+    Arena scratch, table;
     PinnedBuffer results;
     BatchTables tables;
 };
+
+// Records every field's stages and captures their stage-batched replay on
+// the capture stream; the parameter table is uploaded first and kept.
+template <class Enqueue>
+static void capture_stage_batched(BatchStreams& bs, int groups, CachedGraph& cg, Arena& table_arena,
+                                  std::vector<unsigned char>&& key, uint32_t count, Enqueue enqueue) {
+    groups = int(std::min<uint32_t>(uint32_t(groups), count));
+    std::vector<Recorder> recs(groups);
+    for (uint32_t i = 0; i < count; ++i) {
+        Recorder& rec = recs[i % uint32_t(groups)];
+        rec.begin_field();
+        Sink sink{bs.cap, &rec, true};
+        enqueue(i, sink);
+    }
+    std::vector<BatchPlan> plans;
+    std::vector<size_t> at;
+    size_t total = 0;
+    for (const Recorder& rec : recs) {
+        plans.push_back(BatchPlan::make(rec));
+        at.push_back(total);
+        total += (plans.back().bytes() + 255) & ~size_t(255);
+    }
+    unsigned char* table = reinterpret_cast<unsigned char*>(table_arena.reserve(total));
+    for (size_t g = 0; g < plans.size(); ++g)
+        check(cudaMemcpy(table + at[g], plans[g].host.data(), plans[g].bytes(), cudaMemcpyHostToDevice),
+              "batch table upload");
+    capture_batch(bs, groups == 1 ? 0 : groups, cg, std::move(key), [&](cudaStream_t* s) {
+        for (size_t g = 0; g < plans.size(); ++g) plans[g].execute(table + at[g], s[g]);
+    });
+}
 static thread_local BatchCompressState t_bc;
 
 template <class T>
@@ -1456,8 +1483,9 @@ static void compress_batch(const waltz_b200_chunk* items, uint32_t count, uint64
     std::vector<unsigned char> key(reinterpret_cast<const unsigned char*>(items),
                                    reinterpret_cast<const unsigned char*>(items + count));
     key.push_back(uint8_t(sizeof(T)));
-    const int branches = t_branches;
-    append_key(key, branches);
+    const BatchConfig cfg = t_batch_cfg;
+    append_key(key, cfg.mode);
+    append_key(key, cfg.width);
     char* base = st.scratch.reserve(total);
     append_key(key, base); // the scratch must not have moved since the graph was captured
     uint64_t* results = reinterpret_cast<uint64_t*>(base + results_at);
@@ -1465,14 +1493,19 @@ static void compress_batch(const waltz_b200_chunk* items, uint32_t count, uint64
         std::vector<const uint16_t*> rank(count);
         for (uint32_t i = 0; i < count; ++i)
             rank[i] = st.tables.get(jobs[i].nx, jobs[i].ny, jobs[i].nz, jobs[i].g.bz, false, bs.cap);
-        capture_batch(bs, branches, st.graph, std::move(key), [&](cudaStream_t* work) {
-            for (uint32_t i = 0; i < count; ++i) {
-                cudaStream_t w = work[i % branches];
-                jobs[i].enqueue(base + offset[i], rank[i], w);
-                check(cudaMemcpyAsync(results + 9 * size_t(i), jobs[i].result(base + offset[i]), 9 * 8,
-                                      cudaMemcpyDeviceToDevice, w), "result copy");
-            }
-        });
+        if (cfg.mode == WALTZ_B200_BATCH_STAGES) {
+            capture_stage_batched(bs, cfg.width, st.graph, st.table, std::move(key), count,
+                                  [&](uint32_t i, Sink& sink) {
+                                      jobs[i].enqueue(base + offset[i], rank[i], sink, results + 9 * size_t(i));
+                                  });
+        } else {
+            capture_batch(bs, cfg.width, st.graph, std::move(key), [&](cudaStream_t* work) {
+                for (uint32_t i = 0; i < count; ++i) {
+                    Sink sink{work[i % uint32_t(cfg.width)]};
+                    jobs[i].enqueue(base + offset[i], rank[i], sink, results + 9 * size_t(i));
+                }
+            });
+        }
     }
     check(cudaGraphLaunch(st.graph.exec, stream), "graph launch");
     uint64_t* host = st.results.get<uint64_t>(size_t(count) * 9);
@@ -1501,7 +1534,7 @@ __global__ void gather_headers_kernel(const uint8_t* const* archives, uint8_t* h
 
 struct BatchDecodeState {
     CachedGraph graph;
-    Arena scratch;
+    Arena scratch, table;
     PinnedBuffer stage; // job table, then archive pointers / headers / status words
     BatchTables tables;
 };
@@ -1545,12 +1578,15 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
         }
     }
     // Scratch: job table, status words, archive pointers, gathered headers,
-    // the duplicate-check bitmap, then C / bank1 / bank2 per branch, sized by
-    // the largest field on that branch.
-    const int branches = t_branches;
-    uint64_t branch_n[kMaxBranches] = {};
-    for (uint32_t i = 0; i < count; ++i)
-        branch_n[i % branches] = std::max<uint64_t>(branch_n[i % branches], list[i].g.n);
+    // the duplicate-check bitmap, then C / bank1 / bank2 per lane: one lane
+    // per field when stage-batched (all fields run at once), else one per
+    // branch sized by the largest field on it.
+    const BatchConfig cfg = t_batch_cfg;
+    const bool staged = cfg.mode == WALTZ_B200_BATCH_STAGES;
+    const uint32_t lanes = staged ? count : uint32_t(cfg.width);
+    auto lane_of = [&](uint32_t i) { return staged ? i : i % uint32_t(cfg.width); };
+    std::vector<uint64_t> lane_n(lanes, 0);
+    for (uint32_t i = 0; i < count; ++i) lane_n[lane_of(i)] = std::max<uint64_t>(lane_n[lane_of(i)], list[i].g.n);
     Carver plan{nullptr};
     auto carve = [&](Carver& c) {
         struct P {
@@ -1559,17 +1595,17 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
             const uint8_t** ptrs;
             uint8_t* headers;
             uint32_t* seen;
-            T *C[kMaxBranches], *b1[kMaxBranches], *b2[kMaxBranches];
+            std::vector<T*> C, b1, b2;
         } p;
         p.jobs = c.take<DecodeJob>(count);
         p.status = c.take<uint32_t>(count);
         p.ptrs = c.take<const uint8_t*>(count);
         p.headers = c.take<uint8_t>(size_t(count) * 32);
         p.seen = c.take<uint32_t>((max_n + 31) / 32 + 1);
-        for (int k = 0; k < branches; ++k) {
-            p.C[k] = c.take<T>(branch_n[k]);
-            p.b1[k] = c.take<T>(branch_n[k]);
-            p.b2[k] = c.take<T>(branch_n[k]);
+        for (uint32_t k = 0; k < lanes; ++k) {
+            p.C.push_back(c.take<T>(lane_n[k]));
+            p.b1.push_back(c.take<T>(lane_n[k]));
+            p.b2.push_back(c.take<T>(lane_n[k]));
         }
         return p;
     };
@@ -1620,7 +1656,8 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
 
     std::vector<unsigned char> key;
     key.push_back(uint8_t(sizeof(T)));
-    append_key(key, branches);
+    append_key(key, cfg.mode);
+    append_key(key, cfg.width);
     append_key(key, count);
     append_key(key, static_cast<const void*>(P.jobs));
     for (uint32_t i = 0; i < count; ++i) {
@@ -1638,17 +1675,25 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
             irank[i] = st.tables.get(g.nx, g.ny, g.nz, g.bz, true, bs.cap);
             if (list[i].h.flags & kMatrixFlag) t_zmat.get(g.nz, true, false, bs.cap); // upload before capture
         }
-        capture_batch(bs, branches, st.graph, std::move(key), [&](cudaStream_t* work) {
-            for (uint32_t i = 0; i < count; ++i) {
-                const int k = int(i % branches);
-                const Geometry& g = list[i].g;
-                const DecodeJob* job = P.jobs + i;
-                JobOut<T> fin{job, list[i].sy, list[i].sz, P.status + i};
-                JobPatch<T> patch{job, g.nx, g.ny, list[i].sy, list[i].sz};
-                decode_launch<T>(JobRef{job, {}}, (list[i].h.flags & kMatrixFlag) != 0, g, irank[i], P.C[k], P.b1[k],
-                                 P.b2[k], fin, patch, P.status + i, work[k]);
-            }
-        });
+        auto enqueue = [&](uint32_t i, Sink& sink) {
+            const uint32_t k = lane_of(i);
+            const Geometry& g = list[i].g;
+            const DecodeJob* job = P.jobs + i;
+            JobOut<T> fin{job, list[i].sy, list[i].sz, P.status + i};
+            JobPatch<T> patch{job, g.nx, g.ny, list[i].sy, list[i].sz};
+            decode_launch<T>(JobRef{job, {}}, (list[i].h.flags & kMatrixFlag) != 0, g, irank[i], P.C[k], P.b1[k],
+                             P.b2[k], fin, patch, P.status + i, sink);
+        };
+        if (staged) {
+            capture_stage_batched(bs, cfg.width, st.graph, st.table, std::move(key), count, enqueue);
+        } else {
+            capture_batch(bs, cfg.width, st.graph, std::move(key), [&](cudaStream_t* work) {
+                for (uint32_t i = 0; i < count; ++i) {
+                    Sink sink{work[i % uint32_t(cfg.width)]};
+                    enqueue(i, sink);
+                }
+            });
+        }
     }
     check(cudaGraphLaunch(st.graph.exec, stream), "graph launch");
     check(cudaMemcpyAsync(status, P.status, size_t(count) * 4, cudaMemcpyDeviceToHost, stream), "readback");
@@ -1738,11 +1783,14 @@ int waltz_b200_compress_batch(const waltz_b200_chunk* chunks, uint32_t count, in
     }
 }
 
-int waltz_b200_batch_branches(int branches) {
+int waltz_b200_batch_config(int mode, int width) {
     using namespace wb;
-    const int prev = t_branches;
-    if (branches >= 1 && branches <= kMaxBranches) t_branches = branches;
-    return prev;
+    if ((mode != WALTZ_B200_BATCH_STAGES && mode != WALTZ_B200_BATCH_FIELDS) || width < 1 || width > kMaxBranches) {
+        std::snprintf(t_error, sizeof(t_error), "invalid batch configuration (mode %d, width %d)", mode, width);
+        return -1;
+    }
+    t_batch_cfg = BatchConfig{mode, width};
+    return 0;
 }
 
 int waltz_b200_decompress_batch(const waltz_b200_archive* archives, uint32_t count, int width, void* stream) {
@@ -1832,11 +1880,13 @@ extern "C" int waltz_b200_transform(void* d_data, int width, uint32_t nx, uint32
             auto P = plan(real);
             check(cudaMemsetAsync(P.status, 0, 4, s), "memset");
             if (!inverse) {
-                forward<T>(g, data, P.C, P.a, P.b, P.inter, P.status, s);
+                Sink sink{s};
+                forward<T>(g, data, P.C, P.a, P.b, P.inter, P.status, sink);
                 check(cudaMemcpyAsync(data, P.C, g.n * sizeof(T), cudaMemcpyDeviceToDevice, s), "copy");
             } else {
                 check(cudaMemcpyAsync(P.C, data, g.n * sizeof(T), cudaMemcpyDeviceToDevice, s), "copy");
-                wb::inverse<T>(g, P.C, P.inter, P.bank2, StoreOut<T>{data, nx, size_t(nx) * ny}, P.status, s);
+                Sink sink{s};
+                wb::inverse<T>(g, P.C, P.inter, P.bank2, StoreOut<T>{data, nx, size_t(nx) * ny}, P.status, sink);
             }
             uint32_t st = 0;
             check(cudaMemcpyAsync(&st, P.status, 4, cudaMemcpyDeviceToHost, s), "readback");
@@ -1875,11 +1925,11 @@ extern "C" int waltz_b200_wzp_encode(const uint16_t* d_mag, const uint32_t* d_si
         check(cudaMemsetAsync(P.state, 0, size_t(chunks) * 8, s), "memset");
         WzpEncodeArgs wa{n, static_cast<uint8_t*>(d_out), capacity, P.ticket, P.state, P.sizes, P.status, 1u << 22,
                          0xffffffffu};
-        launch_wzp_encode(wa, MagArrays{d_mag, d_sign}, chunks, s);
+        Sink sink{s};
+        launch_wzp_encode(wa, MagArrays{d_mag, d_sign}, chunks, sink);
         const uint32_t groups = wzp_groups(n);
-        wzp_directory_kernel<<<(groups + 255) / 256, 256, 0, s>>>(static_cast<uint8_t*>(d_out), n, P.state, P.sizes,
-                                                                  P.total); note_launch();
-        check(cudaGetLastError(), "wzp launch");
+        sink.run<WzpDirectoryOp>(WzpDirectoryOp::Params{static_cast<uint8_t*>(d_out), n, P.state, P.sizes, P.total},
+                                 (groups + 255) / 256);
         uint64_t* h = pinned();
         check(cudaMemcpyAsync(h, P.total, 8, cudaMemcpyDeviceToHost, s), "readback");
         check(cudaMemcpyAsync(h + 1, P.status, 4, cudaMemcpyDeviceToHost, s), "readback");
@@ -1950,10 +2000,10 @@ extern "C" int waltz_b200_wzp_encode_noalloc(const uint16_t* d_mag, const uint32
         check(cudaMemsetAsync(state, 0, size_t(chunks) * 8, s), "memset");
         WzpEncodeArgs wa{n, static_cast<uint8_t*>(d_out), capacity, ticket, state, sizes, status, 1u << 22,
                          0xffffffffu};
-        launch_wzp_encode(wa, MagArrays{d_mag, d_sign}, chunks, s);
-        wzp_directory_kernel<<<(groups + 255) / 256, 256, 0, s>>>(static_cast<uint8_t*>(d_out), n, state, sizes,
-                                                                  total); note_launch();
-        check(cudaGetLastError(), "wzp launch");
+        Sink sink{s};
+        launch_wzp_encode(wa, MagArrays{d_mag, d_sign}, chunks, sink);
+        sink.run<WzpDirectoryOp>(WzpDirectoryOp::Params{static_cast<uint8_t*>(d_out), n, state, sizes, total},
+                                 (groups + 255) / 256);
         uint64_t host[2] = {0, 0}; // pageable: the copy completes before cudaMemcpyAsync returns
         check(cudaMemcpyAsync(host, base, 16, cudaMemcpyDeviceToHost, s), "readback");
         check(cudaStreamSynchronize(s), "wzp encode");
@@ -1984,7 +2034,8 @@ extern "C" int waltz_b200_zmatrix(float* d_data, uint32_t nx, uint32_t ny, uint3
         Carver real{t_arena.reserve(cv.used)};
         auto P = plan(real);
         check(cudaMemsetAsync(P.status, 0, 4, s), "memset");
-        zmatrix_apply(d_data, nx, ny, nz, inverse != 0, ZmStore<float>{P.out}, P.status, false, s);
+        Sink sink{s};
+        zmatrix_apply(d_data, nx, ny, nz, inverse != 0, ZmStore<float>{P.out}, P.status, false, sink);
         check(cudaMemcpyAsync(d_data, P.out, n * 4, cudaMemcpyDeviceToDevice, s), "copy");
         uint32_t st = 0;
         check(cudaMemcpyAsync(&st, P.status, 4, cudaMemcpyDeviceToHost, s), "readback");

@@ -56,17 +56,36 @@ template <class T> struct InvLevel {
     Dims a;         // level dims
 };
 
+template <class T, int UX, int UY, int UZ, class Out> struct InvTileOp {
+    static constexpr int kThreads = 256, kMinBlocks = 2;
+    static constexpr bool kGridConstant = true;
+    struct Params {
+        CUtensorMap cmap, lmap;
+        InvLevel<T> lv;
+        uint32_t tiles_x, tiles_y;
+        Out out;
+        uint32_t* status;
+    };
+    static __device__ __forceinline__ void run(const Params& P, uint32_t block, uint32_t);
+    static __device__ __forceinline__ void acquire_maps(const Params& P) {
+        tensormap_acquire(&P.cmap);
+        if (P.lv.low) tensormap_acquire(&P.lmap);
+    }
+};
+
 template <class T, int UX, int UY, int UZ, class Out>
-__global__ void __launch_bounds__(256, 2)
-    inv_tile_kernel(InvLevel<T> lv, const __grid_constant__ CUtensorMap cmap, const __grid_constant__ CUtensorMap lmap,
-                    uint32_t tiles_x, uint32_t tiles_y, Out out, uint32_t* status) {
+__device__ __forceinline__ void InvTileOp<T, UX, UY, UZ, Out>::run(const Params& P, uint32_t block, uint32_t) {
+    const InvLevel<T> lv = P.lv;
+    const uint32_t tiles_x = P.tiles_x, tiles_y = P.tiles_y;
+    const Out out = P.out;
+    uint32_t* const status = P.status;
     using S = InvShape<T, UX, UY, UZ>;
     extern __shared__ __align__(128) unsigned char inv_smem[];
     T* Bx = reinterpret_cast<T*>(inv_smem + ((128 - (smem_u32(inv_smem) & 127)) & 127));
     uint64_t* bar = reinterpret_cast<uint64_t*>(Bx + 8 * S::BOX);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const Dims a = lv.a;
-    const uint32_t bx = blockIdx.x % tiles_x, by = (blockIdx.x / tiles_x) % tiles_y, bz = blockIdx.x / (tiles_x * tiles_y);
+    const uint32_t bx = block % tiles_x, by = (block / tiles_x) % tiles_y, bz = block / (tiles_x * tiles_y);
     const uint32_t ox = bx * UX, oy = by * UY, oz = bz * UZ;
     const uint32_t hx = half_len(a.x), hy = half_len(a.y), hz = half_len(a.z);
 
@@ -86,7 +105,7 @@ __global__ void __launch_bounds__(256, 2)
         for (int b = 0; b < 8; ++b) {
             const int xp = b & 1, yp = (b >> 1) & 1, zp = b >> 2;
             const bool from_low = b == 0 && lv.low != nullptr;
-            tma_load_3d(Bx + b * S::BOX, from_low ? &lmap : &cmap, x0 + (xp ? int(hx) : 0), y0 + (yp ? int(hy) : 0),
+            tma_load_3d(Bx + b * S::BOX, from_low ? &P.lmap : &P.cmap, x0 + (xp ? int(hx) : 0), y0 + (yp ? int(hy) : 0),
                         z0 + (zp ? int(hz) : 0), bar);
         }
     }

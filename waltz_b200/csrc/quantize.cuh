@@ -83,12 +83,18 @@ __device__ __forceinline__ T quantize_one(T c, T inv, T q, int32_t& m, bool& neg
     return Lift<T>::mul(T(neg ? -m : m), q);
 }
 
+template <class T> struct QuantizeOp {
+    static constexpr int kThreads = kQuantThreads, kMinBlocks = 0; // no occupancy floor: the compiler picks the register budget
+    using Params = QuantArgs<T>;
+    static __device__ __forceinline__ void run(const Params P, uint32_t block, uint32_t);
+};
+
 template <class T>
-__global__ void __launch_bounds__(kQuantThreads) quantize_kernel(QuantArgs<T> A) {
+__device__ __forceinline__ void QuantizeOp<T>::run(const Params A, uint32_t block, uint32_t) {
     __shared__ __align__(16) uint16_t smag[kChunk];
     __shared__ __align__(16) uint8_t ssign[kChunk];
     const Bricks& B = A.b;
-    const uint64_t bi = blockIdx.x;
+    const uint64_t bi = block;
     const uint32_t bxi = uint32_t(bi % B.nbx), byi = uint32_t((bi / B.nbx) % B.nby), bzi = uint32_t(bi / (uint64_t(B.nbx) * B.nby));
     const uint32_t ex = min(16u, B.nx - bxi * 16), ey = min(16u, B.ny - byi * 16), ez = min(B.bz, B.nz - bzi * B.bz);
     const uint32_t slot = (ex != 16) | ((ey != 16) << 1) | ((ez != B.bz) << 2);
@@ -153,24 +159,24 @@ __global__ void __launch_bounds__(kQuantThreads) quantize_kernel(QuantArgs<T> A)
 }
 
 // Copy with a finiteness check (zero-level transform: coefficients = input).
-template <class T>
-__global__ void copy_finite_kernel(const T* in, T* out, uint64_t n, uint32_t* status) {
-    bool bad = false;
-    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
-        const T v = in[i];
-        bad |= !finite_bits(v);
-        out[i] = v;
+template <class T> struct CopyFiniteOp {
+    static constexpr int kThreads = 256, kMinBlocks = 0; // no occupancy floor: the compiler picks the register budget
+    struct Params {
+        const T* in;
+        T* out;
+        uint64_t n;
+        uint32_t* status;
+    };
+    static __device__ __forceinline__ void run(const Params P, uint32_t block, uint32_t blocks) {
+        bool bad = false;
+        for (uint64_t i = block * uint64_t(kThreads) + threadIdx.x; i < P.n; i += uint64_t(blocks) * kThreads) {
+            const T v = P.in[i];
+            bad |= !finite_bits(v);
+            P.out[i] = v;
+        }
+        if (bad) atomicOr(P.status, ST_NONFINITE_INPUT);
     }
-    if (bad) atomicOr(status, ST_NONFINITE_INPUT);
-}
-
-template <class T>
-__global__ void check_finite_kernel(const T* in, uint64_t n, uint32_t* status) {
-    bool bad = false;
-    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
-        bad |= !finite_bits(in[i]);
-    if (bad) atomicOr(status, ST_NONFINITE_INPUT);
-}
+};
 
 // Encoder repair emitter for the finest synthesis: err = T(value - orig);
 // a sample is patched iff |err| > T(eb); the corrected value must be finite
@@ -248,29 +254,42 @@ template <class T> struct JobOut {
 // (index, value) records: pass 1 counts per block, pass 2 scans the block
 // counts (single CTA) and lays out the archive, pass 3 writes. Ordered by
 // construction, no sort. Both record lists (repair records, q-outliers) go
-// through each pass together: blockIdx.y selects the list.
+// through each pass together: the second half of the grid takes the
+// q-outlier list.
 constexpr int kCompactThreads = 256;
 constexpr int kCompactWords = kCompactThreads * 4; // bitmap words per block
 
-__global__ void compact_count_kernel(const uint32_t* pbits, const uint32_t* qbits, uint64_t words, uint32_t* counts_p,
-                                     uint32_t* counts_q) {
-    __shared__ uint32_t tmp[40];
-    const uint32_t* bits = blockIdx.y ? qbits : pbits;
-    const uint64_t w0 = uint64_t(blockIdx.x) * kCompactWords + threadIdx.x * 4;
-    uint32_t c = 0;
-    for (int k = 0; k < 4; ++k)
-        if (w0 + k < words) c += __popc(bits[w0 + k]);
-    const uint32_t total = block_sum<kCompactThreads>(c, tmp);
-    if (threadIdx.x == 0) (blockIdx.y ? counts_q : counts_p)[blockIdx.x] = total;
-}
+// Grid: 2 x cblocks blocks, the second half on the q-outlier list.
+struct CompactCountOp {
+    static constexpr int kThreads = kCompactThreads, kMinBlocks = 0; // no occupancy floor: the compiler picks the register budget
+    struct Params {
+        const uint32_t *pbits, *qbits;
+        uint64_t words;
+        uint32_t *counts_p, *counts_q;
+        uint32_t cblocks;
+    };
+    static __device__ __forceinline__ void run(const Params P, uint32_t block, uint32_t) {
+        __shared__ uint32_t tmp[40];
+        const bool q = block >= P.cblocks;
+        const uint32_t bx = q ? block - P.cblocks : block;
+        const uint32_t* bits = q ? P.qbits : P.pbits;
+        const uint64_t w0 = uint64_t(bx) * kCompactWords + threadIdx.x * 4;
+        uint32_t c = 0;
+        for (int k = 0; k < 4; ++k)
+            if (w0 + k < P.words) c += __popc(bits[w0 + k]);
+        const uint32_t total = block_sum<kCompactThreads>(c, tmp);
+        if (threadIdx.x == 0) (q ? P.counts_q : P.counts_p)[bx] = total;
+    }
+};
 
 // Record sink: indices as u32 LE, values of sizeof(V) bytes, both at
 // device-side offsets inside the archive (given by `layout`).
 template <class V>
-__device__ __forceinline__ void compact_write_block(const uint32_t* bits, uint64_t words, const uint32_t* offsets,
-                                                    const V* values, uint8_t* archive, const uint64_t* layout,
-                                                    int idx_slot, int val_slot, uint64_t cap_records, uint32_t* tmp) {
-    const uint64_t w0 = uint64_t(blockIdx.x) * kCompactWords + threadIdx.x * 4;
+__device__ __forceinline__ void compact_write_block(uint32_t bx, const uint32_t* bits, uint64_t words,
+                                                    const uint32_t* offsets, const V* values, uint8_t* archive,
+                                                    const uint64_t* layout, int idx_slot, int val_slot,
+                                                    uint64_t cap_records, uint32_t* tmp) {
+    const uint64_t w0 = uint64_t(bx) * kCompactWords + threadIdx.x * 4;
     uint32_t wv[4];
     uint32_t c = 0;
     for (int k = 0; k < 4; ++k) {
@@ -278,7 +297,7 @@ __device__ __forceinline__ void compact_write_block(const uint32_t* bits, uint64
         c += __popc(wv[k]);
     }
     uint32_t total;
-    uint32_t r = offsets[blockIdx.x] + block_excl_scan<kCompactThreads>(c, tmp, total);
+    uint32_t r = offsets[bx] + block_excl_scan<kCompactThreads>(c, tmp, total);
     if (layout[7]) return; // layout overflow: nothing is written
     uint8_t* idx = archive + layout[idx_slot];
     uint8_t* val = archive + layout[val_slot];
@@ -299,26 +318,63 @@ __device__ __forceinline__ void compact_write_block(const uint32_t* bits, uint64
         }
 }
 
-template <class T>
-__global__ void compact_write_kernel(const uint32_t* pbits, const uint32_t* qbits, uint64_t words,
-                                     const uint32_t* offsets_p, const uint32_t* offsets_q, const T* perr,
-                                     const uint32_t* qval, uint8_t* archive, const uint64_t* layout,
-                                     uint64_t cap_records) {
-    __shared__ uint32_t tmp[40];
-    if (blockIdx.y == 0)
-        compact_write_block<T>(pbits, words, offsets_p, perr, archive, layout, 0, 1, cap_records, tmp);
-    else
-        compact_write_block<uint32_t>(qbits, words, offsets_q, qval, archive, layout, 2, 3, cap_records, tmp);
-}
+// Grid: 2 x cblocks blocks, the second half on the q-outlier list.
+template <class T> struct CompactWriteOp {
+    static constexpr int kThreads = kCompactThreads, kMinBlocks = 0; // no occupancy floor: the compiler picks the register budget
+    struct Params {
+        const uint32_t *pbits, *qbits;
+        uint64_t words;
+        const uint32_t *offsets_p, *offsets_q;
+        const T* perr;
+        const uint32_t* qval;
+        uint8_t* archive;
+        const uint64_t* layout;
+        uint64_t cap_records;
+        uint32_t cblocks;
+    };
+    static __device__ __forceinline__ void run(const Params P, uint32_t block, uint32_t) {
+        __shared__ uint32_t tmp[40];
+        if (block < P.cblocks)
+            compact_write_block<T>(block, P.pbits, P.words, P.offsets_p, P.perr, P.archive, P.layout, 0, 1,
+                                   P.cap_records, tmp);
+        else
+            compact_write_block<uint32_t>(block - P.cblocks, P.qbits, P.words, P.offsets_q, P.qval, P.archive,
+                                          P.layout, 2, 3, P.cap_records, tmp);
+    }
+};
 
 // Exclusive scan of both lists' block counts in place, then the archive
 // layout from the totals. layout[]: 0 pi, 1 pv, 2 qi, 3 qv, 4 end, 5 np,
 // 6 nq, 7 overflow flag, 8 the pipeline's status word. Also writes the
 // 32-byte header and zeroes every padding byte between sections.
-__global__ void compact_scan_layout_kernel(uint32_t* counts_p, uint32_t* counts_q, uint32_t count,
-                                           const uint64_t* wzp_total, const uint32_t* status, uint8_t* archive,
-                                           size_t capacity, uint32_t width, uint8_t flags, uint8_t lxy, uint8_t lz,
-                                           uint8_t bz, double quantum, uint64_t* layout) {
+struct ScanLayoutOp {
+    static constexpr int kThreads = kCompactThreads, kMinBlocks = 0; // no occupancy floor: the compiler picks the register budget
+    struct Params {
+        uint32_t *counts_p, *counts_q;
+        uint32_t count;
+        const uint64_t* wzp_total;
+        const uint32_t* status;
+        uint8_t* archive;
+        size_t capacity;
+        uint32_t width;
+        uint8_t flags, lxy, lz, bz;
+        double quantum;
+        uint64_t* layout;
+    };
+    static __device__ __forceinline__ void run(const Params P, uint32_t, uint32_t);
+};
+
+__device__ __forceinline__ void ScanLayoutOp::run(const Params P, uint32_t, uint32_t) {
+    uint32_t* const counts_p = P.counts_p;
+    uint32_t* const counts_q = P.counts_q;
+    const uint32_t count = P.count, width = P.width;
+    const uint64_t* wzp_total = P.wzp_total;
+    const uint32_t* status = P.status;
+    uint8_t* const archive = P.archive;
+    const size_t capacity = P.capacity;
+    const uint8_t flags = P.flags, lxy = P.lxy, lz = P.lz, bz = P.bz;
+    const double quantum = P.quantum;
+    uint64_t* const layout = P.layout;
     __shared__ uint32_t tmp[40];
     uint32_t totals[2];
     for (int list = 0; list < 2; ++list) {
@@ -377,12 +433,26 @@ __global__ void compact_scan_layout_kernel(uint32_t* counts_p, uint32_t* counts_
 // duplicate check) and patches q-outliers: coeff = +-T(v) * q with the sign of
 // the clamped value already in place. Grid-stride over the archive's count,
 // which a graph-replayed launch reads from device memory.
+template <class T> struct QPatchOp {
+    static constexpr int kThreads = 256, kMinBlocks = 0; // no occupancy floor: the compiler picks the register budget
+    struct Params {
+        JobRef job;
+        uint64_t n;
+        T* coeff;
+        uint32_t* status;
+    };
+    static __device__ __forceinline__ void run(const Params P, uint32_t block, uint32_t blocks);
+};
+
 template <class T>
-__global__ void qpatch_kernel(JobRef job, uint64_t n, T* coeff, uint32_t* status) {
-    const DecodeJob J = job.get();
+__device__ __forceinline__ void QPatchOp<T>::run(const Params P, uint32_t block, uint32_t blocks) {
+    const uint64_t n = P.n;
+    T* const coeff = P.coeff;
+    uint32_t* const status = P.status;
+    const DecodeJob J = P.job.get();
     const uint8_t *qi = J.base + J.qi, *qv = J.base + J.qv;
     const T q = T(J.q);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < J.nq; i += gridDim.x * blockDim.x) {
+    for (uint32_t i = block * kThreads + threadIdx.x; i < J.nq; i += blocks * kThreads) {
         uint32_t at, v, prev = 0;
         memcpy(&at, qi + 4 * uint64_t(i), 4);
         memcpy(&v, qv + 4 * uint64_t(i), 4);
@@ -412,11 +482,25 @@ template <class T> struct JobPatch {
 };
 
 // Repair records: validate, then out[i] -= err (after synthesis).
+template <class T, class Patch> struct RPatchOp {
+    static constexpr int kThreads = 256, kMinBlocks = 0; // no occupancy floor: the compiler picks the register budget
+    struct Params {
+        JobRef job;
+        uint64_t n;
+        Patch patch;
+        uint32_t* status;
+    };
+    static __device__ __forceinline__ void run(const Params P, uint32_t block, uint32_t blocks);
+};
+
 template <class T, class Patch>
-__global__ void rpatch_kernel(JobRef job, uint64_t n, Patch patch, uint32_t* status) {
-    const DecodeJob J = job.get();
+__device__ __forceinline__ void RPatchOp<T, Patch>::run(const Params P, uint32_t block, uint32_t blocks) {
+    const uint64_t n = P.n;
+    const Patch patch = P.patch;
+    uint32_t* const status = P.status;
+    const DecodeJob J = P.job.get();
     const uint8_t *pi = J.base + J.pi, *pv = J.base + J.pv;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < J.np; i += gridDim.x * blockDim.x) {
+    for (uint32_t i = block * kThreads + threadIdx.x; i < J.np; i += blocks * kThreads) {
         uint32_t at, prev = 0;
         T err;
         memcpy(&at, pi + 4 * uint64_t(i), 4);

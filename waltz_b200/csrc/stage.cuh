@@ -70,17 +70,34 @@ __device__ __forceinline__ void load_window(int64_t s, uint32_t m, T (&e)[P], T 
 // lifts lines of length z[l]; high bands go to `dst` at their split
 // positions, low bands stay in shared memory for the next level; the last
 // level writes both. With `status`, the input is checked for finiteness.
+template <class T> struct ZStageFwdOp {
+    static constexpr int kThreads = kZStageThreads, kMinBlocks = 0; // no occupancy floor: the compiler picks the register budget
+    struct Params {
+        const T* in;
+        size_t sy, sz;
+        uint32_t nx, ny, nz;
+        StageLevels lv;
+        T* dst;
+        uint32_t* status;
+    };
+    static __device__ __forceinline__ void run(const Params P, uint32_t block, uint32_t);
+};
+
 template <class T>
-__global__ void __launch_bounds__(kZStageThreads) zstage_fwd_kernel(const T* in, size_t sy, size_t sz, uint32_t nx,
-                                                                     uint32_t ny, uint32_t nz, StageLevels lv,
-                                                                     T* dst, uint32_t* status) {
+__device__ __forceinline__ void ZStageFwdOp<T>::run(const Params Pm, uint32_t block, uint32_t) {
+    const T* in = Pm.in;
+    const size_t sy = Pm.sy, sz = Pm.sz;
+    const uint32_t nx = Pm.nx, ny = Pm.ny, nz = Pm.nz;
+    const StageLevels& lv = Pm.lv;
+    T* const dst = Pm.dst;
+    uint32_t* const status = Pm.status;
     constexpr int CX = ZCols<T>::CX, C = ZCols<T>::C;
     constexpr int W = 16, P = W / 2 + 4;
     extern __shared__ __align__(16) unsigned char zstage_raw[];
     T* buf[2] = {reinterpret_cast<T*>(zstage_raw), reinterpret_cast<T*>(zstage_raw) + size_t(C) * nz};
     const uint32_t tiles_x = (nx + CX - 1) / CX;
     const int c = threadIdx.x % C;
-    const uint32_t x = (blockIdx.x % tiles_x) * CX + c % CX, y = (blockIdx.x / tiles_x) * ZCols<T>::CY + c / CX;
+    const uint32_t x = (block % tiles_x) * CX + c % CX, y = (block / tiles_x) * ZCols<T>::CY + c / CX;
     const bool live = x < nx && y < ny;
     const size_t col = size_t(y) * sy + x;
     bool bad = false;
@@ -120,17 +137,32 @@ __global__ void __launch_bounds__(kZStageThreads) zstage_fwd_kernel(const T* in,
 // level l reads one buffer and writes its spatial output over the low part of
 // the other, which is the next finer level's low band. The finest level hands
 // every sample to `out`.
+template <class T, class Out> struct ZStageInvOp {
+    static constexpr int kThreads = kZStageThreads, kMinBlocks = 0; // no occupancy floor: the compiler picks the register budget
+    struct Params {
+        const T* coef;
+        size_t sy, sz;
+        uint32_t nx, ny, nz;
+        StageLevels lv;
+        Out out;
+    };
+    static __device__ __forceinline__ void run(const Params P, uint32_t block, uint32_t);
+};
+
 template <class T, class Out>
-__global__ void __launch_bounds__(kZStageThreads) zstage_inv_kernel(const T* coef, size_t sy, size_t sz, uint32_t nx,
-                                                                     uint32_t ny, uint32_t nz, StageLevels lv,
-                                                                     Out out) {
+__device__ __forceinline__ void ZStageInvOp<T, Out>::run(const Params Pm, uint32_t block, uint32_t) {
+    const T* coef = Pm.coef;
+    const size_t sy = Pm.sy, sz = Pm.sz;
+    const uint32_t nx = Pm.nx, ny = Pm.ny, nz = Pm.nz;
+    const StageLevels& lv = Pm.lv;
+    const Out out = Pm.out;
     constexpr int CX = ZCols<T>::CX, C = ZCols<T>::C;
     constexpr int W = inverse_zwin<T>(), P = W / 2 + 4;
     extern __shared__ __align__(16) unsigned char zstage_raw[];
     T* buf[2] = {reinterpret_cast<T*>(zstage_raw), reinterpret_cast<T*>(zstage_raw) + size_t(C) * nz};
     const uint32_t tiles_x = (nx + CX - 1) / CX;
     const int c = threadIdx.x % C;
-    const uint32_t x = (blockIdx.x % tiles_x) * CX + c % CX, y = (blockIdx.x / tiles_x) * ZCols<T>::CY + c / CX;
+    const uint32_t x = (block % tiles_x) * CX + c % CX, y = (block / tiles_x) * ZCols<T>::CY + c / CX;
     const bool live = x < nx && y < ny;
     const size_t col = size_t(y) * sy + x;
     for (uint32_t z = threadIdx.x / C; z < nz; z += kZStageThreads / C) {
@@ -173,16 +205,34 @@ __global__ void __launch_bounds__(kZStageThreads) zstage_inv_kernel(const T* coe
 // lifting (Q -> P in the level's split layout), then the high bands (all of
 // the box at the last level) are copied out row by row; the low corner of P
 // is the next level's input. With `status`, the input is checked.
+template <class T> struct XYStageFwdOp {
+    static constexpr int kThreads = kXYStageThreads, kMinBlocks = 0; // no occupancy floor: the compiler picks the register budget
+    struct Params {
+        const T* in;
+        size_t sy, sz;
+        uint32_t nx, ny;
+        StageLevels lv;
+        T* dst;
+        size_t dsy, dsz;
+        uint32_t* status;
+    };
+    static __device__ __forceinline__ void run(const Params Pm, uint32_t block, uint32_t);
+};
+
 template <class T>
-__global__ void __launch_bounds__(kXYStageThreads) xystage_fwd_kernel(const T* in, size_t sy, size_t sz, uint32_t nx,
-                                                                       uint32_t ny, StageLevels lv, T* dst,
-                                                                       size_t dsy, size_t dsz, uint32_t* status) {
+__device__ __forceinline__ void XYStageFwdOp<T>::run(const Params Pm, uint32_t block, uint32_t) {
+    const T* in = Pm.in;
+    const size_t sy = Pm.sy, sz = Pm.sz, dsy = Pm.dsy, dsz = Pm.dsz;
+    const uint32_t nx = Pm.nx, ny = Pm.ny;
+    const StageLevels& lv = Pm.lv;
+    T* const dst = Pm.dst;
+    uint32_t* const status = Pm.status;
     constexpr int W = 16, P = W / 2 + 4;
     extern __shared__ __align__(16) unsigned char xystage_raw[];
     const uint32_t PX = xy_pitch(nx);
     T* Pb = reinterpret_cast<T*>(xystage_raw);
     T* Qb = Pb + size_t(PX) * ny;
-    const uint32_t z = blockIdx.x;
+    const uint32_t z = block;
     const T* plane = in + size_t(z) * sz;
     bool bad = false;
     for (uint32_t i = threadIdx.x; i < nx * ny; i += kXYStageThreads) {
@@ -246,16 +296,32 @@ __global__ void __launch_bounds__(kXYStageThreads) xystage_fwd_kernel(const T* i
 // (coarsest first): X lifting of the box's coefficient rows (P -> Q), then Y
 // lifting of Q's columns read through the split layout, written spatially
 // over P's box (the next finer level's low corner), or to `out` at level 0.
+template <class T, class Out> struct XYStageInvOp {
+    static constexpr int kThreads = kXYStageThreads, kMinBlocks = 0; // no occupancy floor: the compiler picks the register budget
+    struct Params {
+        const T* coef;
+        size_t sy, sz;
+        uint32_t nx, ny;
+        StageLevels lv;
+        Out out;
+    };
+    static __device__ __forceinline__ void run(const Params Pm, uint32_t block, uint32_t);
+};
+
 template <class T, class Out>
-__global__ void __launch_bounds__(kXYStageThreads) xystage_inv_kernel(const T* coef, size_t sy, size_t sz, uint32_t nx,
-                                                                       uint32_t ny, StageLevels lv, Out out) {
+__device__ __forceinline__ void XYStageInvOp<T, Out>::run(const Params Pm, uint32_t block, uint32_t) {
+    const T* coef = Pm.coef;
+    const size_t sy = Pm.sy, sz = Pm.sz;
+    const uint32_t nx = Pm.nx, ny = Pm.ny;
+    const StageLevels& lv = Pm.lv;
+    const Out out = Pm.out;
     constexpr int WX = 16, PXW = WX / 2 + 4;
     constexpr int WY = 8, PYW = WY / 2 + 4;
     extern __shared__ __align__(16) unsigned char xystage_raw[];
     const uint32_t PX = xy_pitch(nx);
     T* Pb = reinterpret_cast<T*>(xystage_raw);
     T* Qb = Pb + size_t(PX) * ny;
-    const uint32_t z = blockIdx.x;
+    const uint32_t z = block;
     const T* plane = coef + size_t(z) * sz;
     for (uint32_t i = threadIdx.x; i < nx * ny; i += kXYStageThreads) {
         const uint32_t y = i / nx, x = i - y * nx;

@@ -65,10 +65,31 @@ __device__ __forceinline__ bool nonfinite_max(unsigned long long m) { return m >
 // Tma: stage planes with per-plane tensor-map boxes; otherwise with batched
 // ordinary loads. `status` receives ST_WAIT_TIMEOUT if a copy never
 // completes within the wait bound (the block then stops as a whole).
+template <class T, int UX, int UY, int Q, bool Tma> struct FwdStreamOp {
+    static constexpr int kThreads = 256, kMinBlocks = 3;
+    static constexpr bool kGridConstant = true;
+    struct Params {
+        CUtensorMap map;
+        FwdSrc<T> src;
+        Dims a;
+        uint32_t tiles_x, tiles_y, zrange;
+        FwdOut<T> out;
+        uint32_t* status;
+    };
+    static __device__ __forceinline__ void run(const Params& P, uint32_t block, uint32_t);
+    static __device__ __forceinline__ void acquire_maps(const Params& P) {
+        if (Tma) tensormap_acquire(&P.map);
+    }
+};
+
 template <class T, int UX, int UY, int Q, bool Tma>
-__global__ void __launch_bounds__(256, 3)
-    fwd_stream_kernel(FwdSrc<T> src, const __grid_constant__ CUtensorMap map, Dims a, uint32_t tiles_x,
-                      uint32_t tiles_y, uint32_t zrange, FwdOut<T> out, uint32_t* status) {
+__device__ __forceinline__ void FwdStreamOp<T, UX, UY, Q, Tma>::run(const Params& P, uint32_t block, uint32_t) {
+    const FwdSrc<T> src = P.src;
+    const Dims a = P.a;
+    const uint32_t tiles_x = P.tiles_x, tiles_y = P.tiles_y, zrange = P.zrange;
+    const FwdOut<T> out = P.out;
+    uint32_t* const status = P.status;
+    const CUtensorMap* map = &P.map;
     using S = StreamShape<T, UX, UY, Q>;
     using L = Lift<T>;
     using Bits = decltype(abs_bits(T(0)));
@@ -77,8 +98,8 @@ __global__ void __launch_bounds__(256, 3)
     T* Mid = In + S::IN;                                                                  // [Q][UY][YP]
     uint64_t* bar = reinterpret_cast<uint64_t*>(Mid + S::MID);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint32_t bx = blockIdx.x % tiles_x, by = (blockIdx.x / tiles_x) % tiles_y;
-    const uint32_t bzr = blockIdx.x / (tiles_x * tiles_y);
+    const uint32_t bx = block % tiles_x, by = (block / tiles_x) % tiles_y;
+    const uint32_t bzr = block / (tiles_x * tiles_y);
     const uint32_t ox = bx * UX, oy = by * UY;
     const uint32_t z0 = bzr * zrange, z1 = min(a.z, z0 + zrange);
     if (z0 >= z1) return;
@@ -112,7 +133,7 @@ __global__ void __launch_bounds__(256, 3)
         mbar_expect_tx(bar, uint32_t(Q * S::FY * S::FX * sizeof(T)));
 #pragma unroll 1
         for (int q = 0; q < Q; ++q)
-            tma_load_3d(In + q * S::FY * S::FX, &map, int(ox) - 4, int(oy) - 4, int(mirror(zb + q, a.z)), bar);
+            tma_load_3d(In + q * S::FY * S::FX, map, int(ox) - 4, int(oy) - 4, int(mirror(zb + q, a.z)), bar);
     };
     uint32_t phase = 0;
     if constexpr (Tma) {

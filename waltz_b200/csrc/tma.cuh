@@ -62,6 +62,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32
 
 constexpr uint32_t kWaitBound = 1u << 22;
 
+// A tensor map read from global memory (a batched launch's parameter table)
+// is acquired by the tensor-map proxy before its first use, by the thread
+// that issues the copies; maps in kernel parameter space need nothing.
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* map) {
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(map))
+                 : "memory");
+}
+
 // ------------------------------------------------------------------ host
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,

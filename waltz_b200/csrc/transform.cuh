@@ -157,15 +157,29 @@ constexpr size_t level_smem() {
     return (a + b) * sizeof(T);
 }
 
-// Level kernel (1-D grid of grid.x * grid.y * grid.z tiles). Src: FwdSrc/InvSrc (positions are spatial in box a and are
+// Level op (1-D grid of grid.x * grid.y * grid.z tiles). Src: FwdSrc/InvSrc (positions are spatial in box a and are
 // reflected / coefficient-mapped on load). Out: functor (x,y,z,value).
+template <class T, bool Inverse, int Mask, int UX, int UY, int UZ, class Src, class Out> struct LevelOp {
+    static constexpr int kThreads = 256, kMinBlocks = 0; // no occupancy floor: the compiler picks the register budget
+    struct Params {
+        Src src;
+        Dims a, grid;
+        Out out;
+    };
+    static __device__ __forceinline__ void run(const Params P, uint32_t block, uint32_t);
+};
+
 template <class T, bool Inverse, int Mask, int UX, int UY, int UZ, class Src, class Out>
-__global__ void __launch_bounds__(256) level_kernel(Src src, Dims a, Dims grid, Out out) {
+__device__ __forceinline__ void LevelOp<T, Inverse, Mask, UX, UY, UZ, Src, Out>::run(const Params P, uint32_t block,
+                                                                                      uint32_t) {
+    const Src src = P.src;
+    const Dims a = P.a, grid = P.grid;
+    const Out out = P.out;
     using S = LevelShape<T, Inverse, Mask, UX, UY, UZ>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* A = reinterpret_cast<T*>(smem_raw);
     T* B = A + size_t(S::FPX) * S::FY * S::FZ;
-    const uint32_t bx = blockIdx.x % grid.x, by = (blockIdx.x / grid.x) % grid.y, bz = blockIdx.x / (grid.x * grid.y);
+    const uint32_t bx = block % grid.x, by = (block / grid.x) % grid.y, bz = block / (grid.x * grid.y);
     const uint32_t ox = bx * UX, oy = by * UY, oz = bz * UZ;
     const int hx = (Mask & AX) ? 4 : 0, hy = (Mask & AY) ? 4 : 0, hz = (Mask & AZ) ? 4 : 0;
 

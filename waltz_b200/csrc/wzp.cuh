@@ -187,8 +187,19 @@ template <class T> struct QuantBricks {
     }
 };
 
+template <class Src> struct WzpEncodeOp {
+    static constexpr int kThreads = kWzpThreads, kMinBlocks = 0; // no occupancy floor: the compiler picks the register budget
+    struct Params {
+        WzpEncodeArgs A;
+        Src src;
+    };
+    static __device__ __forceinline__ void run(const Params P, uint32_t, uint32_t);
+};
+
 template <class Src>
-__global__ void __launch_bounds__(kWzpThreads) wzp_encode_kernel(WzpEncodeArgs A, Src src) {
+__device__ __forceinline__ void WzpEncodeOp<Src>::run(const Params P, uint32_t, uint32_t) {
+    const WzpEncodeArgs& A = P.A;
+    const Src& src = P.src;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WzpEncodeSmem& S = *reinterpret_cast<WzpEncodeSmem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -416,10 +427,24 @@ __global__ void __launch_bounds__(kWzpThreads) wzp_encode_kernel(WzpEncodeArgs A
 }
 
 // Group directory: payload offset of the first byte of every nonempty group.
-__global__ void wzp_directory_kernel(uint8_t* out, uint32_t n, const uint64_t* state, const uint64_t* sizes,
-                                     uint64_t* total) {
+struct WzpDirectoryOp {
+    static constexpr int kThreads = 256, kMinBlocks = 0; // no occupancy floor: the compiler picks the register budget
+    struct Params {
+        uint8_t* out;
+        uint32_t n;
+        const uint64_t *state, *sizes;
+        uint64_t* total;
+    };
+    static __device__ __forceinline__ void run(const Params P, uint32_t block, uint32_t);
+};
+
+__device__ __forceinline__ void WzpDirectoryOp::run(const Params P, uint32_t block, uint32_t) {
+    uint8_t* const out = P.out;
+    const uint32_t n = P.n;
+    const uint64_t *state = P.state, *sizes = P.sizes;
+    uint64_t* const total = P.total;
     const uint32_t chunks = wzp_chunks(n), groups = wzp_groups(n);
-    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t g = block * kThreads + threadIdx.x;
     if (g >= groups) return;
     const uint32_t f = g * kGroup, l = min(f + kGroup, chunks) - 1;
     const uint64_t start = (state[f] & kValueMask) - sizes[f];
@@ -530,14 +555,20 @@ template <class T> struct WzpDecodeArgs {
     uint32_t* status;
 };
 
+template <class T> struct WzpDecodeOp {
+    static constexpr int kThreads = kWzpThreads, kMinBlocks = 0; // no occupancy floor: the compiler picks the register budget
+    using Params = WzpDecodeArgs<T>;
+    static __device__ __forceinline__ void run(const Params A, uint32_t block, uint32_t);
+};
+
 template <class T>
-__global__ void __launch_bounds__(kWzpThreads) wzp_decode_kernel(WzpDecodeArgs<T> A) {
+__device__ __forceinline__ void WzpDecodeOp<T>::run(const Params A, uint32_t block, uint32_t) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WzpDecodeSmem& S = *reinterpret_cast<WzpDecodeSmem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = kWzpThreads / 32;
     const uint32_t chunks = wzp_chunks(A.n), groups = wzp_groups(A.n);
-    const uint32_t c = blockIdx.x;
+    const uint32_t c = block;
     const uint32_t first = c * kChunk, count = min(kChunk, A.n - first);
     const size_t header = size_t(groups) * 4 + size_t(chunks) * 3;
     const DecodeJob J = A.job.get();
