@@ -118,6 +118,8 @@ def gpu_arm(args, rank, world, local_rank):
     stream = torch.cuda.current_stream()
     sp = C.c_void_p(stream.cuda_stream)
     shape = tuple(args.shape)
+    from waltz_b200 import autotune
+    knobs = autotune.apply_single(lib, shape, 4)  # committed tuning table (never changes the bytes)
     field = power_law_field_device(shape, SEED, device=dev).contiguous()
     n = field.numel()
     nbytes = n * 4
@@ -237,7 +239,7 @@ def gpu_arm(args, rank, world, local_rank):
                    "global_batch": world, "seq_len": None, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (512 MiB field)", "archive_bytes": a_bytes,
                    "compression_ratio": round(nbytes / a_bytes, 4), "max_abs_error": max_err, "abs_bound": eb,
-                   "repair_records": n_repairs, "q_outliers": n_qout},
+                   "repair_records": n_repairs, "q_outliers": n_qout, "tuning": knobs},
         "compress_gbs": round(nbytes / t_c / 1e9, 3),
         "decompress_gbs": round(nbytes / t_d / 1e9, 3),
         "compress_hbm_frac": round((nbytes + a_bytes) / t_c / 1e9 / hbm, 4),
@@ -265,7 +267,8 @@ def gpu_arm(args, rank, world, local_rank):
         result["tc_form"] = tc_form_comparison(dev, lib, args.steps, tuple(args.tc_shape))
     if not args.no_batch and world == 1:
         torch.cuda.empty_cache()
-        result["batched_form"] = batch_comparison(dev, lib, args.steps)
+        result["batched_form"] = batch_comparison(dev, lib, args.steps,
+                                                  cpu=rank == 0 and not args.no_cpu_baseline)
     return result
 
 
@@ -351,7 +354,7 @@ def tc_form_comparison(dev, lib, steps, shape=(64, 1024, 1024)):
     return report
 
 
-def batch_comparison(dev, lib, steps, count=512):
+def batch_comparison(dev, lib, steps, count=512, cpu=False):
     """Batched form against one call per chunk on the uneven-chunk workload:
     512 float32 chunks, per-axis sides drawn from {32,48,64,96,128} (seed 4),
     k^-11/3 fields each rescaled to a range drawn log-uniformly in [1e-2,1e3],
@@ -422,6 +425,8 @@ def batch_comparison(dev, lib, steps, count=512):
             ms.append(e0.elapsed_time(e1))
         return ms
 
+    from waltz_b200 import autotune
+    batch_knobs = autotune.apply_batch(lib, [tuple(f.shape) for f in fields], 4)
     comp_batch()
     first = [bytes(arch[offs[i]:offs[i] + written[i]].cpu().numpy()) for i in range(0, count, 37)]
     for i, f in enumerate(fields):
@@ -439,6 +444,9 @@ def batch_comparison(dev, lib, steps, count=512):
         dec_batch()
     cb = timed(comp_batch, reps)
     db = timed(dec_batch, reps)
+    # the one-call-per-chunk path with the library defaults
+    lib.waltz_b200_set_option(autotune.OPT_STAGE_KERNELS, 1)
+    lib.waltz_b200_set_option(autotune.OPT_ZMARCH_PLANES, 0)
     ce = timed(comp_each, max(3, steps // 4))
     de = timed(dec_each, max(3, steps // 4))
     # per-chunk archives equal the batched ones
@@ -456,11 +464,16 @@ def batch_comparison(dev, lib, steps, count=512):
                     "ranges log-uniform in [1e-2,1e3], REL 1e-3 per chunk",
         "samples": sum(sizes), "bytes": nbytes, "archive_bytes": archive_bytes,
         "compression_ratio": round(nbytes / archive_bytes, 4), "max_err_over_bound": round(worst, 6),
+        "batch_tuning": batch_knobs,
         "compress": {"batched": stats(cb), "per_chunk": stats(ce)},
         "decompress": {"batched": stats(db), "per_chunk": stats(de)},
     }
     for k in ("compress", "decompress"):
         report[k]["speedup"] = round(report[k]["batched"]["gbs"] / report[k]["per_chunk"]["gbs"], 3)
+    # compress + decompress throughput of the batched form, as the CPU line measures it
+    report["batched_gbs"] = round(nbytes / ((statistics.median(cb) + statistics.median(db)) / 1e3) / 1e9, 3)
+    if cpu:
+        report["cpu_baseline"] = cpu_batch_baseline([f.cpu().numpy() for f in fields], bounds)
     return report
 
 
@@ -537,6 +550,36 @@ def cpu_baseline(field, eb, budget_s=12.0):
     return {"value": round(done / secs / 1e9, 4), "unit": "GB/s", "cores": 1, "kind": kind,
             "sample": f"{i} of the field's eight 256^3 octants, compress + decompress each, "
                       f"reference CPU codec AVX2 backend, 1 thread ({secs:.1f} s)"}
+
+
+def cpu_batch_baseline(chunks, bounds, budget_s=10.0):
+    """Reference CPU codec (oracle/_ref, AVX2) over the chunk list with one
+    workspace per thread (up to 8 threads), compress + decompress per chunk,
+    until the list or about `budget_s` seconds are done."""
+    import os
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import oracle as O
+    kind = "reference" if O.ref_available() else "port"
+    threads = max(1, min(8, os.cpu_count() or 1))
+    local = __import__("threading").local()
+    t0 = time.perf_counter()
+
+    def work(i):
+        if time.perf_counter() - t0 > budget_s:
+            return 0
+        if not hasattr(local, "codec"):
+            local.codec = _codec(kind)
+        a = local.codec.compress(chunks[i], bounds[i])
+        local.codec.decompress(a, chunks[i].shape, chunks[i].dtype)
+        return chunks[i].nbytes
+
+    with ThreadPoolExecutor(threads) as pool:
+        sizes = list(pool.map(work, range(len(chunks))))
+    secs = time.perf_counter() - t0
+    done = sum(sizes)
+    return {"value": round(done / secs / 1e9, 4), "unit": "GB/s", "cores": threads, "kind": kind,
+            "sample": f"{sum(1 for x in sizes if x)} of {len(chunks)} chunks, compress + decompress each, reference "
+                      f"CPU codec AVX2 backend, one workspace per thread ({secs:.1f} s)"}
 
 
 def reference_arm(args):

@@ -96,6 +96,16 @@ int waltz_b200_decompress_batch(const waltz_b200_archive* archives, uint32_t cou
  * WALTZ_B200_BATCH_FIELDS: each field's own launches, fields round-robin on
  *   `width` parallel graph branches. Default, width 32.
  * width 1..64. Returns 0, or -1 for an invalid configuration. */
+/* Tuning options of the calling thread (performance knobs: results do not
+ * depend on them). Returns 0, or -1 for an unknown option or value.
+ * WALTZ_B200_OPT_STAGE_KERNELS (1 default, 0): plane schedule, run a whole Z
+ *   or XY stage in one kernel where its lines or planes fit in shared memory.
+ * WALTZ_B200_OPT_ZMARCH_PLANES (0 = automatic, else >= 16): planes per CTA of
+ *   the forward dyadic z-march (work per tile against the 8-plane halo). */
+#define WALTZ_B200_OPT_STAGE_KERNELS 1
+#define WALTZ_B200_OPT_ZMARCH_PLANES 2
+int waltz_b200_set_option(int option, int value);
+
 #define WALTZ_B200_BATCH_STAGES 0
 #define WALTZ_B200_BATCH_FIELDS 1
 int waltz_b200_batch_config(int mode, int width);

@@ -456,3 +456,45 @@ def test_batch_config_rejects_invalid_forms():
     assert lib.waltz_b200_batch_config(1, 65) == -1
     assert b"invalid batch configuration" in lib.waltz_b200_last_error()
     assert lib.waltz_b200_batch_config(1, 32) == 0
+
+
+def test_tuning_knobs_never_change_the_bytes():
+    """Every knob value of the tuning table gives the same archives and the
+    same decoded samples (single fields of both schedules and both dtypes,
+    and a batch in every execution form)."""
+    torch = _torch()
+    import waltz_b200
+    from waltz_b200 import autotune as A
+    from waltz_b200 import synthetic as S
+    lib = _lib()
+    cases = [((40, 72, 96), np.float32), ((24, 96, 64), np.float32), ((33, 40, 48), np.float64),
+             ((20, 200, 136), np.float32)]
+    try:
+        for shape, dt in cases:
+            f = torch.from_numpy(S.power_law_field(shape, 3).astype(dt)).cuda()
+            ref = waltz_b200.compress_tensor(f, 1e-3, tuned=False)
+            dref = waltz_b200.decompress_tensor(ref, shape, f.dtype, tuned=False)
+            for k in A.SINGLE_CANDIDATES:
+                assert lib.waltz_b200_set_option(A.OPT_STAGE_KERNELS, k["stage_kernels"]) == 0
+                assert lib.waltz_b200_set_option(A.OPT_ZMARCH_PLANES, k["zmarch"]) == 0
+                arc = waltz_b200.compress_tensor(f, 1e-3, tuned=False)
+                assert torch.equal(arc, ref), (shape, k)
+                assert torch.equal(waltz_b200.decompress_tensor(arc, shape, f.dtype, tuned=False), dref), (shape, k)
+        lib.waltz_b200_set_option(A.OPT_STAGE_KERNELS, 1)
+        lib.waltz_b200_set_option(A.OPT_ZMARCH_PLANES, 0)
+        fields, bounds = _uneven_batch(torch, 8, 10)
+        ref = [waltz_b200.compress_tensor(f, eb, tuned=False) for f, eb in zip(fields, bounds)]
+        for k in A.BATCH_CANDIDATES:
+            assert lib.waltz_b200_batch_config(k["mode"], k["width"]) == 0
+            assert lib.waltz_b200_set_option(A.OPT_STAGE_KERNELS, k["stage_kernels"]) == 0
+            arcs = waltz_b200.compress_batch(fields, bounds, tuned=False)
+            assert all(torch.equal(a, r) for a, r in zip(arcs, ref)), k
+            dec = waltz_b200.decompress_batch(arcs, [tuple(f.shape) for f in fields], torch.float32, tuned=False)
+            for d, r, f in zip(dec, ref, fields):
+                assert torch.equal(d, waltz_b200.decompress_tensor(r, tuple(f.shape), torch.float32, tuned=False))
+        assert lib.waltz_b200_set_option(99, 1) == -1
+        assert lib.waltz_b200_set_option(A.OPT_ZMARCH_PLANES, -1) == -1
+    finally:
+        lib.waltz_b200_set_option(A.OPT_STAGE_KERNELS, 1)
+        lib.waltz_b200_set_option(A.OPT_ZMARCH_PLANES, 0)
+        lib.waltz_b200_batch_config(1, 32)

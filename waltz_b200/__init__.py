@@ -15,6 +15,7 @@ import operator
 
 import numpy as np
 
+from . import autotune
 from ._lib import Archive, BatchShape, Chunk, WaltzError, checked, lib
 
 __all__ = ["compress", "decompress", "compress_tensor", "decompress_tensor", "compress_batch", "decompress_batch", "extrema",
@@ -59,18 +60,33 @@ def _stream(torch, stream):
 FORMS = {"plain": 0, "matrix": 1}
 
 
-def compress_tensor(field, abs_error: float, *, form: str = "plain", stream=None):
+def _matrix_ok(shape, itemsize):
+    nx, ny, nz = _geometry(shape, itemsize)
+    lxy, lz = (autotune._levels(min(nx, ny)), autotune._levels(nz))
+    return itemsize == 4 and lxy != lz and lz >= 1 and nz <= 64 and (nx * ny) % 4 == 0
+
+
+def compress_tensor(field, abs_error: float, *, form: str = "plain", stream=None, tuned=True):
     """Compress a contiguous float32/float64 CUDA tensor of shape (z,y,x) or
     (y,x). Returns a uint8 CUDA tensor holding the archive.
 
     form="plain" is the default profile (byte-identical to the reference CPU
     codec); form="matrix" is the precision form, whose Z stage runs as one
-    matrix on the tensor cores (float, plane schedule, nz <= 64)."""
+    matrix on the tensor cores (float, plane schedule, nz <= 64); form="auto"
+    takes the matrix form where it applies and the tuning table measured it
+    faster. With `tuned`, the tuning table's knobs for the field's class are
+    applied first (they never change the output)."""
     torch = _torch()
     if not field.is_cuda or not field.is_contiguous():
         raise ValueError("expected a contiguous CUDA tensor")
-    if form not in FORMS:
-        raise ValueError(f"form must be one of {sorted(FORMS)}")
+    if form not in FORMS and form != "auto":
+        raise ValueError(f"form must be one of {sorted(FORMS) + ['auto']}")
+    itemsize = field.element_size()
+    if form == "auto":
+        form = "matrix" if _matrix_ok(field.shape, itemsize) and autotune.matrix_preferred(
+            tuple(field.shape), itemsize) else "plain"
+    if tuned:
+        autotune.apply_single(lib(), tuple(_geometry(field.shape, itemsize))[::-1], itemsize)
     nx, ny, nz = _geometry(field.shape, field.element_size())
     cap = compressed_capacity(field.numel(), field.element_size())
     out = torch.empty(cap, dtype=torch.uint8, device=field.device)
@@ -81,7 +97,7 @@ def compress_tensor(field, abs_error: float, *, form: str = "plain", stream=None
     return out[:written.value]
 
 
-def decompress_tensor(archive, shape, dtype, *, out=None, stream=None):
+def decompress_tensor(archive, shape, dtype, *, out=None, stream=None, tuned=True):
     """Decode a uint8 CUDA tensor archive into a (z,y,x) CUDA tensor."""
     torch = _torch()
     dtype = {np.float32: torch.float32, np.float64: torch.float64}.get(dtype, dtype)
@@ -89,6 +105,8 @@ def decompress_tensor(archive, shape, dtype, *, out=None, stream=None):
         raise TypeError("Waltz requires float32 or float64")
     itemsize = 4 if dtype == torch.float32 else 8
     nx, ny, nz = _geometry(shape, itemsize)
+    if tuned:
+        autotune.apply_single(lib(), (nz, ny, nx), itemsize)
     if out is None:
         out = torch.empty(tuple(shape), dtype=dtype, device=archive.device)
     if not archive.is_cuda or not archive.is_contiguous():
@@ -99,7 +117,7 @@ def decompress_tensor(archive, shape, dtype, *, out=None, stream=None):
     return out
 
 
-def compress_batch(fields, abs_errors, *, out=None, stream=None):
+def compress_batch(fields, abs_errors, *, out=None, stream=None, tuned=True):
     """Compress many contiguous CUDA tensors (one dtype, any shapes) in one
     call: one CUDA graph, kept and replayed while the fields, bounds and
     output buffer stay the same. Returns one uint8 archive tensor per field,
@@ -131,11 +149,13 @@ def compress_batch(fields, abs_errors, *, out=None, stream=None):
         items[k] = Chunk(f.data_ptr(), nx, ny, nz, _bound(eb), out.data_ptr() + off,
                          compressed_capacity(f.numel(), itemsize))
     written = (C.c_uint64 * len(fields))()
+    if tuned:
+        autotune.apply_batch(lib(), [tuple(f.shape) for f in fields], itemsize)
     checked(lib().waltz_b200_compress_batch(items, len(fields), itemsize, written, _stream(torch, stream)))
     return [out[off:off + written[k]] for k, off in enumerate(offsets)]
 
 
-def decompress_batch(archives, shapes, dtype, *, out=None, headers=None, stream=None):
+def decompress_batch(archives, shapes, dtype, *, out=None, headers=None, stream=None, tuned=True):
     """Decode many archives (uint8 CUDA tensors, e.g. views of one staging
     buffer) of any shapes in one call, through one CUDA graph that is replayed
     while the shapes, forms and outputs stay the same. `out` is either one
@@ -182,6 +202,8 @@ def decompress_batch(archives, shapes, dtype, *, out=None, headers=None, stream=
             keep.append(buf)
             hdr = C.cast(buf, C.c_void_p)
         items[k] = Archive(a.data_ptr(), a.numel(), hdr, nx, ny, nz, v.data_ptr(), v.numel() * itemsize)
+    if tuned:
+        autotune.apply_batch(lib(), shapes, itemsize)
     checked(lib().waltz_b200_decompress_batch(items, len(archives), itemsize, _stream(torch, stream)))
     return views
 

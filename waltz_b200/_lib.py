@@ -27,6 +27,7 @@ SIGNATURES = {
                                            C.c_int, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t), C.c_void_p]),
     "waltz_b200_compress_batch": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int, C.POINTER(C.c_uint64), C.c_void_p]),
     "waltz_b200_batch_config": (C.c_int, [C.c_int, C.c_int]),
+    "waltz_b200_set_option": (C.c_int, [C.c_int, C.c_int]),
     "waltz_b200_decompress_batch": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int, C.c_void_p]),
     "waltz_b200_decompress": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_uint32, C.c_uint32, C.c_uint32,
                                         C.c_void_p, C.c_size_t, C.c_void_p]),

@@ -1,0 +1,228 @@
+"""Autotuner of the codec's performance knobs, and the committed table it
+writes (``tuning.json`` beside this file).
+
+Knobs (none changes a byte of the output, so a choice is a pure timing
+question and the table can be applied blindly):
+ * single fields: the plane schedule's whole-stage kernels on or off
+   (WALTZ_B200_OPT_STAGE_KERNELS) and the forward z-march depth, the planes
+   per CTA tile of the dyadic forward levels (WALTZ_B200_OPT_ZMARCH_PLANES);
+ * batches: the execution form of the batch graph (stage-batched groups or
+   per-field chains, and their width, waltz_b200_batch_config) and the stage
+   kernels knob;
+ * the transform form (lifting or the tensor-core matrix form) of fields the
+   matrix form serves: recorded per class and used only when a caller asks
+   for form="auto", since the matrix form sets its own header flag.
+The WZP group size (16 chunks of 8192 samples) is part of the archive
+format the reference decoders read, so it is not a knob.
+
+Classes: single fields by (dtype, schedule, round(log2 n)); batches by
+(dtype, round(log2 count), round(log2 mean chunk size)). A lookup takes the
+nearest measured class of the same dtype and kind.
+
+Run on a GPU:  python -m waltz_b200.autotune [--quick]
+"""
+from __future__ import annotations
+
+import json
+import math
+import statistics
+import time
+from pathlib import Path
+
+TABLE = Path(__file__).with_name("tuning.json")
+
+OPT_STAGE_KERNELS, OPT_ZMARCH_PLANES = 1, 2
+BATCH_STAGES, BATCH_FIELDS = 0, 1
+DEFAULT_SINGLE = {"stage_kernels": 1, "zmarch": 0}
+MATRIX_MARGIN = 0.97  # the matrix form changes the header flag: take it only for a clear gain
+DEFAULT_BATCH = {"mode": BATCH_FIELDS, "width": 32, "stage_kernels": 1}
+
+SINGLE_CANDIDATES = [{"stage_kernels": s, "zmarch": z} for s in (1, 0) for z in (0, 32, 64)]
+BATCH_CANDIDATES = ([{"mode": BATCH_STAGES, "width": w, "stage_kernels": s} for w in (1, 4, 16) for s in (1, 0)] +
+                    [{"mode": BATCH_FIELDS, "width": w, "stage_kernels": s} for w in (16, 32, 64) for s in (1, 0)])
+
+
+def _levels(n):
+    l = 0
+    while n > 8 and l < 5:
+        n -= n // 2
+        l += 1
+    return l
+
+
+def single_class(shape, itemsize):
+    nz, ny, nx = shape
+    sched = "dyadic" if _levels(min(nx, ny)) == _levels(nz) else "plane"
+    return {"kind": "single", "dtype": "f32" if itemsize == 4 else "f64", "schedule": sched,
+            "log2n": round(math.log2(max(1, nx * ny * nz)))}
+
+
+def batch_class(shapes, itemsize):
+    mean = sum(math.prod(s) for s in shapes) / max(1, len(shapes))
+    return {"kind": "batch", "dtype": "f32" if itemsize == 4 else "f64",
+            "log2count": round(math.log2(max(1, len(shapes)))), "log2mean": round(math.log2(max(1.0, mean)))}
+
+
+_cache = {}
+
+
+def load(path=TABLE):
+    key = str(path)
+    if key not in _cache:
+        try:
+            _cache[key] = json.loads(Path(path).read_text())
+        except (OSError, ValueError):
+            _cache[key] = {"entries": []}
+    return _cache[key]
+
+
+def lookup(cls, path=TABLE):
+    """Knobs of the nearest measured class (same kind, dtype and schedule),
+    or the built-in defaults."""
+    best, dist = None, None
+    for e in load(path).get("entries", []):
+        c = e["class"]
+        if c["kind"] != cls["kind"] or c["dtype"] != cls["dtype"] or c.get("schedule") != cls.get("schedule"):
+            continue
+        d = sum(abs(c[k] - cls[k]) for k in ("log2n", "log2count", "log2mean") if k in cls)
+        if dist is None or d < dist:
+            best, dist = e, d
+    if best is None:
+        return dict(DEFAULT_SINGLE if cls["kind"] == "single" else DEFAULT_BATCH)
+    return dict(best["choice"])
+
+
+def apply_single(lib, shape, itemsize):
+    k = lookup(single_class(shape, itemsize))
+    lib.waltz_b200_set_option(OPT_STAGE_KERNELS, int(k.get("stage_kernels", 1)))
+    lib.waltz_b200_set_option(OPT_ZMARCH_PLANES, int(k.get("zmarch", 0)))
+    return k
+
+
+def apply_batch(lib, shapes, itemsize):
+    k = lookup(batch_class(shapes, itemsize))
+    lib.waltz_b200_batch_config(int(k["mode"]), int(k["width"]))
+    lib.waltz_b200_set_option(OPT_STAGE_KERNELS, int(k.get("stage_kernels", 1)))
+    lib.waltz_b200_set_option(OPT_ZMARCH_PLANES, 0)
+    return k
+
+
+def matrix_preferred(shape, itemsize):
+    """Whether the measured class prefers the matrix form (form="auto")."""
+    return bool(lookup(single_class(shape, itemsize)).get("matrix", False))
+
+
+# ------------------------------------------------------------------ tuning
+def _time(torch, fn, reps):
+    fn()
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    return statistics.median(ms)
+
+
+def _tune_single(torch, lib, shape, dtype, reps, rel=1e-3):
+    import waltz_b200
+    from .synthetic import power_law_field_device
+    f = power_law_field_device(shape, 11, dtype=dtype).contiguous()
+    lo, hi = waltz_b200.extrema(f)
+    eb = rel * (hi - lo)
+    itemsize = f.element_size()
+    results = []
+    for cand in SINGLE_CANDIDATES:
+        lib.waltz_b200_set_option(OPT_STAGE_KERNELS, cand["stage_kernels"])
+        lib.waltz_b200_set_option(OPT_ZMARCH_PLANES, cand["zmarch"])
+        arc = waltz_b200.compress_tensor(f, eb, tuned=False)
+        tc = _time(torch, lambda: waltz_b200.compress_tensor(f, eb, tuned=False), reps)
+        td = _time(torch, lambda: waltz_b200.decompress_tensor(arc, shape, dtype, tuned=False), reps)
+        results.append({"knobs": cand, "compress_ms": round(tc, 4), "decompress_ms": round(td, 4)})
+    entry = {"class": single_class(shape, itemsize), "workload": f"{dtype} {shape} k^-11/3 REL {rel:g}",
+             "measured": results}
+    choice = min(results, key=lambda r: r["compress_ms"] + r["decompress_ms"])["knobs"]
+    entry["choice"] = dict(choice)
+    # the matrix form where it applies: timed with the chosen knobs
+    nz, ny, nx = shape
+    if dtype == torch.float32 and entry["class"]["schedule"] == "plane" and nz <= 64 and (nx * ny) % 4 == 0:
+        lib.waltz_b200_set_option(OPT_STAGE_KERNELS, choice["stage_kernels"])
+        lib.waltz_b200_set_option(OPT_ZMARCH_PLANES, choice["zmarch"])
+        arc = waltz_b200.compress_tensor(f, eb, form="matrix", tuned=False)
+        tc = _time(torch, lambda: waltz_b200.compress_tensor(f, eb, form="matrix", tuned=False), reps)
+        td = _time(torch, lambda: waltz_b200.decompress_tensor(arc, shape, dtype, tuned=False), reps)
+        best = min(results, key=lambda r: r["compress_ms"] + r["decompress_ms"])
+        entry["matrix_form"] = {"compress_ms": round(tc, 4), "decompress_ms": round(td, 4)}
+        entry["choice"]["matrix"] = tc + td < MATRIX_MARGIN * (best["compress_ms"] + best["decompress_ms"])
+    lib.waltz_b200_set_option(OPT_STAGE_KERNELS, 1)
+    lib.waltz_b200_set_option(OPT_ZMARCH_PLANES, 0)
+    return entry
+
+
+def _tune_batch(torch, lib, fields, label, reps, rel=1e-3):
+    import waltz_b200
+    bounds = []
+    for f in fields:
+        lo, hi = waltz_b200.extrema(f)
+        bounds.append(rel * (hi - lo))
+    shapes = [tuple(f.shape) for f in fields]
+    itemsize = fields[0].element_size()
+    cap = sum(waltz_b200.compressed_capacity(f.numel(), itemsize) + 16 for f in fields)
+    out = torch.empty(cap, dtype=torch.uint8, device=fields[0].device)
+    dec = torch.empty(sum(f.numel() for f in fields), dtype=fields[0].dtype, device=fields[0].device)
+    results = []
+    for cand in BATCH_CANDIDATES:
+        lib.waltz_b200_batch_config(cand["mode"], cand["width"])
+        lib.waltz_b200_set_option(OPT_STAGE_KERNELS, cand["stage_kernels"])
+        arcs = waltz_b200.compress_batch(fields, bounds, out=out, tuned=False)
+        tc = _time(torch, lambda: waltz_b200.compress_batch(fields, bounds, out=out, tuned=False), reps)
+        td = _time(torch, lambda: waltz_b200.decompress_batch(arcs, shapes, fields[0].dtype, out=dec, tuned=False),
+                   reps)
+        results.append({"knobs": cand, "compress_ms": round(tc, 4), "decompress_ms": round(td, 4)})
+    lib.waltz_b200_batch_config(*[DEFAULT_BATCH[k] for k in ("mode", "width")])
+    lib.waltz_b200_set_option(OPT_STAGE_KERNELS, 1)
+    choice = min(results, key=lambda r: r["compress_ms"] + r["decompress_ms"])["knobs"]
+    return {"class": batch_class(shapes, itemsize), "workload": label, "measured": results, "choice": dict(choice)}
+
+
+def tune(quick=False, reps=5, path=TABLE):
+    """Measure every candidate on the standard workloads and write the table."""
+    import torch
+    from . import _lib
+    from .synthetic import power_law_field_device, uneven_chunks_device
+    lib = _lib.lib()
+    entries = []
+    singles = [((64, 64, 64), torch.float32), ((256, 256, 256), torch.float32), ((512, 512, 512), torch.float32),
+               ((32, 128, 128), torch.float32), ((64, 1024, 1024), torch.float32), ((96, 256, 384), torch.float64)]
+    if quick:
+        singles = singles[:2] + singles[3:5]
+    for shape, dtype in singles:
+        t = time.time()
+        entries.append(_tune_single(torch, lib, shape, dtype, reps))
+        print(f"single {dtype} {shape}: {entries[-1]['choice']} ({time.time() - t:.1f} s)", flush=True)
+    batches = [("512 f32 chunks, sides from {32,48,64,96,128} (seed 4), k^-11/3, ranges log-uniform [1e-2,1e3]",
+                lambda: uneven_chunks_device(512 if not quick else 128, 4)),
+               ("512 f32 chunks 32^3", lambda: [power_law_field_device((32, 32, 32), 100 + i) for i in range(512)]),
+               ("64 f32 chunks 128^3", lambda: [power_law_field_device((128, 128, 128), 200 + i) for i in range(64)])]
+    for label, make in batches:
+        t = time.time()
+        fields = [f.contiguous() for f in make()]
+        entries.append(_tune_batch(torch, lib, fields, label, reps))
+        print(f"batch {label[:40]}: {entries[-1]['choice']} ({time.time() - t:.1f} s)", flush=True)
+        del fields
+        torch.cuda.empty_cache()
+    table = {"device": torch.cuda.get_device_name(), "reps": reps,
+             "note": "median CUDA-event times per candidate through the Python API (same call overhead for "
+                     "every candidate); choice = least compress + decompress time",
+             "entries": entries}
+    Path(path).write_text(json.dumps(table, indent=1) + "\n")
+    _cache.pop(str(path), None)
+    return table
+
+
+if __name__ == "__main__":
+    import sys
+    tune(quick="--quick" in sys.argv, path=Path(sys.argv[sys.argv.index("--out") + 1]) if "--out" in sys.argv else TABLE)

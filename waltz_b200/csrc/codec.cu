@@ -196,6 +196,14 @@ template <> struct Tiles<double> {
     static constexpr int Z[3] = {32, 8, 8};
 };
 
+// Tuning options of the calling thread (performance only: results do not
+// depend on them; set through waltz_b200_set_option).
+struct Options {
+    bool stage_kernels = true; // plane schedule: whole-stage kernels where they fit
+    uint32_t zmarch = 0;       // forward z-march planes per CTA: 0 = automatic
+};
+static thread_local Options t_opt;
+
 template <class T, bool Inverse, int Mask, int UX, int UY, int UZ, class Src, class Out>
 static void launch_level(const Src& src, Dims a, const Out& out, Sink& sink) {
     using Op = LevelOp<T, Inverse, Mask, UX, UY, UZ, Src, Out>;
@@ -247,7 +255,9 @@ static void level_fwd_stream(const FwdSrc<T>& src, Dims a, const FwdOut<T>& out,
     const uint32_t tx = (a.x + UX - 1) / UX, ty = (a.y + UY - 1) / UY;
     const uint64_t tiles = uint64_t(tx) * ty;
     uint32_t zrange = a.z + (a.z & 1);
-    if (!sink.many) {
+    if (t_opt.zmarch) {
+        zrange = std::min(zrange, std::max<uint32_t>(16, t_opt.zmarch + (t_opt.zmarch & 1)));
+    } else if (!sink.many) {
         // maximise (filled share of the last wave) x (planes kept out of the
         // 8-plane halo a range re-reads), over up to 16 ranges of >= 16 planes
         static thread_local int device = -1;
@@ -365,9 +375,11 @@ static StageLevels xy_levels(const Geometry& g) {
     }
     return lv;
 }
-template <class T> static bool zstage_ok(const Geometry& g) { return g.lz && zstage_smem<T>(g.nz) <= kStageSmemCap; }
+template <class T> static bool zstage_ok(const Geometry& g) {
+    return t_opt.stage_kernels && g.lz && zstage_smem<T>(g.nz) <= kStageSmemCap;
+}
 template <class T> static bool xystage_ok(const Geometry& g) {
-    return g.lxy && xystage_smem<T>(g.nx, g.ny) <= kStageSmemCap;
+    return t_opt.stage_kernels && g.lxy && xystage_smem<T>(g.nx, g.ny) <= kStageSmemCap;
 }
 
 static unsigned zstage_grid(const Geometry& g, int cx, int cy) {
@@ -1486,6 +1498,8 @@ static void compress_batch(const waltz_b200_chunk* items, uint32_t count, uint64
     const BatchConfig cfg = t_batch_cfg;
     append_key(key, cfg.mode);
     append_key(key, cfg.width);
+    append_key(key, t_opt.stage_kernels);
+    append_key(key, t_opt.zmarch);
     char* base = st.scratch.reserve(total);
     append_key(key, base); // the scratch must not have moved since the graph was captured
     uint64_t* results = reinterpret_cast<uint64_t*>(base + results_at);
@@ -1658,6 +1672,8 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
     key.push_back(uint8_t(sizeof(T)));
     append_key(key, cfg.mode);
     append_key(key, cfg.width);
+    append_key(key, t_opt.stage_kernels);
+    append_key(key, t_opt.zmarch);
     append_key(key, count);
     append_key(key, static_cast<const void*>(P.jobs));
     for (uint32_t i = 0; i < count; ++i) {
@@ -1781,6 +1797,24 @@ int waltz_b200_compress_batch(const waltz_b200_chunk* chunks, uint32_t count, in
     } catch (const std::exception& e) {
         return fail(e);
     }
+}
+
+int waltz_b200_set_option(int option, int value) {
+    using namespace wb;
+    switch (option) {
+    case WALTZ_B200_OPT_STAGE_KERNELS:
+        if (value != 0 && value != 1) break;
+        t_opt.stage_kernels = value != 0;
+        return 0;
+    case WALTZ_B200_OPT_ZMARCH_PLANES:
+        if (value < 0 || value > 65536) break;
+        t_opt.zmarch = uint32_t(value);
+        return 0;
+    default:
+        break;
+    }
+    std::snprintf(t_error, sizeof(t_error), "invalid option %d or value %d", option, value);
+    return -1;
 }
 
 int waltz_b200_batch_config(int mode, int width) {

@@ -365,6 +365,8 @@ class _Decoder:
                 at = base + (((side * batch.count + i) * fz + o[0]) * fy * fx + o[1] * fx + o[2]) * width
                 # header: the host copy of the archive in the payload tensor
                 items[k] = Archive(buf.data_ptr() + off, size, host + off, s[2], s[1], s[0], at, end - at, fx, fx * fy)
+            from . import autotune
+            autotune.apply_batch(lib(), [s for _, _, _, s, _, _ in batch.chunks], width)
             checked(lib().waltz_b200_decompress_batch(items, len(batch.chunks), width, C.c_void_p(caller.cuda_stream)))
         return (outs[0], outs[1]) if d.lead else outs[0]
 
