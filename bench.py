@@ -477,6 +477,45 @@ def batch_comparison(dev, lib, steps, count=512, cpu=False):
     return report
 
 
+def batch_only(dev, lib, args, count=512):
+    """The batched form alone on the uneven-chunk workload: `warmup` + `steps`
+    batched compress + decompress calls (the first captures the graphs)."""
+    import torch
+    import waltz_b200
+    from waltz_b200 import autotune
+    from waltz_b200.synthetic import uneven_chunks_device
+    fields = uneven_chunks_device(count, 4, device=dev)
+    bounds = []
+    for f in fields:
+        lo, hi = waltz_b200.extrema(f)
+        bounds.append(REL * (hi - lo))
+    shapes = [tuple(f.shape) for f in fields]
+    out = torch.empty(sum(waltz_b200.compressed_capacity(f.numel(), 4) + 16 for f in fields), dtype=torch.uint8,
+                      device=dev)
+    dec = torch.empty(sum(f.numel() for f in fields), dtype=torch.float32, device=dev)
+    if args.batch_config:
+        mode, width = (int(v) for v in args.batch_config.split(":"))
+        knobs = {"mode": mode, "width": width, "stage_kernels": 1}
+    else:
+        knobs = autotune.lookup(autotune.batch_class(shapes, 4))
+    lib.waltz_b200_batch_config(knobs["mode"], knobs["width"])
+    lib.waltz_b200_set_option(autotune.OPT_STAGE_KERNELS, int(knobs.get("stage_kernels", 1)))
+    ms = []
+    for k in range(args.warmup + max(1, args.steps)):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        arcs = waltz_b200.compress_batch(fields, bounds, out=out, tuned=False)
+        waltz_b200.decompress_batch(arcs, shapes, torch.float32, out=dec, tuned=False)
+        b.record()
+        torch.cuda.synchronize()
+        if k >= args.warmup:
+            ms.append(a.elapsed_time(b))
+    nbytes = 4 * sum(f.numel() for f in fields)
+    return {"workload": f"{count} uneven f32 chunks (seed 4), REL 1e-3, batched compress + decompress",
+            "knobs": knobs, "ms_per_step": round(statistics.median(ms), 4),
+            "gbs": round(nbytes / (statistics.median(ms) / 1e3) / 1e9, 3)}
+
+
 def algorithmic_bytes(n, s, a, fused=True):
     """Bytes each timed stage must move at least (its inputs read once and its
     outputs written once); a = archive bytes. Level kernels of the dyadic
@@ -636,6 +675,10 @@ def main():
                     help="field of the tensor-core comparison (z y x); smaller shapes serve profiler captures")
     ap.add_argument("--shape", type=int, nargs=3, default=list(SHAPE), metavar=("NZ", "NY", "NX"),
                     help="field shape (z y x); smaller shapes serve profiler captures")
+    ap.add_argument("--batch-only", action="store_true",
+                    help="run only the batched form on the uneven-chunk workload (profiler captures)")
+    ap.add_argument("--batch-config", default=None, metavar="MODE:WIDTH",
+                    help="batch execution form instead of the tuning table's (0 = stage-batched, 1 = field chains)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -652,6 +695,12 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
+    if args.batch_only:
+        import torch
+        from waltz_b200 import _lib
+        torch.cuda.set_device(local_rank)
+        print(json.dumps(batch_only(torch.device("cuda", local_rank), _lib.lib(), args)))
+        return
     try:
         result = gpu_arm(args, rank, world, local_rank)
         if rank == 0:
