@@ -179,6 +179,19 @@ __device__ __forceinline__ void ZStageInvOp<T, Out>::run(const Params Pm, uint32
         const uint32_t wins = (m + W - 1) / W;
         for (uint32_t w = threadIdx.x / C; w < wins; w += kZStageThreads / C) {
             const uint32_t s = w * W;
+            // finest level with a prefetching emitter: the originals of the
+            // window's outputs are requested before the lifting
+            T pe[P], po[P];
+            if constexpr (Out::kPrefetch) {
+                if (l == 0 && live) {
+#pragma unroll
+                    for (int j = 2; j < P - 2; ++j) {
+                        const uint32_t u = s + 2 * (j - 2);
+                        pe[j] = u < m ? out.fetch(x, y, u) : T(0);
+                        po[j] = u + 1 < m ? out.fetch(x, y, u + 1) : T(0);
+                    }
+                }
+            }
             T e[P], o[P];
             load_window<T, P>(int64_t(s), m, e, o,
                               [&](uint32_t p) { return src[size_t(split_of(p, m)) * C + c]; });
@@ -190,8 +203,13 @@ __device__ __forceinline__ void ZStageInvOp<T, Out>::run(const Params Pm, uint32
                     if (u < m) nxt[size_t(u) * C + c] = e[j];
                     if (u + 1 < m) nxt[size_t(u + 1) * C + c] = o[j];
                 } else if (live) {
-                    if (u < m) out(x, y, u, e[j]);
-                    if (u + 1 < m) out(x, y, u + 1, o[j]);
+                    if constexpr (Out::kPrefetch) {
+                        if (u < m) out.emit(x, y, u, e[j], pe[j]);
+                        if (u + 1 < m) out.emit(x, y, u + 1, o[j], po[j]);
+                    } else {
+                        if (u < m) out(x, y, u, e[j]);
+                        if (u + 1 < m) out(x, y, u + 1, o[j]);
+                    }
                 }
             }
         }
@@ -354,6 +372,17 @@ __device__ __forceinline__ void XYStageInvOp<T, Out>::run(const Params Pm, uint3
             const uint32_t wins = (my + WY - 1) / WY;
             for (uint32_t it = threadIdx.x; it < mx * wins; it += kXYStageThreads) {
                 const uint32_t cx = it % mx, s = (it / mx) * WY;
+                T pe[PYW], po[PYW];
+                if constexpr (Out::kPrefetch) {
+                    if (l == 0) {
+#pragma unroll
+                        for (int j = 2; j < PYW - 2; ++j) {
+                            const uint32_t u = s + 2 * (j - 2);
+                            pe[j] = u < my ? out.fetch(cx, u, z) : T(0);
+                            po[j] = u + 1 < my ? out.fetch(cx, u + 1, z) : T(0);
+                        }
+                    }
+                }
                 T e[PYW], o[PYW];
                 load_window<T, PYW>(int64_t(s), my, e, o,
                                     [&](uint32_t p) { return Qb[size_t(split_of(p, my)) * PX + cx]; });
@@ -364,6 +393,9 @@ __device__ __forceinline__ void XYStageInvOp<T, Out>::run(const Params Pm, uint3
                     if (l > 0) {
                         if (u < my) Pb[size_t(u) * PX + cx] = e[j];
                         if (u + 1 < my) Pb[size_t(u + 1) * PX + cx] = o[j];
+                    } else if constexpr (Out::kPrefetch) {
+                        if (u < my) out.emit(cx, u, z, e[j], pe[j]);
+                        if (u + 1 < my) out.emit(cx, u + 1, z, o[j], po[j]);
                     } else {
                         if (u < my) out(cx, u, z, e[j]);
                         if (u + 1 < my) out(cx, u + 1, z, o[j]);

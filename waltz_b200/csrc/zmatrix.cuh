@@ -84,18 +84,37 @@ struct ZmPlan {
     __host__ __device__ uint32_t smem() const { return 1024 + 2 * a_bytes + 2 * b_bytes + 64; }
 };
 
-// Destination of the Z stage: z-major store, or a per-sample emitter.
+// Destination of the Z stage: z-major store, or a per-sample emitter. The
+// epilogue hands over one column's group of 16 consecutive z values
+// (z0 .. z0+15, those below nz).
 template <class T> struct ZmStore {
     T* dst;       // z-major: dst[z * ncols + col]
-    __device__ __forceinline__ void operator()(uint32_t col, uint32_t z, size_t ncols, T v) const {
-        dst[size_t(z) * ncols + col] = v;
+    __device__ __forceinline__ void group(uint32_t col, uint32_t z0, uint32_t nz, size_t ncols,
+                                          const uint32_t (&r)[16]) const {
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+            if (z0 + j < nz) dst[size_t(z0 + j) * ncols + col] = __uint_as_float(r[j]);
     }
 };
 template <class Final> struct ZmEmit {
     Final fin;
     uint32_t nx;
-    __device__ __forceinline__ void operator()(uint32_t col, uint32_t z, size_t, float v) const {
-        fin(col % nx, col / nx, z, v);
+    __device__ __forceinline__ void group(uint32_t col, uint32_t z0, uint32_t nz, size_t, const uint32_t (&r)[16]) const {
+        const uint32_t x = col % nx, y = col / nx;
+        if constexpr (Final::kPrefetch) {
+            // every original first, then the emissions: the loads do not wait
+            // behind the emitter's stores
+            float o[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) o[j] = z0 + j < nz ? fin.fetch(x, y, z0 + j) : 0.f;
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+                if (z0 + j < nz) fin.emit(x, y, z0 + j, __uint_as_float(r[j]), o[j]);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+                if (z0 + j < nz) fin(x, y, z0 + j, __uint_as_float(r[j]));
+        }
     }
 };
 
@@ -209,11 +228,7 @@ __global__ void __launch_bounds__(kZmThreads, 2)
             uint32_t r[16];
             tmem_ld16(tmem + (uint32_t(32 * sub) << 16) + c0, r);
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (col < ncols) {
-#pragma unroll
-                for (int j = 0; j < 16; ++j)
-                    if (c0 + j < nz) out(uint32_t(col), c0 + j, ncols, __uint_as_float(r[j]));
-            }
+            if (col < ncols) out.group(uint32_t(col), c0, nz, ncols, r);
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads(); // tensor memory read out, A free: the next tile may overwrite both
