@@ -677,6 +677,8 @@ def main():
                     help="field shape (z y x); smaller shapes serve profiler captures")
     ap.add_argument("--batch-only", action="store_true",
                     help="run only the batched form on the uneven-chunk workload (profiler captures)")
+    ap.add_argument("--tc-only", action="store_true",
+                    help="run only the plain vs tensor-core form comparison at --tc-shape (profiler captures)")
     ap.add_argument("--batch-config", default=None, metavar="MODE:WIDTH",
                     help="batch execution form instead of the tuning table's (0 = stage-batched, 1 = field chains)")
     args = ap.parse_args()
@@ -695,6 +697,13 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
+    if args.tc_only:
+        import torch
+        from waltz_b200 import _lib
+        torch.cuda.set_device(local_rank)
+        print(json.dumps(tc_form_comparison(torch.device("cuda", local_rank), _lib.lib(), args.steps,
+                                            tuple(args.tc_shape))))
+        return
     if args.batch_only:
         import torch
         from waltz_b200 import _lib
