@@ -281,6 +281,8 @@ def tc_form_comparison(dev, lib, steps, shape=(64, 1024, 1024)):
     from waltz_b200 import _lib
     from waltz_b200.synthetic import power_law_field_device
     nz, ny, nx = shape
+    from waltz_b200 import autotune
+    autotune.apply_single(lib, shape, 4)  # this field's class in the tuning table (never changes the bytes)
     f = power_law_field_device(shape, 3, device=dev)
     gen = torch.Generator(device=dev)
     gen.manual_seed(3)

@@ -468,20 +468,18 @@ def test_tuning_knobs_never_change_the_bytes():
     from waltz_b200 import synthetic as S
     lib = _lib()
     cases = [((40, 72, 96), np.float32), ((24, 96, 64), np.float32), ((33, 40, 48), np.float64),
-             ((20, 200, 136), np.float32)]
+             ((20, 200, 136), np.float32), ((96, 96, 96), np.float32), ((64, 80, 48), np.float64)]
     try:
         for shape, dt in cases:
             f = torch.from_numpy(S.power_law_field(shape, 3).astype(dt)).cuda()
             ref = waltz_b200.compress_tensor(f, 1e-3, tuned=False)
             dref = waltz_b200.decompress_tensor(ref, shape, f.dtype, tuned=False)
-            for k in A.SINGLE_CANDIDATES:
-                assert lib.waltz_b200_set_option(A.OPT_STAGE_KERNELS, k["stage_kernels"]) == 0
-                assert lib.waltz_b200_set_option(A.OPT_ZMARCH_PLANES, k["zmarch"]) == 0
+            for k in A.SINGLE_CANDIDATES + [{"small_inv": 0, "small_fwd": 0}, {"small_inv": 1 << 30, "small_fwd": 1 << 30}]:
+                A.set_single(lib, k)
                 arc = waltz_b200.compress_tensor(f, 1e-3, tuned=False)
                 assert torch.equal(arc, ref), (shape, k)
                 assert torch.equal(waltz_b200.decompress_tensor(arc, shape, f.dtype, tuned=False), dref), (shape, k)
-        lib.waltz_b200_set_option(A.OPT_STAGE_KERNELS, 1)
-        lib.waltz_b200_set_option(A.OPT_ZMARCH_PLANES, 0)
+        A.set_single(lib, {})
         fields, bounds = _uneven_batch(torch, 8, 10)
         ref = [waltz_b200.compress_tensor(f, eb, tuned=False) for f, eb in zip(fields, bounds)]
         for k in A.BATCH_CANDIDATES:
@@ -495,6 +493,5 @@ def test_tuning_knobs_never_change_the_bytes():
         assert lib.waltz_b200_set_option(99, 1) == -1
         assert lib.waltz_b200_set_option(A.OPT_ZMARCH_PLANES, -1) == -1
     finally:
-        lib.waltz_b200_set_option(A.OPT_STAGE_KERNELS, 1)
-        lib.waltz_b200_set_option(A.OPT_ZMARCH_PLANES, 0)
+        A.set_single(lib, {})
         lib.waltz_b200_batch_config(1, 32)

@@ -4,8 +4,10 @@ writes (``tuning.json`` beside this file).
 Knobs (none changes a byte of the output, so a choice is a pure timing
 question and the table can be applied blindly):
  * single fields: the plane schedule's whole-stage kernels on or off
-   (WALTZ_B200_OPT_STAGE_KERNELS) and the forward z-march depth, the planes
-   per CTA tile of the dyadic forward levels (WALTZ_B200_OPT_ZMARCH_PLANES);
+   (WALTZ_B200_OPT_STAGE_KERNELS), the forward z-march depth, the planes
+   per CTA tile of the dyadic forward levels (WALTZ_B200_OPT_ZMARCH_PLANES),
+   and the level sizes below which dyadic levels stage tiles with reflecting
+   loads instead of tensor-map copies (WALTZ_B200_OPT_SMALL_LEVEL / _FWD);
  * batches: the execution form of the batch graph (stage-batched groups or
    per-field chains, and their width, waltz_b200_batch_config) and the stage
    kernels knob;
@@ -31,13 +33,14 @@ from pathlib import Path
 
 TABLE = Path(__file__).with_name("tuning.json")
 
-OPT_STAGE_KERNELS, OPT_ZMARCH_PLANES = 1, 2
+OPT_STAGE_KERNELS, OPT_ZMARCH_PLANES, OPT_SMALL_LEVEL, OPT_SMALL_FWD = 1, 2, 3, 4
 BATCH_STAGES, BATCH_FIELDS = 0, 1
-DEFAULT_SINGLE = {"stage_kernels": 1, "zmarch": 0}
+DEFAULT_SINGLE = {"stage_kernels": 1, "zmarch": 0, "small_inv": 1 << 21, "small_fwd": 1 << 26}
 MATRIX_MARGIN = 0.97  # the matrix form changes the header flag: take it only for a clear gain
 DEFAULT_BATCH = {"mode": BATCH_FIELDS, "width": 32, "stage_kernels": 1}
 
-SINGLE_CANDIDATES = [{"stage_kernels": s, "zmarch": z} for s in (1, 0) for z in (0, 32, 64)]
+SINGLE_CANDIDATES = [{"stage_kernels": s, "zmarch": z, "small_inv": 1 << 21, "small_fwd": f}
+                     for s in (1, 0) for z in (0, 32) for f in (1 << 24, 1 << 26, 1 << 28)]
 BATCH_CANDIDATES = ([{"mode": BATCH_STAGES, "width": w, "stage_kernels": s} for w in (1, 4, 16) for s in (1, 0)] +
                     [{"mode": BATCH_FIELDS, "width": w, "stage_kernels": s} for w in (16, 32, 64) for s in (1, 0)])
 
@@ -92,18 +95,24 @@ def lookup(cls, path=TABLE):
     return dict(best["choice"])
 
 
-def apply_single(lib, shape, itemsize):
-    k = lookup(single_class(shape, itemsize))
-    lib.waltz_b200_set_option(OPT_STAGE_KERNELS, int(k.get("stage_kernels", 1)))
-    lib.waltz_b200_set_option(OPT_ZMARCH_PLANES, int(k.get("zmarch", 0)))
+def set_single(lib, k):
+    """Applies single-field knobs (missing ones take their defaults)."""
+    k = {**DEFAULT_SINGLE, **k}
+    lib.waltz_b200_set_option(OPT_STAGE_KERNELS, int(k["stage_kernels"]))
+    lib.waltz_b200_set_option(OPT_ZMARCH_PLANES, int(k["zmarch"]))
+    lib.waltz_b200_set_option(OPT_SMALL_LEVEL, int(k["small_inv"]))
+    lib.waltz_b200_set_option(OPT_SMALL_FWD, int(k["small_fwd"]))
     return k
+
+
+def apply_single(lib, shape, itemsize):
+    return set_single(lib, lookup(single_class(shape, itemsize)))
 
 
 def apply_batch(lib, shapes, itemsize):
     k = lookup(batch_class(shapes, itemsize))
     lib.waltz_b200_batch_config(int(k["mode"]), int(k["width"]))
-    lib.waltz_b200_set_option(OPT_STAGE_KERNELS, int(k.get("stage_kernels", 1)))
-    lib.waltz_b200_set_option(OPT_ZMARCH_PLANES, 0)
+    set_single(lib, {"stage_kernels": int(k.get("stage_kernels", 1))})
     return k
 
 
@@ -136,8 +145,7 @@ def _tune_single(torch, lib, shape, dtype, reps, rel=1e-3):
     itemsize = f.element_size()
     results = []
     for cand in SINGLE_CANDIDATES:
-        lib.waltz_b200_set_option(OPT_STAGE_KERNELS, cand["stage_kernels"])
-        lib.waltz_b200_set_option(OPT_ZMARCH_PLANES, cand["zmarch"])
+        set_single(lib, cand)
         arc = waltz_b200.compress_tensor(f, eb, tuned=False)
         tc = _time(torch, lambda: waltz_b200.compress_tensor(f, eb, tuned=False), reps)
         td = _time(torch, lambda: waltz_b200.decompress_tensor(arc, shape, dtype, tuned=False), reps)
@@ -149,16 +157,14 @@ def _tune_single(torch, lib, shape, dtype, reps, rel=1e-3):
     # the matrix form where it applies: timed with the chosen knobs
     nz, ny, nx = shape
     if dtype == torch.float32 and entry["class"]["schedule"] == "plane" and nz <= 64 and (nx * ny) % 4 == 0:
-        lib.waltz_b200_set_option(OPT_STAGE_KERNELS, choice["stage_kernels"])
-        lib.waltz_b200_set_option(OPT_ZMARCH_PLANES, choice["zmarch"])
+        set_single(lib, choice)
         arc = waltz_b200.compress_tensor(f, eb, form="matrix", tuned=False)
         tc = _time(torch, lambda: waltz_b200.compress_tensor(f, eb, form="matrix", tuned=False), reps)
         td = _time(torch, lambda: waltz_b200.decompress_tensor(arc, shape, dtype, tuned=False), reps)
         best = min(results, key=lambda r: r["compress_ms"] + r["decompress_ms"])
         entry["matrix_form"] = {"compress_ms": round(tc, 4), "decompress_ms": round(td, 4)}
         entry["choice"]["matrix"] = tc + td < MATRIX_MARGIN * (best["compress_ms"] + best["decompress_ms"])
-    lib.waltz_b200_set_option(OPT_STAGE_KERNELS, 1)
-    lib.waltz_b200_set_option(OPT_ZMARCH_PLANES, 0)
+    set_single(lib, {})
     return entry
 
 
@@ -176,14 +182,14 @@ def _tune_batch(torch, lib, fields, label, reps, rel=1e-3):
     results = []
     for cand in BATCH_CANDIDATES:
         lib.waltz_b200_batch_config(cand["mode"], cand["width"])
-        lib.waltz_b200_set_option(OPT_STAGE_KERNELS, cand["stage_kernels"])
+        set_single(lib, {"stage_kernels": cand["stage_kernels"]})
         arcs = waltz_b200.compress_batch(fields, bounds, out=out, tuned=False)
         tc = _time(torch, lambda: waltz_b200.compress_batch(fields, bounds, out=out, tuned=False), reps)
         td = _time(torch, lambda: waltz_b200.decompress_batch(arcs, shapes, fields[0].dtype, out=dec, tuned=False),
                    reps)
         results.append({"knobs": cand, "compress_ms": round(tc, 4), "decompress_ms": round(td, 4)})
     lib.waltz_b200_batch_config(*[DEFAULT_BATCH[k] for k in ("mode", "width")])
-    lib.waltz_b200_set_option(OPT_STAGE_KERNELS, 1)
+    set_single(lib, {})
     choice = min(results, key=lambda r: r["compress_ms"] + r["decompress_ms"])["knobs"]
     return {"class": batch_class(shapes, itemsize), "workload": label, "measured": results, "choice": dict(choice)}
 

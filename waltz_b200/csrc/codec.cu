@@ -201,6 +201,9 @@ template <> struct Tiles<double> {
 struct Options {
     bool stage_kernels = true; // plane schedule: whole-stage kernels where they fit
     uint32_t zmarch = 0;       // forward z-march planes per CTA: 0 = automatic
+    uint64_t small_level = uint64_t(1) << 21; // inverse levels of at most this many samples: direct staging
+    uint64_t small_fwd = uint64_t(1) << 26;   // forward levels of at most this many samples: direct staging,
+                                              // short z ranges (measured on 128^3 .. 512^3 fields)
 };
 static thread_local Options t_opt;
 
@@ -251,15 +254,20 @@ static void level_fwd_stream(const FwdSrc<T>& src, Dims a, const FwdOut<T>& out,
     using OpT = FwdStreamOp<T, UX, UY, Q, true>;
     using OpL = FwdStreamOp<T, UX, UY, Q, false>;
     typename OpT::Params p{};
-    const bool tma = make_map_3d<T>(&p.map, src.p, a.x, a.y, a.z, src.sy, src.sz, S::FX, S::FY, 1);
+    // small levels: almost every tile is an edge tile, whose reflected cells
+    // the TMA path fixes up one by one; direct staging reflects on load
+    const bool small = vol(a) <= t_opt.small_fwd;
+    const bool tma = !small && make_map_3d<T>(&p.map, src.p, a.x, a.y, a.z, src.sy, src.sz, S::FX, S::FY, 1);
     const uint32_t tx = (a.x + UX - 1) / UX, ty = (a.y + UY - 1) / UY;
     const uint64_t tiles = uint64_t(tx) * ty;
+    const uint32_t min_range = small ? 8 : 16;
     uint32_t zrange = a.z + (a.z & 1);
     if (t_opt.zmarch) {
         zrange = std::min(zrange, std::max<uint32_t>(16, t_opt.zmarch + (t_opt.zmarch & 1)));
     } else if (!sink.many) {
         // maximise (filled share of the last wave) x (planes kept out of the
         // 8-plane halo a range re-reads), over up to 16 ranges of >= 16 planes
+        // (>= 8 for small levels, which are latency-bound)
         static thread_local int device = -1;
         static thread_local size_t granted = 0;
         opt_in_smem(op_kernel_for<OpT>(), S::smem, device, granted);
@@ -268,7 +276,7 @@ static void level_fwd_stream(const FwdSrc<T>& src, Dims a, const FwdOut<T>& out,
         for (uint32_t k = 1; k <= 16; ++k) {
             uint32_t r = (a.z + k - 1) / k;
             r += r & 1;
-            if (k > 1 && r < 16) break;
+            if (k > 1 && r < min_range) break;
             const uint64_t blocks = tiles * ((a.z + r - 1) / r);
             const double waves = double((blocks + slots - 1) / slots);
             const double score = double(blocks) / (waves * double(slots)) * double(r) / double(r + 8);
@@ -310,7 +318,7 @@ static void level_inv(const InvSrc<T>& src, Dims a, const Out& out, uint32_t* st
     using S = InvShape<T, UX, UY, UZ>;
     using Op = InvTileOp<T, UX, UY, UZ, Out>;
     typename Op::Params p{};
-    bool tma = half_len(a.x) % S::V == 0 &&
+    bool tma = vol(a) > t_opt.small_level && half_len(a.x) % S::V == 0 &&
                make_map_3d<T>(&p.cmap, src.base, a.x, a.y, a.z, src.sy, src.sz, S::BX, S::HY, S::HZ);
     if (tma && src.low)
         tma = make_map_3d<T>(&p.lmap, src.low, src.lo.x, src.lo.y, src.lo.z, src.lo.x, uint64_t(src.lo.x) * src.lo.y,
@@ -1500,6 +1508,8 @@ static void compress_batch(const waltz_b200_chunk* items, uint32_t count, uint64
     append_key(key, cfg.width);
     append_key(key, t_opt.stage_kernels);
     append_key(key, t_opt.zmarch);
+    append_key(key, t_opt.small_level);
+    append_key(key, t_opt.small_fwd);
     char* base = st.scratch.reserve(total);
     append_key(key, base); // the scratch must not have moved since the graph was captured
     uint64_t* results = reinterpret_cast<uint64_t*>(base + results_at);
@@ -1674,6 +1684,8 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
     append_key(key, cfg.width);
     append_key(key, t_opt.stage_kernels);
     append_key(key, t_opt.zmarch);
+    append_key(key, t_opt.small_level);
+    append_key(key, t_opt.small_fwd);
     append_key(key, count);
     append_key(key, static_cast<const void*>(P.jobs));
     for (uint32_t i = 0; i < count; ++i) {
@@ -1809,6 +1821,14 @@ int waltz_b200_set_option(int option, int value) {
     case WALTZ_B200_OPT_ZMARCH_PLANES:
         if (value < 0 || value > 65536) break;
         t_opt.zmarch = uint32_t(value);
+        return 0;
+    case WALTZ_B200_OPT_SMALL_LEVEL:
+        if (value < 0) break;
+        t_opt.small_level = uint64_t(value);
+        return 0;
+    case WALTZ_B200_OPT_SMALL_FWD:
+        if (value < 0) break;
+        t_opt.small_fwd = uint64_t(value);
         return 0;
     default:
         break;
