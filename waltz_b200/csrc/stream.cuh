@@ -66,7 +66,9 @@ __device__ __forceinline__ bool nonfinite_max(unsigned long long m) { return m >
 // ordinary loads. `status` receives ST_WAIT_TIMEOUT if a copy never
 // completes within the wait bound (the block then stops as a whole).
 template <class T, int UX, int UY, int Q, bool Tma> struct FwdStreamOp {
-    static constexpr int kThreads = 256, kMinBlocks = 3;
+    // four CTAs per SM (64 registers): measured faster than three with more
+    // registers, for both staging forms
+    static constexpr int kThreads = 256, kMinBlocks = 4;
     static constexpr bool kGridConstant = true;
     struct Params {
         CUtensorMap map;

@@ -188,7 +188,7 @@ template <class T> struct QuantBricks {
 };
 
 template <class Src> struct WzpEncodeOp {
-    static constexpr int kThreads = kWzpThreads, kMinBlocks = 0; // no occupancy floor: the compiler picks the register budget
+    static constexpr int kThreads = kWzpThreads, kMinBlocks = 4; // 32 registers: four CTAs per SM
     struct Params {
         WzpEncodeArgs A;
         Src src;
