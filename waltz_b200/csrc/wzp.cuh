@@ -49,6 +49,57 @@ constexpr uint64_t kValueMask = (1ull << 62) - 1;
 // 16384 + 2048 + 256 + 32 + 4 payload bytes, plus slack for word-wide copies.
 constexpr uint32_t kEncBytes = 2 * kChunk + 2048 + 256 + 32 + 4 + 28;
 
+// Bit planes in shared memory: the stream's natural layout puts plane p's
+// u16 word b at p * blocks + b, so the 16 lanes that hold the 16 planes of one
+// 32-sample group would all hit one bank. The decoder therefore reads them
+// from a padded layout, plane p at u32 word p * kPlanePitch + group, filled
+// from the natural layout by a conflict-free pass (consecutive threads on
+// consecutive natural words).
+constexpr uint32_t kPlanePitch = kChunk / 32 + 1; // u32 words per padded plane
+
+// natural -> padded (dir = true) or padded -> natural, in place in `buf`
+// (room for 16 * kPlanePitch words); the caller syncs before and after.
+__device__ __forceinline__ void planes_repack(uint8_t* buf, uint32_t blocks, bool to_padded, int tid) {
+    constexpr int PER = (16 * kChunk / 16 / 2 + kWzpThreads - 1) / kWzpThreads; // u32 words per thread
+    uint32_t* w = reinterpret_cast<uint32_t*>(buf);
+    if (blocks == 0) return; // no whole block: no planes (uniform across the block)
+    if ((blocks & 1u) == 0) {
+        const uint32_t per_plane = blocks / 2, words = 16 * per_plane;
+        uint32_t v[PER];
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const uint32_t q = tid + k * kWzpThreads;
+            const uint32_t p = q / per_plane, g = q - p * per_plane;
+            if (q < words) v[k] = to_padded ? w[q] : w[p * kPlanePitch + g];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const uint32_t q = tid + k * kWzpThreads;
+            const uint32_t p = q / per_plane, g = q - p * per_plane;
+            if (q < words) (to_padded ? w[p * kPlanePitch + g] : w[q]) = v[k];
+        }
+    } else {
+        // an odd number of 16-sample blocks (a field's last chunk): u16 steps
+        uint16_t* h = reinterpret_cast<uint16_t*>(buf);
+        const uint32_t halves = 16 * blocks;
+        uint16_t v[2 * PER];
+#pragma unroll
+        for (int k = 0; k < 2 * PER; ++k) {
+            const uint32_t q = tid + k * kWzpThreads;
+            const uint32_t p = q / blocks, b = q - p * blocks;
+            if (q < halves) v[k] = to_padded ? h[q] : h[2 * p * kPlanePitch + b];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 2 * PER; ++k) {
+            const uint32_t q = tid + k * kWzpThreads;
+            const uint32_t p = q / blocks, b = q - p * blocks;
+            if (q < halves) (to_padded ? h[2 * p * kPlanePitch + b] : h[q]) = v[k];
+        }
+    }
+}
+
 struct WzpEncodeSmem {
     uint16_t m[kChunk + 8];            // magnitudes (+ slack for word-wide copies)
     union {
@@ -244,6 +295,8 @@ __device__ __forceinline__ void WzpEncodeOp<Src>::run(const Params P, uint32_t, 
                     if (lane == p) mine = r;
                 }
             }
+            // natural layout (the 16 stores share a bank; a padded layout and a
+            // repacking pass measured slower here, stores do not stall the warp)
             uint16_t* pl = reinterpret_cast<uint16_t*>(S.planes);
             if (lane < 16) {
                 pl[lane * blocks + 2 * g] = uint16_t(mine >> 16);
@@ -500,7 +553,7 @@ struct WzpDecodeSmem {
     uint16_t m[kChunk + 16];           // staged magnitude bytes, then the decoded magnitudes
     uint8_t sb[1024 + 32];             // staged sign bytes
     uint32_t xsel[16];                 // byte_perm selectors: spread 4-bit-mask bytes into place
-    uint8_t planes[2 * kChunk];
+    uint8_t planes[16 * kPlanePitch * 4]; // natural planes, then the padded layout
     uint8_t lv[2048 + 256 + 32 + 4];
     uint32_t gprefix[kChunk / 32];
     uint32_t tmp[40];
@@ -744,16 +797,24 @@ __device__ __forceinline__ void WzpDecodeOp<T>::run(const Params A, uint32_t blo
             out[1] = make_uint4(words[4], words[5], words[6], words[7]);
         }
         __syncthreads();
+        // the verbatim tail (samples past the last whole block) while the
+        // planes are still in the natural layout
+        const uint16_t* pl = reinterpret_cast<const uint16_t*>(S.planes);
+        uint16_t tail = 0;
+        const uint32_t ti = blocks * 16 + tid;
+        if (ti < count) tail = pl[ti];
+        planes_repack(S.planes, blocks, true, tid);
+        __syncthreads();
         // ---- inverse bit planes: lane p < 16 holds plane p of the group's 32
         // magnitudes (bit e = magnitude e's bit 15-p); a 32x32 bit transpose
         // across the warp (five butterfly exchanges) leaves magnitude e in lane e
-        const uint16_t* pl = reinterpret_cast<const uint16_t*>(S.planes);
         for (int g = warp; g < int(kChunk / 32); g += NW) {
             if (uint32_t(g * 32) >= blocks * 16) break;
             uint32_t x = 0;
             if (lane < 16) {
-                uint32_t w = uint32_t(pl[lane * blocks + 2 * g]) << 16;
-                if (uint32_t(2 * g + 1) < blocks) w |= pl[lane * blocks + 2 * g + 1];
+                uint32_t w = __funnelshift_l(reinterpret_cast<const uint32_t*>(S.planes)[lane * kPlanePitch + g],
+                                             reinterpret_cast<const uint32_t*>(S.planes)[lane * kPlanePitch + g], 16);
+                if (uint32_t(2 * g + 1) >= blocks) w &= 0xffff0000u;
                 x = __brev(w);
             }
 #pragma unroll
@@ -767,7 +828,7 @@ __device__ __forceinline__ void WzpDecodeOp<T>::run(const Params A, uint32_t blo
             if (uint32_t(e) < blocks * 16) S.m[e] = uint16_t(__brev(x) >> 16);
         }
         for (uint32_t i = blocks * 16 + tid; i < kChunk; i += kWzpThreads)
-            S.m[i] = i < count ? pl[i] : 0;
+            S.m[i] = i == ti ? tail : 0;
     }
     __syncthreads();
 
