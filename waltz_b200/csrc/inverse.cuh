@@ -83,7 +83,7 @@ __device__ __forceinline__ void InvTileOp<T, UX, UY, UZ, Out>::run(const Params&
     extern __shared__ __align__(128) unsigned char inv_smem[];
     T* Bx = reinterpret_cast<T*>(inv_smem + ((128 - (smem_u32(inv_smem) & 127)) & 127));
     uint64_t* bar = reinterpret_cast<uint64_t*>(Bx + 8 * S::BOX);
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5;
     const Dims a = lv.a;
     const uint32_t bx = block % tiles_x, by = (block / tiles_x) % tiles_y, bz = block / (tiles_x * tiles_y);
     const uint32_t ox = bx * UX, oy = by * UY, oz = bz * UZ;
@@ -119,28 +119,52 @@ __device__ __forceinline__ void InvTileOp<T, UX, UY, UZ, Out>::run(const Params&
     // ---- edge tiles: out-of-range cells from their reflections
     const bool edge = ox < 4 || ox + UX + 4 > a.x || oy < 4 || oy + UY + 4 > a.y || oz < 4 || oz + UZ + 4 > a.z;
     if (edge) {
-        for (int r = warp; r < S::FY * S::FZ; r += 8) {
-            const int fy = r % S::FY, fz = r / S::FY;
-            const int64_t py = int64_t(oy) + fy - 4, pz = int64_t(oz) + fz - 4;
-            const bool row_in = py >= 0 && py < int64_t(a.y) && pz >= 0 && pz < int64_t(a.z);
-            for (int fx = lane; fx < S::FX; fx += 32) {
-                const int64_t px = int64_t(ox) + fx - 4;
-                if (row_in && px >= 0 && px < int64_t(a.x)) continue;
-                const uint32_t mx = mirror(px, a.x), my = mirror(py, a.y), mz = mirror(pz, a.z);
-                const int64_t gx = int64_t(mx) - (int64_t(ox) - 4), gy = int64_t(my) - (int64_t(oy) - 4),
-                              gz = int64_t(mz) - (int64_t(oz) - 4);
-                T v;
-                if (gx >= 0 && gx < S::FX && gy >= 0 && gy < S::FY && gz >= 0 && gz < S::FZ) {
-                    v = *cell(int(gx), int(gy), int(gz));
+        // only the cells outside the array: the in-range footprint is the box
+        // [f*_lo, f*_hi); cells of in-range rows left or right of it (A), and
+        // whole rows outside it in y or z (B), as one flat list
+        const int fx_lo = ox < 4 ? int(4 - ox) : 0, fx_hi = min(S::FX, int(a.x - ox) + 4);
+        const int fy_lo = oy < 4 ? int(4 - oy) : 0, fy_hi = min(S::FY, int(a.y - oy) + 4);
+        const int fz_lo = oz < 4 ? int(4 - oz) : 0, fz_hi = min(S::FZ, int(a.z - oz) + 4);
+        const int nx_out = fx_lo + (S::FX - fx_hi), ny_in = fy_hi - fy_lo, nz_in = fz_hi - fz_lo;
+        const int ny_out = S::FY - ny_in, nz_out = S::FZ - nz_in;
+        const int na = ny_in * nz_in * nx_out;
+        const int nb = (nz_out * S::FY + nz_in * ny_out) * S::FX;
+        for (int i = tid; i < na + nb; i += 256) {
+            int fx, fy, fz;
+            if (i < na) {
+                const int k = i % nx_out, row = i / nx_out;
+                fy = fy_lo + row % ny_in;
+                fz = fz_lo + row / ny_in;
+                fx = k < fx_lo ? k : fx_hi + (k - fx_lo);
+            } else {
+                const int j = i - na;
+                fx = j % S::FX;
+                const int rr = j / S::FX;
+                if (rr < nz_out * S::FY) {
+                    const int zs = rr / S::FY;
+                    fy = rr % S::FY;
+                    fz = zs < fz_lo ? zs : fz_hi + (zs - fz_lo);
                 } else {
-                    const uint32_t cx = split_of(mx, a.x), cy = split_of(my, a.y), cz = split_of(mz, a.z);
-                    if (lv.low && cx < lv.lo.x && cy < lv.lo.y && cz < lv.lo.z)
-                        v = lv.low[(size_t(cz) * lv.lo.y + cy) * lv.lo.x + cx];
-                    else
-                        v = lv.base[size_t(cz) * lv.sz + size_t(cy) * lv.sy + cx];
+                    const int r2 = rr - nz_out * S::FY, ks = r2 % ny_out;
+                    fz = fz_lo + r2 / ny_out;
+                    fy = ks < fy_lo ? ks : fy_hi + (ks - fy_lo);
                 }
-                *cell(fx, fy, fz) = v;
             }
+            const int64_t px = int64_t(ox) + fx - 4, py = int64_t(oy) + fy - 4, pz = int64_t(oz) + fz - 4;
+            const uint32_t mx = mirror(px, a.x), my = mirror(py, a.y), mz = mirror(pz, a.z);
+            const int64_t gx = int64_t(mx) - (int64_t(ox) - 4), gy = int64_t(my) - (int64_t(oy) - 4),
+                          gz = int64_t(mz) - (int64_t(oz) - 4);
+            T v;
+            if (gx >= 0 && gx < S::FX && gy >= 0 && gy < S::FY && gz >= 0 && gz < S::FZ) {
+                v = *cell(int(gx), int(gy), int(gz));
+            } else {
+                const uint32_t cx = split_of(mx, a.x), cy = split_of(my, a.y), cz = split_of(mz, a.z);
+                if (lv.low && cx < lv.lo.x && cy < lv.lo.y && cz < lv.lo.z)
+                    v = lv.low[(size_t(cz) * lv.lo.y + cy) * lv.lo.x + cx];
+                else
+                    v = lv.base[size_t(cz) * lv.sz + size_t(cy) * lv.sy + cx];
+            }
+            *cell(fx, fy, fz) = v;
         }
         __syncthreads();
     }

@@ -111,6 +111,8 @@ __device__ __forceinline__ void FwdStreamOp<T, UX, UY, Q, Tma>::run(const Params
     const int64_t zin1 = 2 * (int64_t((z1 - 1) / 2) + 2) + 2;
     const bool check = src.status != nullptr;
     const bool edge = ox < 4 || ox + UX + 4 > a.x || oy < 4 || oy + UY + 4 > a.y;
+    const int fx_lo = ox < 4 ? int(4 - ox) : 0, fx_hi = min(S::FX, int(a.x - ox) + 4);
+    const int fy_lo = oy < 4 ? int(4 - oy) : 0, fy_hi = min(S::FY, int(a.y - oy) + 4);
 
     // per-thread output columns: x/y parts of the split addresses
     size_t hi_off[S::CPT], lo_off[S::CPT];
@@ -158,24 +160,35 @@ __device__ __forceinline__ void FwdStreamOp<T, UX, UY, Q, Tma>::run(const Params
             }
             phase ^= 1;
             if (edge) {
-                // cells outside the array: reflect from inside the box, or
-                // load when the reflected cell lies outside it
-                for (int r = warp; r < Q * S::FY; r += 8) {
-                    const int q = r / S::FY, fy = r % S::FY;
-                    const int64_t y = int64_t(oy) + fy - 4;
-                    const bool yin = y >= 0 && y < int64_t(a.y);
-                    for (int fx = lane; fx < S::FX; fx += 32) {
-                        const int64_t x = int64_t(ox) + fx - 4;
-                        if (yin && x >= 0 && x < int64_t(a.x)) continue;
-                        const uint32_t mx = mirror(x, a.x), my = mirror(y, a.y);
-                        const int64_t bxm = int64_t(mx) - (int64_t(ox) - 4), bym = int64_t(my) - (int64_t(oy) - 4);
-                        T v;
-                        if (bxm >= 0 && bxm < S::FX && bym >= 0 && bym < S::FY)
-                            v = In[(q * S::FY + int(bym)) * S::FX + int(bxm)];
-                        else
-                            v = src.get(src.row(my, mirror(zb + q, a.z)), mx);
-                        In[r * S::FX + fx] = v;
+                // cells outside the array only (the in-range box of a plane
+                // is [f*_lo, f*_hi)): cells of in-range rows left or right of
+                // it, then whole out-of-range rows, as one flat list; each is
+                // reflected from inside the box, or loaded when its reflection
+                // lies outside the box
+                const int nx_out = fx_lo + (S::FX - fx_hi), ny_in = fy_hi - fy_lo, ny_out = S::FY - ny_in;
+                const int na = Q * ny_in * nx_out, nb = Q * ny_out * S::FX;
+                for (int i = tid; i < na + nb; i += 256) {
+                    int fx, fy, q;
+                    if (i < na) {
+                        const int k = i % nx_out, row = i / nx_out;
+                        fy = fy_lo + row % ny_in;
+                        q = row / ny_in;
+                        fx = k < fx_lo ? k : fx_hi + (k - fx_lo);
+                    } else {
+                        const int j = i - na, rr = j / S::FX, ks = rr % ny_out;
+                        fx = j % S::FX;
+                        q = rr / ny_out;
+                        fy = ks < fy_lo ? ks : fy_hi + (ks - fy_lo);
                     }
+                    const int64_t x = int64_t(ox) + fx - 4, y = int64_t(oy) + fy - 4;
+                    const uint32_t mx = mirror(x, a.x), my = mirror(y, a.y);
+                    const int64_t bxm = int64_t(mx) - (int64_t(ox) - 4), bym = int64_t(my) - (int64_t(oy) - 4);
+                    T v;
+                    if (bxm >= 0 && bxm < S::FX && bym >= 0 && bym < S::FY)
+                        v = In[(q * S::FY + int(bym)) * S::FX + int(bxm)];
+                    else
+                        v = src.get(src.row(my, mirror(zb + q, a.z)), mx);
+                    In[(q * S::FY + fy) * S::FX + fx] = v;
                 }
                 fence_proxy_async(); // these writes precede the next copy into In
                 __syncthreads();
