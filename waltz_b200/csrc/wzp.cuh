@@ -288,11 +288,27 @@ __device__ __forceinline__ void WzpEncodeOp<Src>::run(const Params P, uint32_t, 
         if (uint32_t(g * 32) < blocks * 16) {
             const int top = 32 - __clz(__reduce_or_sync(0xffffffffu, v)); // planes 16-top .. 15 may be set
             uint32_t mine = 0;
+            if (top > 4) {
+                // 32x32 bit transpose across the warp (five butterfly
+                // exchanges): lane p ends with plane p (bit 31-e = bit 15-p of
+                // magnitude e), the decoder's transform run backwards
+                uint32_t x = __brev(v << 16);
 #pragma unroll
-            for (int p = 0; p < 16; ++p) {
-                if (15 - p < top) {
-                    const uint32_t r = __brev(__ballot_sync(0xffffffffu, (v >> (15 - p)) & 1u));
-                    if (lane == p) mine = r;
+                for (int j = 16; j >= 1; j >>= 1) {
+                    const uint32_t m = j == 16 ? 0x0000ffffu : j == 8 ? 0x00ff00ffu : j == 4 ? 0x0f0f0f0fu
+                                     : j == 2  ? 0x33333333u : 0x55555555u;
+                    const uint32_t y = __shfl_xor_sync(0xffffffffu, x, j);
+                    x = (lane & j) ? ((x & ~m) | ((y >> j) & m)) : ((x & m) | ((y << j) & ~m));
+                }
+                mine = __brev(x);
+            } else {
+                // few planes: one ballot each
+#pragma unroll
+                for (int p = 12; p < 16; ++p) {
+                    if (15 - p < top) {
+                        const uint32_t r = __brev(__ballot_sync(0xffffffffu, (v >> (15 - p)) & 1u));
+                        if (lane == p) mine = r;
+                    }
                 }
             }
             // natural layout (the 16 stores share a bank; a padded layout and a
