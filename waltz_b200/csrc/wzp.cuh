@@ -109,6 +109,7 @@ struct WzpEncodeSmem {
     uint8_t lv[2048 + 256 + 32 + 4 + 4]; // nonzero bitmap and its reductions
     uint32_t sgn[kChunk / 32 + 1];     // compacted sign bits (+ slack)
     uint32_t gcount[kChunk / 32];      // nonzero magnitudes per 32-group
+    uint32_t gsign[kChunk / 32];       // per 32-group: sign bits of its nonzero magnitudes, compacted
     uint32_t nsign[kChunk / 32];       // natural sign words of the chunk
     uint32_t bbase[32];                // row-major bases of the chunk's bricks (quantising source)
     uint32_t sel[16];                  // byte_perm selectors: compact the bytes of a 4-bit mask
@@ -284,7 +285,15 @@ __device__ __forceinline__ void WzpEncodeOp<Src>::run(const Params P, uint32_t, 
         const int e = g * 32 + lane;
         const uint32_t v = S.m[e];
         const uint32_t nzmask = __ballot_sync(0xffffffffu, v != 0);
-        if (lane == 0) S.gcount[g] = __popc(nzmask);
+        // the group's nonzero magnitudes' sign bits packed in order (merged
+        // at the group's rank below)
+        const uint32_t pos = __popc(nzmask & ((1u << lane) - 1u));
+        const uint32_t packed =
+            __reduce_or_sync(0xffffffffu, (v != 0 && ((S.nsign[g] >> lane) & 1u)) ? 1u << pos : 0u);
+        if (lane == 0) {
+            S.gcount[g] = __popc(nzmask);
+            S.gsign[g] = packed;
+        }
         if (uint32_t(g * 32) < blocks * 16) {
             const int top = 32 - __clz(__reduce_or_sync(0xffffffffu, v)); // planes 16-top .. 15 may be set
             uint32_t mine = 0;
@@ -325,29 +334,19 @@ __device__ __forceinline__ void WzpEncodeOp<Src>::run(const Params P, uint32_t, 
         reinterpret_cast<uint16_t*>(S.planes)[i] = S.m[i];
     __syncthreads();
 
-    // ---- signs: rank of every nonzero magnitude inside the chunk
+    // ---- signs: each group's packed sign bits go to its rank offset (at most
+    // two words)
     uint32_t nnz;
     {
         const uint32_t gc = tid < int(kChunk / 32) ? S.gcount[tid] : 0;
-        const uint32_t gp = block_excl_scan<kWzpThreads>(gc, S.tmp, nnz);
-        __syncthreads();
-        if (tid < int(kChunk / 32)) S.gcount[tid] = gp; // now the group prefix
-        __syncthreads();
-    }
-    // Each 32-group packs its nonzero magnitudes' sign bits with one warp OR
-    // reduction and merges them at its bit offset (at most two words).
-    for (int g = warp; g < int(kChunk / 32); g += NW) {
-        if (uint32_t(g * 32) >= count) break;
-        const int e = g * 32 + lane;
-        const uint32_t v = S.m[e];
-        const uint32_t nzmask = __ballot_sync(0xffffffffu, v != 0);
-        const uint32_t word = S.nsign[g];
-        const uint32_t pos = __popc(nzmask & ((1u << lane) - 1u));
-        const uint32_t packed = __reduce_or_sync(0xffffffffu, (v != 0 && ((word >> lane) & 1u)) ? 1u << pos : 0u);
-        if (lane == 0 && packed) {
-            const uint32_t r = S.gcount[g], sh = r & 31;
-            atomicOr(&S.sgn[r >> 5], packed << sh);
-            if (sh && (packed >> (32 - sh))) atomicOr(&S.sgn[(r >> 5) + 1], packed >> (32 - sh));
+        const uint32_t r = block_excl_scan<kWzpThreads>(gc, S.tmp, nnz);
+        if (tid < int(kChunk / 32)) {
+            const uint32_t packed = S.gsign[tid];
+            if (packed) {
+                const uint32_t sh = r & 31;
+                atomicOr(&S.sgn[r >> 5], packed << sh);
+                if (sh && (packed >> (32 - sh))) atomicOr(&S.sgn[(r >> 5) + 1], packed >> (32 - sh));
+            }
         }
     }
     __syncthreads();
