@@ -840,15 +840,22 @@ __device__ __forceinline__ void WzpDecodeOp<T>::run(const Params A, uint32_t blo
                 x = (lane & j) ? ((x & ~m) | ((y >> j) & m)) : ((x & m) | ((y << j) & ~m));
             }
             const int e = g * 32 + lane;
-            if (uint32_t(e) < blocks * 16) S.m[e] = uint16_t(__brev(x) >> 16);
+            const uint32_t mag = __brev(x) >> 16;
+            if (uint32_t(e) < blocks * 16) S.m[e] = uint16_t(mag);
+            // groups wholly inside the planes: their nonzero count now
+            if (uint32_t(g * 32 + 32) <= blocks * 16) {
+                const uint32_t nzm = __ballot_sync(0xffffffffu, mag != 0);
+                if (lane == 0) S.gprefix[g] = __popc(nzm);
+            }
         }
         for (uint32_t i = blocks * 16 + tid; i < kChunk; i += kWzpThreads)
             S.m[i] = i == ti ? tail : 0;
     }
     __syncthreads();
 
-    // ---- signs and dequantisation
-    for (int g = warp; g < int(kChunk / 32); g += NW) {
+    // ---- signs and dequantisation: nonzero counts of the remaining groups
+    const int counted = (mbytes != 0 && !S.raw) ? int(blocks * 16 / 32) : 0;
+    for (int g = counted + warp; g < int(kChunk / 32); g += NW) {
         const uint32_t nzm = __ballot_sync(0xffffffffu, S.m[g * 32 + lane] != 0);
         if (lane == 0) S.gprefix[g] = __popc(nzm);
     }
