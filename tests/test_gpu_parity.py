@@ -495,3 +495,30 @@ def test_tuning_knobs_never_change_the_bytes():
     finally:
         A.set_single(lib, {})
         lib.waltz_b200_batch_config(1, 32)
+
+
+def test_unaligned_archive_addresses():
+    """Archives written to and decoded from odd device addresses give the same
+    bytes and samples (the side-record sections then take byte-wide paths)."""
+    torch = _torch()
+    import waltz_b200
+    from waltz_b200 import _lib as L
+    from waltz_b200 import synthetic as S
+    lib = _lib()
+    for shape, dt in [((48, 64, 80), np.float32), ((20, 33, 40), np.float64)]:
+        f = torch.from_numpy(S.power_law_field(shape, 21).astype(dt)).cuda()
+        ref = waltz_b200.compress_tensor(f, 1e-4)  # many repair records at this bound
+        assert int.from_bytes(bytes(ref[24:28].cpu().numpy()), "little") > 0
+        nz, ny, nx = shape
+        w = f.element_size()
+        cap = waltz_b200.compressed_capacity(f.numel(), w)
+        buf = torch.zeros(cap + 16, dtype=torch.uint8, device="cuda")
+        written = C.c_size_t()
+        for off in (1, 3):
+            L.checked(lib.waltz_b200_compress(C.c_void_p(f.data_ptr()), w, nx, ny, nz, 1e-4,
+                                              C.c_void_p(buf.data_ptr() + off), cap, C.byref(written), _stream()))
+            assert torch.equal(buf[off:off + written.value], ref)
+            out = torch.empty_like(f)
+            L.checked(lib.waltz_b200_decompress(C.c_void_p(buf.data_ptr() + off), written.value, w, nx, ny, nz,
+                                                C.c_void_p(out.data_ptr()), out.numel() * w, _stream()))
+            assert torch.equal(out, waltz_b200.decompress_tensor(ref, shape, f.dtype))

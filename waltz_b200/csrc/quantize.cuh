@@ -301,18 +301,25 @@ __device__ __forceinline__ void compact_write_block(uint32_t bx, const uint32_t*
     if (layout[7]) return; // layout overflow: nothing is written
     uint8_t* idx = archive + layout[idx_slot];
     uint8_t* val = archive + layout[val_slot];
+    const bool aligned = (reinterpret_cast<uintptr_t>(archive) & 7u) == 0;
     for (int k = 0; k < 4; ++k)
         for (uint32_t b = wv[k]; b; b &= b - 1) {
             const uint64_t i = (w0 + k) * 32 + (__ffs(b) - 1);
             if (r < cap_records) {
                 const uint32_t ii = uint32_t(i);
-                idx[4 * uint64_t(r) + 0] = uint8_t(ii);
-                idx[4 * uint64_t(r) + 1] = uint8_t(ii >> 8);
-                idx[4 * uint64_t(r) + 2] = uint8_t(ii >> 16);
-                idx[4 * uint64_t(r) + 3] = uint8_t(ii >> 24);
                 const V v = values[i];
-                const uint8_t* vb = reinterpret_cast<const uint8_t*>(&v);
-                for (int j = 0; j < int(sizeof(V)); ++j) val[sizeof(V) * uint64_t(r) + j] = vb[j];
+                if (aligned) {
+                    // sections start on 8-byte offsets: whole-word stores
+                    reinterpret_cast<uint32_t*>(idx)[r] = ii;
+                    reinterpret_cast<V*>(val)[r] = v;
+                } else {
+                    idx[4 * uint64_t(r) + 0] = uint8_t(ii);
+                    idx[4 * uint64_t(r) + 1] = uint8_t(ii >> 8);
+                    idx[4 * uint64_t(r) + 2] = uint8_t(ii >> 16);
+                    idx[4 * uint64_t(r) + 3] = uint8_t(ii >> 24);
+                    const uint8_t* vb = reinterpret_cast<const uint8_t*>(&v);
+                    for (int j = 0; j < int(sizeof(V)); ++j) val[sizeof(V) * uint64_t(r) + j] = vb[j];
+                }
             }
             ++r;
         }
@@ -451,12 +458,19 @@ __device__ __forceinline__ void QPatchOp<T>::run(const Params P, uint32_t block,
     uint32_t* const status = P.status;
     const DecodeJob J = P.job.get();
     const uint8_t *qi = J.base + J.qi, *qv = J.base + J.qv;
+    const bool aligned = (reinterpret_cast<uintptr_t>(J.base) & 7u) == 0; // sections on 8-byte offsets
     const T q = T(J.q);
     for (uint32_t i = block * kThreads + threadIdx.x; i < J.nq; i += blocks * kThreads) {
         uint32_t at, v, prev = 0;
-        memcpy(&at, qi + 4 * uint64_t(i), 4);
-        memcpy(&v, qv + 4 * uint64_t(i), 4);
-        if (i) memcpy(&prev, qi + 4 * uint64_t(i - 1), 4);
+        if (aligned) {
+            at = reinterpret_cast<const uint32_t*>(qi)[i];
+            v = reinterpret_cast<const uint32_t*>(qv)[i];
+            if (i) prev = reinterpret_cast<const uint32_t*>(qi)[i - 1];
+        } else {
+            memcpy(&at, qi + 4 * uint64_t(i), 4);
+            memcpy(&v, qv + 4 * uint64_t(i), 4);
+            if (i) memcpy(&prev, qi + 4 * uint64_t(i - 1), 4);
+        }
         if (at >= n) { atomicOr(status, ST_BAD_INDEX); continue; }
         if (i && prev >= at) atomicOr(status, ST_UNORDERED);
         if (v <= 65535u || v > 0x7fffffffu) { atomicOr(status, ST_BAD_QOUT); continue; }
@@ -500,12 +514,19 @@ __device__ __forceinline__ void RPatchOp<T, Patch>::run(const Params P, uint32_t
     uint32_t* const status = P.status;
     const DecodeJob J = P.job.get();
     const uint8_t *pi = J.base + J.pi, *pv = J.base + J.pv;
+    const bool aligned = (reinterpret_cast<uintptr_t>(J.base) & 7u) == 0; // sections on 8-byte offsets
     for (uint32_t i = block * kThreads + threadIdx.x; i < J.np; i += blocks * kThreads) {
         uint32_t at, prev = 0;
         T err;
-        memcpy(&at, pi + 4 * uint64_t(i), 4);
-        memcpy(&err, pv + sizeof(T) * uint64_t(i), sizeof(T));
-        if (i) memcpy(&prev, pi + 4 * uint64_t(i - 1), 4);
+        if (aligned) {
+            at = reinterpret_cast<const uint32_t*>(pi)[i];
+            err = reinterpret_cast<const T*>(pv)[i];
+            if (i) prev = reinterpret_cast<const uint32_t*>(pi)[i - 1];
+        } else {
+            memcpy(&at, pi + 4 * uint64_t(i), 4);
+            memcpy(&err, pv + sizeof(T) * uint64_t(i), sizeof(T));
+            if (i) memcpy(&prev, pi + 4 * uint64_t(i - 1), 4);
+        }
         if (at >= n) { atomicOr(status, ST_BAD_INDEX); continue; }
         if (i && prev >= at) atomicOr(status, ST_UNORDERED);
         if (!finite_bits(err)) { atomicOr(status, ST_BAD_REPAIR); continue; }
