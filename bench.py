@@ -340,7 +340,7 @@ def gpu_arm(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(field.cpu().numpy(), eb)
     if not args.no_tc_form and world == 1:
-        del field, out, archive, host_in, host_arch, host_out
+        del field, out, archive, host_in
         torch.cuda.empty_cache()
         result["tc_form"] = tc_form_comparison(dev, lib, args.steps, tuple(args.tc_shape))
     if not args.no_batch and world == 1:
