@@ -624,7 +624,7 @@ template <class T> struct WzpDecodeArgs {
 };
 
 template <class T> struct WzpDecodeOp {
-    static constexpr int kThreads = kWzpThreads, kMinBlocks = 0; // no occupancy floor: the compiler picks the register budget
+    static constexpr int kThreads = kWzpThreads, kMinBlocks = 4; // 32 registers: four CTAs per SM
     using Params = WzpDecodeArgs<T>;
     static __device__ __forceinline__ void run(const Params A, uint32_t block, uint32_t);
 };
