@@ -602,11 +602,11 @@ def batch_only(dev, lib, args, count=512):
 # scaled by the sample ratio 512^3 / (256*384*384) = 3.5556; traffic grows in
 # proportion to the samples processed.
 TRAFFIC_512 = {
-    "compress:fwd_l0": 992205027,
-    "compress:wzp_encode": 976033109,
-    "compress:inv_l0_repair": 1287420131,
-    "decompress:wzp_decode": 444504291,
-    "decompress:inv_l0": 965358023,
+    "compress:fwd_l0": 1011955940,
+    "compress:wzp_encode": 982265401,
+    "compress:inv_l0_repair": 1287945330,
+    "decompress:wzp_decode": 442284260,
+    "decompress:inv_l0": 966507634,
 }
 
 
