@@ -56,6 +56,13 @@ constexpr uint32_t kEncBytes = 2 * kChunk + 2048 + 256 + 32 + 4 + 28;
 // from the natural layout by a conflict-free pass (consecutive threads on
 // consecutive natural words).
 constexpr uint32_t kPlanePitch = kChunk / 32 + 1; // u32 words per padded plane
+// The encoder's full chunks store their planes at a pitch of 260 u32 words:
+// lane p's word of group g lands in bank (4p + g) mod 32 (two lanes per bank
+// instead of sixteen), and a thread's 32 consecutive natural bytes (8 words
+// of one plane) stay 16-byte aligned and contiguous at natural word 8t plus
+// 4 * (t / 32), so the zero elimination reads them in place, no repacking.
+constexpr uint32_t kEncPitch = kChunk / 32 + 4;
+static_assert(16 * kEncPitch * 4 <= kEncBytes, "padded encoder planes fit the plane buffer");
 
 // natural -> padded (dir = true) or padded -> natural, in place in `buf`
 // (room for 16 * kPlanePitch words); the caller syncs before and after.
@@ -320,12 +327,17 @@ __device__ __forceinline__ void WzpEncodeOp<Src>::run(const Params P, uint32_t, 
                     }
                 }
             }
-            // natural layout (the 16 stores share a bank; a padded layout and a
-            // repacking pass measured slower here, stores do not stall the warp)
-            uint16_t* pl = reinterpret_cast<uint16_t*>(S.planes);
+            // full chunks: one word per plane at the padded pitch (blocks 2g
+            // and 2g+1 in its low and high halves); a partial chunk keeps the
+            // natural layout, u16 words at p * blocks + b
             if (lane < 16) {
-                pl[lane * blocks + 2 * g] = uint16_t(mine >> 16);
-                if (uint32_t(2 * g + 1) < blocks) pl[lane * blocks + 2 * g + 1] = uint16_t(mine & 0xffffu);
+                if (blocks == kChunk / 16) {
+                    reinterpret_cast<uint32_t*>(S.planes)[lane * kEncPitch + g] = __funnelshift_l(mine, mine, 16);
+                } else {
+                    uint16_t* pl = reinterpret_cast<uint16_t*>(S.planes);
+                    pl[lane * blocks + 2 * g] = uint16_t(mine >> 16);
+                    if (uint32_t(2 * g + 1) < blocks) pl[lane * blocks + 2 * g + 1] = uint16_t(mine & 0xffffu);
+                }
             }
         }
     }
@@ -357,7 +369,8 @@ __device__ __forceinline__ void WzpEncodeOp<Src>::run(const Params P, uint32_t, 
     {
         const uint32_t b0 = tid * 32;
         uint32_t w[8];
-        const uint4* q = reinterpret_cast<const uint4*>(S.planes + b0);
+        const uint32_t pad = blocks == kChunk / 16 ? 4 * (kEncPitch - kChunk / 32) * (uint32_t(tid) >> 5) : 0u;
+        const uint4* q = reinterpret_cast<const uint4*>(S.planes + b0 + pad);
         const uint4 q0 = q[0], q1 = q[1];
         w[0] = q0.x; w[1] = q0.y; w[2] = q0.z; w[3] = q0.w;
         w[4] = q1.x; w[5] = q1.y; w[6] = q1.z; w[7] = q1.w;
