@@ -51,17 +51,18 @@ constexpr uint32_t kEncBytes = 2 * kChunk + 2048 + 256 + 32 + 4 + 28;
 
 // Bit planes in shared memory: the stream's natural layout puts plane p's
 // u16 word b at p * blocks + b, so the 16 lanes that hold the 16 planes of one
-// 32-sample group would all hit one bank. The decoder therefore reads them
-// from a padded layout, plane p at u32 word p * kPlanePitch + group, filled
-// from the natural layout by a conflict-free pass (consecutive threads on
+// 32-sample group would all hit one bank. Both directions therefore keep the
+// planes of a full chunk (512 blocks) at a padded pitch of kEncPitch u32
+// words: lane p's word of group g lands in bank (4p + g) mod 32 (two lanes per
+// bank instead of sixteen), and a thread's 32 consecutive natural bytes
+// (8 words of one plane) stay 16-byte aligned and contiguous at natural word
+// 8t plus 4 * (t / 32), so the zero elimination reads them, and the decoder's
+// byte spreading writes them, in place. A partial chunk (a field's last)
+// keeps the natural layout; the decoder repacks it to plane p at u32 word
+// p * kPlanePitch + group by a conflict-free pass (consecutive threads on
 // consecutive natural words).
-constexpr uint32_t kPlanePitch = kChunk / 32 + 1; // u32 words per padded plane
-// The encoder's full chunks store their planes at a pitch of 260 u32 words:
-// lane p's word of group g lands in bank (4p + g) mod 32 (two lanes per bank
-// instead of sixteen), and a thread's 32 consecutive natural bytes (8 words
-// of one plane) stay 16-byte aligned and contiguous at natural word 8t plus
-// 4 * (t / 32), so the zero elimination reads them in place, no repacking.
-constexpr uint32_t kEncPitch = kChunk / 32 + 4;
+constexpr uint32_t kPlanePitch = kChunk / 32 + 1; // u32 words per padded plane, partial chunks
+constexpr uint32_t kEncPitch = kChunk / 32 + 4;   // u32 words per padded plane, full chunks
 static_assert(16 * kEncPitch * 4 <= kEncBytes, "padded encoder planes fit the plane buffer");
 
 // natural -> padded (dir = true) or padded -> natural, in place in `buf`
@@ -135,6 +136,24 @@ struct WzpEncodeArgs {
     uint32_t spin_cap;  // lookback wait bound (polls of ~0.2 us)
     uint32_t skip_publish; // test hook: this chunk never publishes (0xffffffff = none)
 };
+
+// 32x32 bit transpose across a warp (five butterfly exchanges): on return
+// lane i holds in bit j what lane j held in bit i. The half-word and byte
+// exchanges are byte permutes; the nibble, pair and bit exchanges are shifts
+// under the stage's mask.
+__device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, int lane) {
+    uint32_t y = __shfl_xor_sync(0xffffffffu, x, 16);
+    x = __byte_perm(x, y, (lane & 16) ? 0x3276u : 0x5410u);
+    y = __shfl_xor_sync(0xffffffffu, x, 8);
+    x = __byte_perm(x, y, (lane & 8) ? 0x3715u : 0x6240u);
+#pragma unroll
+    for (int j = 4; j >= 1; j >>= 1) {
+        const uint32_t m = j == 4 ? 0x0f0f0f0fu : j == 2 ? 0x33333333u : 0x55555555u;
+        y = __shfl_xor_sync(0xffffffffu, x, j);
+        x = (lane & j) ? ((x & ~m) | ((y >> j) & m)) : ((x & m) | ((y << j) & ~m));
+    }
+    return x;
+}
 
 // 4-bit mask of the nonzero bytes of w (bit k = byte k).
 __device__ __forceinline__ uint32_t nonzero_nibble(uint32_t w) { return (__vsetne4(w, 0u) * 0x01020408u) >> 24; }
@@ -286,58 +305,55 @@ __device__ __forceinline__ void WzpEncodeOp<Src>::run(const Params P, uint32_t, 
     for (int i = tid; i < int(kChunk / 32) + 1; i += kWzpThreads) S.sgn[i] = 0;
     __syncthreads();
 
-    // ---- per 32-group nonzero counts, bit planes (warp ballots; planes above
-    // the group's highest set bit are zero and skip their ballots)
-    for (int g = warp; g < int(kChunk / 32); g += NW) {
-        const int e = g * 32 + lane;
-        const uint32_t v = S.m[e];
-        const uint32_t nzmask = __ballot_sync(0xffffffffu, v != 0);
-        // the group's nonzero magnitudes' sign bits packed in order (merged
+    // ---- per 32-group nonzero counts and sign bits, and the bit planes, two
+    // groups per warp step: one 32x32 transpose turns the pair's 16-bit
+    // magnitudes (group g in the high half of each lane's word, g+1 in the
+    // low half) into plane p of g in lane p and of g+1 in lane 16+p
+    const uint32_t in_planes = blocks * 16;
+    for (int k = warp; k < int(kChunk / 64); k += NW) {
+        const int g0 = 2 * k, e0 = g0 * 32 + lane;
+        const uint32_t v = S.m[e0], u = S.m[e0 + 32];
+        const uint32_t nz0 = __ballot_sync(0xffffffffu, v != 0), nz1 = __ballot_sync(0xffffffffu, u != 0);
+        // each group's nonzero magnitudes' sign bits packed in order (merged
         // at the group's rank below)
-        const uint32_t pos = __popc(nzmask & ((1u << lane) - 1u));
-        const uint32_t packed =
-            __reduce_or_sync(0xffffffffu, (v != 0 && ((S.nsign[g] >> lane) & 1u)) ? 1u << pos : 0u);
-        if (lane == 0) {
-            S.gcount[g] = __popc(nzmask);
-            S.gsign[g] = packed;
+        const uint32_t below = (1u << lane) - 1u;
+        const uint32_t s0 = __reduce_or_sync(
+            0xffffffffu, (v != 0 && ((S.nsign[g0] >> lane) & 1u)) ? 1u << __popc(nz0 & below) : 0u);
+        const uint32_t s1 = __reduce_or_sync(
+            0xffffffffu, (u != 0 && ((S.nsign[g0 + 1] >> lane) & 1u)) ? 1u << __popc(nz1 & below) : 0u);
+        if (lane < 2) {
+            S.gcount[g0 + lane] = __popc(lane ? nz1 : nz0);
+            S.gsign[g0 + lane] = lane ? s1 : s0;
         }
-        if (uint32_t(g * 32) < blocks * 16) {
-            const int top = 32 - __clz(__reduce_or_sync(0xffffffffu, v)); // planes 16-top .. 15 may be set
+        if (uint32_t(g0 * 32) < in_planes) {
+            const uint32_t va = uint32_t(e0) < in_planes ? v : 0u, ua = uint32_t(e0 + 32) < in_planes ? u : 0u;
+            const int top = 32 - __clz(__reduce_or_sync(0xffffffffu, va | ua)); // planes 16-top .. 15 may be set
             uint32_t mine = 0;
-            if (top > 4) {
-                // 32x32 bit transpose across the warp (five butterfly
-                // exchanges): lane p ends with plane p (bit 31-e = bit 15-p of
-                // magnitude e), the decoder's transform run backwards
-                uint32_t x = __brev(v << 16);
-#pragma unroll
-                for (int j = 16; j >= 1; j >>= 1) {
-                    const uint32_t m = j == 16 ? 0x0000ffffu : j == 8 ? 0x00ff00ffu : j == 4 ? 0x0f0f0f0fu
-                                     : j == 2  ? 0x33333333u : 0x55555555u;
-                    const uint32_t y = __shfl_xor_sync(0xffffffffu, x, j);
-                    x = (lane & j) ? ((x & ~m) | ((y >> j) & m)) : ((x & m) | ((y << j) & ~m));
-                }
-                mine = __brev(x);
+            if (top > 2) {
+                mine = __brev(warp_transpose32(__brev((va << 16) | ua), lane));
             } else {
-                // few planes: one ballot each
+                // one or two planes: a ballot each (bit 31-e = magnitude e's bit)
 #pragma unroll
-                for (int p = 12; p < 16; ++p) {
+                for (int p = 14; p < 16; ++p) {
                     if (15 - p < top) {
-                        const uint32_t r = __brev(__ballot_sync(0xffffffffu, (v >> (15 - p)) & 1u));
-                        if (lane == p) mine = r;
+                        const uint32_t r0 = __brev(__ballot_sync(0xffffffffu, (va >> (15 - p)) & 1u));
+                        const uint32_t r1 = __brev(__ballot_sync(0xffffffffu, (ua >> (15 - p)) & 1u));
+                        if (lane == p) mine = r0;
+                        if (lane == 16 + p) mine = r1;
                     }
                 }
             }
-            // full chunks: one word per plane at the padded pitch (blocks 2g
-            // and 2g+1 in its low and high halves); a partial chunk keeps the
-            // natural layout, u16 words at p * blocks + b
-            if (lane < 16) {
-                if (blocks == kChunk / 16) {
-                    reinterpret_cast<uint32_t*>(S.planes)[lane * kEncPitch + g] = __funnelshift_l(mine, mine, 16);
-                } else {
-                    uint16_t* pl = reinterpret_cast<uint16_t*>(S.planes);
-                    pl[lane * blocks + 2 * g] = uint16_t(mine >> 16);
-                    if (uint32_t(2 * g + 1) < blocks) pl[lane * blocks + 2 * g + 1] = uint16_t(mine & 0xffffu);
-                }
+            // lane l holds plane l % 16 of group g0 + l / 16 (blocks 2g, 2g+1 in
+            // its high and low halves); full chunks: one word at the padded
+            // pitch; a partial chunk keeps the natural layout, u16 words at
+            // p * blocks + b
+            const uint32_t g = uint32_t(g0) + (uint32_t(lane) >> 4), pl_ = uint32_t(lane) & 15u;
+            if (blocks == kChunk / 16) {
+                reinterpret_cast<uint32_t*>(S.planes)[pl_ * kEncPitch + g] = __funnelshift_l(mine, mine, 16);
+            } else {
+                uint16_t* pl = reinterpret_cast<uint16_t*>(S.planes);
+                if (2 * g < blocks) pl[pl_ * blocks + 2 * g] = uint16_t(mine >> 16);
+                if (2 * g + 1 < blocks) pl[pl_ * blocks + 2 * g + 1] = uint16_t(mine & 0xffffu);
             }
         }
     }
@@ -581,7 +597,9 @@ struct WzpDecodeSmem {
     uint16_t m[kChunk + 16];           // staged magnitude bytes, then the decoded magnitudes
     uint8_t sb[1024 + 32];             // staged sign bytes
     uint32_t xsel[16];                 // byte_perm selectors: spread 4-bit-mask bytes into place
-    uint8_t planes[16 * kPlanePitch * 4]; // natural planes, then the padded layout
+    // full chunks: planes at pitch kEncPitch; a partial chunk: natural, then
+    // repacked to pitch kPlanePitch
+    uint8_t planes[16 * (kEncPitch > kPlanePitch ? kEncPitch : kPlanePitch) * 4];
     uint8_t lv[2048 + 256 + 32 + 4];
     uint32_t gprefix[kChunk / 32];
     uint32_t tmp[40];
@@ -820,46 +838,45 @@ __device__ __forceinline__ void WzpDecodeOp<T>::run(const Params A, uint32_t blo
                 r += __popc(m4);
             }
             __syncthreads(); // every thread has read the staged bytes it needs
-            uint4* out = reinterpret_cast<uint4*>(S.planes + b0);
+            // full chunks write the padded layout (plane t / 32 at pitch
+            // kEncPitch) straight away; a partial chunk writes the natural one
+            const uint32_t pad = blocks == kChunk / 16 ? 4 * (kEncPitch - kChunk / 32) * (uint32_t(tid) >> 5) : 0u;
+            uint4* out = reinterpret_cast<uint4*>(S.planes + b0 + pad);
             out[0] = make_uint4(words[0], words[1], words[2], words[3]);
             out[1] = make_uint4(words[4], words[5], words[6], words[7]);
         }
         __syncthreads();
-        // the verbatim tail (samples past the last whole block) while the
-        // planes are still in the natural layout
+        // the verbatim tail (samples past the last whole block) while a
+        // partial chunk's planes are still in the natural layout
         const uint16_t* pl = reinterpret_cast<const uint16_t*>(S.planes);
         uint16_t tail = 0;
         const uint32_t ti = blocks * 16 + tid;
         if (ti < count) tail = pl[ti];
-        planes_repack(S.planes, blocks, true, tid);
+        const bool full = blocks == kChunk / 16;
+        if (!full) planes_repack(S.planes, blocks, true, tid);
         __syncthreads();
-        // ---- inverse bit planes: lane p < 16 holds plane p of the group's 32
-        // magnitudes (bit e = magnitude e's bit 15-p); a 32x32 bit transpose
-        // across the warp (five butterfly exchanges) leaves magnitude e in lane e
-        for (int g = warp; g < int(kChunk / 32); g += NW) {
-            if (uint32_t(g * 32) >= blocks * 16) break;
-            uint32_t x = 0;
-            if (lane < 16) {
-                uint32_t w = __funnelshift_l(reinterpret_cast<const uint32_t*>(S.planes)[lane * kPlanePitch + g],
-                                             reinterpret_cast<const uint32_t*>(S.planes)[lane * kPlanePitch + g], 16);
-                if (uint32_t(2 * g + 1) >= blocks) w &= 0xffff0000u;
-                x = __brev(w);
+        // ---- inverse bit planes, two groups per warp step: lane l holds plane
+        // l % 16 of group g0 + l / 16 (bit 31-e = magnitude e's bit 15-p); one
+        // 32x32 transpose leaves magnitude e of g0 in the high half of lane e's
+        // word and of g0 + 1 in the low half
+        const uint32_t pitch = full ? kEncPitch : kPlanePitch, in_planes = blocks * 16;
+        for (int k = warp; k < int(kChunk / 64); k += NW) {
+            const int g0 = 2 * k;
+            if (uint32_t(g0 * 32) >= in_planes) break;
+            const uint32_t g = uint32_t(g0) + (uint32_t(lane) >> 4);
+            uint32_t w = 0;
+            if (2 * g < blocks) {
+                const uint32_t word = reinterpret_cast<const uint32_t*>(S.planes)[(uint32_t(lane) & 15u) * pitch + g];
+                w = __funnelshift_l(word, word, 16);
+                if (2 * g + 1 >= blocks) w &= 0xffff0000u;
             }
-#pragma unroll
-            for (int j = 16; j >= 1; j >>= 1) {
-                const uint32_t m = j == 16 ? 0x0000ffffu : j == 8 ? 0x00ff00ffu : j == 4 ? 0x0f0f0f0fu
-                                 : j == 2  ? 0x33333333u : 0x55555555u;
-                const uint32_t y = __shfl_xor_sync(0xffffffffu, x, j);
-                x = (lane & j) ? ((x & ~m) | ((y >> j) & m)) : ((x & m) | ((y << j) & ~m));
-            }
-            const int e = g * 32 + lane;
-            const uint32_t mag = __brev(x) >> 16;
-            if (uint32_t(e) < blocks * 16) S.m[e] = uint16_t(mag);
-            // groups wholly inside the planes: their nonzero count now
-            if (uint32_t(g * 32 + 32) <= blocks * 16) {
-                const uint32_t nzm = __ballot_sync(0xffffffffu, mag != 0);
-                if (lane == 0) S.gprefix[g] = __popc(nzm);
-            }
+            const uint32_t r = __brev(warp_transpose32(__brev(w), lane));
+            const uint32_t e0 = uint32_t(g0) * 32 + lane, m0 = r >> 16, m1 = r & 0xffffu;
+            if (e0 < in_planes) S.m[e0] = uint16_t(m0);
+            if (e0 + 32 < in_planes) S.m[e0 + 32] = uint16_t(m1);
+            // groups wholly inside the planes: their nonzero counts now
+            const uint32_t nzm0 = __ballot_sync(0xffffffffu, m0 != 0), nzm1 = __ballot_sync(0xffffffffu, m1 != 0);
+            if (lane < 2 && (uint32_t(g0) + lane) * 32 + 32 <= in_planes) S.gprefix[g0 + lane] = __popc(lane ? nzm1 : nzm0);
         }
         for (uint32_t i = blocks * 16 + tid; i < kChunk; i += kWzpThreads)
             S.m[i] = i == ti ? tail : 0;
