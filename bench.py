@@ -15,7 +15,13 @@ time over ranks.
 
 `--impl reference` times the reference's own CPU codec (compiled from its
 sources into oracle/_ref, AVX2 backend) on the host cores with one thread
-per core, on the same field split into its eight 256^3 octants.
+per core, on the same field split into its eight 256^3 octants (64 blocks of
+128^3 with more than 8 threads).
+
+Beside the line's own numbers: `cpu_baseline` (the reference CPU codec, one
+core, a bounded sample) and `gpu_baseline` (the reference's own CUDA library,
+built from its sources for sm_100a, on the same field, bound and GPU, with
+its archive compared byte for byte with ours).
 """
 from __future__ import annotations
 
@@ -339,6 +345,8 @@ def gpu_arm(args, rank, world, local_rank):
         result["roofline"]["traffic"] = TRAFFIC_512[dom]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(field.cpu().numpy(), eb)
+    if rank == 0 and world == 1 and not args.no_gpu_baseline:
+        result["gpu_baseline"] = gpu_baseline(field, eb, archive[:a_bytes], min(args.steps, 10))
     if not args.no_tc_form and world == 1:
         del field, out, archive, host_in
         torch.cuda.empty_cache()
@@ -685,6 +693,47 @@ def cpu_baseline(field, eb, budget_s=12.0):
                       f"reference CPU codec AVX2 backend, 1 thread ({secs:.1f} s)"}
 
 
+def gpu_baseline(field, eb, ours, steps):
+    """The reference's own CUDA library (oracle/_ref/libwaltz_refgpu.so, its
+    src/waltz.cu and src/lossless/wzp.cu compiled for sm_100a) on the same
+    field, bound and GPU: device-resident input, one compress and one
+    decompress per step, CUDA events around each call, median over `steps`
+    after two warm-up steps. Its archive is compared with ours byte for byte."""
+    import torch
+    from oracle import oracle as O
+    if not O.refgpu_available():
+        return {"unavailable": "reference CUDA library not built (make -C oracle refgpu)"}
+    lib = O.refgpu_lib()
+    shape, width = tuple(field.shape), field.element_size()
+    src = field.clone()  # the reference takes a mutable input pointer
+    arch = torch.empty(lib.refgpu_capacity(field.numel(), width), dtype=torch.uint8, device=field.device)
+    out = torch.empty_like(field)
+    stream = torch.cuda.current_stream().cuda_stream
+    tc, td, size = [], [], 0
+    for it in range(2 + steps):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record()
+        size = O.refgpu_compress(src.data_ptr(), width, shape, eb, arch.data_ptr(), stream)
+        e[1].record()
+        O.refgpu_decompress(arch.data_ptr(), width, shape, out.data_ptr(), stream)
+        e[2].record()
+        torch.cuda.synchronize()
+        if it >= 2:
+            tc.append(e[0].elapsed_time(e[1]))
+            td.append(e[1].elapsed_time(e[2]))
+    nbytes = field.numel() * width
+    t_c, t_d = statistics.median(tc), statistics.median(td)
+    identical = size == ours.numel() and bool(torch.equal(arch[:size], ours))
+    worst = float((out.double() - field.double()).abs().max())
+    del src, arch, out
+    return {"value": round(nbytes / ((t_c + t_d) / 1e3) / 1e9, 3), "unit": "GB/s",
+            "compress_gbs": round(nbytes / (t_c / 1e3) / 1e9, 3),
+            "decompress_gbs": round(nbytes / (t_d / 1e3) / 1e9, 3),
+            "ms_per_step": round(t_c + t_d, 4), "archive_bytes": size, "archive_identical_to_ours": identical,
+            "max_abs_error": worst, "kind": "reference CUDA library, same GPU",
+            "sample": f"same field and bound, {steps} steps after 2 warm-up, device-resident"}
+
+
 def cpu_batch_baseline(chunks, bounds, budget_s=10.0):
     """Reference CPU codec (oracle/_ref, AVX2) over the chunk list with one
     workspace per thread (up to 8 threads), compress + decompress per chunk,
@@ -772,6 +821,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-gpu-baseline", action="store_true",
+                    help="skip the reference CUDA library timed on the same GPU")
     ap.add_argument("--no-tc-form", action="store_true", help="skip the plain vs tensor-core form comparison")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched vs per-chunk comparison")
     ap.add_argument("--tc-shape", type=int, nargs=3, default=[64, 1024, 1024], metavar=("NZ", "NY", "NX"),

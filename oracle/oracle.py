@@ -8,10 +8,13 @@ Two libraries live here:
 * ``_ref/libwaltz_ref.so`` -- the reference CPU codec compiled from its own
   sources (``make -C oracle ref``); present only where the reference sources
   were available when it was built.
+* ``_ref/libwaltz_refgpu.so`` -- the reference's own CUDA library compiled for
+  sm_100a from its sources (``make -C oracle refgpu``): a second checker on the
+  GPU (its archives must equal the product's) and the same-GPU baseline.
 
-Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
-``bench.py`` import this module, and only as the checker. The GPU product
-never imports it.
+Only tests/, ``__graft_entry__.smoke()`` and the baseline legs of
+``bench.py`` import this module, and only as the checker or the baseline.
+The GPU product never imports it.
 """
 from __future__ import annotations
 
@@ -26,6 +29,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "liboracle.so"
 REF_SO = HERE / "_ref" / "libwaltz_ref.so"
+REFGPU_SO = HERE / "_ref" / "libwaltz_refgpu.so"
 
 
 class WoConfig(C.Structure):
@@ -103,6 +107,48 @@ def ref_lib():
         fn = getattr(lib, name)
         fn.restype, fn.argtypes = res, args
     return lib
+
+
+def refgpu_available() -> bool:
+    return REFGPU_SO.exists()
+
+
+@lru_cache(maxsize=1)
+def refgpu_lib():
+    """The reference CUDA library (device pointers; see ref_gpu_shim.cu)."""
+    if not REFGPU_SO.exists():
+        raise FileNotFoundError("reference CUDA library not built (make -C oracle refgpu)")
+    lib = C.CDLL(str(REFGPU_SO))
+    p, u32 = C.c_void_p, C.c_uint32
+    sig = {
+        "refgpu_last_error": (C.c_char_p, []),
+        "refgpu_capacity": (C.c_size_t, [C.c_uint64, C.c_int]),
+        "refgpu_compress": (C.c_int, [p, C.c_int, u32, u32, u32, C.c_double, p, C.POINTER(C.c_size_t), p]),
+        "refgpu_decompress": (C.c_int, [p, C.c_int, u32, u32, u32, p, p]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype, fn.argtypes = res, args
+    return lib
+
+
+def refgpu_compress(d_in: int, width: int, shape, abs_error: float, d_out: int, stream: int) -> int:
+    """Archive bytes the reference CUDA library writes at d_out (device
+    pointers, (z, y, x) shape)."""
+    nz, ny, nx = shape
+    w = C.c_size_t()
+    lib = refgpu_lib()
+    if lib.refgpu_compress(C.c_void_p(d_in), width, nx, ny, nz, abs_error, C.c_void_p(d_out), C.byref(w),
+                           C.c_void_p(stream)):
+        raise RuntimeError(lib.refgpu_last_error().decode())
+    return w.value
+
+
+def refgpu_decompress(d_archive: int, width: int, shape, d_out: int, stream: int) -> None:
+    nz, ny, nx = shape
+    lib = refgpu_lib()
+    if lib.refgpu_decompress(C.c_void_p(d_archive), width, nx, ny, nz, C.c_void_p(d_out), C.c_void_p(stream)):
+        raise RuntimeError(lib.refgpu_last_error().decode())
 
 
 def _ptr(a: np.ndarray):
