@@ -247,12 +247,12 @@ template <class K> static uint64_t resident_slots(K kernel, size_t smem, int thr
 // ranges only as far as needed to give every resident CTA slot work (one
 // range per column tile when many fields share the GPU). Planes are staged by
 // TMA when the source rows meet the copy engine's alignment.
-template <class T>
+template <class T, bool Z = true>
 static void level_fwd_stream(const FwdSrc<T>& src, Dims a, const FwdOut<T>& out, uint32_t* status, Sink& sink) {
     constexpr int UX = StreamTile<T>::UX, UY = StreamTile<T>::UY, Q = StreamTile<T>::Q;
     using S = StreamShape<T, UX, UY, Q>;
-    using OpT = FwdStreamOp<T, UX, UY, Q, true>;
-    using OpL = FwdStreamOp<T, UX, UY, Q, false>;
+    using OpT = FwdStreamOp<T, UX, UY, Q, true, Z>;
+    using OpL = FwdStreamOp<T, UX, UY, Q, false, Z>;
     typename OpT::Params p{};
     // small levels: almost every tile is an edge tile, whose reflected cells
     // the TMA path fixes up one by one; direct staging reflects on load
@@ -260,7 +260,10 @@ static void level_fwd_stream(const FwdSrc<T>& src, Dims a, const FwdOut<T>& out,
     const bool tma = !small && make_map_3d<T>(&p.map, src.p, a.x, a.y, a.z, src.sy, src.sz, S::FX, S::FY, 1);
     const uint32_t tx = (a.x + UX - 1) / UX, ty = (a.y + UY - 1) / UY;
     const uint64_t tiles = uint64_t(tx) * ty;
-    const uint32_t min_range = small ? 8 : 16;
+    const uint32_t min_range = small || !Z ? 8 : 16;
+    // planes a z range re-reads besides its own: the z halo of the pipeline
+    // (none for an XY level, whose ranges only repeat the CTA's set-up)
+    const double reread = Z ? 8.0 : 1.0;
     uint32_t zrange = a.z + (a.z & 1);
     if (t_opt.zmarch) {
         zrange = std::min(zrange, std::max<uint32_t>(16, t_opt.zmarch + (t_opt.zmarch & 1)));
@@ -279,7 +282,7 @@ static void level_fwd_stream(const FwdSrc<T>& src, Dims a, const FwdOut<T>& out,
             if (k > 1 && r < min_range) break;
             const uint64_t blocks = tiles * ((a.z + r - 1) / r);
             const double waves = double((blocks + slots - 1) / slots);
-            const double score = double(blocks) / (waves * double(slots)) * double(r) / double(r + 8);
+            const double score = double(blocks) / (waves * double(slots)) * double(r) / (double(r) + reread);
             if (score > best + 1e-9) {
                 best = score;
                 zrange = r;
@@ -325,6 +328,35 @@ static void level_inv(const InvSrc<T>& src, Dims a, const Out& out, uint32_t* st
                              S::BX, S::HY, S::HZ);
     if (!tma) {
         level<T, true, AX | AY | AZ>(src, a, out, sink);
+        return;
+    }
+    const uint32_t tx = (a.x + UX - 1) / UX, ty = (a.y + UY - 1) / UY, tz = (a.z + UZ - 1) / UZ;
+    const uint64_t blocks = uint64_t(tx) * ty * tz;
+    need(blocks < (1ull << 31), "Waltz: level grid too large");
+    p.lv = InvLevel<T>{src.base, src.sy, src.sz, src.low, src.lo, a};
+    p.tiles_x = tx;
+    p.tiles_y = ty;
+    p.out = out;
+    p.status = status;
+    sink.run<Op>(p, uint32_t(blocks), S::smem);
+}
+
+// One inverse XY level of the plane schedule from TMA-staged parity boxes
+// when the coefficient rows meet the copy engine's alignment; the generic
+// level kernel otherwise.
+template <class T, class Out>
+static void level_inv_xy(const InvSrc<T>& src, Dims a, const Out& out, uint32_t* status, Sink& sink) {
+    constexpr int UX = InvTileXY<T>::UX, UY = InvTileXY<T>::UY, UZ = InvTileXY<T>::UZ;
+    using S = InvXYShape<T, UX, UY, UZ>;
+    using Op = InvTileXYOp<T, UX, UY, UZ, Out>;
+    typename Op::Params p{};
+    bool tma = vol(a) > t_opt.small_level && half_len(a.x) % S::V == 0 &&
+               make_map_3d<T>(&p.cmap, src.base, a.x, a.y, a.z, src.sy, src.sz, S::BX, S::HY, UZ);
+    if (tma && src.low)
+        tma = make_map_3d<T>(&p.lmap, src.low, src.lo.x, src.lo.y, src.lo.z, src.lo.x, uint64_t(src.lo.x) * src.lo.y,
+                             S::BX, S::HY, UZ);
+    if (!tma) {
+        level<T, true, AX | AY>(src, a, out, sink);
         return;
     }
     const uint32_t tx = (a.x + UX - 1) / UX, ty = (a.y + UY - 1) / UY, tz = (a.z + UZ - 1) / UZ;
@@ -498,7 +530,7 @@ static void forward(const Geometry& g, const T* in, T* C, T* lowA, T* lowB, T* i
         const Dims a = g.xyl[l], lo = halve(a, AX | AY);
         const bool last = l + 1 == g.lxy;
         FwdOut<T> out{C, sy, sz, last ? nullptr : lows[l & 1], lo, a, AX | AY};
-        level<T, false, AX | AY>(src, a, out, sink);
+        level_fwd_stream<T, false>(src, a, out, status, sink);
         src = FwdSrc<T>{lows[l & 1], lo.x, size_t(lo.x) * lo.y};
     }
     if (g.lxy) sink.mark("fwd_xy");
@@ -569,14 +601,14 @@ static void inverse(const Geometry& g, T* C, T* bank1, T* bank2, const Final& fi
             InvSrc<T> src{C, sy, sz, low, halve(a, AX | AY)};
             if (l > 0) {
                 T* dst = halves[l & 1];
-                level<T, true, AX | AY>(src, a, StoreOut<T>{dst, a.x, size_t(a.x) * a.y}, sink);
+                level_inv_xy<T>(src, a, StoreOut<T>{dst, a.x, size_t(a.x) * a.y}, status, sink);
                 low = dst;
             } else if (g.lz) {
-                level<T, true, AX | AY>(src, a, StoreOut<T>{bank1, sy, sz}, sink);
+                level_inv_xy<T>(src, a, StoreOut<T>{bank1, sy, sz}, status, sink);
                 zbase = bank1;
                 zping[1] = C; // the coefficients are no longer read
             } else {
-                level<T, true, AX | AY>(src, a, fin, sink);
+                level_inv_xy<T>(src, a, fin, status, sink);
             }
         }
         sink.mark("inv_xy");

@@ -1,4 +1,6 @@
-// Forward dyadic level as a z-march (all three axes in one kernel).
+// Forward dyadic level as a z-march (all three axes in one kernel), and the
+// same march for an XY level of the plane schedule (Z = false: Y and X per
+// plane, no z pipeline and no z halo).
 //
 // The forward analysis is window independent (every output depends only on
 // its reflected neighbourhood, cpu/src/transform.cpp:136-146), so a level can
@@ -65,7 +67,7 @@ __device__ __forceinline__ bool nonfinite_max(unsigned long long m) { return m >
 // Tma: stage planes with per-plane tensor-map boxes; otherwise with batched
 // ordinary loads. `status` receives ST_WAIT_TIMEOUT if a copy never
 // completes within the wait bound (the block then stops as a whole).
-template <class T, int UX, int UY, int Q, bool Tma> struct FwdStreamOp {
+template <class T, int UX, int UY, int Q, bool Tma, bool Z = true> struct FwdStreamOp {
     // four CTAs per SM (64 registers): measured faster than three with more
     // registers, for both staging forms
     static constexpr int kThreads = 256, kMinBlocks = 4;
@@ -84,8 +86,8 @@ template <class T, int UX, int UY, int Q, bool Tma> struct FwdStreamOp {
     }
 };
 
-template <class T, int UX, int UY, int Q, bool Tma>
-__device__ __forceinline__ void FwdStreamOp<T, UX, UY, Q, Tma>::run(const Params& P, uint32_t block, uint32_t) {
+template <class T, int UX, int UY, int Q, bool Tma, bool Z>
+__device__ __forceinline__ void FwdStreamOp<T, UX, UY, Q, Tma, Z>::run(const Params& P, uint32_t block, uint32_t) {
     const FwdSrc<T> src = P.src;
     const Dims a = P.a;
     const uint32_t tiles_x = P.tiles_x, tiles_y = P.tiles_y, zrange = P.zrange;
@@ -105,10 +107,10 @@ __device__ __forceinline__ void FwdStreamOp<T, UX, UY, Q, Tma>::run(const Params
     const uint32_t ox = bx * UX, oy = by * UY;
     const uint32_t z0 = bzr * zrange, z1 = min(a.z, z0 + zrange);
     if (z0 >= z1) return;
-    // input planes [zin0, zin1): pairs from z0 - 4 until the pair that
-    // completes output z1 - 1
-    const int64_t zin0 = int64_t(z0) - 4;
-    const int64_t zin1 = 2 * (int64_t((z1 - 1) / 2) + 2) + 2;
+    // input planes [zin0, zin1): with Z, pairs from z0 - 4 until the pair
+    // that completes output z1 - 1; an XY level reads its output planes only
+    const int64_t zin0 = Z ? int64_t(z0) - 4 : int64_t(z0);
+    const int64_t zin1 = Z ? 2 * (int64_t((z1 - 1) / 2) + 2) + 2 : int64_t(z1);
     const bool check = src.status != nullptr;
     const bool edge = ox < 4 || ox + UX + 4 > a.x || oy < 4 || oy + UY + 4 > a.y;
     const int fx_lo = ox < 4 ? int(4 - ox) : 0, fx_hi = min(S::FX, int(a.x - ox) + 4);
@@ -283,35 +285,55 @@ __device__ __forceinline__ void FwdStreamOp<T, UX, UY, Q, Tma>::run(const Params
             }
         }
         __syncthreads();
-        // ---- Z: feed the Q lifted planes pair by pair into the column pipes
+        if constexpr (!Z) {
+            // ---- an XY level: every lifted plane is an output plane
 #pragma unroll
-        for (int c = 0; c < S::CPT; ++c) {
-            const int k = tid + c * 256;
-            if (k >= S::COLS) break;
-            const int x = k % UX, y = k / UX;
-            const bool inside = ox + x < a.x && oy + y < a.y;
-            const T* s = Mid + y * S::YP + x;
-            ZPipe<T>& p = pipe[c];
+            for (int c = 0; c < S::CPT; ++c) {
+                const int k = tid + c * 256;
+                if (k >= S::COLS) break;
+                const int x = k % UX, y = k / UX;
+                if (ox + x >= a.x || oy + y >= a.y) continue;
+                const T* s = Mid + y * S::YP + x;
 #pragma unroll
-            for (int q = 0; q < Q; q += 2) {
-                const T en = s[q * UY * S::YP], on = s[(q + 1) * UY * S::YP];
-                const T o1 = L::fma(K97<T>::a, L::add(p.e, en), p.o);
-                const T e2 = L::fma(K97<T>::b, L::add(p.o1, o1), p.e);
-                const T o3 = L::fma(K97<T>::g, L::add(p.e2, e2), p.o1);
-                const T e4 = L::fma(K97<T>::d, L::add(p.o3, o3), p.e2);
-                const int64_t zo = zb + q - 4; // even output plane of this pair
-                if (inside && zo >= int64_t(z0) && zo < int64_t(z1)) {
-                    const size_t cz = size_t(zo) >> 1;
-                    const T ev = L::mul(e4, K97<T>::k);
-                    if (even_xy[c]) out.low[cz * lo_plane + lo_off[c]] = ev;
-                    else out.dst[cz * out.sz + hi_off[c]] = ev;
-                    if (zo + 1 < int64_t(z1)) out.dst[(zhalf + cz) * out.sz + hi_off[c]] = L::mul(o3, -K97<T>::ik);
+                for (int q = 0; q < Q; ++q) {
+                    const int64_t zo = zb + q;
+                    if (zo >= int64_t(z1)) break;
+                    const T v = s[q * UY * S::YP];
+                    if (even_xy[c]) out.low[size_t(zo) * lo_plane + lo_off[c]] = v;
+                    else out.dst[size_t(zo) * out.sz + hi_off[c]] = v;
                 }
-                p.o3 = o3;
-                p.e2 = e2;
-                p.o1 = o1;
-                p.e = en;
-                p.o = on;
+            }
+        } else {
+            // ---- Z: feed the Q lifted planes pair by pair into the column pipes
+#pragma unroll
+            for (int c = 0; c < S::CPT; ++c) {
+                const int k = tid + c * 256;
+                if (k >= S::COLS) break;
+                const int x = k % UX, y = k / UX;
+                const bool inside = ox + x < a.x && oy + y < a.y;
+                const T* s = Mid + y * S::YP + x;
+                ZPipe<T>& p = pipe[c];
+#pragma unroll
+                for (int q = 0; q < Q; q += 2) {
+                    const T en = s[q * UY * S::YP], on = s[(q + 1) * UY * S::YP];
+                    const T o1 = L::fma(K97<T>::a, L::add(p.e, en), p.o);
+                    const T e2 = L::fma(K97<T>::b, L::add(p.o1, o1), p.e);
+                    const T o3 = L::fma(K97<T>::g, L::add(p.e2, e2), p.o1);
+                    const T e4 = L::fma(K97<T>::d, L::add(p.o3, o3), p.e2);
+                    const int64_t zo = zb + q - 4; // even output plane of this pair
+                    if (inside && zo >= int64_t(z0) && zo < int64_t(z1)) {
+                        const size_t cz = size_t(zo) >> 1;
+                        const T ev = L::mul(e4, K97<T>::k);
+                        if (even_xy[c]) out.low[cz * lo_plane + lo_off[c]] = ev;
+                        else out.dst[cz * out.sz + hi_off[c]] = ev;
+                        if (zo + 1 < int64_t(z1)) out.dst[(zhalf + cz) * out.sz + hi_off[c]] = L::mul(o3, -K97<T>::ik);
+                    }
+                    p.o3 = o3;
+                    p.e2 = e2;
+                    p.o1 = o1;
+                    p.e = en;
+                    p.o = on;
+                }
             }
         }
         // the next iteration's barrier vote orders these Mid reads before the
