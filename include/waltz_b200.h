@@ -103,11 +103,12 @@ int waltz_b200_decompress_batch(const waltz_b200_archive* archives, uint32_t cou
  * WALTZ_B200_OPT_ZMARCH_PLANES (0 = automatic, else >= 16): planes per CTA of
  *   the forward dyadic z-march (work per tile against the 8-plane halo).
  * WALTZ_B200_OPT_SMALL_LEVEL (samples, default 2^18, 0 = none): inverse
- *   dyadic levels of at most this many samples stage their tiles with
- *   reflecting loads instead of tensor-map copies (their tiles are almost all
- *   edge tiles).
+ *   levels (dyadic, and the plane schedule's XY levels) of at most this many
+ *   samples stage their tiles with reflecting loads instead of tensor-map
+ *   copies (their tiles are almost all edge tiles).
  * WALTZ_B200_OPT_SMALL_FWD (samples, default 2^21, 0 = none): the same for
- *   forward dyadic levels, whose z-march may then also use 8-plane ranges. */
+ *   forward levels (dyadic and XY), whose z-march may then also use 8-plane
+ *   ranges. */
 #define WALTZ_B200_OPT_STAGE_KERNELS 1
 #define WALTZ_B200_OPT_ZMARCH_PLANES 2
 #define WALTZ_B200_OPT_SMALL_LEVEL 3

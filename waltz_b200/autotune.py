@@ -6,8 +6,9 @@ question and the table can be applied blindly):
  * single fields: the plane schedule's whole-stage kernels on or off
    (WALTZ_B200_OPT_STAGE_KERNELS), the forward z-march depth, the planes
    per CTA tile of the dyadic forward levels (WALTZ_B200_OPT_ZMARCH_PLANES),
-   and the level sizes below which dyadic levels stage tiles with reflecting
-   loads instead of tensor-map copies (WALTZ_B200_OPT_SMALL_LEVEL / _FWD);
+   and the level sizes below which dyadic and XY levels stage tiles with
+   reflecting loads instead of tensor-map copies (WALTZ_B200_OPT_SMALL_LEVEL /
+   _FWD);
  * batches: the execution form of the batch graph (stage-batched groups or
    per-field chains, and their width, waltz_b200_batch_config) and the stage
    kernels knob;

@@ -265,7 +265,7 @@ static void level_fwd_stream(const FwdSrc<T>& src, Dims a, const FwdOut<T>& out,
     // (none for an XY level, whose ranges only repeat the CTA's set-up)
     const double reread = Z ? 8.0 : 1.0;
     uint32_t zrange = a.z + (a.z & 1);
-    if (t_opt.zmarch) {
+    if (Z && t_opt.zmarch) {
         zrange = std::min(zrange, std::max<uint32_t>(16, t_opt.zmarch + (t_opt.zmarch & 1)));
     } else if (!sink.many) {
         // maximise (filled share of the last wave) x (planes kept out of the
