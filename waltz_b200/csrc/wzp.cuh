@@ -194,6 +194,23 @@ __device__ __forceinline__ void copy_to_global(uint8_t* dst, const uint8_t* src,
     }
 }
 
+// Four consecutive samples through 16-byte accesses (p 16-byte aligned).
+__device__ __forceinline__ void load4(const float* p, float (&v)[4]) {
+    const float4 a = *reinterpret_cast<const float4*>(p);
+    v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w;
+}
+__device__ __forceinline__ void load4(const double* p, double (&v)[4]) {
+    const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+    v[0] = a.x, v[1] = a.y, v[2] = b.x, v[3] = b.y;
+}
+__device__ __forceinline__ void store4(float* p, const float (&v)[4]) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void store4(double* p, const double (&v)[4]) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+}
+
 // Magnitude sources of the encoder. Each fills S.m[0, 8192) (zeros past
 // the chunk's end) and S.nsign (the chunk's natural sign words).
 
@@ -239,18 +256,43 @@ template <class T> struct QuantBricks {
         }
         __syncthreads();
         uint32_t bad = 0;
-        for (uint32_t e = tid; e < nb * bsz; e += kWzpThreads) {
-            const uint32_t j = e >> lb, i = e & (bsz - 1u);
-            const uint32_t at = S.bbase[j] + (i >> 8) * plane + ((i >> 4) & 15u) * nx + (i & 15u);
-            int32_t m;
-            bool neg;
-            coeff[at] = quantize_one<T>(coeff[at], inv, q, m, neg, bad);
-            const uint32_t slot = (j << lb) + rank[i];
+        auto place = [&](uint32_t at, uint32_t slot, int32_t m, bool neg) {
             S.m[slot] = uint16_t(m > 65535 ? 65535 : m);
             S.sneg[slot] = neg && m;
             if (m > 65535) {
                 atomicOr(&qbits[at >> 5], 1u << (at & 31));
                 qval[at] = uint32_t(m);
+            }
+        };
+        if (((reinterpret_cast<uintptr_t>(coeff) & 15u) | (reinterpret_cast<uintptr_t>(rank) & 7u)) == 0) {
+            // four consecutive samples of a brick row per step (16 | nx, so a
+            // row's quarter is 16-byte aligned): one vector load and store of
+            // the coefficients, one 8-byte load of their four ranks
+            for (uint32_t e = 4 * uint32_t(tid); e < nb * bsz; e += 4 * kWzpThreads) {
+                const uint32_t j = e >> lb, i = e & (bsz - 1u);
+                const uint32_t at = S.bbase[j] + (i >> 8) * plane + ((i >> 4) & 15u) * nx + (i & 15u);
+                T v[4];
+                load4(coeff + at, v);
+                const uint2 rk = *reinterpret_cast<const uint2*>(rank + i);
+                const uint32_t base = j << lb;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    int32_t m;
+                    bool neg;
+                    v[k] = quantize_one<T>(v[k], inv, q, m, neg, bad);
+                    const uint32_t r = ((k < 2 ? rk.x : rk.y) >> (16 * (k & 1))) & 0xffffu;
+                    place(at + k, base + r, m, neg);
+                }
+                store4(coeff + at, v);
+            }
+        } else {
+            for (uint32_t e = tid; e < nb * bsz; e += kWzpThreads) {
+                const uint32_t j = e >> lb, i = e & (bsz - 1u);
+                const uint32_t at = S.bbase[j] + (i >> 8) * plane + ((i >> 4) & 15u) * nx + (i & 15u);
+                int32_t m;
+                bool neg;
+                coeff[at] = quantize_one<T>(coeff[at], inv, q, m, neg, bad);
+                place(at, (j << lb) + rank[i], m, neg);
             }
         }
         if (bad) atomicOr(status, ST_QUANT_DOMAIN);
