@@ -1176,7 +1176,8 @@ static DecodeJob decode_job(const uint8_t* d_in, const Header& h, const Layout& 
 // `job.ptr` set (graph capture) the side-record kernels are always launched
 // on a fixed grid, as the counts are only known on the device.
 template <class T, class Final, class Patch>
-static void decode_launch(const JobRef& job, bool matrix, const Geometry& g, const uint16_t* irank, T* C, T* bank1,
+static void decode_launch(const JobRef& job, bool matrix, const Geometry& g, const uint16_t* irank,
+                          const uint16_t* frank, T* C, T* bank1,
                           T* bank2, const Final& fin, const Patch& patch, uint32_t* status, Sink& sink) {
     const uint32_t n = uint32_t(g.n);
     if (!sink.rec) stage_clock().begin(sink.stream);
@@ -1184,7 +1185,7 @@ static void decode_launch(const JobRef& job, bool matrix, const Geometry& g, con
     sink.run<DirectoryCheckOp>(DirectoryCheckOp::Params{job, n, status}, 1);
     {
         sink.phase(PH_DECODE);
-        BrickMap map{g.nx, g.ny, g.nz, g.bz, irank, false, 0};
+        BrickMap map{g.nx, g.ny, g.nz, g.bz, irank, frank, false, 0};
         const uint32_t bsz = 256 * g.bz;
         if (g.nx % 16 == 0 && g.ny % 16 == 0 && g.nz % g.bz == 0 && (bsz & (bsz - 1)) == 0 && bsz <= kChunk &&
             kChunk / bsz <= 32) {
@@ -1288,10 +1289,11 @@ static void decompress(const uint8_t* d_in, size_t bytes, uint32_t nx, uint32_t 
     Carver real{t_arena.reserve(cv.used)};
     auto P = plan(real);
     const uint16_t* irank = t_inv_tables.get(nx, ny, nz, g.bz, true, stream);
+    const uint16_t* frank = t_fwd_tables.get(nx, ny, nz, g.bz, false, stream);
     check(cudaMemsetAsync(P.status, 0, 4, stream), "memset");
     FinalOut<T> fin{d_out, nx, size_t(nx) * ny, P.status};
     Sink sink{stream};
-    decode_launch<T>(JobRef{nullptr, decode_job(d_in, h, L)}, (h.flags & kMatrixFlag) != 0, g, irank, P.C, P.bank1,
+    decode_launch<T>(JobRef{nullptr, decode_job(d_in, h, L)}, (h.flags & kMatrixFlag) != 0, g, irank, frank, P.C, P.bank1,
                      P.bank2, fin, RowPatch<T>{d_out}, P.status, sink);
     check(cudaMemcpyAsync(pin + 8, P.status, 4, cudaMemcpyDeviceToHost, stream), "readback");
     check(cudaStreamSynchronize(stream), "decompress");
@@ -1729,10 +1731,11 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
         key.push_back(list[i].h.flags & kMatrixFlag);
     }
     if (!st.graph.valid(key)) {
-        std::vector<const uint16_t*> irank(count);
+        std::vector<const uint16_t*> irank(count), frank(count);
         for (uint32_t i = 0; i < count; ++i) {
             const Geometry& g = list[i].g;
             irank[i] = st.tables.get(g.nx, g.ny, g.nz, g.bz, true, bs.cap);
+            frank[i] = st.tables.get(g.nx, g.ny, g.nz, g.bz, false, bs.cap);
             if (list[i].h.flags & kMatrixFlag) t_zmat.get(g.nz, true, false, bs.cap); // upload before capture
         }
         auto enqueue = [&](uint32_t i, Sink& sink) {
@@ -1741,7 +1744,7 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
             const DecodeJob* job = P.jobs + i;
             JobOut<T> fin{job, list[i].sy, list[i].sz, P.status + i};
             JobPatch<T> patch{job, g.nx, g.ny, list[i].sy, list[i].sz};
-            decode_launch<T>(JobRef{job, {}}, (list[i].h.flags & kMatrixFlag) != 0, g, irank[i], P.C[k], P.b1[k],
+            decode_launch<T>(JobRef{job, {}}, (list[i].h.flags & kMatrixFlag) != 0, g, irank[i], frank[i], P.C[k], P.b1[k],
                              P.b2[k], fin, patch, P.status + i, sink);
         };
         if (staged) {

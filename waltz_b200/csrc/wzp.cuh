@@ -599,6 +599,8 @@ __device__ __forceinline__ void WzpDirectoryOp::run(const Params P, uint32_t blo
 struct BrickMap {
     uint32_t nx, ny, nz, bz;
     const uint16_t* local; // 8 slots x 256*bz: rank -> packed brick-local (x | y << 4 | z << 8)
+    const uint16_t* rank;  // 8 slots x 256*bz: brick-local row-major index -> rank (slot 0: whole
+                           // bricks), or null (the decoder then scatters through `local`)
     // Fast map: every brick whole (16 | nx, 16 | ny, bz | nz) and 256*bz a power
     // of two (lb = its log2), so a chunk is a run of whole bricks.
     bool fast;
@@ -644,6 +646,7 @@ struct WzpDecodeSmem {
     uint8_t planes[16 * (kEncPitch > kPlanePitch ? kEncPitch : kPlanePitch) * 4];
     uint8_t lv[2048 + 256 + 32 + 4];
     uint32_t gprefix[kChunk / 32];
+    uint32_t gmask[kChunk / 32];       // nonzero magnitudes of each 32-group
     uint32_t tmp[40];
     uint32_t off, mbytes, sbytes, raw, bad;
 };
@@ -918,7 +921,10 @@ __device__ __forceinline__ void WzpDecodeOp<T>::run(const Params A, uint32_t blo
             if (e0 + 32 < in_planes) S.m[e0 + 32] = uint16_t(m1);
             // groups wholly inside the planes: their nonzero counts now
             const uint32_t nzm0 = __ballot_sync(0xffffffffu, m0 != 0), nzm1 = __ballot_sync(0xffffffffu, m1 != 0);
-            if (lane < 2 && (uint32_t(g0) + lane) * 32 + 32 <= in_planes) S.gprefix[g0 + lane] = __popc(lane ? nzm1 : nzm0);
+            if (lane < 2 && (uint32_t(g0) + lane) * 32 + 32 <= in_planes) {
+                S.gprefix[g0 + lane] = __popc(lane ? nzm1 : nzm0);
+                S.gmask[g0 + lane] = lane ? nzm1 : nzm0;
+            }
         }
         for (uint32_t i = blocks * 16 + tid; i < kChunk; i += kWzpThreads)
             S.m[i] = i == ti ? tail : 0;
@@ -929,7 +935,10 @@ __device__ __forceinline__ void WzpDecodeOp<T>::run(const Params A, uint32_t blo
     const int counted = (mbytes != 0 && !S.raw) ? int(blocks * 16 / 32) : 0;
     for (int g = counted + warp; g < int(kChunk / 32); g += NW) {
         const uint32_t nzm = __ballot_sync(0xffffffffu, S.m[g * 32 + lane] != 0);
-        if (lane == 0) S.gprefix[g] = __popc(nzm);
+        if (lane == 0) {
+            S.gprefix[g] = __popc(nzm);
+            S.gmask[g] = nzm;
+        }
     }
     if (A.map.fast && tid < int(kChunk >> A.map.lb)) S.bbase[tid] = A.map.brick_base((first >> A.map.lb) + tid);
     __syncthreads();
@@ -944,22 +953,44 @@ __device__ __forceinline__ void WzpDecodeOp<T>::run(const Params A, uint32_t blo
         else if ((nnz & 7) && (sgn[sbytes - 1] >> (nnz & 7))) bad = true;
     }
     __syncthreads();
-    for (int g = warp; g < int(kChunk / 32); g += NW) {
-        if (uint32_t(g * 32) >= count) break;
-        const int e = g * 32 + lane;
-        const uint32_t v = S.m[e];
-        const uint32_t nzmask = __ballot_sync(0xffffffffu, v != 0);
-        bool neg = false;
-        if (v && !bad) {
-            const uint32_t rank = S.gprefix[g] + __popc(nzmask & ((1u << lane) - 1u));
-            if (rank < 8 * sbytes) neg = (sgn[rank >> 3] >> (rank & 7)) & 1u;
+    // sign of the magnitude at Morton slot e: the sign bit at its rank among
+    // the chunk's nonzero magnitudes
+    auto negative = [&](uint32_t e, uint32_t v) {
+        if (!v || bad) return false;
+        const uint32_t rank = S.gprefix[e >> 5] + __popc(S.gmask[e >> 5] & ((1u << (e & 31u)) - 1u));
+        return rank < 8 * sbytes && ((sgn[rank >> 3] >> (rank & 7)) & 1u);
+    };
+    if (A.map.fast && A.map.rank &&
+        ((reinterpret_cast<uintptr_t>(A.coeff) & 15u) | (reinterpret_cast<uintptr_t>(A.map.rank) & 7u)) == 0) {
+        // whole bricks: four consecutive samples of a brick row per step,
+        // gathered from their Morton slots, one 16-byte store
+        const uint32_t bsz = 1u << A.map.lb, plane = A.map.nx * A.map.ny;
+        for (uint32_t e = 4 * uint32_t(tid); e < count; e += 4 * kWzpThreads) {
+            const uint32_t j = e >> A.map.lb, i = e & (bsz - 1u);
+            const uint32_t at = S.bbase[j] + (i >> 8) * plane + ((i >> 4) & 15u) * A.map.nx + (i & 15u);
+            const uint2 rk = *reinterpret_cast<const uint2*>(A.map.rank + i);
+            T v4[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const uint32_t slot = (j << A.map.lb) + (((k < 2 ? rk.x : rk.y) >> (16 * (k & 1))) & 0xffffu);
+                const uint32_t v = S.m[slot];
+                const T mag = Lift<T>::mul(T(v), q);
+                v4[k] = negative(slot, v) ? -mag : mag;
+            }
+            store4(A.coeff + at, v4);
         }
-        if (uint32_t(e) < count) {
-            const T mag = Lift<T>::mul(T(v), q);
-            const uint32_t at = A.map.fast ? A.map.in_full_brick(S.bbase[uint32_t(e) >> A.map.lb],
-                                                                 uint32_t(e) & ((1u << A.map.lb) - 1u))
-                                           : A.map.rowmajor(first + uint32_t(e));
-            A.coeff[at] = neg ? -mag : mag;
+    } else {
+        for (int g = warp; g < int(kChunk / 32); g += NW) {
+            if (uint32_t(g * 32) >= count) break;
+            const int e = g * 32 + lane;
+            const uint32_t v = S.m[e];
+            if (uint32_t(e) < count) {
+                const T mag = Lift<T>::mul(T(v), q);
+                const uint32_t at = A.map.fast ? A.map.in_full_brick(S.bbase[uint32_t(e) >> A.map.lb],
+                                                                     uint32_t(e) & ((1u << A.map.lb) - 1u))
+                                               : A.map.rowmajor(first + uint32_t(e));
+                A.coeff[at] = negative(uint32_t(e), v) ? -mag : mag;
+            }
         }
     }
     if (bad) atomicOr(A.status, ST_BAD_STREAM);
