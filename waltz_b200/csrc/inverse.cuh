@@ -57,7 +57,9 @@ template <class T> struct InvLevel {
 };
 
 template <class T, int UX, int UY, int UZ, class Out> struct InvTileOp {
-    static constexpr int kThreads = 256, kMinBlocks = 2;
+    // float tiles: 16 warps per CTA, two CTAs per SM (the passes have 512 to
+    // 960 items); double tiles are half as wide and keep 8 warps
+    static constexpr int kThreads = sizeof(T) == 4 ? 512 : 256, kMinBlocks = 2;
     static constexpr bool kGridConstant = true;
     struct Params {
         CUtensorMap cmap, lmap;
@@ -129,7 +131,7 @@ __device__ __forceinline__ void InvTileOp<T, UX, UY, UZ, Out>::run(const Params&
         const int ny_out = S::FY - ny_in, nz_out = S::FZ - nz_in;
         const int na = ny_in * nz_in * nx_out;
         const int nb = (nz_out * S::FY + nz_in * ny_out) * S::FX;
-        for (int i = tid; i < na + nb; i += 256) {
+        for (int i = tid; i < na + nb; i += kThreads) {
             int fx, fy, fz;
             if (i < na) {
                 const int k = i % nx_out, row = i / nx_out;
@@ -175,7 +177,7 @@ __device__ __forceinline__ void InvTileOp<T, UX, UY, UZ, Out>::run(const Params&
     constexpr int ZS = S::HY * S::BX; // z-slot stride inside a box
     {
         constexpr int P = UZ / 2 + 4;
-        for (int L = tid; L < S::FX * S::FY; L += 256) {
+        for (int L = tid; L < S::FX * S::FY; L += kThreads) {
             // x index fastest inside one (x parity, y parity) box
             const int i = L % (S::FX / 2), k = (L / (S::FX / 2)) % (S::FY / 2);
             const int par = L / ((S::FX / 2) * (S::FY / 2)); // x parity + 2 * y parity
@@ -201,7 +203,7 @@ __device__ __forceinline__ void InvTileOp<T, UX, UY, UZ, Out>::run(const Params&
     {
         constexpr int P = UX / 2 + 4;
         constexpr int NV = S::BX / S::V; // 16-byte vectors per box row
-        for (int L = tid; L < S::FY * UZ; L += 256) {
+        for (int L = tid; L < S::FY * UZ; L += kThreads) {
             const int fy = L % S::FY, fz = 4 + L / S::FY;
             T* re = Bx + ((fz & 1) * 4 + (fy & 1) * 2) * S::BOX + ((fz >> 1) * S::HY + (fy >> 1)) * S::BX;
             T* ro = re + S::BOX;
@@ -240,7 +242,7 @@ __device__ __forceinline__ void InvTileOp<T, UX, UY, UZ, Out>::run(const Params&
         constexpr int P = 8 / 2 + 4;
         constexpr int WIN = UY / 8;
         constexpr int K = S::HY; // y slots per parity
-        for (int L = tid; L < UX * UZ; L += 256) {
+        for (int L = tid; L < UX * UZ; L += kThreads) {
             const int zrow = L / UX, xr = L % UX;
             const int u_x = 2 * (xr % (UX / 2)) + xr / (UX / 2); // first half of a row: even x
             const int fx = u_x + 4, fz = zrow + 4;
@@ -385,7 +387,7 @@ __device__ __forceinline__ void InvTileXYOp<T, UX, UY, UZ, Out>::run(const Param
         const int fy_lo = oy < 4 ? int(4 - oy) : 0, fy_hi = min(S::FY, int(a.y - oy) + 4);
         const int nx_out = fx_lo + (S::FX - fx_hi), ny_in = fy_hi - fy_lo, ny_out = S::FY - ny_in;
         const int na = ny_in * nx_out, per = na + ny_out * S::FX;
-        for (int i = tid; i < per * nz; i += 256) {
+        for (int i = tid; i < per * nz; i += kThreads) {
             const int z = i / per, r = i - z * per;
             int fx, fy;
             if (r < na) {
@@ -418,7 +420,7 @@ __device__ __forceinline__ void InvTileXYOp<T, UX, UY, UZ, Out>::run(const Param
     {
         constexpr int P = UX / 2 + 4;
         constexpr int NV = S::BX / S::V;
-        for (int L = tid; L < S::FY * nz; L += 256) {
+        for (int L = tid; L < S::FY * nz; L += kThreads) {
             const int fy = L % S::FY, z = L / S::FY;
             T* re = Bx + ((fy & 1) * 2) * S::BOX + (z * S::HY + (fy >> 1)) * S::BX;
             T* ro = re + S::BOX;
@@ -455,7 +457,7 @@ __device__ __forceinline__ void InvTileXYOp<T, UX, UY, UZ, Out>::run(const Param
         constexpr int P = 8 / 2 + 4;
         constexpr int WIN = UY / 8;
         constexpr int K = S::HY;
-        for (int L = tid; L < UX * nz; L += 256) {
+        for (int L = tid; L < UX * nz; L += kThreads) {
             const int zrow = L / UX, xr = L % UX;
             const int u_x = 2 * (xr % (UX / 2)) + xr / (UX / 2);
             const int fx = u_x + 4;
