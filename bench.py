@@ -350,21 +350,25 @@ def gpu_arm(args, rank, world, local_rank):
     if not args.no_tc_form and world == 1:
         del field, out, archive, host_in
         torch.cuda.empty_cache()
-        result["tc_form"] = tc_form_comparison(dev, lib, args.steps, tuple(args.tc_shape))
+        result["tc_form"] = tc_form_comparison(dev, lib, args.steps, tuple(args.tc_shape),
+                                               ref_gpu=rank == 0 and not args.no_gpu_baseline)
     if not args.no_batch and world == 1:
         torch.cuda.empty_cache()
         result["batched_form"] = batch_comparison(dev, lib, args.steps,
-                                                  cpu=rank == 0 and not args.no_cpu_baseline)
+                                                  cpu=rank == 0 and not args.no_cpu_baseline,
+                                                  ref_gpu=rank == 0 and not args.no_gpu_baseline)
     return result
 
 
-def tc_form_comparison(dev, lib, steps, shape=(64, 1024, 1024)):
+def tc_form_comparison(dev, lib, steps, shape=(64, 1024, 1024), ref_gpu=True):
     """Plain lifting against the precision form (tensor-core Z stage) on the
     tensor-core configuration: float32 1024x1024x64 (z=64) k^-11/3 random field
     (seed 3) with 1 % salt spikes of magnitude 50, REL 1e-3 and 1e-5; device
-    resident, CUDA events, median of `steps` after one warm-up. Also the Z-stage
-    coefficient error of the tensor-core matrix against the float64 lifting
-    transform on 16384 columns of the field."""
+    resident, CUDA events, median of `steps` after one warm-up; beside them the
+    reference's own CUDA library (its default profile, the plain form's bytes)
+    on the same field and bound. Also the Z-stage coefficient error of the
+    tensor-core matrix against the float64 lifting transform on 16384 columns
+    of the field."""
     import torch
     import waltz_b200
     from waltz_b200 import _lib
@@ -420,7 +424,12 @@ def tc_form_comparison(dev, lib, steps, shape=(64, 1024, 1024)):
                            "compression_ratio": round(nbytes / size, 4),
                            "repair_records": int.from_bytes(header[24:28], "little"),
                            "max_abs_error": err, "abs_bound": eb}
+            if form == "plain":
+                plain_arch = arch[:size].clone()
         entry["ratio_change"] = round(entry["matrix"]["compression_ratio"] / entry["plain"]["compression_ratio"] - 1, 5)
+        if ref_gpu:
+            entry["reference_gpu"] = gpu_baseline(f, eb, plain_arch, max(1, steps))
+        del plain_arch
         report[f"rel_{rel:g}"] = entry
     # coefficient error of the tensor-core Z stage against the float64 lifting
     cols = min(16384, nx * ny)
@@ -442,7 +451,7 @@ def tc_form_comparison(dev, lib, steps, shape=(64, 1024, 1024)):
     return report
 
 
-def batch_comparison(dev, lib, steps, count=512, cpu=False):
+def batch_comparison(dev, lib, steps, count=512, cpu=False, ref_gpu=False):
     """Batched form against one call per chunk on the uneven-chunk workload:
     512 float32 chunks, per-axis sides drawn from {32,48,64,96,128} (seed 4),
     k^-11/3 fields each rescaled to a range drawn log-uniformly in [1e-2,1e3],
@@ -562,7 +571,55 @@ def batch_comparison(dev, lib, steps, count=512, cpu=False):
     report["batched_gbs"] = round(nbytes / ((statistics.median(cb) + statistics.median(db)) / 1e3) / 1e9, 3)
     if cpu:
         report["cpu_baseline"] = cpu_batch_baseline([f.cpu().numpy() for f in fields], bounds)
+    if ref_gpu:
+        report["gpu_baseline"] = gpu_batch_baseline(fields, bounds, arch, offs, written)
     return report
+
+
+def gpu_batch_baseline(fields, bounds, ours, offs, written, reps=2):
+    """The reference's own CUDA library over the same chunk list on the same
+    GPU: it has no batched compressor, so one d_compress and one d_decompress
+    per chunk (its public API), device-resident, CUDA events around the whole
+    list; every archive compared byte for byte with ours."""
+    import torch
+    from oracle import oracle as O
+    if not O.refgpu_available():
+        return {"unavailable": "reference CUDA library not built (make -C oracle refgpu)"}
+    lib = O.refgpu_lib()
+    stream = torch.cuda.current_stream().cuda_stream
+    caps = [lib.refgpu_capacity(f.numel(), 4) for f in fields]
+    arch = torch.empty(max(caps), dtype=torch.uint8, device=fields[0].device)
+    srcs = [f.clone() for f in fields]  # the reference takes mutable input pointers
+    out = torch.empty(max(f.numel() for f in fields), dtype=torch.float32, device=fields[0].device)
+    identical = True
+    for i, f in enumerate(srcs):
+        size = O.refgpu_compress(f.data_ptr(), 4, tuple(f.shape), bounds[i], arch.data_ptr(), stream)
+        torch.cuda.synchronize()
+        identical &= size == written[i] and bool(torch.equal(arch[:size], ours[offs[i]:offs[i] + size]))
+    cmp_ms, dec_ms = [], []
+    nbytes = 4 * sum(f.numel() for f in fields)
+    for _ in range(reps):
+        tc = td = 0.0
+        for i, f in enumerate(srcs):
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            e[0].record()
+            O.refgpu_compress(f.data_ptr(), 4, tuple(f.shape), bounds[i], arch.data_ptr(), stream)
+            e[1].record()
+            O.refgpu_decompress(arch.data_ptr(), 4, tuple(f.shape), out.data_ptr(), stream)
+            e[2].record()
+            torch.cuda.synchronize()
+            tc += e[0].elapsed_time(e[1])
+            td += e[1].elapsed_time(e[2])
+        cmp_ms.append(tc)
+        dec_ms.append(td)
+    t_c, t_d = min(cmp_ms), min(dec_ms)
+    del srcs, arch, out
+    return {"value": round(nbytes / ((t_c + t_d) / 1e3) / 1e9, 3), "unit": "GB/s",
+            "compress_gbs": round(nbytes / (t_c / 1e3) / 1e9, 3),
+            "decompress_gbs": round(nbytes / (t_d / 1e3) / 1e9, 3),
+            "chunks_per_s": round(len(fields) / ((t_c + t_d) / 1e3), 1),
+            "archives_identical_to_ours": identical, "kind": "reference CUDA library, same GPU, one call per chunk",
+            "sample": f"all {len(fields)} chunks, best of {reps} passes"}
 
 
 def batch_only(dev, lib, args, count=512):
@@ -856,7 +913,7 @@ def main():
         from waltz_b200 import _lib
         torch.cuda.set_device(local_rank)
         print(json.dumps(tc_form_comparison(torch.device("cuda", local_rank), _lib.lib(), args.steps,
-                                            tuple(args.tc_shape))))
+                                            tuple(args.tc_shape), ref_gpu=False)))
         return
     if args.batch_only:
         import torch

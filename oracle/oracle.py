@@ -122,6 +122,7 @@ def refgpu_lib():
     p, u32 = C.c_void_p, C.c_uint32
     sig = {
         "refgpu_last_error": (C.c_char_p, []),
+        "refgpu_report": (None, [C.c_int]),
         "refgpu_capacity": (C.c_size_t, [C.c_uint64, C.c_int]),
         "refgpu_compress": (C.c_int, [p, C.c_int, u32, u32, u32, C.c_double, p, C.POINTER(C.c_size_t), p]),
         "refgpu_decompress": (C.c_int, [p, C.c_int, u32, u32, u32, p, p]),

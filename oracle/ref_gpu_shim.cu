@@ -7,7 +7,8 @@
 // Wrapped reference interfaces:
 //   WALTZ::d_compress<T> / d_decompress<T>          include/waltz.hpp:47-81
 //   WALTZ::compressed_buffer_capacity<T>            include/waltz.hpp:21-34
-//   WALTZ::Waltz_report_enabled (stage tables off)  include/utils/Statistics.hpp:118
+//   WALTZ::Waltz_report_enabled (stage tables, off unless refgpu_report(1))
+//                                                   include/utils/Statistics.hpp:118
 #include "waltz.hpp"
 
 #include <cstdio>
@@ -15,6 +16,7 @@
 
 namespace {
 thread_local char g_error[256];
+thread_local bool g_report = false; // the reference's per-stage timing tables
 int fail_with(const std::exception& e) {
     std::snprintf(g_error, sizeof(g_error), "%s", e.what());
     return -1;
@@ -24,6 +26,10 @@ int fail_with(const std::exception& e) {
 extern "C" {
 
 const char* refgpu_last_error(void) { return g_error; }
+
+// Lets the reference print its own per-stage timing tables on later calls of
+// this thread (off by default).
+void refgpu_report(int on) { g_report = on != 0; }
 
 size_t refgpu_capacity(uint64_t n, int width) {
     try {
@@ -39,7 +45,7 @@ size_t refgpu_capacity(uint64_t n, int width) {
 int refgpu_compress(void* d_in, int width, uint32_t nx, uint32_t ny, uint32_t nz, double abs_error, void* d_out,
                     size_t* written, void* stream) {
     try {
-        WALTZ::Waltz_report_enabled = false;
+        WALTZ::Waltz_report_enabled = g_report;
         WALTZ::Config conf(nx, ny, nz);
         conf.errorBoundMode = WALTZ::EB_ABS;
         conf.absErrorBound = abs_error;
@@ -56,7 +62,7 @@ int refgpu_compress(void* d_in, int width, uint32_t nx, uint32_t ny, uint32_t nz
 
 int refgpu_decompress(void* d_archive, int width, uint32_t nx, uint32_t ny, uint32_t nz, void* d_out, void* stream) {
     try {
-        WALTZ::Waltz_report_enabled = false;
+        WALTZ::Waltz_report_enabled = g_report;
         WALTZ::Config conf(nx, ny, nz);
         if (width == 4)
             WALTZ::d_decompress<float>(conf, static_cast<char*>(d_archive), static_cast<float*>(d_out), nullptr,
