@@ -39,10 +39,12 @@ int waltz_b200_compress(const void* d_input, int width, uint32_t nx, uint32_t ny
  * the plane schedule's Z stage (all Z levels) runs as one nz x nz matrix on
  * the tensor cores (TF32 hi/lo halves, FP32 accumulation) and the repair pass
  * restores the bound; such archives set header flag bit 6, which the
- * reference's decoders reject. MATRIX needs float data in the plane schedule
- * (Z levels differ from XY levels) with 1 <= nz <= 64 and nx*ny a multiple of
- * 4. New surface: the reference has no counterpart (its header reserves the
- * bit, include/utils/Blob.hpp:46-53). */
+ * reference's decoders reject. MATRIX needs the plane schedule (Z levels
+ * differ from XY levels) with 1 <= nz <= 128 and nx*ny a multiple of 4; float
+ * and double fields (the transform is fp32-accurate for both; a double
+ * field's quantisation and repair decisions stay in double). New surface:
+ * the reference has no counterpart (its header reserves the bit,
+ * include/utils/Blob.hpp:46-53). */
 #define WALTZ_B200_FORM_PLAIN 0
 #define WALTZ_B200_FORM_MATRIX 1
 int waltz_b200_compress_form(const void* d_input, int width, uint32_t nx, uint32_t ny, uint32_t nz,
@@ -142,13 +144,16 @@ int waltz_b200_transform(void* d_data, int width, uint32_t nx, uint32_t ny, uint
                          void* stream);
 int waltz_b200_wzp_encode(const uint16_t* d_mag, const uint32_t* d_sign, uint32_t n, void* d_out,
                           size_t capacity, size_t* written, void* stream);
-/* waltz_b200_zmatrix: the precision form's Z transform in place on a z-major
- *   float field (nx*ny a multiple of 4, 1 <= nz <= 64): all Z levels of the
- *   CDF 9/7 analysis (inverse = 0, coefficients in split-band order) or
- *   synthesis (inverse = 1) as one nz x nz matrix on the tensor cores (TF32
- *   hi/lo halves, FP32 accumulation). Counterpart of the reference's plane
- *   schedule Z stage, include/transformers/all_halo.cuh:143-224. */
+/* waltz_b200_zmatrix / _f64: the precision form's Z transform in place on a
+ *   z-major float / double field (nx*ny a multiple of 4, 1 <= nz <= 128): all
+ *   Z levels of the CDF 9/7 analysis (inverse = 0, coefficients in split-band
+ *   order) or synthesis (inverse = 1) as one nz x nz matrix on the tensor
+ *   cores (TF32 hi/lo halves, FP32 accumulation; double input is rounded to
+ *   float first, results are written back in the field's type). Counterpart
+ *   of the reference's plane schedule Z stage,
+ *   include/transformers/all_halo.cuh:143-224. */
 int waltz_b200_zmatrix(float* d_data, uint32_t nx, uint32_t ny, uint32_t nz, int inverse, void* stream);
+int waltz_b200_zmatrix_f64(double* d_data, uint32_t nx, uint32_t ny, uint32_t nz, int inverse, void* stream);
 /* Allocation-free variant of waltz_b200_wzp_encode (same arguments, same
  * stream bytes), for callers that cannot allocate device memory when they
  * call: a framework whose allocator owns the device budget, a plugin or filter

@@ -281,20 +281,25 @@ def _z_matrix_f64(nz: int, inverse: bool) -> np.ndarray:
     return np.linalg.inv(m) if inverse else m
 
 
-@pytest.mark.parametrize("nxyz", [(64, 64, 64), (32, 24, 40), (16, 20, 33), (256, 4, 17), (20, 20, 9)])
-def test_tensor_core_z_transform_matches_float64(nxyz):
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("nxyz", [(64, 64, 64), (32, 24, 40), (16, 20, 33), (256, 4, 17), (20, 20, 9), (24, 16, 65),
+                                  (16, 16, 96), (20, 12, 128)])
+def test_tensor_core_z_transform_matches_float64(nxyz, dtype):
     """The precision form's tensor-core Z transform (TF32 hi/lo halves, FP32
-    accumulation) against the float64 matrix of the lifting transform; the
-    coefficient error is a few 2^-20 of the row-weighted input."""
+    accumulation; a double field rounded to float first) against the float64
+    matrix of the lifting transform, for columns of up to 128 samples (two
+    MMA passes of 64 planes above 64); the coefficient error is a few 2^-20
+    of the row-weighted input."""
     torch = _torch()
     nx, ny, nz = nxyz
     rng = np.random.default_rng(nx * 7 + nz)
-    a = rng.standard_normal((nz, ny, nx)).astype(np.float32)
+    a = rng.standard_normal((nz, ny, nx)).astype(dtype)
+    entry = _lib().waltz_b200_zmatrix if dtype == np.float32 else _lib().waltz_b200_zmatrix_f64
     for inverse in (False, True):
         m = _z_matrix_f64(nz, inverse)
         expect = (m @ a.reshape(nz, -1).astype(np.float64)).reshape(a.shape)
         d = torch.from_numpy(a.copy()).cuda()
-        rc = _lib().waltz_b200_zmatrix(C.c_void_p(d.data_ptr()), nx, ny, nz, int(inverse), _stream())
+        rc = entry(C.c_void_p(d.data_ptr()), nx, ny, nz, int(inverse), _stream())
         assert rc == 0, _lib().waltz_b200_last_error()
         got = d.cpu().numpy().astype(np.float64)
         scale = np.abs(m).sum(axis=1).max() * np.abs(a).max()
@@ -303,7 +308,7 @@ def test_tensor_core_z_transform_matches_float64(nxyz):
 
 
 @pytest.mark.parametrize("rel", [1e-3, 1e-5])
-@pytest.mark.parametrize("shape", [(64, 128, 128), (24, 96, 64), (33, 24, 40)])
+@pytest.mark.parametrize("shape", [(64, 128, 128), (24, 96, 64), (33, 24, 40), (96, 64, 96), (128, 32, 64)])
 def test_matrix_form_round_trip(shape, rel):
     """Precision form (tensor-core Z stage): the archive carries header bit 6,
     the reference decoder (the oracle) rejects it, the GPU decoder restores
@@ -336,7 +341,29 @@ def test_matrix_form_rejects_unsuited_fields():
     with pytest.raises(waltz_b200.WaltzError, match="matrix form"):
         waltz_b200.compress(cube, abs_error=1e-3, form="matrix")
     with pytest.raises(waltz_b200.WaltzError, match="matrix form"):
-        waltz_b200.compress(np.zeros((64, 16, 16)), abs_error=1e-3, form="matrix")  # float64
+        waltz_b200.compress(np.zeros((160, 64, 64), np.float32), abs_error=1e-3, form="matrix")  # nz > 128
+
+
+@pytest.mark.parametrize("shape,eb", [((96, 32, 48), 1e-6), ((24, 64, 64), 1e-4), ((128, 16, 24), 1e-8)])
+def test_matrix_form_round_trip_float64(shape, eb):
+    """Precision form of a double field (the configuration with nz = 96 in
+    small): fp32-accurate tensor-core Z stage, quantisation and repair
+    decisions in double; every sample within the bound, decodes repeatable,
+    header bit 6 set. The field: k^-5/3 random field plus a tanh front along
+    z, in double."""
+    import waltz_b200
+    from waltz_b200 import synthetic as S
+    nz, ny, nx = shape
+    a = S.power_law_field(shape, 2, slope=-5.0 / 3.0, dtype=np.float64)
+    a += 10.0 * np.tanh((np.arange(nz, dtype=np.float64) - nz / 2) / 2.0)[:, None, None]
+    plain = waltz_b200.compress(a, abs_error=eb)
+    matrix = waltz_b200.compress(a, abs_error=eb, form="matrix")
+    assert matrix[0] == plain[0] | 0x40
+    out1 = waltz_b200.decompress(matrix, shape=a.shape, dtype=np.float64)
+    out2 = waltz_b200.decompress(matrix, shape=a.shape, dtype=np.float64)
+    assert out1.tobytes() == out2.tobytes()
+    err = np.abs(out1.astype(np.longdouble) - a.astype(np.longdouble)).max()
+    assert err <= np.longdouble(eb)
 
 
 BATCH_FORMS = [(0, 1), (0, 3), (1, 32)]  # (stage-batched | field chains, width)

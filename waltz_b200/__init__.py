@@ -63,7 +63,7 @@ FORMS = {"plain": 0, "matrix": 1}
 def _matrix_ok(shape, itemsize):
     nx, ny, nz = _geometry(shape, itemsize)
     lxy, lz = (autotune._levels(min(nx, ny)), autotune._levels(nz))
-    return itemsize == 4 and lxy != lz and lz >= 1 and nz <= 64 and (nx * ny) % 4 == 0
+    return itemsize in (4, 8) and lxy != lz and lz >= 1 and nz <= 128 and (nx * ny) % 4 == 0
 
 
 def compress_tensor(field, abs_error: float, *, form: str = "plain", stream=None, tuned=True):
@@ -72,7 +72,7 @@ def compress_tensor(field, abs_error: float, *, form: str = "plain", stream=None
 
     form="plain" is the default profile (byte-identical to the reference CPU
     codec); form="matrix" is the precision form, whose Z stage runs as one
-    matrix on the tensor cores (float, plane schedule, nz <= 64); form="auto"
+    matrix on the tensor cores (plane schedule, nz <= 128); form="auto"
     takes the matrix form where it applies and the tuning table measured it
     faster. With `tuned`, the tuning table's knobs for the field's class are
     applied first (they never change the output)."""

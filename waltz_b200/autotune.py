@@ -157,7 +157,7 @@ def _tune_single(torch, lib, shape, dtype, reps, rel=1e-3):
     entry["choice"] = dict(choice)
     # the matrix form where it applies: timed with the chosen knobs
     nz, ny, nx = shape
-    if dtype == torch.float32 and entry["class"]["schedule"] == "plane" and nz <= 64 and (nx * ny) % 4 == 0:
+    if entry["class"]["schedule"] == "plane" and nz <= 128 and (nx * ny) % 4 == 0:
         set_single(lib, choice)
         arc = waltz_b200.compress_tensor(f, eb, form="matrix", tuned=False)
         tc = _time(torch, lambda: waltz_b200.compress_tensor(f, eb, form="matrix", tuned=False), reps)

@@ -473,8 +473,8 @@ static TransformScratch scratch_need(const Geometry& g) {
     return s;
 }
 
-template <class Out>
-static void zmatrix_apply(const float* x, uint32_t nx, uint32_t ny, uint32_t nz, bool inverse, const Out& out,
+template <class T, class Out>
+static void zmatrix_apply(const T* x, uint32_t nx, uint32_t ny, uint32_t nz, bool inverse, const Out& out,
                           uint32_t* status, bool check_finite, Sink& sink);
 
 // Forward all-level transform of `in` into the coefficient array C. With
@@ -504,11 +504,9 @@ static void forward(const Geometry& g, const T* in, T* C, T* lowA, T* lowB, T* i
     }
     FwdSrc<T> src{in, sy, sz, status};
     T* zdst = g.lxy ? inter : C;
-    if constexpr (std::is_same_v<T, float>) {
-        if (matrix) {
-            zmatrix_apply(in, g.nx, g.ny, g.nz, false, ZmStore<float>{zdst}, status, true, sink);
-            sink.mark("fwd_z_matrix");
-        }
+    if (matrix) {
+        zmatrix_apply<T>(in, g.nx, g.ny, g.nz, false, ZmStore<T>{zdst}, status, true, sink);
+        sink.mark("fwd_z_matrix");
     }
     const bool zstage = !matrix && zstage_ok<T>(g);
     if (zstage) zstage_forward<T>(in, sy, sz, g, zdst, status, sink);
@@ -613,12 +611,10 @@ static void inverse(const Geometry& g, T* C, T* bank1, T* bank2, const Final& fi
         }
         sink.mark("inv_xy");
     }
-    if constexpr (std::is_same_v<T, float>) {
-        if (matrix && g.lz) {
-            zmatrix_apply(zbase, g.nx, g.ny, g.nz, true, ZmEmit<Final>{fin, g.nx}, status, false, sink);
-            sink.mark("inv_z_matrix");
-            return;
-        }
+    if (matrix && g.lz) {
+        zmatrix_apply<T>(zbase, g.nx, g.ny, g.nz, true, ZmEmit<T, Final>{fin, g.nx}, status, false, sink);
+        sink.mark("inv_z_matrix");
+        return;
     }
     if (zstage_ok<T>(g)) {
         zstage_inverse<T>(zbase, sy, sz, g, fin, sink);
@@ -777,20 +773,20 @@ struct ZMatrixCache {
 };
 static thread_local ZMatrixCache t_zmat;
 
-// Applies the all-levels Z analysis (or synthesis) matrix to a z-major f32
-// field of nx*ny columns on the tensor cores; `out(col, z, ncols, v)` takes
-// every result. nz <= 64, nx*ny a multiple of 4.
-template <class Out>
-static void zmatrix_apply(const float* x, uint32_t nx, uint32_t ny, uint32_t nz, bool inverse, const Out& out,
+// Applies the all-levels Z analysis (or synthesis) matrix to a z-major float
+// or double field of nx*ny columns on the tensor cores; `out.group` takes
+// every result. nz <= 128, nx*ny a multiple of 4.
+template <class T, class Out>
+static void zmatrix_apply(const T* x, uint32_t nx, uint32_t ny, uint32_t nz, bool inverse, const Out& out,
                           uint32_t* status, bool check_finite, Sink& sink) {
-    need(nz >= 1 && nz <= uint32_t(kZmMaxK), "Waltz: matrix form needs 1 <= nz <= 64");
+    need(nz >= 1 && nz <= uint32_t(kZmMaxK), "Waltz: matrix form needs 1 <= nz <= 128");
     const uint64_t ncols = uint64_t(nx) * ny;
     const ZmPlan P = ZmPlan::make(nz);
     const float* bhi = t_zmat.get(nz, inverse, false, sink.stream);
     const float* blo = t_zmat.get(nz, inverse, true, sink.stream);
     // no batched form: every field keeps its own persistent launch
     sink.direct([=](cudaStream_t stream) {
-        auto kernel = zmatrix_kernel<Out>;
+        auto kernel = zmatrix_kernel<T, Out>;
         const uint32_t smem_max = ZmPlan::make(kZmMaxK).smem();
         static thread_local int configured_device = -1;
         int dev = 0;
@@ -801,7 +797,12 @@ static void zmatrix_apply(const float* x, uint32_t nx, uint32_t ny, uint32_t nz,
             configured_device = dev;
         }
         const uint64_t tiles = (ncols + kZmCols - 1) / kZmCols;
-        const unsigned grid = unsigned(std::min<uint64_t>(tiles, resident_slots(kernel, P.smem())));
+        // resident CTAs at this column length's shared memory (one or two per SM)
+        int sms = 0, occ = 0;
+        check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+        check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kZmThreads, P.smem()), "occupancy");
+        const uint64_t slots = uint64_t(sms) * uint64_t(occ > 0 ? occ : 1);
+        const unsigned grid = unsigned(std::min<uint64_t>(tiles, slots));
         kernel<<<grid, kZmThreads, P.smem(), stream>>>(x, bhi, blo, nz, ncols, out, status, check_finite ? 1u : 0u);
         note_launch();
         check(cudaGetLastError(), "matrix kernel launch");
@@ -833,10 +834,11 @@ struct EncodeOptions {
 // the reference decoders reject such archives and the default bytes stay).
 constexpr uint8_t kMatrixFlag = 0x40;
 
-// Fields the matrix form serves: float, plane schedule with Z levels,
-// 1 <= nz <= 64 and nx*ny a multiple of 4 (16-byte planes).
+// Fields the matrix form serves: float or double, plane schedule with Z
+// levels, 1 <= nz <= 128 and nx*ny a multiple of 4.
 static bool matrix_form_ok(const Geometry& g, size_t width) {
-    return width == 4 && !g.dyadic && g.lz >= 1 && g.nz <= uint32_t(kZmMaxK) && (uint64_t(g.nx) * g.ny) % 4 == 0;
+    return (width == 4 || width == 8) && !g.dyadic && g.lz >= 1 && g.nz <= uint32_t(kZmMaxK) &&
+           (uint64_t(g.nx) * g.ny) % 4 == 0;
 }
 
 // ------------------------------------------------------------------ encode
@@ -879,7 +881,7 @@ template <class T> struct CompressJob {
         need(capacity >= 32 + wzp_header(uint32_t(n)), "Waltz: archive capacity too small");
         CompressJob j{d_in, nx, ny, nz, eb, d_out, capacity, opt, Geometry::make(nx, ny, nz), n};
         need(!opt.matrix || matrix_form_ok(j.g, sizeof(T)),
-             "Waltz: the matrix form needs float data in the plane schedule with 1 <= nz <= 64 and nx*ny a multiple of 4");
+             "Waltz: the matrix form needs the plane schedule with 1 <= nz <= 128 and nx*ny a multiple of 4");
         return j;
     }
 
@@ -2106,30 +2108,45 @@ extern "C" int waltz_b200_wzp_encode_noalloc(const uint16_t* d_mag, const uint32
     }
 }
 
-// Diagnostic entry of the tensor-core Z transform (declared in include/waltz_b200.h).
+// Diagnostic entries of the tensor-core Z transform (declared in include/waltz_b200.h).
+template <class T>
+static void zmatrix_in_place(T* d_data, uint32_t nx, uint32_t ny, uint32_t nz, int inverse, void* stream) {
+    need(d_data && nx && ny && nz, "invalid matrix transform arguments");
+    auto s = reinterpret_cast<cudaStream_t>(stream);
+    const uint64_t n = uint64_t(nx) * ny * nz;
+    Carver cv{nullptr};
+    auto plan = [&](Carver& c) {
+        struct P { T* out; uint32_t* status; } p;
+        p.out = c.take<T>(n);
+        p.status = c.take<uint32_t>(1);
+        return p;
+    };
+    plan(cv);
+    Carver real{t_arena.reserve(cv.used)};
+    auto P = plan(real);
+    check(cudaMemsetAsync(P.status, 0, 4, s), "memset");
+    Sink sink{s};
+    zmatrix_apply<T>(d_data, nx, ny, nz, inverse != 0, ZmStore<T>{P.out}, P.status, false, sink);
+    check(cudaMemcpyAsync(d_data, P.out, n * sizeof(T), cudaMemcpyDeviceToDevice, s), "copy");
+    uint32_t st = 0;
+    check(cudaMemcpyAsync(&st, P.status, 4, cudaMemcpyDeviceToHost, s), "readback");
+    check(cudaStreamSynchronize(s), "matrix transform");
+    if (st & ST_WAIT_TIMEOUT) throw Error("Waltz: asynchronous copy wait exceeded its bound");
+}
+
 extern "C" int waltz_b200_zmatrix(float* d_data, uint32_t nx, uint32_t ny, uint32_t nz, int inverse, void* stream) {
     try {
-        need(d_data && nx && ny && nz, "invalid matrix transform arguments");
-        auto s = reinterpret_cast<cudaStream_t>(stream);
-        const uint64_t n = uint64_t(nx) * ny * nz;
-        Carver cv{nullptr};
-        auto plan = [&](Carver& c) {
-            struct P { float* out; uint32_t* status; } p;
-            p.out = c.take<float>(n);
-            p.status = c.take<uint32_t>(1);
-            return p;
-        };
-        plan(cv);
-        Carver real{t_arena.reserve(cv.used)};
-        auto P = plan(real);
-        check(cudaMemsetAsync(P.status, 0, 4, s), "memset");
-        Sink sink{s};
-        zmatrix_apply(d_data, nx, ny, nz, inverse != 0, ZmStore<float>{P.out}, P.status, false, sink);
-        check(cudaMemcpyAsync(d_data, P.out, n * 4, cudaMemcpyDeviceToDevice, s), "copy");
-        uint32_t st = 0;
-        check(cudaMemcpyAsync(&st, P.status, 4, cudaMemcpyDeviceToHost, s), "readback");
-        check(cudaStreamSynchronize(s), "matrix transform");
-        if (st & ST_WAIT_TIMEOUT) throw Error("Waltz: asynchronous copy wait exceeded its bound");
+        zmatrix_in_place<float>(d_data, nx, ny, nz, inverse, stream);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+extern "C" int waltz_b200_zmatrix_f64(double* d_data, uint32_t nx, uint32_t ny, uint32_t nz, int inverse,
+                                      void* stream) {
+    try {
+        zmatrix_in_place<double>(d_data, nx, ny, nz, inverse, stream);
         return 0;
     } catch (const std::exception& e) {
         return fail(e);

@@ -7,10 +7,14 @@
 // row of D per column of the field, computed here on the 5th-generation
 // tensor cores:
 //   * a CTA takes 128 field columns at a time (UMMA M = 128): its threads
-//     read the K = nz planes of those columns (coalesced rows of 128) and
-//     split every value into TF32 halves (hi = fp32 truncated to TF32,
-//     lo = x - hi, exact) written transposed into the K-major no-swizzle
-//     operand layout (8-row x 16-byte core matrices);
+//     read the K = nz planes of those columns (coalesced rows of 128) in
+//     chunks of up to 64 planes and split every value into TF32 halves
+//     (hi = fp32 truncated to TF32, lo = x - hi, exact) written transposed
+//     into the K-major no-swizzle operand layout (8-row x 16-byte core
+//     matrices); chunks accumulate into the same tensor-memory tile. Double
+//     fields are rounded to fp32 first (the precision form's transform is
+//     fp32-accurate for both types; the quantisation and repair decisions of
+//     double fields stay in double, outside this kernel);
 //   * Mz's halves are prepared on the host in the same layout and loaded once
 //     per CTA; D = Ahi*Bhi + Ahi*Blo + Alo*Bhi, three tcgen05.mma kind::tf32
 //     per 8-deep K step, FP32 accumulation in tensor memory;
@@ -26,7 +30,8 @@
 namespace wb {
 
 constexpr int kZmCols = 128;   // field columns per tile (UMMA M)
-constexpr int kZmMaxK = 64;    // largest nz handled (operands stay in shared memory)
+constexpr int kZmMaxK = 128;   // largest nz handled (the whole matrix stays in shared memory)
+constexpr int kZmChunk = 64;   // planes of A staged per MMA pass
 constexpr int kZmThreads = 256;
 
 // Instruction descriptor of tcgen05.mma kind::tf32: D f32, A and B tf32,
@@ -68,16 +73,19 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
 }
 
 // Shared-memory plan of one CTA (bytes from a 1024-byte aligned base): the
-// A halves (128 x kp each) and the B halves (np x kp each), all fp32.
+// A halves (128 x one chunk of up to 64 planes each) and the B halves
+// (np x kp each), all fp32.
 struct ZmPlan {
     uint32_t kp, np;          // padded K (multiple of 8) and N (multiple of 16)
-    uint32_t a_bytes;         // one A half: 128 x kp x 4 B
+    uint32_t kc;              // planes per A chunk (multiple of 8, <= kZmChunk)
+    uint32_t a_bytes;         // one A half: 128 x kc x 4 B
     uint32_t b_bytes;         // one B half: np x kp x 4 B
     __host__ __device__ static ZmPlan make(uint32_t nz) {
         ZmPlan p;
         p.kp = (nz + 7) / 8 * 8;
         p.np = (nz + 15) / 16 * 16;
-        p.a_bytes = 128 * p.kp * 4;
+        p.kc = p.kp < uint32_t(kZmChunk) ? p.kp : uint32_t(kZmChunk);
+        p.a_bytes = 128 * p.kc * 4;
         p.b_bytes = p.np * p.kp * 4;
         return p;
     }
@@ -93,10 +101,10 @@ template <class T> struct ZmStore {
                                           const uint32_t (&r)[16]) const {
 #pragma unroll
         for (int j = 0; j < 16; ++j)
-            if (z0 + j < nz) dst[size_t(z0 + j) * ncols + col] = __uint_as_float(r[j]);
+            if (z0 + j < nz) dst[size_t(z0 + j) * ncols + col] = T(__uint_as_float(r[j]));
     }
 };
-template <class Final> struct ZmEmit {
+template <class T, class Final> struct ZmEmit {
     Final fin;
     uint32_t nx;
     __device__ __forceinline__ void group(uint32_t col, uint32_t z0, uint32_t nz, size_t, const uint32_t (&r)[16]) const {
@@ -104,16 +112,16 @@ template <class Final> struct ZmEmit {
         if constexpr (Final::kPrefetch) {
             // every original first, then the emissions: the loads do not wait
             // behind the emitter's stores
-            float o[16];
+            T o[16];
 #pragma unroll
-            for (int j = 0; j < 16; ++j) o[j] = z0 + j < nz ? fin.fetch(x, y, z0 + j) : 0.f;
+            for (int j = 0; j < 16; ++j) o[j] = z0 + j < nz ? fin.fetch(x, y, z0 + j) : T(0);
 #pragma unroll
             for (int j = 0; j < 16; ++j)
-                if (z0 + j < nz) fin.emit(x, y, z0 + j, __uint_as_float(r[j]), o[j]);
+                if (z0 + j < nz) fin.emit(x, y, z0 + j, T(__uint_as_float(r[j])), o[j]);
         } else {
 #pragma unroll
             for (int j = 0; j < 16; ++j)
-                if (z0 + j < nz) fin(x, y, z0 + j, __uint_as_float(r[j]));
+                if (z0 + j < nz) fin(x, y, z0 + j, T(__uint_as_float(r[j])));
         }
     }
 };
@@ -121,9 +129,9 @@ template <class Final> struct ZmEmit {
 // B halves: device arrays of np * kp floats each in the K-major no-swizzle
 // core layout (core (n/8, k/4) at ((n/8) * kp/4 + k/4) * 128 B, element
 // (n%8, k%4) at (n%8) * 16 + (k%4) * 4 inside it).
-template <class Out>
+template <class T, class Out>
 __global__ void __launch_bounds__(kZmThreads, 2)
-    zmatrix_kernel(const float* x, const float* bhi, const float* blo, uint32_t nz, uint64_t ncols, Out out,
+    zmatrix_kernel(const T* x, const float* bhi, const float* blo, uint32_t nz, uint64_t ncols, Out out,
                    uint32_t* status, uint32_t check_finite) {
     extern __shared__ __align__(1024) unsigned char zm_smem[];
     const ZmPlan P = ZmPlan::make(nz);
@@ -158,67 +166,78 @@ __global__ void __launch_bounds__(kZmThreads, 2)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
     const uint32_t idesc = zm_idesc(P.np);
-    const uint32_t sbo = (P.kp / 4) * 128; // 8-row groups of the K-major operands
-    const uint32_t kh = P.kp / 2;          // planes per half of the threads
+    const uint32_t sbo_b = (P.kp / 4) * 128; // 8-row groups of the K-major B operand
 
     uint32_t phase = 0;
-    bool bad = false;
-    for (uint64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        // split and transpose: thread t takes field column c = t % 128 and the
-        // t / 128 half of the planes; element (c, k) goes to core (c/8, k/4)
-        // at ((c/8) * kp/4 + k/4) * 128 B, row c%8
-        {
-            const int c = tid % kZmCols, half = tid / kZmCols;
-            const uint64_t col = tile * kZmCols + c;
-            const bool live = col < ncols;
-            const float* xcol = x + col;
-            unsigned char* hrow = Ahi + (c / 8) * sbo + (c % 8) * 16;
-            unsigned char* lrow = Alo + (c / 8) * sbo + (c % 8) * 16;
-            float v[kZmMaxK / 2];
+    bool bad = false, stop = false;
+    for (uint64_t tile = blockIdx.x; tile < tiles && !stop; tile += gridDim.x) {
+        for (uint32_t k0 = 0; k0 < P.kp; k0 += P.kc) {
+            const uint32_t kc = min(P.kc, P.kp - k0); // planes of this chunk (multiple of 8)
+            const uint32_t sbo_a = (kc / 4) * 128, kh = kc / 2;
+            // split and transpose: thread t takes field column c = t % 128 and the
+            // t / 128 half of the chunk's planes; element (c, k) goes to core
+            // (c/8, k/4) at ((c/8) * kc/4 + k/4) * 128 B, row c%8
+            {
+                const int c = tid % kZmCols, half = tid / kZmCols;
+                const uint64_t col = tile * kZmCols + c;
+                const bool live = col < ncols;
+                const T* xcol = x + col;
+                unsigned char* hrow = Ahi + (c / 8) * sbo_a + (c % 8) * 16;
+                unsigned char* lrow = Alo + (c / 8) * sbo_a + (c % 8) * 16;
+                float v[kZmChunk / 2];
 #pragma unroll
-            for (int j = 0; j < kZmMaxK / 2; ++j) {
-                const uint32_t k = half * kh + j;
-                v[j] = (j < int(kh) && k < nz && live) ? xcol[size_t(k) * ncols] : 0.f;
-            }
+                for (int j = 0; j < kZmChunk / 2; ++j) {
+                    const uint32_t k = k0 + half * kh + j;
+                    T w = T(0);
+                    if (j < int(kh) && k < nz && live) w = xcol[size_t(k) * ncols];
+                    if (check_finite) bad |= !finite_bits(w);
+                    v[j] = float(w);
+                }
 #pragma unroll
-            for (int j = 0; j < kZmMaxK / 2; j += 4) {
-                if (j < int(kh)) {
-                    uint32_t h[4], l[4];
+                for (int j = 0; j < kZmChunk / 2; j += 4) {
+                    if (j < int(kh)) {
+                        uint32_t h[4], l[4];
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        if (check_finite) bad |= !finite_bits(v[j + q]);
-                        h[q] = __float_as_uint(v[j + q]) & 0xffffe000u;
-                        l[q] = __float_as_uint(__fsub_rn(v[j + q], __uint_as_float(h[q])));
+                        for (int q = 0; q < 4; ++q) {
+                            h[q] = __float_as_uint(v[j + q]) & 0xffffe000u;
+                            l[q] = __float_as_uint(__fsub_rn(v[j + q], __uint_as_float(h[q])));
+                        }
+                        const uint32_t kq = (half * kh + j) / 4;
+                        *reinterpret_cast<uint4*>(hrow + kq * 128) = make_uint4(h[0], h[1], h[2], h[3]);
+                        *reinterpret_cast<uint4*>(lrow + kq * 128) = make_uint4(l[0], l[1], l[2], l[3]);
                     }
-                    const uint32_t kq = (half * kh + j) / 4;
-                    *reinterpret_cast<uint4*>(hrow + kq * 128) = make_uint4(h[0], h[1], h[2], h[3]);
-                    *reinterpret_cast<uint4*>(lrow + kq * 128) = make_uint4(l[0], l[1], l[2], l[3]);
                 }
             }
-        }
-        fence_proxy_async();
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            // A and B: K-major, no swizzle; cores 128 B apart along K (LBO),
-            // 8-row groups kp/4 cores apart (SBO); a K step of 8 is two cores
-            const uint32_t a0 = smem_u32(Ahi), a1 = smem_u32(Alo), b0 = smem_u32(Bhi), b1 = smem_u32(Blo);
-            for (uint32_t s = 0; s < P.kp / 8; ++s) {
-                const uint64_t dah = zm_sdesc(a0 + s * 256, 128, sbo, 0);
-                const uint64_t dal = zm_sdesc(a1 + s * 256, 128, sbo, 0);
-                const uint64_t dbh = zm_sdesc(b0 + s * 256, 128, sbo, 0);
-                const uint64_t dbl = zm_sdesc(b1 + s * 256, 128, sbo, 0);
-                zm_mma(tmem, dah, dbh, idesc, s > 0);
-                zm_mma(tmem, dah, dbl, idesc, 1);
-                zm_mma(tmem, dal, dbh, idesc, 1);
+            fence_proxy_async();
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncthreads();
+            if (tid == 0) {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                // A and B: K-major, no swizzle; cores 128 B apart along K (LBO),
+                // 8-row groups kc/4 (A) or kp/4 (B) cores apart (SBO); a K step
+                // of 8 is two cores
+                const uint32_t a0 = smem_u32(Ahi), a1 = smem_u32(Alo);
+                const uint32_t b0 = smem_u32(Bhi) + (k0 / 8) * 256, b1 = smem_u32(Blo) + (k0 / 8) * 256;
+                for (uint32_t s = 0; s < kc / 8; ++s) {
+                    const uint64_t dah = zm_sdesc(a0 + s * 256, 128, sbo_a, 0);
+                    const uint64_t dal = zm_sdesc(a1 + s * 256, 128, sbo_a, 0);
+                    const uint64_t dbh = zm_sdesc(b0 + s * 256, 128, sbo_b, 0);
+                    const uint64_t dbl = zm_sdesc(b1 + s * 256, 128, sbo_b, 0);
+                    zm_mma(tmem, dah, dbh, idesc, (k0 > 0 || s > 0) ? 1u : 0u);
+                    zm_mma(tmem, dah, dbl, idesc, 1);
+                    zm_mma(tmem, dal, dbh, idesc, 1);
+                }
+                zm_commit(mma_bar);
             }
-            zm_commit(mma_bar);
+            // the chunk's MMAs have read A before the next chunk overwrites it
+            if (!__syncthreads_and(warp != 0 || mbar_wait(mma_bar, phase, kWaitBound))) {
+                if (tid == 0) atomicOr(status, ST_WAIT_TIMEOUT);
+                stop = true;
+                break;
+            }
+            phase ^= 1;
         }
-        if (!__syncthreads_and(warp != 0 || mbar_wait(mma_bar, phase, kWaitBound))) {
-            if (tid == 0) atomicOr(status, ST_WAIT_TIMEOUT);
-            break;
-        }
+        if (stop) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         // epilogue: warp w reads lanes 32 (w % 4) .. (lane = field column) and
         // every other 16-coefficient group, starting at group w / 4
@@ -231,8 +250,7 @@ __global__ void __launch_bounds__(kZmThreads, 2)
             if (col < ncols) out.group(uint32_t(col), c0, nz, ncols, r);
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads(); // tensor memory read out, A free: the next tile may overwrite both
-        phase ^= 1;
+        __syncthreads(); // tensor memory read out: the next tile's MMAs may overwrite it
     }
     if (check_finite && __syncthreads_or(bad) && tid == 0) atomicOr(status, ST_NONFINITE_INPUT);
     __syncthreads();
