@@ -21,7 +21,10 @@ per core, on the same field split into its eight 256^3 octants (64 blocks of
 Beside the line's own numbers: `cpu_baseline` (the reference CPU codec, one
 core, a bounded sample) and `gpu_baseline` (the reference's own CUDA library,
 built from its sources for sm_100a, on the same field, bound and GPU, with
-its archive compared byte for byte with ours).
+its archive compared byte for byte with ours); `tc_form` / `tc_form_f64`
+compare the plain and precision forms on the float 1024x1024x64 and double
+384x256x96 plane-schedule configurations; `batched_form` the batched form on
+512 uneven chunks.
 """
 from __future__ import annotations
 
@@ -352,12 +355,104 @@ def gpu_arm(args, rank, world, local_rank):
         torch.cuda.empty_cache()
         result["tc_form"] = tc_form_comparison(dev, lib, args.steps, tuple(args.tc_shape),
                                                ref_gpu=rank == 0 and not args.no_gpu_baseline)
+        torch.cuda.empty_cache()
+        result["tc_form_f64"] = tc_form_f64(dev, lib, args.steps, ref_gpu=rank == 0 and not args.no_gpu_baseline)
     if not args.no_batch and world == 1:
         torch.cuda.empty_cache()
         result["batched_form"] = batch_comparison(dev, lib, args.steps,
                                                   cpu=rank == 0 and not args.no_cpu_baseline,
                                                   ref_gpu=rank == 0 and not args.no_gpu_baseline)
     return result
+
+
+def _form_entries(dev, lib, f, eb, steps, ref_gpu):
+    """Plain lifting and the precision form on one device-resident field at
+    one absolute bound: compress / decompress GB/s (median of `steps` after
+    one warm-up), ratio, repair records, worst error; beside them the
+    reference's own CUDA library (the plain form's bytes)."""
+    import torch
+    import waltz_b200
+    from waltz_b200 import _lib
+    nz, ny, nx = f.shape
+    width = f.element_size()
+    n = f.numel()
+    nbytes = n * width
+    cap = waltz_b200.compressed_capacity(n, width)
+    arch = torch.empty(cap, dtype=torch.uint8, device=dev)
+    out = torch.empty_like(f)
+    sp = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    written = C.c_size_t()
+    entry = {}
+    plain_arch = None
+    for form, code in (("plain", 0), ("matrix", 1)):
+        def comp():
+            _lib.checked(lib.waltz_b200_compress_form(C.c_void_p(f.data_ptr()), width, nx, ny, nz, eb, code,
+                                                      C.c_void_p(arch.data_ptr()), cap, C.byref(written), sp))
+            return written.value
+
+        def dec(size):
+            _lib.checked(lib.waltz_b200_decompress(C.c_void_p(arch.data_ptr()), size, width, nx, ny, nz,
+                                                   C.c_void_p(out.data_ptr()), nbytes, sp))
+        try:
+            size = comp()
+        except _lib.WaltzError as e:  # the form cannot serve this field at this bound
+            entry[form] = {"error": str(e), "abs_bound": eb}
+            continue
+        dec(size)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        tc, td = [], []
+        for _ in range(max(1, steps)):
+            ev[0].record()
+            size = comp()
+            ev[1].record()
+            dec(size)
+            ev[2].record()
+            torch.cuda.synchronize()
+            tc.append(ev[0].elapsed_time(ev[1]))
+            td.append(ev[1].elapsed_time(ev[2]))
+        header = arch[:32].cpu().numpy().tobytes()
+        err = float((out.double() - f.double()).abs().max())
+        assert err <= eb, f"{form} form violates the bound: {err} > {eb}"
+        entry[form] = {"compress_gbs": round(nbytes / (statistics.median(tc) / 1e3) / 1e9, 3),
+                       "decompress_gbs": round(nbytes / (statistics.median(td) / 1e3) / 1e9, 3),
+                       "compression_ratio": round(nbytes / size, 4),
+                       "repair_records": int.from_bytes(header[24:28], "little"),
+                       "max_abs_error": err, "abs_bound": eb}
+        if form == "plain":
+            plain_arch = arch[:size].clone()
+    if "compression_ratio" in entry["matrix"] and "compression_ratio" in entry["plain"]:
+        entry["ratio_change"] = round(entry["matrix"]["compression_ratio"] / entry["plain"]["compression_ratio"] - 1,
+                                      5)
+    if ref_gpu and plain_arch is not None:
+        entry["reference_gpu"] = gpu_baseline(f, eb, plain_arch, max(1, steps))
+    del plain_arch, arch, out
+    return entry
+
+
+def _z_coefficient_error(dev, lib, f):
+    """Largest error of the tensor-core Z stage against the float64 lifting on
+    up to 16384 columns of the field (absolute, and relative to the largest
+    coefficient of each column)."""
+    import torch
+    from waltz_b200 import _lib
+    nz, ny, nx = f.shape
+    sp = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    cols = min(16384, nx * ny)
+    x = f.reshape(nz, -1)[:, :cols].contiguous()
+    eye = torch.eye(nz, dtype=torch.float64, device=dev).reshape(nz, nz, 1, 1)
+    m = torch.empty(nz, nz, dtype=torch.float64, device=dev)
+    for k in range(nz):
+        e = eye[:, k].contiguous()
+        _lib.checked(lib.waltz_b200_transform(C.c_void_p(e.data_ptr()), 8, 1, 1, nz, 0, sp))
+        m[:, k] = e.reshape(nz)
+    ref = m @ x.double()
+    tcx = x.clone()
+    entry = lib.waltz_b200_zmatrix if f.element_size() == 4 else lib.waltz_b200_zmatrix_f64
+    _lib.checked(entry(C.c_void_p(tcx.data_ptr()), cols, 1, nz, 0, sp))
+    diff = (tcx.double() - ref).abs()
+    return {"max_abs": float(diff.max()),
+            "max_rel_to_column_max": float((diff.max(0).values / ref.abs().max(0).values.clamp_min(1e-30)).max()),
+            "columns": cols}
 
 
 def tc_form_comparison(dev, lib, steps, shape=(64, 1024, 1024), ref_gpu=True):
@@ -371,10 +466,8 @@ def tc_form_comparison(dev, lib, steps, shape=(64, 1024, 1024), ref_gpu=True):
     of the field."""
     import torch
     import waltz_b200
-    from waltz_b200 import _lib
-    from waltz_b200.synthetic import power_law_field_device
-    nz, ny, nx = shape
     from waltz_b200 import autotune
+    from waltz_b200.synthetic import power_law_field_device
     autotune.apply_single(lib, shape, 4)  # this field's class in the tuning table (never changes the bytes)
     f = power_law_field_device(shape, 3, device=dev)
     gen = torch.Generator(device=dev)
@@ -382,72 +475,33 @@ def tc_form_comparison(dev, lib, steps, shape=(64, 1024, 1024), ref_gpu=True):
     spikes = torch.rand(shape, device=dev, generator=gen) < 0.01
     signs = torch.where(torch.rand(shape, device=dev, generator=gen) < 0.5, -50.0, 50.0)
     f = torch.where(spikes, signs, f).to(torch.float32).contiguous()
-    n = f.numel()
-    nbytes = n * 4
-    cap = waltz_b200.compressed_capacity(n, 4)
-    arch = torch.empty(cap, dtype=torch.uint8, device=dev)
-    out = torch.empty_like(f)
-    sp = C.c_void_p(torch.cuda.current_stream().cuda_stream)
-    written = C.c_size_t()
     lo, hi = waltz_b200.extrema(f)
     report = {"workload": "f32 %dx%dx%d (z,y,x) k^-11/3 GRF seed 3 + 1%% spikes of 50, plane schedule" % shape}
     for rel in (1e-3, 1e-5):
-        eb = rel * (hi - lo)
-        entry = {}
-        for form, code in (("plain", 0), ("matrix", 1)):
-            def comp():
-                _lib.checked(lib.waltz_b200_compress_form(C.c_void_p(f.data_ptr()), 4, nx, ny, nz, eb, code,
-                                                          C.c_void_p(arch.data_ptr()), cap, C.byref(written), sp))
-                return written.value
+        report[f"rel_{rel:g}"] = _form_entries(dev, lib, f, rel * (hi - lo), steps, ref_gpu)
+    report["z_coefficient_error_vs_float64"] = _z_coefficient_error(dev, lib, f)
+    return report
 
-            def dec(size):
-                _lib.checked(lib.waltz_b200_decompress(C.c_void_p(arch.data_ptr()), size, 4, nx, ny, nz,
-                                                       C.c_void_p(out.data_ptr()), nbytes, sp))
-            size = comp()
-            dec(size)
-            ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-            tc, td = [], []
-            for _ in range(max(1, steps)):
-                ev[0].record()
-                size = comp()
-                ev[1].record()
-                dec(size)
-                ev[2].record()
-                torch.cuda.synchronize()
-                tc.append(ev[0].elapsed_time(ev[1]))
-                td.append(ev[1].elapsed_time(ev[2]))
-            header = arch[:32].cpu().numpy().tobytes()
-            err = float((out.double() - f.double()).abs().max())
-            assert err <= eb, f"{form} form violates the bound: {err} > {eb}"
-            entry[form] = {"compress_gbs": round(nbytes / (statistics.median(tc) / 1e3) / 1e9, 3),
-                           "decompress_gbs": round(nbytes / (statistics.median(td) / 1e3) / 1e9, 3),
-                           "compression_ratio": round(nbytes / size, 4),
-                           "repair_records": int.from_bytes(header[24:28], "little"),
-                           "max_abs_error": err, "abs_bound": eb}
-            if form == "plain":
-                plain_arch = arch[:size].clone()
-        entry["ratio_change"] = round(entry["matrix"]["compression_ratio"] / entry["plain"]["compression_ratio"] - 1, 5)
-        if ref_gpu:
-            entry["reference_gpu"] = gpu_baseline(f, eb, plain_arch, max(1, steps))
-        del plain_arch
-        report[f"rel_{rel:g}"] = entry
-    # coefficient error of the tensor-core Z stage against the float64 lifting
-    cols = min(16384, nx * ny)
-    x = f.reshape(nz, -1)[:, :cols].contiguous()
-    eye = torch.eye(nz, dtype=torch.float64, device=dev).reshape(nz, nz, 1, 1)
-    m = torch.empty(nz, nz, dtype=torch.float64, device=dev)
-    for k in range(nz):
-        e = eye[:, k].contiguous()
-        _lib.checked(lib.waltz_b200_transform(C.c_void_p(e.data_ptr()), 8, 1, 1, nz, 0, sp))
-        m[:, k] = e.reshape(nz)
-    ref = m @ x.double()
-    tcx = x.clone()
-    _lib.checked(lib.waltz_b200_zmatrix(C.c_void_p(tcx.data_ptr()), cols, 1, nz, 0, sp))
-    diff = (tcx.double() - ref).abs()
-    report["z_coefficient_error_vs_float64"] = {"max_abs": float(diff.max()),
-                                                "max_rel_to_column_max": float((diff.max(0).values /
-                                                                                ref.abs().max(0).values.clamp_min(1e-30)).max()),
-                                                "columns": cols}
+
+def tc_form_f64(dev, lib, steps, shape=(96, 256, 384), ref_gpu=True):
+    """The same comparison on the double configuration: float64 384x256x96
+    (z=96) k^-5/3 random field (seed 2) plus a front 10*tanh((z-48)/2) along
+    z, ABS 1e-4, 1e-5 and 1e-6. The precision form's Z stage is fp32-accurate; its
+    quantisation and repair decisions stay in double, and the repair pass
+    restores the bound."""
+    import torch
+    from waltz_b200 import autotune
+    from waltz_b200.synthetic import front_field
+    autotune.apply_single(lib, shape, 8)
+    f = torch.from_numpy(front_field(shape, 2)).to(dev).contiguous()
+    report = {"workload": "f64 %dx%dx%d (z,y,x) k^-5/3 GRF seed 2 + 10*tanh((z-48)/2), plane schedule" % shape}
+    # at ABS 1e-6 this field's coefficients exceed 65535 quanta so often that
+    # the q-outlier list passes the portable side-channel cap (2^20 records for
+    # fields over 2^20 samples) in either form, as in the reference; the entry
+    # records the refusal, the looser bounds measure both forms
+    for eb in (1e-4, 1e-5, 1e-6):
+        report[f"abs_{eb:g}"] = _form_entries(dev, lib, f, eb, steps, ref_gpu)
+    report["z_coefficient_error_vs_float64"] = _z_coefficient_error(dev, lib, f)
     return report
 
 
