@@ -289,6 +289,7 @@ static void level_fwd_stream(const FwdSrc<T>& src, Dims a, const FwdOut<T>& out,
             }
         }
     }
+    if (!Z && sink.many) zrange = std::min<uint32_t>(zrange, 16); // many fields: XY ranges re-read no halo
     const uint64_t blocks = tiles * ((a.z + zrange - 1) / zrange);
     need(blocks < (1ull << 31), "Waltz: level grid too large");
     p.src = src;
