@@ -721,11 +721,11 @@ def batch_only(dev, lib, args, count=512):
 # scaled by the sample ratio 512^3 / (256*384*384) = 3.5556; traffic grows in
 # proportion to the samples processed.
 TRAFFIC_512 = {
-    "compress:fwd_l0": 1011955940,
-    "compress:wzp_encode": 982265401,
-    "compress:inv_l0_repair": 1287945330,
-    "decompress:wzp_decode": 442284260,
-    "decompress:inv_l0": 966507634,
+    "compress:fwd_l0": 1010748985,
+    "compress:wzp_encode": 974181717,
+    "compress:inv_l0_repair": 1288321252,
+    "decompress:wzp_decode": 453289756,
+    "decompress:inv_l0": 968155136,
 }
 
 
