@@ -357,6 +357,9 @@ def gpu_arm(args, rank, world, local_rank):
                                                ref_gpu=rank == 0 and not args.no_gpu_baseline)
         torch.cuda.empty_cache()
         result["tc_form_f64"] = tc_form_f64(dev, lib, args.steps, ref_gpu=rank == 0 and not args.no_gpu_baseline)
+    if not args.no_batch and world > 1:
+        torch.cuda.empty_cache()
+        result["batched_form_sharded"] = batch_sharded(dev, lib, args.steps, rank, world)
     if not args.no_batch and world == 1:
         torch.cuda.empty_cache()
         result["batched_form"] = batch_comparison(dev, lib, args.steps,
@@ -676,6 +679,63 @@ def gpu_batch_baseline(fields, bounds, ours, offs, written, reps=2):
             "sample": f"all {len(fields)} chunks, best of {reps} passes"}
 
 
+def batch_sharded(dev, lib, steps, rank, world, count=512):
+    """The uneven-chunk batch shared across the ranks (one GPU each): every
+    rank builds the same chunk list, takes its share (balanced by bytes,
+    waltz_b200.shard.partition) and runs batched compress + decompress of it;
+    no data-path collective, only the archive sizes are exchanged once (the
+    metadata a shared container needs). Time per step = max over ranks;
+    value = the whole batch's bytes / that time (the batch is fixed as the
+    ranks grow: strong scaling)."""
+    import torch
+    import waltz_b200
+    from waltz_b200 import autotune, shard
+    from waltz_b200.synthetic import uneven_chunks_device
+    fields = uneven_chunks_device(count, 4, device=dev)
+    sizes = [f.numel() * 4 for f in fields]
+    mine = shard.partition(sizes, world)[rank]
+    local = [fields[i].contiguous() for i in mine]
+    del fields
+    bounds = []
+    for f in local:
+        lo, hi = waltz_b200.extrema(f)
+        bounds.append(REL * (hi - lo))
+    shapes = [tuple(f.shape) for f in local]
+    cap = sum(waltz_b200.compressed_capacity(f.numel(), 4) + 256 for f in local)
+    arch_buf = torch.empty(max(cap, 1), dtype=torch.uint8, device=dev)
+    out = torch.empty(max(sum(f.numel() for f in local), 1), dtype=torch.float32, device=dev)
+    autotune.apply_batch(lib, shapes, 4)
+    arcs = []
+
+    def step():
+        nonlocal arcs
+        if local:
+            arcs = waltz_b200.compress_batch(local, bounds, out=arch_buf)
+            waltz_b200.decompress_batch(arcs, shapes, torch.float32, out=out)
+    for _ in range(2):
+        step()
+    ms = []
+    for _ in range(max(3, steps)):
+        dist_barrier(world)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step()
+        e1.record()
+        torch.cuda.synchronize()
+        ms.append(dist_max(e0.elapsed_time(e1), world))
+    sizes_all, _ = shard.exchange_sizes({i: a.numel() for i, a in zip(mine, arcs)}) if world > 1 else (
+        {i: a.numel() for i, a in zip(mine, arcs)}, None)
+    t = statistics.median(ms)
+    loads = [sum(sizes[i] for i in share) for share in shard.partition(sizes, world)]
+    return {"workload": f"{count} f32 chunks, sides per axis from {{32,48,64,96,128}} (seed 4), REL 1e-3 per chunk, "
+                        f"shared across {world} ranks by bytes",
+            "value": round(sum(sizes) / (t / 1e3) / 1e9, 3), "unit": "GB/s", "ms_per_step": round(t, 4),
+            "scaling": "strong", "ranks": world, "chunks_this_rank": len(mine),
+            "max_rank_bytes_over_mean": round(max(loads) / (sum(loads) / world), 4),
+            "archive_bytes": int(sum(sizes_all.values())), "chunks_compressed": len(sizes_all)}
+
+
 def batch_only(dev, lib, args, count=512):
     """The batched form alone on the uneven-chunk workload: `warmup` + `steps`
     batched compress + decompress calls (the first captures the graphs)."""
@@ -756,7 +816,7 @@ def dist_max(x, world):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
