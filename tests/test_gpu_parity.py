@@ -342,6 +342,11 @@ def test_matrix_form_rejects_unsuited_fields():
         waltz_b200.compress(cube, abs_error=1e-3, form="matrix")
     with pytest.raises(waltz_b200.WaltzError, match="matrix form"):
         waltz_b200.compress(np.zeros((160, 64, 64), np.float32), abs_error=1e-3, form="matrix")  # nz > 128
+    big = np.zeros((24, 64, 64))
+    big[5, 6, 7] = 1e39  # a double the float transform cannot hold
+    with pytest.raises(waltz_b200.WaltzError, match="float range"):
+        waltz_b200.compress(big, abs_error=1e-3, form="matrix")
+    assert len(waltz_b200.compress(big, abs_error=1e30)) > 32  # the plain form takes it
 
 
 @pytest.mark.parametrize("shape,eb", [((96, 32, 48), 1e-6), ((24, 64, 64), 1e-4), ((128, 16, 24), 1e-8)])

@@ -1008,6 +1008,7 @@ template <class T> struct CompressJob {
         const uint32_t status = uint32_t(h[8]);
         const uint64_t np = h[5], nq = h[6];
         if (status & ST_NONFINITE_INPUT) throw Error("nonfinite input is unsupported");
+        if (status & ST_MATRIX_RANGE) throw Error("Waltz: the matrix form needs samples within the float range");
         if (status & ST_QUANT_DOMAIN) throw Error("coefficient exceeds portable integer conversion domain");
         if (status & ST_BOUND) throw Error("native repair cannot meet strict bound or nonfinite reconstruction");
         if (status & ST_LOOKBACK_TIMEOUT) throw Error("Waltz: WZP lookback wait exceeded its bound");

@@ -95,6 +95,7 @@ enum Status : uint32_t {
     ST_BAD_REPAIR = 1u << 9,        // nonfinite repair value
     ST_DIRECTORY = 1u << 10,        // WZP directory not in canonical order
     ST_WAIT_TIMEOUT = 1u << 11,     // a bounded wait for an asynchronous copy expired
+    ST_MATRIX_RANGE = 1u << 12,     // precision form: a double sample beyond the float range
 };
 
 // ------------------------------------------------------------ geometry

@@ -25,6 +25,8 @@
 // memory and returns. Nothing here multicasts.
 #pragma once
 #include "common.cuh"
+
+#include <cfloat>
 #include "tma.cuh"
 
 namespace wb {
@@ -169,7 +171,7 @@ __global__ void __launch_bounds__(kZmThreads, 2)
     const uint32_t sbo_b = (P.kp / 4) * 128; // 8-row groups of the K-major B operand
 
     uint32_t phase = 0;
-    bool bad = false, stop = false;
+    bool bad = false, range_bad = false, stop = false;
     for (uint64_t tile = blockIdx.x; tile < tiles && !stop; tile += gridDim.x) {
         for (uint32_t k0 = 0; k0 < P.kp; k0 += P.kc) {
             const uint32_t kc = min(P.kc, P.kp - k0); // planes of this chunk (multiple of 8)
@@ -190,7 +192,10 @@ __global__ void __launch_bounds__(kZmThreads, 2)
                     const uint32_t k = k0 + half * kh + j;
                     T w = T(0);
                     if (j < int(kh) && k < nz && live) w = xcol[size_t(k) * ncols];
-                    if (check_finite) bad |= !finite_bits(w);
+                    if (check_finite) {
+                        bad |= !finite_bits(w);
+                        if constexpr (sizeof(T) == 8) range_bad |= finite_bits(w) && fabs(w) > double(FLT_MAX);
+                    }
                     v[j] = float(w);
                 }
 #pragma unroll
@@ -253,6 +258,7 @@ __global__ void __launch_bounds__(kZmThreads, 2)
         __syncthreads(); // tensor memory read out: the next tile's MMAs may overwrite it
     }
     if (check_finite && __syncthreads_or(bad) && tid == 0) atomicOr(status, ST_NONFINITE_INPUT);
+    if (check_finite && __syncthreads_or(range_bad) && tid == 0) atomicOr(status, ST_MATRIX_RANGE);
     __syncthreads();
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
