@@ -431,7 +431,7 @@ def test_batch_decompress_equals_single_calls(batch_form):
     import waltz_b200
     from waltz_b200 import synthetic as S
     fields, bounds = _uneven_batch(torch, 5, 12)
-    # two precision-form archives (plane schedule, nz <= 64)
+    # two precision-form archives (plane schedule, nz <= 128)
     for shape in [(24, 96, 64), (33, 24, 40)]:
         fields.append(torch.from_numpy(S.power_law_field(shape, 9)).cuda())
         bounds.append(1e-3)
