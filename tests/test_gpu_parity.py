@@ -431,11 +431,12 @@ def test_batch_decompress_equals_single_calls(batch_form):
     import waltz_b200
     from waltz_b200 import synthetic as S
     fields, bounds = _uneven_batch(torch, 5, 12)
-    # two precision-form archives (plane schedule, nz <= 128)
-    for shape in [(24, 96, 64), (33, 24, 40)]:
+    # three precision-form archives (plane schedule, nz <= 128; the last in
+    # two MMA passes of up to 64 planes)
+    for shape in [(24, 96, 64), (33, 24, 40), (96, 32, 48)]:
         fields.append(torch.from_numpy(S.power_law_field(shape, 9)).cuda())
         bounds.append(1e-3)
-    forms = ["plain"] * 12 + ["matrix"] * 2
+    forms = ["plain"] * 12 + ["matrix"] * 3
     shapes = [tuple(f.shape) for f in fields]
     total = sum(f.numel() for f in fields)
     out = torch.full((total,), float("nan"), dtype=torch.float32, device="cuda")
@@ -466,19 +467,21 @@ def test_batch_decompress_f64_and_errors(batch_form):
     import waltz_b200
     from waltz_b200 import synthetic as S
     fields = [torch.from_numpy(S.power_law_field(s, 11).astype(np.float64)).cuda()
-              for s in [(16, 16, 16), (20, 33, 18), (40, 24, 32)]]
-    archives = [waltz_b200.compress_tensor(f, 1e-6) for f in fields]
+              for s in [(16, 16, 16), (20, 33, 18), (40, 24, 32), (96, 32, 48)]]
+    # the last in the precision form (a double field, nz = 96)
+    archives = [waltz_b200.compress_tensor(f, 1e-6, form="matrix" if k == 3 else "plain")
+                for k, f in enumerate(fields)]
     shapes = [tuple(f.shape) for f in fields]
     got = waltz_b200.decompress_batch(archives, shapes, torch.float64)
     for a, s, g in zip(archives, shapes, got):
         assert torch.equal(g, waltz_b200.decompress_tensor(a, s, torch.float64))
     # a truncated archive is reported with its index
-    bad = archives[:2] + [archives[2][:-8]]
+    bad = archives[:2] + [archives[2][:-8]] + archives[3:]
     with pytest.raises(waltz_b200.WaltzError, match="batch item 2"):
         waltz_b200.decompress_batch(bad, shapes, torch.float64)
     # a shape that does not match the archive's levels
     with pytest.raises(waltz_b200.WaltzError, match="batch item 1"):
-        waltz_b200.decompress_batch(archives, [shapes[0], (64, 64, 64), shapes[2]], torch.float64)
+        waltz_b200.decompress_batch(archives, [shapes[0], (64, 64, 64)] + shapes[2:], torch.float64)
 
 
 def test_batch_config_rejects_invalid_forms():
