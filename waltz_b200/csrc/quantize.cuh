@@ -384,18 +384,23 @@ __device__ __forceinline__ void ScanLayoutOp::run(const Params P, uint32_t, uint
     uint64_t* const layout = P.layout;
     __shared__ uint32_t tmp[40];
     uint32_t totals[2];
+    // each thread takes a run of consecutive block counts: its run's sum, one
+    // block scan for the runs' offsets, then the run rewritten as exclusive
+    // prefixes (two block scans in all instead of one per kCompactThreads)
+    const uint32_t per = (count + kCompactThreads - 1) / kCompactThreads;
+    const uint32_t b0 = min(count, threadIdx.x * per), b1 = min(count, b0 + per);
     for (int list = 0; list < 2; ++list) {
         uint32_t* counts = list ? counts_q : counts_p;
-        uint32_t carry = 0;
-        for (uint32_t base = 0; base < count; base += kCompactThreads) {
-            const uint32_t i = base + threadIdx.x;
-            const uint32_t v = i < count ? counts[i] : 0;
-            uint32_t sum;
-            const uint32_t ex = block_excl_scan<kCompactThreads>(v, tmp, sum);
-            if (i < count) counts[i] = carry + ex;
-            carry += sum;
+        uint32_t run = 0;
+        for (uint32_t i = b0; i < b1; ++i) run += counts[i];
+        uint32_t sum;
+        uint32_t at = block_excl_scan<kCompactThreads>(run, tmp, sum);
+        for (uint32_t i = b0; i < b1; ++i) {
+            const uint32_t v = counts[i];
+            counts[i] = at;
+            at += v;
         }
-        totals[list] = carry;
+        totals[list] = sum;
     }
     if (threadIdx.x != 0) return;
     const uint64_t wb = *wzp_total; // includes the WZP header
