@@ -247,12 +247,12 @@ template <class K> static uint64_t resident_slots(K kernel, size_t smem, int thr
 // ranges only as far as needed to give every resident CTA slot work (one
 // range per column tile when many fields share the GPU). Planes are staged by
 // TMA when the source rows meet the copy engine's alignment.
-template <class T, bool Z = true>
-static void level_fwd_stream(const FwdSrc<T>& src, Dims a, const FwdOut<T>& out, uint32_t* status, Sink& sink) {
+template <class T, bool Z, int NT>
+static void level_fwd_stream_nt(const FwdSrc<T>& src, Dims a, const FwdOut<T>& out, uint32_t* status, Sink& sink) {
     constexpr int UX = StreamTile<T>::UX, UY = StreamTile<T>::UY, Q = StreamTile<T>::Q;
-    using S = StreamShape<T, UX, UY, Q>;
-    using OpT = FwdStreamOp<T, UX, UY, Q, true, Z>;
-    using OpL = FwdStreamOp<T, UX, UY, Q, false, Z>;
+    using S = StreamShape<T, UX, UY, Q, NT>;
+    using OpT = FwdStreamOp<T, UX, UY, Q, true, Z, NT>;
+    using OpL = FwdStreamOp<T, UX, UY, Q, false, Z, NT>;
     typename OpT::Params p{};
     // small levels: almost every tile is an edge tile, whose reflected cells
     // the TMA path fixes up one by one; direct staging reflects on load
@@ -312,6 +312,16 @@ static void level_fwd_stream(const FwdSrc<T>& src, Dims a, const FwdOut<T>& out,
         q.status = status;
         sink.run<OpL>(q, uint32_t(blocks), S::smem);
     }
+}
+
+// Thread count of a z-march CTA: float dyadic levels of one field up to
+// 2^24 samples run 512 threads per CTA, the rest 256.
+template <class T, bool Z = true>
+static void level_fwd_stream(const FwdSrc<T>& src, Dims a, const FwdOut<T>& out, uint32_t* status, Sink& sink) {
+    if (sizeof(T) == 4 && Z && !sink.many && !sink.rec && vol(a) <= (uint64_t(1) << 24))
+        level_fwd_stream_nt<T, Z, 512>(src, a, out, status, sink);
+    else
+        level_fwd_stream_nt<T, Z, 256>(src, a, out, status, sink);
 }
 
 // One dyadic inverse level from TMA-staged parity boxes when the coefficient

@@ -41,14 +41,14 @@ template <> struct StreamTile<double> {
     static constexpr int UX = 16, UY = 16, Q = 8;
 };
 
-template <class T, int UX, int UY, int Q> struct StreamShape {
+template <class T, int UX, int UY, int Q, int NT = 256> struct StreamShape {
     static constexpr int FX = UX + 8, FY = UY + 8;
     static constexpr int YP = UX + 9 - (UX + 8) % 2; // odd pitch of the lifted rows
     static constexpr int IN = Q * FY * FX;          // staged planes
     static constexpr int MID = Q * UY * YP;          // Y-lifted planes
     static constexpr size_t smem = size_t(IN + MID) * sizeof(T) + 128 + 16; // + alignment + barrier
     static constexpr int COLS = UX * UY;
-    static constexpr int CPT = (COLS + 255) / 256;   // columns per thread
+    static constexpr int CPT = (COLS + NT - 1) / NT; // columns per thread
 };
 
 template <class T> struct ZPipe {
@@ -67,10 +67,13 @@ __device__ __forceinline__ bool nonfinite_max(unsigned long long m) { return m >
 // Tma: stage planes with per-plane tensor-map boxes; otherwise with batched
 // ordinary loads. `status` receives ST_WAIT_TIMEOUT if a copy never
 // completes within the wait bound (the block then stops as a whole).
-template <class T, int UX, int UY, int Q, bool Tma, bool Z = true> struct FwdStreamOp {
-    // four CTAs per SM (64 registers): measured faster than three with more
-    // registers, for both staging forms
-    static constexpr int kThreads = 256, kMinBlocks = 4;
+// NT threads per CTA: 256 (four CTAs per SM) for the large levels; 512 (two
+// CTAs per SM, every Y item of a batch of planes in one round) measured
+// faster on the coarser levels, slower on the finest.
+template <class T, int UX, int UY, int Q, bool Tma, bool Z = true, int NT = 256> struct FwdStreamOp {
+    // 256 threads: four CTAs per SM (64 registers), measured faster than
+    // three with more registers, for both staging forms
+    static constexpr int kThreads = NT, kMinBlocks = NT == 512 ? 2 : 4;
     static constexpr bool kGridConstant = true;
     struct Params {
         CUtensorMap map;
@@ -86,15 +89,15 @@ template <class T, int UX, int UY, int Q, bool Tma, bool Z = true> struct FwdStr
     }
 };
 
-template <class T, int UX, int UY, int Q, bool Tma, bool Z>
-__device__ __forceinline__ void FwdStreamOp<T, UX, UY, Q, Tma, Z>::run(const Params& P, uint32_t block, uint32_t) {
+template <class T, int UX, int UY, int Q, bool Tma, bool Z, int NT>
+__device__ __forceinline__ void FwdStreamOp<T, UX, UY, Q, Tma, Z, NT>::run(const Params& P, uint32_t block, uint32_t) {
     const FwdSrc<T> src = P.src;
     const Dims a = P.a;
     const uint32_t tiles_x = P.tiles_x, tiles_y = P.tiles_y, zrange = P.zrange;
     const FwdOut<T> out = P.out;
     uint32_t* const status = P.status;
     const CUtensorMap* map = &P.map;
-    using S = StreamShape<T, UX, UY, Q>;
+    using S = StreamShape<T, UX, UY, Q, NT>;
     using L = Lift<T>;
     using Bits = decltype(abs_bits(T(0)));
     extern __shared__ __align__(128) unsigned char stream_smem[];
@@ -122,7 +125,7 @@ __device__ __forceinline__ void FwdStreamOp<T, UX, UY, Q, Tma, Z>::run(const Par
     ZPipe<T> pipe[S::CPT];
 #pragma unroll
     for (int c = 0; c < S::CPT; ++c) {
-        const int k = tid + c * 256;
+        const int k = tid + c * NT;
         const uint32_t x = ox + k % UX, y = oy + k / UX;
         const uint32_t cx = split_of(x, a.x), cy = split_of(y, a.y);
         hi_off[c] = size_t(cy) * out.sy + cx;
@@ -169,7 +172,7 @@ __device__ __forceinline__ void FwdStreamOp<T, UX, UY, Q, Tma, Z>::run(const Par
                 // lies outside the box
                 const int nx_out = fx_lo + (S::FX - fx_hi), ny_in = fy_hi - fy_lo, ny_out = S::FY - ny_in;
                 const int na = Q * ny_in * nx_out, nb = Q * ny_out * S::FX;
-                for (int i = tid; i < na + nb; i += 256) {
+                for (int i = tid; i < na + nb; i += NT) {
                     int fx, fy, q;
                     if (i < na) {
                         const int k = i % nx_out, row = i / nx_out;
@@ -201,11 +204,11 @@ __device__ __forceinline__ void FwdStreamOp<T, UX, UY, Q, Tma, Z>::run(const Par
             constexpr int kBatch = 6;
             const uint32_t x0 = mirror(int64_t(ox) + lane - 4, a.x), x1 = mirror(int64_t(ox) + lane + 28, a.x);
             const bool has0 = lane < S::FX, has1 = lane + 32 < S::FX;
-            for (int r0 = warp; r0 < ROWS; r0 += 8 * kBatch) {
+            for (int r0 = warp; r0 < ROWS; r0 += (NT / 32) * kBatch) {
                 T v0[kBatch], v1[kBatch];
 #pragma unroll
                 for (int u = 0; u < kBatch; ++u) {
-                    const int r = r0 + u * 8;
+                    const int r = r0 + u * (NT / 32);
                     v0[u] = T(0);
                     v1[u] = T(0);
                     if (r < ROWS) {
@@ -217,7 +220,7 @@ __device__ __forceinline__ void FwdStreamOp<T, UX, UY, Q, Tma, Z>::run(const Par
                 }
 #pragma unroll
                 for (int u = 0; u < kBatch; ++u) {
-                    const int r = r0 + u * 8;
+                    const int r = r0 + u * (NT / 32);
                     if (r < ROWS) {
                         T* dst = In + r * S::FX;
                         if (has0) dst[lane] = v0[u];
@@ -231,7 +234,7 @@ __device__ __forceinline__ void FwdStreamOp<T, UX, UY, Q, Tma, Z>::run(const Par
         // sample is read here exactly once, so the finiteness check rides along
         {
             constexpr int P = UY / 2 + 4;
-            for (int item = tid; item < Q * S::FX; item += 256) {
+            for (int item = tid; item < Q * S::FX; item += NT) {
                 const int q = item / S::FX, fx = item % S::FX;
                 const T* s = In + q * S::FY * S::FX + fx;
                 T e[P], o[P];
@@ -261,7 +264,7 @@ __device__ __forceinline__ void FwdStreamOp<T, UX, UY, Q, Tma, Z>::run(const Par
         {
             constexpr int WX = 16, P = WX / 2 + 4, WIN = UX / WX;
             constexpr int ITEMS = Q * UY * WIN;
-            static_assert(ITEMS <= 256, "one X window per thread");
+            static_assert(ITEMS <= NT, "one X window per thread");
             const int item = tid;
             T e[P], o[P];
             T* rowp = nullptr;
@@ -289,7 +292,7 @@ __device__ __forceinline__ void FwdStreamOp<T, UX, UY, Q, Tma, Z>::run(const Par
             // ---- an XY level: every lifted plane is an output plane
 #pragma unroll
             for (int c = 0; c < S::CPT; ++c) {
-                const int k = tid + c * 256;
+                const int k = tid + c * NT;
                 if (k >= S::COLS) break;
                 const int x = k % UX, y = k / UX;
                 if (ox + x >= a.x || oy + y >= a.y) continue;
@@ -307,7 +310,7 @@ __device__ __forceinline__ void FwdStreamOp<T, UX, UY, Q, Tma, Z>::run(const Par
             // ---- Z: feed the Q lifted planes pair by pair into the column pipes
 #pragma unroll
             for (int c = 0; c < S::CPT; ++c) {
-                const int k = tid + c * 256;
+                const int k = tid + c * NT;
                 if (k >= S::COLS) break;
                 const int x = k % UX, y = k / UX;
                 const bool inside = ox + x < a.x && oy + y < a.y;
