@@ -1106,7 +1106,7 @@ static Layout validate_header(const Header& h, const Geometry& g, size_t bytes, 
 // verifies canonical (increasing) order on the device; anything else is
 // checked on the host like cpu/src/wzp_cpu.cpp:720-761.
 struct DirectoryCheckOp {
-    static constexpr int kThreads = 256, kMinBlocks = 0; // no occupancy floor: the compiler picks the register budget
+    static constexpr int kThreads = 1024, kMinBlocks = 0; // no occupancy floor: the compiler picks the register budget
     struct Params {
         JobRef job;
         uint32_t n;
@@ -1127,11 +1127,15 @@ __device__ __forceinline__ void DirectoryCheckOp::run(const Params P, uint32_t, 
     const uint8_t* meta = in + size_t(groups) * 4;
     uint64_t carry = 0;
     uint32_t st = 0;
-    for (uint32_t base = 0; base < groups; base += 256) {
+    for (uint32_t base = 0; base < groups; base += kThreads) {
         const uint32_t g = base + threadIdx.x;
         uint32_t len = 0, off = 0;
         if (g < groups) {
-            for (uint32_t c = g * kGroup; c < min(chunks, (g + 1) * kGroup); ++c) {
+            // the group's 16 metadata words are independent loads: all in flight at once
+#pragma unroll
+            for (uint32_t k = 0; k < kGroup; ++k) {
+                const uint32_t c = g * kGroup + k;
+                if (c >= chunks) break;
                 const WzpChunkInfo ci = wzp_meta(load_u24(meta + size_t(c) * 3), min(kChunk, n - c * kChunk));
                 if (!ci.ok) st |= ST_BAD_STREAM;
                 len += ci.mbytes + ci.sbytes;
@@ -1140,7 +1144,7 @@ __device__ __forceinline__ void DirectoryCheckOp::run(const Params P, uint32_t, 
             if (off > payload || len > payload - off || (!len && off)) st |= ST_BAD_STREAM;
         }
         uint32_t sum;
-        const uint32_t ex = block_excl_scan<256>(len, tmp, sum);
+        const uint32_t ex = block_excl_scan<kThreads>(len, tmp, sum);
         if (g < groups && len && uint64_t(off) != carry + ex) st |= ST_DIRECTORY;
         carry += sum;
     }
