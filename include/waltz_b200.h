@@ -104,11 +104,11 @@ int waltz_b200_decompress_batch(const waltz_b200_archive* archives, uint32_t cou
  *   or XY stage in one kernel where its lines or planes fit in shared memory.
  * WALTZ_B200_OPT_ZMARCH_PLANES (0 = automatic, else >= 16): planes per CTA of
  *   the forward dyadic z-march (work per tile against the 8-plane halo).
- * WALTZ_B200_OPT_SMALL_LEVEL (samples, default 2^18, 0 = none): inverse
+ * WALTZ_B200_OPT_SMALL_LEVEL (samples, default 2^15, 0 = none): inverse
  *   levels (dyadic, and the plane schedule's XY levels) of at most this many
  *   samples stage their tiles with reflecting loads instead of tensor-map
  *   copies (their tiles are almost all edge tiles).
- * WALTZ_B200_OPT_SMALL_FWD (samples, default 2^21, 0 = none): the same for
+ * WALTZ_B200_OPT_SMALL_FWD (samples, default 2^20, 0 = none): the same for
  *   forward levels (dyadic and XY), whose z-march may then also use 8-plane
  *   ranges. */
 #define WALTZ_B200_OPT_STAGE_KERNELS 1

@@ -36,12 +36,13 @@ TABLE = Path(__file__).with_name("tuning.json")
 
 OPT_STAGE_KERNELS, OPT_ZMARCH_PLANES, OPT_SMALL_LEVEL, OPT_SMALL_FWD = 1, 2, 3, 4
 BATCH_STAGES, BATCH_FIELDS = 0, 1
-DEFAULT_SINGLE = {"stage_kernels": 1, "zmarch": 0, "small_inv": 1 << 18, "small_fwd": 1 << 21}
+DEFAULT_SINGLE = {"stage_kernels": 1, "zmarch": 0, "small_inv": 1 << 15, "small_fwd": 1 << 20}
 MATRIX_MARGIN = 0.97  # the matrix form changes the header flag: take it only for a clear gain
 DEFAULT_BATCH = {"mode": BATCH_FIELDS, "width": 32, "stage_kernels": 1}
 
 SINGLE_CANDIDATES = [{"stage_kernels": s, "zmarch": z, "small_inv": i, "small_fwd": f}
-                     for s in (1, 0) for z in (0, 32) for i in (1 << 18, 1 << 21) for f in (1 << 21, 1 << 24, 1 << 26)]
+                     for s in (1, 0) for z in (0, 32) for i in (1 << 15, 1 << 18, 1 << 21)
+                     for f in (1 << 20, 1 << 21, 1 << 24, 1 << 26)]
 BATCH_CANDIDATES = ([{"mode": BATCH_STAGES, "width": w, "stage_kernels": s} for w in (1, 4, 16) for s in (1, 0)] +
                     [{"mode": BATCH_FIELDS, "width": w, "stage_kernels": s} for w in (16, 32, 64) for s in (1, 0)])
 

@@ -201,8 +201,8 @@ template <> struct Tiles<double> {
 struct Options {
     bool stage_kernels = true; // plane schedule: whole-stage kernels where they fit
     uint32_t zmarch = 0;       // forward z-march planes per CTA: 0 = automatic
-    uint64_t small_level = uint64_t(1) << 18; // inverse levels of at most this many samples: direct staging
-    uint64_t small_fwd = uint64_t(1) << 21;   // forward levels of at most this many samples: direct staging,
+    uint64_t small_level = uint64_t(1) << 15; // inverse levels of at most this many samples: direct staging
+    uint64_t small_fwd = uint64_t(1) << 20;   // forward levels of at most this many samples: direct staging,
                                               // short z ranges (measured on 128^3 .. 512^3 fields)
 };
 static thread_local Options t_opt;
