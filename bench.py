@@ -347,7 +347,13 @@ def gpu_arm(args, rank, world, local_rank):
     if shape == SHAPE and dom in TRAFFIC_512:
         result["roofline"]["traffic"] = TRAFFIC_512[dom]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        result["cpu_baseline"] = cpu_baseline(field.cpu().numpy(), eb)
+        host_field = field.cpu().numpy()
+        result["cpu_baseline"] = cpu_baseline(host_field, eb)
+        result["archive_identical_to_cpu"] = cpu_identical(host_field, eb, first)
+    if world == 1:
+        rel2 = 1e-4
+        result[f"rel_{rel2:g}"] = bound_entry(lib, field, rel2 * (hi - lo), min(args.steps, 10), hbm,
+                                              host_field if rank == 0 and not args.no_cpu_baseline else None)
     if rank == 0 and world == 1 and not args.no_gpu_baseline:
         result["gpu_baseline"] = gpu_baseline(field, eb, archive[:a_bytes], min(args.steps, 10))
     if not args.no_tc_form and world == 1:
@@ -366,6 +372,63 @@ def gpu_arm(args, rank, world, local_rank):
                                                   cpu=rank == 0 and not args.no_cpu_baseline,
                                                   ref_gpu=rank == 0 and not args.no_gpu_baseline)
     return result
+
+
+def cpu_identical(host_field, eb, ours):
+    """Whether our archive equals the reference CPU codec's (oracle/_ref, AVX2,
+    whose bytes equal its scalar backend's) for the same field and bound."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        return None
+    expect = O.RefCodec(O.AVX2).compress(host_field, eb)
+    return len(expect) == ours.numel() and expect == ours.cpu().numpy().tobytes()
+
+
+def bound_entry(lib, field, eb, steps, hbm, host_field=None):
+    """Compress and decompress throughput of the device-resident field at
+    another bound: CUDA events around each call, median over `steps` after two
+    warm-up steps; the archive compared with the reference CPU codec's when
+    `host_field` is given."""
+    import torch
+    import waltz_b200
+    from waltz_b200 import _lib
+    n = field.numel()
+    nbytes = n * field.element_size()
+    nz, ny, nx = field.shape
+    cap = waltz_b200.compressed_capacity(n, 4)
+    arch = torch.empty(cap, dtype=torch.uint8, device=field.device)
+    out = torch.empty_like(field)
+    sp = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    w = C.c_size_t()
+    tc, td = [], []
+    for it in range(2 + steps):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record()
+        _lib.checked(lib.waltz_b200_compress(C.c_void_p(field.data_ptr()), 4, nx, ny, nz, eb,
+                                             C.c_void_p(arch.data_ptr()), cap, C.byref(w), sp))
+        e[1].record()
+        _lib.checked(lib.waltz_b200_decompress(C.c_void_p(arch.data_ptr()), w.value, 4, nx, ny, nz,
+                                               C.c_void_p(out.data_ptr()), nbytes, sp))
+        e[2].record()
+        torch.cuda.synchronize()
+        if it >= 2:
+            tc.append(e[0].elapsed_time(e[1]))
+            td.append(e[1].elapsed_time(e[2]))
+    a = w.value
+    t_c, t_d = statistics.median(tc) / 1e3, statistics.median(td) / 1e3
+    header = arch[:32].cpu().numpy().tobytes()
+    entry = {"abs_bound": eb, "archive_bytes": a, "compression_ratio": round(nbytes / a, 4),
+             "compress_gbs": round(nbytes / t_c / 1e9, 3), "decompress_gbs": round(nbytes / t_d / 1e9, 3),
+             "compress_hbm_frac": round((nbytes + a) / t_c / 1e9 / hbm, 4),
+             "decompress_hbm_frac": round((nbytes + a) / t_d / 1e9 / hbm, 4),
+             "value": round(nbytes / (t_c + t_d) / 1e9, 3),
+             "repair_records": int.from_bytes(header[24:28], "little"),
+             "q_outliers": int.from_bytes(header[28:32], "little"),
+             "max_abs_error": float((out.double() - field.double()).abs().max())}
+    if host_field is not None:
+        entry["archive_identical_to_cpu"] = cpu_identical(host_field, eb, arch[:a])
+    del arch, out
+    return entry
 
 
 def _form_entries(dev, lib, f, eb, steps, ref_gpu):
@@ -470,14 +533,9 @@ def tc_form_comparison(dev, lib, steps, shape=(64, 1024, 1024), ref_gpu=True):
     import torch
     import waltz_b200
     from waltz_b200 import autotune
-    from waltz_b200.synthetic import power_law_field_device
+    from waltz_b200.synthetic import spiky_field_device
     autotune.apply_single(lib, shape, 4)  # this field's class in the tuning table (never changes the bytes)
-    f = power_law_field_device(shape, 3, device=dev)
-    gen = torch.Generator(device=dev)
-    gen.manual_seed(3)
-    spikes = torch.rand(shape, device=dev, generator=gen) < 0.01
-    signs = torch.where(torch.rand(shape, device=dev, generator=gen) < 0.5, -50.0, 50.0)
-    f = torch.where(spikes, signs, f).to(torch.float32).contiguous()
+    f = spiky_field_device(shape, 3, device=dev)
     lo, hi = waltz_b200.extrema(f)
     report = {"workload": "f32 %dx%dx%d (z,y,x) k^-11/3 GRF seed 3 + 1%% spikes of 50, plane schedule" % shape}
     for rel in (1e-3, 1e-5):

@@ -122,7 +122,9 @@ int waltz_b200_set_option(int option, int value);
 int waltz_b200_batch_config(int mode, int width);
 
 /* Decode an archive of `bytes` bytes into nx*ny*nz samples (the archive does
- * not store its dimensions); either form. */
+ * not store its dimensions); either form. bytes == 0 takes the length from
+ * the archive's 32-byte header (its section sizes), as the reference's
+ * d_decompress does, which has no length argument (src/waltz.cu:612-626). */
 int waltz_b200_decompress(const void* d_archive, size_t bytes, int width, uint32_t nx, uint32_t ny,
                           uint32_t nz, void* d_output, size_t output_bytes, void* stream);
 
@@ -162,7 +164,9 @@ int waltz_b200_zmatrix_f64(double* d_data, uint32_t nx, uint32_t ny, uint32_t nz
  * device array of about 256 KiB that every GPU loading the library holds
  * until exit; n is limited to 134217728 magnitudes (16384 chunks) and larger
  * n is rejected with an error. The first call on a device looks up the
- * array's device address (make that first call before any stream capture).
+ * array's device address (make that first call before any stream capture);
+ * the address stays valid for the life of the device's context, so a
+ * cudaDeviceReset of that device voids it for the rest of the process.
  * Calls share the array, so calls that overlap on the GPU (other streams,
  * threads or processes sharing a context) race: serialise them. */
 int waltz_b200_wzp_encode_noalloc(const uint16_t* d_mag, const uint32_t* d_sign, uint32_t n, void* d_out,

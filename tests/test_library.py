@@ -11,9 +11,15 @@ import pytest
 ROOT = Path(__file__).resolve().parents[1]
 
 
-def declared_functions():
+# The HDF5 filter plugin is its own library (waltz_b200/plugins/libwaltz_h5z.so).
+PLUGIN_HEADERS = {"waltz_h5z.h"}
+
+
+def declared_functions(headers=None):
     names = set()
-    for header in (ROOT / "include").glob("*.h"):
+    for header in sorted((ROOT / "include").glob("*.h")):
+        if (header.name in PLUGIN_HEADERS) != (headers == "plugin"):
+            continue
         text = re.sub(r"/\*.*?\*/", "", header.read_text(), flags=re.S)
         for m in re.finditer(r"\b([a-z_][a-z0-9_]*)\s*\(", text):
             name = m.group(1)
@@ -34,6 +40,15 @@ def test_library_loads_and_exports_every_declared_symbol():
     lib = ctypes.CDLL(str(lib_path))
     missing = [n for n in sorted(declared_functions()) if not hasattr(lib, n)]
     assert not missing, missing
+
+
+def test_plugin_exports_every_declared_symbol():
+    from waltz_b200 import build
+    build.build()
+    lib = ctypes.CDLL(str(build.PLUGIN))
+    names = declared_functions("plugin")
+    assert names == {"waltz_b200_h5z_filter"}
+    assert all(hasattr(lib, n) for n in names | {"H5PLget_plugin_type", "H5PLget_plugin_info"})
 
 
 def test_binding_covers_every_declared_symbol():

@@ -17,7 +17,10 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libwaltz_b200.so"
-SOURCES = ["codec.cu"]
+SOURCES = ["codec.cu", "cxx_api.cu"]
+# HDF5 filter plugin (filter 61197), a separate library linked to LIB.
+PLUGIN = PKG / "plugins" / "libwaltz_h5z.so"
+PLUGIN_SOURCES = ["h5z_filter.cu"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -35,22 +38,27 @@ def nvcc() -> str:
     return path
 
 
-def _stale() -> bool:
-    if not LIB.exists():
+def _stale(target: Path, sources) -> bool:
+    if not target.exists():
         return True
-    newest = max(p.stat().st_mtime for p in list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh"))
-                 + list((PKG.parent / "include").glob("*.h")))
-    return newest > LIB.stat().st_mtime
+    deps = [CSRC / s for s in sources] + list(CSRC.glob("*.cuh")) + list((PKG.parent / "include").glob("*.h*"))
+    return max(p.stat().st_mtime for p in deps) > target.stat().st_mtime
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
-    if not force and not _stale():
-        return LIB
-    srcs = [str(CSRC / s) for s in SOURCES if (CSRC / s).exists()]
-    tmp = LIB.with_suffix(".so.tmp")
-    cmd = [nvcc(), *NVCC_FLAGS, *(["-Xptxas", "-v"] if verbose else []), "-o", str(tmp), *srcs]
-    subprocess.run(cmd, check=True)
-    os.replace(tmp, LIB)
+    if force or _stale(LIB, SOURCES):
+        srcs = [str(CSRC / s) for s in SOURCES]
+        tmp = LIB.with_suffix(".so.tmp")
+        cmd = [nvcc(), *NVCC_FLAGS, *(["-Xptxas", "-v"] if verbose else []), "-o", str(tmp), *srcs]
+        subprocess.run(cmd, check=True)
+        os.replace(tmp, LIB)
+    if force or _stale(PLUGIN, PLUGIN_SOURCES) or PLUGIN.stat().st_mtime < LIB.stat().st_mtime:
+        PLUGIN.parent.mkdir(exist_ok=True)
+        tmp = PLUGIN.with_suffix(".so.tmp")
+        cmd = [nvcc(), *NVCC_FLAGS, "-o", str(tmp), *[str(CSRC / s) for s in PLUGIN_SOURCES],
+               f"-L{PKG}", "-lwaltz_b200", "-Xlinker", "-rpath,$ORIGIN/.."]
+        subprocess.run(cmd, check=True)
+        os.replace(tmp, PLUGIN)
     return LIB
 
 

@@ -1068,6 +1068,15 @@ struct Layout {
     uint64_t pi, pv, qi, qv, end;
 };
 
+// Archive length implied by the header's section sizes (BlobLayout of
+// include/utils/Blob.hpp:62-90): header, WZP stream, repair indices and
+// values, q-outlier indices and values, each padded to 8 bytes. Sizes beyond
+// the format's limits give a length the header checks then reject.
+static uint64_t archive_end(const Header& h) {
+    if (h.wzp > (uint64_t(1) << 60)) return 0;
+    return 32 + pad8(h.wzp) + pad8(uint64_t(h.np) * 4) + pad8(h.pwe_bytes) + 2 * pad8(uint64_t(h.nq) * 4);
+}
+
 // Header checks of the reference CPU decoder (cpu/src/codec.cpp:276-293);
 // `canonical` adds the exact-profile checks of src/waltz.cu:631-646.
 template <class T>
@@ -1273,11 +1282,7 @@ static void decompress(const uint8_t* d_in, size_t bytes, uint32_t nx, uint32_t 
     need(n <= 0xffffffffull / sizeof(T), "Waltz: volume exceeds the archive section limits");
     need(d_in && d_out, "Waltz: null buffer");
     need(out_bytes >= n * sizeof(T), "output capacity too small");
-    need(bytes >= 32, "invalid Waltz archive header");
-    {
-        const uintptr_t a = reinterpret_cast<uintptr_t>(d_in), b = reinterpret_cast<uintptr_t>(d_out);
-        need(!(a < b + n * sizeof(T) && b < a + bytes), "Waltz: input and output buffers overlap");
-    }
+    need(bytes >= 32 || (bytes == 0 && !canonical), "invalid Waltz archive header");
     const Geometry g = Geometry::make(nx, ny, nz);
     Header h;
     uint64_t* pin = pinned();
@@ -1287,6 +1292,14 @@ static void decompress(const uint8_t* d_in, size_t bytes, uint32_t nx, uint32_t 
         check(cudaMemcpyAsync(pin, d_in, 32, cudaMemcpyDeviceToHost, stream), "header readback");
         check(cudaStreamSynchronize(stream), "header readback");
         h = Header::parse(reinterpret_cast<const uint8_t*>(pin));
+    }
+    // bytes == 0: the caller does not know the archive length (the reference's
+    // d_decompress takes none, src/waltz.cu:612-626); the header's section
+    // sizes give it, and every later check runs against that length.
+    if (bytes == 0) bytes = size_t(archive_end(h));
+    {
+        const uintptr_t a = reinterpret_cast<uintptr_t>(d_in), b = reinterpret_cast<uintptr_t>(d_out);
+        need(!(a < b + n * sizeof(T) && b < a + bytes), "Waltz: input and output buffers overlap");
     }
     const Layout L = validate_header<T>(h, g, bytes, canonical);
     const uint64_t words = (n + 31) / 32;
@@ -1964,6 +1977,17 @@ const char* waltz_cuda_decode_chunk(uint32_t nx, uint32_t ny, uint32_t nz, int w
 
 } // extern "C"
 
+namespace wb {
+// Status word of a standalone WZP encode -> diagnostic (capacity, a
+// lookback wait that hit its bound, anything else).
+static void wzp_encode_status(uint32_t st) {
+    if (st & ST_CAPACITY) throw Error("WZP output capacity is too small");
+    if (st & ST_LOOKBACK_TIMEOUT) throw Error("Waltz: WZP lookback wait exceeded its bound");
+    if (st & ST_WAIT_TIMEOUT) throw Error("Waltz: asynchronous copy wait exceeded its bound");
+    if (st) throw Error("WZP encode failed");
+}
+} // namespace wb
+
 // Diagnostic stage entry points (declared in include/waltz_b200.h).
 extern "C" int waltz_b200_transform(void* d_data, int width, uint32_t nx, uint32_t ny, uint32_t nz, int inverse,
                                     void* stream) {
@@ -2041,8 +2065,7 @@ extern "C" int waltz_b200_wzp_encode(const uint16_t* d_mag, const uint32_t* d_si
         check(cudaMemcpyAsync(h, P.total, 8, cudaMemcpyDeviceToHost, s), "readback");
         check(cudaMemcpyAsync(h + 1, P.status, 4, cudaMemcpyDeviceToHost, s), "readback");
         check(cudaStreamSynchronize(s), "wzp encode");
-        if (uint32_t(h[1]) & ST_CAPACITY) throw Error("WZP output capacity is too small");
-        if (uint32_t(h[1])) throw Error("WZP encode failed");
+        wzp_encode_status(uint32_t(h[1]));
         *written = size_t(h[0]);
         return 0;
     } catch (const std::exception& e) {
@@ -2115,8 +2138,7 @@ extern "C" int waltz_b200_wzp_encode_noalloc(const uint16_t* d_mag, const uint32
         check(cudaMemcpyAsync(host, base, 16, cudaMemcpyDeviceToHost, s), "readback");
         check(cudaStreamSynchronize(s), "wzp encode");
         const uint32_t st = uint32_t(host[0] >> 32);
-        if (st & ST_CAPACITY) throw Error("WZP output capacity is too small");
-        if (st) throw Error("WZP encode failed");
+        wzp_encode_status(st);
         *written = size_t(host[1]);
         return 0;
     } catch (const std::exception& e) {

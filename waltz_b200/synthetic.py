@@ -95,6 +95,20 @@ def spiky_field(shape=(64, 1024, 1024), seed=3, fraction=0.01, magnitude=50.0, d
     return field.astype(dtype)
 
 
+def spiky_field_device(shape=(64, 1024, 1024), seed=3, fraction=0.01, magnitude=50.0, device="cuda"):
+    """spiky_field built with torch on a GPU: a device k^-11/3 field (seed)
+    with each sample replaced by +-magnitude with probability `fraction`
+    (signs equally likely), from a torch generator seeded with `seed`.
+    Returns a contiguous float32 CUDA tensor."""
+    import torch
+    f = power_law_field_device(shape, seed, device=device)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    spikes = torch.rand(shape, device=device, generator=gen) < fraction
+    signs = torch.where(torch.rand(shape, device=device, generator=gen) < 0.5, -magnitude, magnitude)
+    return torch.where(spikes, signs, f).to(torch.float32).contiguous()
+
+
 def uneven_chunks(count=512, seed=4, sides=(32, 48, 64, 96, 128), dtype=np.float32):
     """List of k^-11/3 chunks with per-axis sides drawn from `sides` and each
     chunk rescaled to a value range drawn log-uniformly in [1e-2, 1e3]."""
