@@ -211,11 +211,131 @@ __device__ __forceinline__ void store4(double* p, const double (&v)[4]) {
     reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
 }
 
+
+// ---------------------------------------------------------------------------
+// 16-sample blocks. The stream's bit planes are per 16 consecutive Morton
+// slots (a "block"): plane p of block b is a u16 whose bit 15-j is bit 15-p
+// of the block's magnitude j. In a whole 16 x 16 x bz brick (bz a power of
+// two) a block is an aligned 4 x 2 x 2 box when bz = 16 and an aligned
+// 4 x 4 x 1 box when bz <= 8 (the recursive octant order of morton_rank), so
+// one thread can own a block: load it as four 16-byte rows, hold its 16
+// magnitudes in registers and move between magnitudes and planes with one
+// 16 x 16 bit transpose.
+
+// 16 x 16 bit transpose, rows packed in pairs (w[i] = row 2i | row 2i+1 << 16,
+// bit 15 of a row = column 0): on return row p holds column p. Its own
+// inverse. Four block-swap stages (Hacker's Delight 7-3); the stages of
+// width 8, 4 and 2 act on both halves of a word pair at once, the stage of
+// width 1 inside each word.
+__device__ __forceinline__ void bit_transpose16(uint32_t (&w)[8]) {
+#pragma unroll
+    for (int j = 8; j >= 2; j >>= 1) {
+        const uint32_t m = j == 8 ? 0x00ff00ffu : j == 4 ? 0x0f0f0f0fu : 0x33333333u;
+        const int h = j / 2; // word distance of rows k and k + j
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            if (i & h) continue;
+            const uint32_t t = (w[i] ^ (w[i + h] >> j)) & m;
+            w[i] ^= t;
+            w[i + h] ^= t << j;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const uint32_t t = (w[i] ^ (w[i] >> 17)) & 0x5555u;
+        w[i] ^= t ^ (t << 17);
+    }
+}
+
+// Element layout of a block: row r (0..3) of the block's four 16-byte rows
+// holds magnitudes e0(r), e0(r)+1 (x = 0, 1) and e0(r)+d, e0(r)+d+1 (x = 2, 3);
+// its offset from the block origin is dz * plane + dy * nx.
+struct BlockShape {
+    bool tall; // bz = 16: 4 x 2 x 2 (rows dy + 2 dz); else 4 x 4 x 1 (rows dy)
+    __device__ __forceinline__ uint32_t e0(int r) const {
+        return tall ? uint32_t(2 * r) : uint32_t(((r & 1) << 1) | ((r >> 1) << 3));
+    }
+    __device__ __forceinline__ uint32_t d() const { return tall ? 8u : 4u; }
+    __device__ __forceinline__ uint32_t row_offset(int r, uint32_t nx, uint32_t plane) const {
+        return tall ? uint32_t(r >> 1) * plane + uint32_t(r & 1) * nx : uint32_t(r) * nx;
+    }
+};
+
+// Origin (x, y, z) inside a 16 x 16 x 2^zb brick of the block holding Morton
+// ranks 16k .. 16k+15: the rank's bits come in levels from the bottom, 4 - zb
+// levels of (x, y) bits, then zb levels of (x, y, z) bits; the block index
+// drops the lowest four bits.
+__device__ __forceinline__ void block_origin(uint32_t k, uint32_t zb, uint32_t& x, uint32_t& y, uint32_t& z) {
+    uint32_t r = k << 4, bit = 0;
+    x = y = z = 0;
+    uint32_t zl = 0;
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+        const bool withz = uint32_t(l) >= 4 - zb;
+        x |= ((r >> bit) & 1u) << l;
+        y |= ((r >> (bit + 1)) & 1u) << l;
+        bit += 2;
+        if (withz) {
+            z |= ((r >> bit) & 1u) << zl;
+            ++zl;
+            ++bit;
+        }
+    }
+}
+
+// Bits of x selected by mask, packed towards bit 0 in order (16-bit
+// compress, Hacker's Delight 7-4).
+__device__ __forceinline__ uint32_t compress16(uint32_t x, uint32_t m) {
+    x &= m;
+    uint32_t mk = (~m << 1) & 0xffffu;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        uint32_t mp = mk ^ (mk << 1);
+        mp ^= mp << 2;
+        mp ^= mp << 4;
+        mp ^= mp << 8;
+        mp &= 0xffffu;
+        const uint32_t mv = mp & m;
+        m = (m ^ mv) | (mv >> (1 << i));
+        const uint32_t t = x & mv;
+        x = (x ^ t) | (t >> (1 << i));
+        mk &= ~mp;
+    }
+    return x;
+}
+
+// The low popc(m) bits of x spread to the set positions of m, in order
+// (16-bit expand, the inverse of compress16).
+__device__ __forceinline__ uint32_t expand16(uint32_t x, uint32_t m) {
+    uint32_t a[4];
+    const uint32_t m0 = m;
+    uint32_t mk = (~m << 1) & 0xffffu;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        uint32_t mp = mk ^ (mk << 1);
+        mp ^= mp << 2;
+        mp ^= mp << 4;
+        mp ^= mp << 8;
+        mp &= 0xffffu;
+        const uint32_t mv = mp & m;
+        a[i] = mv;
+        m = (m ^ mv) | (mv >> (1 << i));
+        mk &= ~mp;
+    }
+#pragma unroll
+    for (int i = 3; i >= 0; --i) {
+        const uint32_t mv = a[i], t = x << (1 << i);
+        x = (x & ~mv) | (t & mv);
+    }
+    return x & m0;
+}
+
 // Magnitude sources of the encoder. Each fills S.m[0, 8192) (zeros past
 // the chunk's end) and S.nsign (the chunk's natural sign words).
 
 // Morton-packed u16 magnitudes and a natural sign bitmap in global memory.
 struct MagArrays {
+    static constexpr bool kBlockPlanes = false;
     const uint16_t* mag;
     const uint32_t* sign;
     __device__ __forceinline__ void load(WzpEncodeSmem& S, uint32_t first, uint32_t count, int tid) const {
@@ -236,6 +356,7 @@ struct MagArrays {
 // rewritten (dequantised) row by row, its magnitudes and negative flags placed
 // at their Morton ranks, and q-outliers recorded as in quantize_kernel.
 template <class T> struct QuantBricks {
+    static constexpr bool kBlockPlanes = true;
     T* coeff;
     uint32_t nx, ny, bz, lb;
     const uint16_t* rank; // full-brick slot: brick-local row-major index -> rank
@@ -243,6 +364,76 @@ template <class T> struct QuantBricks {
     uint32_t* qbits;
     uint32_t* qval;
     uint32_t* status;
+
+    // One thread per 16-sample block (thread t: Morton slots 16t .. 16t+15 of
+    // the chunk): quantise the block's four rows (dequantised values written
+    // back), then write its magnitudes to S.m, its 16 bit planes to S.planes
+    // (full chunks at the padded pitch, a partial chunk in the natural
+    // layout), and per 32-group the nonzero count and the compacted sign bits
+    // of its nonzero magnitudes (the even thread of each pair). Blocks past
+    // the chunk's end are zero.
+    __device__ __forceinline__ void block_planes(WzpEncodeSmem& S, uint32_t first, uint32_t count, int tid) const {
+        const uint32_t blocks = count >> 4, t = uint32_t(tid);
+        uint32_t w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        uint32_t zm = 0, nm = 0;
+        if (t < blocks) {
+            const BlockShape sh{bz == 16};
+            const uint32_t plane = nx * ny;
+            const uint32_t b = (first >> lb) + ((t << 4) >> lb), k = t & ((1u << (lb - 4)) - 1u);
+            const uint32_t nbx = nx / 16, nby = ny / 16;
+            const uint32_t bxi = b % nbx, tb = b / nbx, byi = tb % nby, slab = tb / nby;
+            uint32_t lx, ly, lz;
+            block_origin(k, lb - 8, lx, ly, lz);
+            const uint32_t at0 = (slab * bz + lz) * plane + (byi * 16 + ly) * nx + bxi * 16 + lx;
+            uint32_t bad = 0;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const uint32_t at = at0 + sh.row_offset(r, nx, plane);
+                const uint32_t e0 = sh.e0(r), e1 = e0 + sh.d();
+                T v[4];
+                load4(coeff + at, v);
+                uint32_t mg[4];
+#pragma unroll
+                for (int x = 0; x < 4; ++x) {
+                    int32_t m;
+                    bool neg;
+                    v[x] = quantize_one<T>(v[x], inv, q, m, neg, bad);
+                    const uint32_t e = (x < 2 ? e0 : e1) + (x & 1);
+                    mg[x] = uint32_t(m > 65535 ? 65535 : m);
+                    zm |= uint32_t(m != 0) << e;
+                    nm |= uint32_t(neg && m) << e;
+                    if (m > 65535) {
+                        atomicOr(&qbits[(at + x) >> 5], 1u << ((at + x) & 31));
+                        qval[at + x] = uint32_t(m);
+                    }
+                }
+                store4(coeff + at, v);
+                // e0 and e1 are even: each pair fills one packed word
+                w[e0 >> 1] = mg[0] | (mg[1] << 16);
+                w[e1 >> 1] = mg[2] | (mg[3] << 16);
+            }
+            if (bad) atomicOr(status, ST_QUANT_DOMAIN);
+        }
+        uint4* dm = reinterpret_cast<uint4*>(S.m + 16 * t);
+        dm[0] = make_uint4(w[0], w[1], w[2], w[3]);
+        dm[1] = make_uint4(w[4], w[5], w[6], w[7]);
+        // group statistics: this block's count and compacted signs, merged
+        // with the odd neighbour's by the even thread of the pair
+        const uint32_t cnt = __popc(zm), cs = compress16(nm, zm);
+        const uint32_t cnt1 = __shfl_xor_sync(0xffffffffu, cnt, 1), cs1 = __shfl_xor_sync(0xffffffffu, cs, 1);
+        if (!(t & 1) && t < kChunk / 16) {
+            S.gcount[t >> 1] = cnt + cnt1;
+            S.gsign[t >> 1] = cs | (cs1 << cnt);
+        }
+        if (t < blocks) {
+            if ((w[0] | w[1] | w[2] | w[3] | w[4] | w[5] | w[6] | w[7]) != 0) bit_transpose16(w);
+            uint16_t* pl = reinterpret_cast<uint16_t*>(S.planes);
+            const bool full = blocks == kChunk / 16;
+            const uint32_t stride = full ? 2 * kEncPitch : blocks;
+#pragma unroll
+            for (int p = 0; p < 16; ++p) pl[p * stride + t] = uint16_t(p & 1 ? w[p >> 1] >> 16 : w[p >> 1]);
+        }
+    }
     __device__ __forceinline__ void load(WzpEncodeSmem& S, uint32_t first, uint32_t count, int tid) const {
         const uint32_t bsz = 1u << lb, nb = count >> lb, plane = nx * ny;
         if (tid < int(nb)) {
@@ -342,6 +533,13 @@ __device__ __forceinline__ void WzpEncodeOp<Src>::run(const Params P, uint32_t, 
     const uint32_t count = min(kChunk, A.n - first);
     const uint32_t blocks = count / 16;
 
+    if constexpr (Src::kBlockPlanes) {
+        // ---- one thread per 16-sample block: magnitudes, bit planes and
+        // group statistics in one pass
+        src.block_planes(S, first, count, tid);
+        for (int i = tid; i < int(kChunk / 32) + 1; i += kWzpThreads) S.sgn[i] = 0;
+        __syncthreads();
+    } else {
     // ---- magnitudes and natural sign words of the chunk
     src.load(S, first, count, tid);
     for (int i = tid; i < int(kChunk / 32) + 1; i += kWzpThreads) S.sgn[i] = 0;
@@ -403,6 +601,7 @@ __device__ __forceinline__ void WzpEncodeOp<Src>::run(const Params P, uint32_t, 
     for (uint32_t i = blocks * 16 + tid; i < count; i += kWzpThreads)
         reinterpret_cast<uint16_t*>(S.planes)[i] = S.m[i];
     __syncthreads();
+    }
 
     // ---- signs: each group's packed sign bits go to its rank offset (at most
     // two words)
