@@ -250,14 +250,13 @@ __device__ __forceinline__ void bit_transpose16(uint32_t (&w)[8]) {
 // Element layout of a block: row r (0..3) of the block's four 16-byte rows
 // holds magnitudes e0(r), e0(r)+1 (x = 0, 1) and e0(r)+d, e0(r)+d+1 (x = 2, 3);
 // its offset from the block origin is dz * plane + dy * nx.
-struct BlockShape {
-    bool tall; // bz = 16: 4 x 2 x 2 (rows dy + 2 dz); else 4 x 4 x 1 (rows dy)
-    __device__ __forceinline__ uint32_t e0(int r) const {
-        return tall ? uint32_t(2 * r) : uint32_t(((r & 1) << 1) | ((r >> 1) << 3));
-    }
-    __device__ __forceinline__ uint32_t d() const { return tall ? 8u : 4u; }
-    __device__ __forceinline__ uint32_t row_offset(int r, uint32_t nx, uint32_t plane) const {
-        return tall ? uint32_t(r >> 1) * plane + uint32_t(r & 1) * nx : uint32_t(r) * nx;
+// Tall: bz = 16, 4 x 2 x 2 (rows dy + 2 dz); else 4 x 4 x 1 (rows dy). A
+// compile-time shape keeps the packed magnitudes in registers.
+template <bool Tall> struct BlockShape {
+    static __device__ __forceinline__ constexpr int e0(int r) { return Tall ? 2 * r : ((r & 1) << 1) | ((r >> 1) << 3); }
+    static constexpr int d = Tall ? 8 : 4;
+    static __device__ __forceinline__ uint32_t row_offset(int r, uint32_t nx, uint32_t plane) {
+        return Tall ? uint32_t(r >> 1) * plane + uint32_t(r & 1) * nx : uint32_t(r) * nx;
     }
 };
 
@@ -365,6 +364,51 @@ template <class T> struct QuantBricks {
     uint32_t* qval;
     uint32_t* status;
 
+    // Quantises block t of the chunk starting at `first` (its dequantised
+    // values written back): packed magnitudes w (pairs of Morton slots),
+    // nonzero and negative masks (bit j = slot j of the block).
+    template <bool Tall>
+    __device__ __forceinline__ void quantise_block(uint32_t first, uint32_t t, uint32_t (&w)[8], uint32_t& zm,
+                                                   uint32_t& nm) const {
+        using Sh = BlockShape<Tall>;
+        const uint32_t plane = nx * ny;
+        const uint32_t b = (first >> lb) + ((t << 4) >> lb), k = t & ((1u << (lb - 4)) - 1u);
+        const uint32_t nbx = nx / 16, nby = ny / 16;
+        const uint32_t bxi = b % nbx, tb = b / nbx, byi = tb % nby, slab = tb / nby;
+        uint32_t lx, ly, lz;
+        block_origin(k, lb - 8, lx, ly, lz);
+        const uint32_t at0 = (slab * bz + lz) * plane + (byi * 16 + ly) * nx + bxi * 16 + lx;
+        uint32_t bad = 0;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const uint32_t at = at0 + Sh::row_offset(r, nx, plane);
+            constexpr int dd = Sh::d;
+            const int e0 = Sh::e0(r), e1 = e0 + dd;
+            T v[4];
+            load4(coeff + at, v);
+            uint32_t mg[4];
+#pragma unroll
+            for (int x = 0; x < 4; ++x) {
+                int32_t m;
+                bool neg;
+                v[x] = quantize_one<T>(v[x], inv, q, m, neg, bad);
+                const int e = (x < 2 ? e0 : e1) + (x & 1);
+                mg[x] = uint32_t(m > 65535 ? 65535 : m);
+                zm |= uint32_t(m != 0) << e;
+                nm |= uint32_t(neg && m) << e;
+                if (m > 65535) {
+                    atomicOr(&qbits[(at + x) >> 5], 1u << ((at + x) & 31));
+                    qval[at + x] = uint32_t(m);
+                }
+            }
+            store4(coeff + at, v);
+            // e0 and e1 are even: each pair fills one packed word
+            w[e0 >> 1] = mg[0] | (mg[1] << 16);
+            w[e1 >> 1] = mg[2] | (mg[3] << 16);
+        }
+        if (bad) atomicOr(status, ST_QUANT_DOMAIN);
+    }
+
     // One thread per 16-sample block (thread t: Morton slots 16t .. 16t+15 of
     // the chunk): quantise the block's four rows (dequantised values written
     // back), then write its magnitudes to S.m, its 16 bit planes to S.planes
@@ -377,44 +421,11 @@ template <class T> struct QuantBricks {
         uint32_t w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         uint32_t zm = 0, nm = 0;
         if (t < blocks) {
-            const BlockShape sh{bz == 16};
-            const uint32_t plane = nx * ny;
-            const uint32_t b = (first >> lb) + ((t << 4) >> lb), k = t & ((1u << (lb - 4)) - 1u);
-            const uint32_t nbx = nx / 16, nby = ny / 16;
-            const uint32_t bxi = b % nbx, tb = b / nbx, byi = tb % nby, slab = tb / nby;
-            uint32_t lx, ly, lz;
-            block_origin(k, lb - 8, lx, ly, lz);
-            const uint32_t at0 = (slab * bz + lz) * plane + (byi * 16 + ly) * nx + bxi * 16 + lx;
-            uint32_t bad = 0;
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                const uint32_t at = at0 + sh.row_offset(r, nx, plane);
-                const uint32_t e0 = sh.e0(r), e1 = e0 + sh.d();
-                T v[4];
-                load4(coeff + at, v);
-                uint32_t mg[4];
-#pragma unroll
-                for (int x = 0; x < 4; ++x) {
-                    int32_t m;
-                    bool neg;
-                    v[x] = quantize_one<T>(v[x], inv, q, m, neg, bad);
-                    const uint32_t e = (x < 2 ? e0 : e1) + (x & 1);
-                    mg[x] = uint32_t(m > 65535 ? 65535 : m);
-                    zm |= uint32_t(m != 0) << e;
-                    nm |= uint32_t(neg && m) << e;
-                    if (m > 65535) {
-                        atomicOr(&qbits[(at + x) >> 5], 1u << ((at + x) & 31));
-                        qval[at + x] = uint32_t(m);
-                    }
-                }
-                store4(coeff + at, v);
-                // e0 and e1 are even: each pair fills one packed word
-                w[e0 >> 1] = mg[0] | (mg[1] << 16);
-                w[e1 >> 1] = mg[2] | (mg[3] << 16);
-            }
-            if (bad) atomicOr(status, ST_QUANT_DOMAIN);
+            if (bz == 16) quantise_block<true>(first, t, w, zm, nm);
+            else quantise_block<false>(first, t, w, zm, nm);
         }
         uint4* dm = reinterpret_cast<uint4*>(S.m + 16 * t);
+
         dm[0] = make_uint4(w[0], w[1], w[2], w[3]);
         dm[1] = make_uint4(w[4], w[5], w[6], w[7]);
         // group statistics: this block's count and compacted signs, merged
@@ -835,6 +846,34 @@ struct BrickMap {
     }
 };
 
+// Dequantises block t of the chunk starting at `first` (packed magnitudes w,
+// negative mask nm) into the row-major coefficients as four 16-byte rows.
+template <class T, bool Tall>
+__device__ __forceinline__ void store_block(const BrickMap& map, T* coeff, uint32_t first, uint32_t t,
+                                            const uint32_t (&w)[8], uint32_t nm, T q) {
+    using Sh = BlockShape<Tall>;
+    const uint32_t plane = map.nx * map.ny;
+    uint32_t lx, ly, lz;
+    block_origin(t & ((1u << (map.lb - 4)) - 1u), map.lb - 8, lx, ly, lz);
+    const uint32_t b = (first >> map.lb) + ((t << 4) >> map.lb);
+    const uint32_t at0 = map.brick_base(b) + lz * plane + ly * map.nx + lx;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        constexpr int dd = Sh::d;
+        const int e0 = Sh::e0(r), e1 = e0 + dd;
+        const uint32_t pa = w[e0 >> 1], pb = w[e1 >> 1];
+        const uint32_t mg[4] = {pa & 0xffffu, pa >> 16, pb & 0xffffu, pb >> 16};
+        T v4[4];
+#pragma unroll
+        for (int x = 0; x < 4; ++x) {
+            const int e = (x < 2 ? e0 : e1) + (x & 1);
+            const T mag = Lift<T>::mul(T(mg[x]), q);
+            v4[x] = ((nm >> e) & 1u) ? -mag : mag;
+        }
+        store4(coeff + at0 + Sh::row_offset(r, map.nx, plane), v4);
+    }
+}
+
 struct WzpDecodeSmem {
     uint32_t bbase[32];                // row-major base of each whole brick of the chunk (fast map)
     uint16_t m[kChunk + 16];           // staged magnitude bytes, then the decoded magnitudes
@@ -920,6 +959,8 @@ __device__ __forceinline__ void WzpDecodeOp<T>::run(const Params A, uint32_t blo
     const uint8_t* meta = in + size_t(groups) * 4;
     const uint8_t* payload = in + header;
     const size_t payload_bytes = J.wzp - header;
+    // whole bricks (chunks are runs of them): one thread per 16-sample block
+    const bool blockwise = A.map.fast && (reinterpret_cast<uintptr_t>(A.coeff) & 15u) == 0;
 
     if (warp == 0) {
         // Lane k reads the metadata of the group's chunk k; the chunk's payload
@@ -1099,6 +1140,7 @@ __device__ __forceinline__ void WzpDecodeOp<T>::run(const Params A, uint32_t blo
         const bool full = blocks == kChunk / 16;
         if (!full) planes_repack(S.planes, blocks, true, tid);
         __syncthreads();
+        if (!blockwise) { // else each thread transposes its own block below
         // ---- inverse bit planes, two groups per warp step: lane l holds plane
         // l % 16 of group g0 + l / 16 (bit 31-e = magnitude e's bit 15-p); one
         // 32x32 transpose leaves magnitude e of g0 in the high half of lane e's
@@ -1127,8 +1169,57 @@ __device__ __forceinline__ void WzpDecodeOp<T>::run(const Params A, uint32_t blo
         }
         for (uint32_t i = blocks * 16 + tid; i < kChunk; i += kWzpThreads)
             S.m[i] = i == ti ? tail : 0;
+        }
     }
     __syncthreads();
+
+    if (blockwise) {
+        // ---- one thread per 16-sample block (whole bricks): magnitudes from
+        // its 16 bit planes (one transpose) or the verbatim ones, nonzero
+        // ranks by one block scan, signs spread from the sign stream, then the
+        // dequantised block stored as four 16-byte rows
+        const uint32_t t = uint32_t(tid);
+        uint32_t w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        if (t < blocks && mbytes != 0) {
+            if (S.raw) {
+                const uint4* sm = reinterpret_cast<const uint4*>(S.m + 16 * t);
+                const uint4 a = sm[0], b = sm[1];
+                w[0] = a.x, w[1] = a.y, w[2] = a.z, w[3] = a.w, w[4] = b.x, w[5] = b.y, w[6] = b.z, w[7] = b.w;
+            } else {
+                const uint16_t* pl = reinterpret_cast<const uint16_t*>(S.planes);
+                const uint32_t stride = blocks == kChunk / 16 ? 2 * kEncPitch : 2 * kPlanePitch;
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+                    w[i] = uint32_t(pl[2 * i * stride + t]) | (uint32_t(pl[(2 * i + 1) * stride + t]) << 16);
+                if ((w[0] | w[1] | w[2] | w[3] | w[4] | w[5] | w[6] | w[7]) != 0) bit_transpose16(w);
+            }
+        }
+        uint32_t zm = 0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const uint32_t nzh = __vsetne2(w[i], 0u); // 0xffff per nonzero half
+            zm |= ((nzh & 1u) | ((nzh >> 15) & 2u)) << (2 * i);
+        }
+        const uint32_t cnt = __popc(zm);
+        uint32_t nnz;
+        const uint32_t base = block_excl_scan<kWzpThreads>(cnt, S.tmp, nnz);
+        if (mbytes != 0) {
+            if (nnz == 0 || (nnz + 7) / 8 != sbytes) bad = true;
+            else if ((nnz & 7) && (sgn[sbytes - 1] >> (nnz & 7))) bad = true;
+        }
+        if (t < blocks) {
+            uint32_t nm = 0;
+            if (cnt && !bad) {
+                const uint32_t by = base >> 3;
+                const uint32_t bits = uint32_t(sgn[by]) | (uint32_t(sgn[by + 1]) << 8) | (uint32_t(sgn[by + 2]) << 16);
+                nm = expand16((bits >> (base & 7u)) & ((1u << cnt) - 1u), zm);
+            }
+            if (A.map.bz == 16) store_block<T, true>(A.map, A.coeff, first, t, w, nm, q);
+            else store_block<T, false>(A.map, A.coeff, first, t, w, nm, q);
+        }
+        if (bad) atomicOr(A.status, ST_BAD_STREAM);
+        return;
+    }
 
     // ---- signs and dequantisation: nonzero counts of the remaining groups
     const int counted = (mbytes != 0 && !S.raw) ? int(blocks * 16 / 32) : 0;
