@@ -35,18 +35,30 @@ int waltz_b200_compress(const void* d_input, int width, uint32_t nx, uint32_t ny
                         void* stream);
 
 /* Transform forms. PLAIN is the default profile (lifting, archives
- * byte-identical to the reference CPU codec). MATRIX is the precision form:
- * the plane schedule's Z stage (all Z levels) runs as one nz x nz matrix on
- * the tensor cores (TF32 hi/lo halves, FP32 accumulation) and the repair pass
- * restores the bound; such archives set header flag bit 6, which the
- * reference's decoders reject. MATRIX needs the plane schedule (Z levels
- * differ from XY levels) with 1 <= nz <= 128 and nx*ny a multiple of 4; float
- * and double fields (the transform is fp32-accurate for both; a double
- * field's quantisation and repair decisions stay in double). New surface:
- * the reference has no counterpart (its header reserves the bit,
+ * byte-identical to the reference CPU codec). The MATRIX forms are the
+ * precision form: the plane schedule's Z stage (all Z levels) runs as one
+ * nz x nz matrix on the tensor cores and the repair pass restores the bound.
+ * They differ in the tensor-core arithmetic:
+ *   MATRIX        TF32x3: TF32 hi/lo halves, three products, FP32 accumulation
+ *                 (about 21 bits);
+ *   MATRIX_BF16   BF16x3: three bf16 slices, six products, FP32 accumulation
+ *                 (fp32-accurate);
+ *   MATRIX_EXACT  five 7-bit integer slices in bf16 per column and matrix row
+ *                 (power-of-two scaled), every product order accumulated
+ *                 exactly in its own FP32 tile and recombined in double:
+ *                 about 2^-35 relative error, for double fields (nz <= 96).
+ * Such archives set header flag bit 6 and record the form in bits 5 and 7,
+ * which the reference's decoders reject. The matrix forms need the plane
+ * schedule (Z levels differ from XY levels) with 1 <= nz <= 128 (96 for
+ * MATRIX_EXACT) and nx*ny a multiple of 4; float and double fields (TF32x3
+ * and BF16x3 round double samples to float first; a double field's
+ * quantisation and repair decisions stay in double). New surface: the
+ * reference has no counterpart (its header reserves the bits,
  * include/utils/Blob.hpp:46-53). */
 #define WALTZ_B200_FORM_PLAIN 0
 #define WALTZ_B200_FORM_MATRIX 1
+#define WALTZ_B200_FORM_MATRIX_BF16 2
+#define WALTZ_B200_FORM_MATRIX_EXACT 3
 int waltz_b200_compress_form(const void* d_input, int width, uint32_t nx, uint32_t ny, uint32_t nz,
                              double abs_error, int form, void* d_archive, size_t capacity, size_t* written,
                              void* stream);
@@ -156,6 +168,11 @@ int waltz_b200_wzp_encode(const uint16_t* d_mag, const uint32_t* d_sign, uint32_
  *   include/transformers/all_halo.cuh:143-224. */
 int waltz_b200_zmatrix(float* d_data, uint32_t nx, uint32_t ny, uint32_t nz, int inverse, void* stream);
 int waltz_b200_zmatrix_f64(double* d_data, uint32_t nx, uint32_t ny, uint32_t nz, int inverse, void* stream);
+/* waltz_b200_zmatrix_split: the same Z transform of a float (width 4) or
+ *   double (width 8) field in any matrix form (WALTZ_B200_FORM_MATRIX,
+ *   _MATRIX_BF16, _MATRIX_EXACT). */
+int waltz_b200_zmatrix_split(void* d_data, int width, uint32_t nx, uint32_t ny, uint32_t nz, int inverse, int form,
+                             void* stream);
 /* Allocation-free variant of waltz_b200_wzp_encode (same arguments, same
  * stream bytes), for callers that cannot allocate device memory when they
  * call: a framework whose allocator owns the device budget, a plugin or filter

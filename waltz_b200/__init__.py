@@ -57,13 +57,28 @@ def _stream(torch, stream):
     return C.c_void_p(s.cuda_stream)
 
 
-FORMS = {"plain": 0, "matrix": 1}
+# Transform forms: the default lifting profile, and the precision form's
+# tensor-core splits (include/waltz_b200.h, WALTZ_B200_FORM_*).
+FORMS = {"plain": 0, "matrix": 1, "matrix-tf32": 1, "matrix-bf16": 2, "matrix-exact": 3}
 
 
-def _matrix_ok(shape, itemsize):
+def _matrix_ok(shape, itemsize, form="matrix"):
     nx, ny, nz = _geometry(shape, itemsize)
     lxy, lz = (autotune._levels(min(nx, ny)), autotune._levels(nz))
-    return itemsize in (4, 8) and lxy != lz and lz >= 1 and nz <= 128 and (nx * ny) % 4 == 0
+    kmax = 96 if form == "matrix-exact" else 128
+    return itemsize in (4, 8) and lxy != lz and lz >= 1 and nz <= kmax and (nx * ny) % 4 == 0
+
+
+def auto_form(shape, itemsize):
+    """The form form="auto" takes: the precision form where it applies and
+    the tuning table measured it faster, in its most accurate split for the
+    field's type (exact slices for double fields with nz <= 96, BF16x3
+    otherwise); the plain form elsewhere."""
+    if not (_matrix_ok(shape, itemsize) and autotune.matrix_preferred(tuple(shape), itemsize)):
+        return "plain"
+    if itemsize == 8 and _matrix_ok(shape, itemsize, "matrix-exact"):
+        return "matrix-exact"
+    return "matrix-bf16"
 
 
 def compress_tensor(field, abs_error: float, *, form: str = "plain", stream=None, tuned=True):
@@ -71,11 +86,12 @@ def compress_tensor(field, abs_error: float, *, form: str = "plain", stream=None
     (y,x). Returns a uint8 CUDA tensor holding the archive.
 
     form="plain" is the default profile (byte-identical to the reference CPU
-    codec); form="matrix" is the precision form, whose Z stage runs as one
-    matrix on the tensor cores (plane schedule, nz <= 128); form="auto"
-    takes the matrix form where it applies and the tuning table measured it
-    faster. With `tuned`, the tuning table's knobs for the field's class are
-    applied first (they never change the output)."""
+    codec); form="matrix" (TF32x3), "matrix-bf16" (BF16x3) and
+    "matrix-exact" (exact bf16 slices, nz <= 96) are the precision form,
+    whose Z stage runs as one matrix on the tensor cores (plane schedule,
+    nz <= 128); form="auto" takes auto_form(). With `tuned`, the tuning
+    table's knobs for the field's class are applied first (they never change
+    the output)."""
     torch = _torch()
     if not field.is_cuda or not field.is_contiguous():
         raise ValueError("expected a contiguous CUDA tensor")
@@ -83,8 +99,7 @@ def compress_tensor(field, abs_error: float, *, form: str = "plain", stream=None
         raise ValueError(f"form must be one of {sorted(FORMS) + ['auto']}")
     itemsize = field.element_size()
     if form == "auto":
-        form = "matrix" if _matrix_ok(field.shape, itemsize) and autotune.matrix_preferred(
-            tuple(field.shape), itemsize) else "plain"
+        form = auto_form(tuple(field.shape), itemsize)
     if tuned:
         autotune.apply_single(lib(), tuple(_geometry(field.shape, itemsize))[::-1], itemsize)
     nx, ny, nz = _geometry(field.shape, field.element_size())
@@ -226,7 +241,7 @@ def rel_to_abs_bound(field, rel: float, *, stream=None) -> float:
 def compress(array, *, abs_error, form="plain"):
     """Return archive bytes of a float32/float64 (z,y,x) or (y,x) numpy array,
     computed on the current CUDA device: canonical (reference-identical) in
-    the default plain form, tensor-core Z stage with form="matrix"."""
+    the default plain form, tensor-core Z stage with the matrix forms."""
     torch = _torch()
     a = np.ascontiguousarray(np.asarray(array))
     if a.dtype not in (np.float32, np.float64):

@@ -40,6 +40,8 @@ SIGNATURES = {
                                         C.POINTER(C.c_size_t), C.c_void_p]),
     "waltz_b200_zmatrix": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_void_p]),
     "waltz_b200_zmatrix_f64": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_void_p]),
+    "waltz_b200_zmatrix_split": (C.c_int, [C.c_void_p, C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_int,
+                                           C.c_void_p]),
     "waltz_b200_wzp_encode_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_size_t,
                                                 C.POINTER(C.c_size_t), C.c_void_p]),
     "waltz_b200_test_lookback_timeout": (C.c_int, [C.c_void_p, C.c_int, C.c_uint32, C.c_uint32, C.c_uint32,

@@ -8,8 +8,9 @@
 -f / -d select float32 (default) / float64. Raw files hold nx*ny*nz samples,
 x fastest. REL resolves to REL * (max - min) on the GPU before compressing
 (examples/waltz.cu:50-55). With -o during compression the reconstruction is
-written and compared with the input (max error, PSNR, ratio). --form matrix
-selects the precision form; WALTZ_WARMUP=1 runs each call once untimed and
+written and compared with the input (max error, PSNR, ratio). --form matrix,
+matrix-bf16 or matrix-exact selects the precision form (its tensor-core
+split); WALTZ_WARMUP=1 runs each call once untimed and
 WALTZ_REPORT_CE2E=1 prints the device time of the call, as in the reference.
 """
 from __future__ import annotations
@@ -33,7 +34,7 @@ def parse(argv):
     ap.add_argument("-o", dest="output", help="reconstruction; with compression also verified against the input")
     ap.add_argument("-3", dest="dims", nargs=3, type=int, metavar=("NX", "NY", "NZ"), required=True)
     ap.add_argument("-M", dest="mode", nargs=2, metavar=("REL|ABS", "BOUND"))
-    ap.add_argument("--form", choices=["plain", "matrix", "auto"], default="plain")
+    ap.add_argument("--form", choices=["plain", "matrix", "matrix-bf16", "matrix-exact", "auto"], default="plain")
     a = ap.parse_args(argv)
     a.dtype = a.dtype or "f32"
     if any(v <= 0 for v in a.dims):

@@ -485,15 +485,16 @@ static TransformScratch scratch_need(const Geometry& g) {
 }
 
 template <class T, class Out>
-static void zmatrix_apply(const T* x, uint32_t nx, uint32_t ny, uint32_t nz, bool inverse, const Out& out,
+static void zmatrix_apply(const T* x, uint32_t nx, uint32_t ny, uint32_t nz, bool inverse, int zsplit, const Out& out,
                           uint32_t* status, bool check_finite, Sink& sink);
 
-// Forward all-level transform of `in` into the coefficient array C. With
-// `matrix` (the precision form; plane schedule, float) the Z stage is the
+// Forward all-level transform of `in` into the coefficient array C. With a
+// split code `zsplit` (the precision form; plane schedule) the Z stage is the
 // tensor-core matrix transform instead of Z lifting.
 template <class T>
 static void forward(const Geometry& g, const T* in, T* C, T* lowA, T* lowB, T* inter, uint32_t* status,
-                    Sink& sink, bool matrix = false) {
+                    Sink& sink, int zsplit = 0) {
+    const bool matrix = zsplit != 0;
     const size_t sy = g.nx, sz = size_t(g.nx) * g.ny;
     T* lows[2] = {lowA, lowB};
     if (g.lxy == 0 && g.lz == 0) {
@@ -516,7 +517,7 @@ static void forward(const Geometry& g, const T* in, T* C, T* lowA, T* lowB, T* i
     FwdSrc<T> src{in, sy, sz, status};
     T* zdst = g.lxy ? inter : C;
     if (matrix) {
-        zmatrix_apply<T>(in, g.nx, g.ny, g.nz, false, ZmStore<T>{zdst}, status, true, sink);
+        zmatrix_apply<T>(in, g.nx, g.ny, g.nz, false, zsplit, ZmStore<T>{zdst}, status, true, sink);
         sink.mark("fwd_z_matrix");
     }
     const bool zstage = !matrix && zstage_ok<T>(g);
@@ -564,7 +565,8 @@ static uint64_t inverse_low_need(const Geometry& g) {
 // hands every sample to `fin`.
 template <class T, class Final>
 static void inverse(const Geometry& g, T* C, T* bank1, T* bank2, const Final& fin, uint32_t* status,
-                    Sink& sink, const char* final_stage = "inv_l0", bool matrix = false) {
+                    Sink& sink, const char* final_stage = "inv_l0", int zsplit = 0) {
+    const bool matrix = zsplit != 0;
     const size_t sy = g.nx, sz = size_t(g.nx) * g.ny;
     const uint64_t half_off = ((g.n + 1) / 2 + 63) & ~uint64_t(63);
     need(inverse_low_need(g) <= g.n - std::min(g.n, half_off), "Waltz: inverse scratch layout");
@@ -623,7 +625,7 @@ static void inverse(const Geometry& g, T* C, T* bank1, T* bank2, const Final& fi
         sink.mark("inv_xy");
     }
     if (matrix && g.lz) {
-        zmatrix_apply<T>(zbase, g.nx, g.ny, g.nz, true, ZmEmit<T, Final>{fin, g.nx}, status, false, sink);
+        zmatrix_apply<T>(zbase, g.nx, g.ny, g.nz, true, zsplit, ZmEmit<T, Final>{fin, g.nx}, status, false, sink);
         sink.mark("inv_z_matrix");
         return;
     }
@@ -741,80 +743,190 @@ static void pack_tf32_halves(const std::vector<double>& m, uint32_t nz, std::vec
         }
 }
 
-// Device copies of the Z matrices per column length, kept until exit: a
-// captured graph may hold their addresses.
+// Bits of the bf16 nearest to v (round to nearest even; v finite).
+static uint16_t host_bf16(double v) {
+    const float f = float(v);
+    uint32_t b;
+    std::memcpy(&b, &f, 4);
+    b += 0x7fffu + ((b >> 16) & 1u);
+    return uint16_t(b >> 16);
+}
+static double host_bf16_value(uint16_t h) {
+    const uint32_t b = uint32_t(h) << 16;
+    float f;
+    std::memcpy(&f, &b, 4);
+    return f;
+}
+
+// bf16 slices of a matrix in the K-major no-swizzle core layout of
+// zmatrix_slices_kernel (core (n/8, k/8) at ((n/8) * kp/8 + k/8) * 64
+// elements, element (n%8, k%8) at (n%8) * 8 + k%8), slice after slice.
+// BF16x3: m = b0 + b1 + b2 (+ residual), each bf16 of the remaining residual.
+// Exact: row n scaled by 2^-f_n (|m| < 2^f_n over the row) and cut into
+// 7-bit integer slices; scale[n] = 2^(f_n - 14), the epilogue's row factor.
+static void pack_bf16_slices(const std::vector<double>& m, uint32_t nz, bool exact, std::vector<uint16_t>& out,
+                             std::vector<double>& scale) {
+    const uint32_t S = exact ? kZsExactSlices : 3;
+    const ZsPlan P = ZsPlan::make(nz, S);
+    const size_t per = size_t(P.np) * P.kp;
+    out.assign(S * per, 0);
+    scale.assign(P.np, 0.0);
+    for (uint32_t n = 0; n < P.np; ++n) {
+        double rmax = 0.0;
+        for (uint32_t k = 0; k < nz && n < nz; ++k) rmax = std::max(rmax, std::fabs(m[size_t(n) * nz + k]));
+        int f = 0;
+        if (rmax > 0) std::frexp(rmax, &f); // rmax < 2^f
+        scale[n] = n < nz ? std::ldexp(1.0, f - 14) : 0.0;
+        for (uint32_t k = 0; k < P.kp; ++k) {
+            const double v = (n < nz && k < nz) ? m[size_t(n) * nz + k] : 0.0;
+            const size_t at = (size_t(n / 8) * (P.kp / 8) + k / 8) * 64 + (n % 8) * 8 + (k % 8);
+            if (exact) {
+                double u = std::ldexp(v, -f);
+                for (uint32_t sl = 0; sl < S; ++sl) {
+                    const double a = std::nearbyint(u * 128.0);
+                    u = u * 128.0 - a;
+                    out[sl * per + at] = host_bf16(a);
+                }
+            } else {
+                double r = v;
+                for (uint32_t sl = 0; sl < S; ++sl) {
+                    const uint16_t h = host_bf16(r);
+                    out[sl * per + at] = h;
+                    r -= host_bf16_value(h);
+                }
+            }
+        }
+    }
+}
+
+// Device copies of the Z matrices per column length and split form, kept
+// until exit: a captured graph may hold their addresses. TF32x3: the hi and
+// lo halves of the analysis and synthesis matrices; bf16 forms: their slices
+// (and row scales).
 struct ZMatrixCache {
     struct Entry {
         uint32_t nz;
-        float* dev; // fwd hi, fwd lo, inv hi, inv lo
-        size_t half; // floats per half
+        int split;
+        void* dev;
+        size_t bytes[2];  // per direction: operand bytes, then scale bytes
+        size_t off[2][2]; // [inverse][0 operand, 1 scales]
     };
     int device = -1;
     std::vector<Entry> entries;
     ~ZMatrixCache() {
         for (auto& e : entries) cudaFree(e.dev);
     }
-    const float* get(uint32_t n, bool inverse, bool lo, cudaStream_t stream) {
+    const Entry& get(uint32_t n, int split, cudaStream_t stream) {
         int d = 0;
         check(cudaGetDevice(&d), "cudaGetDevice");
         if (d != device) {
             entries.clear(); // matrices of another device's context stay allocated there
             device = d;
         }
-        const Entry* hit = nullptr;
         for (auto& e : entries)
-            if (e.nz == n) hit = &e;
-        if (!hit) {
-            const std::vector<double> M = z_analysis_matrix(n), S = invert_matrix(M, n);
-            std::vector<float> fh, fl, ih, il;
-            pack_tf32_halves(M, n, fh, fl);
-            pack_tf32_halves(S, n, ih, il);
-            Entry e{n, nullptr, fh.size()};
-            check(cudaMalloc(&e.dev, 4 * e.half * sizeof(float)), "Waltz: cannot allocate Z matrices");
-            std::vector<float> all;
-            for (auto* part : {&fh, &fl, &ih, &il}) all.insert(all.end(), part->begin(), part->end());
-            check(cudaMemcpyAsync(e.dev, all.data(), all.size() * 4, cudaMemcpyHostToDevice, stream),
-                  "Z matrix upload");
-            check(cudaStreamSynchronize(stream), "Z matrix upload");
-            entries.push_back(e);
-            hit = &entries.back();
+            if (e.nz == n && e.split == split) return e;
+        const std::vector<double> M = z_analysis_matrix(n), Sy = invert_matrix(M, n);
+        std::vector<unsigned char> all;
+        Entry e{n, split, nullptr, {0, 0}, {{0, 0}, {0, 0}}};
+        auto append = [&](const void* p, size_t bytes) {
+            const size_t at = (all.size() + 255) / 256 * 256;
+            all.resize(at + bytes);
+            std::memcpy(all.data() + at, p, bytes);
+            return at;
+        };
+        for (int inv = 0; inv < 2; ++inv) {
+            const std::vector<double>& mat = inv ? Sy : M;
+            if (split == kZsTf32x3) {
+                std::vector<float> hi, lo;
+                pack_tf32_halves(mat, n, hi, lo);
+                hi.insert(hi.end(), lo.begin(), lo.end());
+                e.off[inv][0] = append(hi.data(), hi.size() * 4);
+            } else {
+                std::vector<uint16_t> sl;
+                std::vector<double> sc;
+                pack_bf16_slices(mat, n, split == kZsExact, sl, sc);
+                e.off[inv][0] = append(sl.data(), sl.size() * 2);
+                e.off[inv][1] = append(sc.data(), sc.size() * 8);
+            }
         }
-        return hit->dev + (size_t(inverse) * 2 + size_t(lo)) * hit->half;
+        check(cudaMalloc(&e.dev, all.size()), "Waltz: cannot allocate Z matrices");
+        check(cudaMemcpyAsync(e.dev, all.data(), all.size(), cudaMemcpyHostToDevice, stream), "Z matrix upload");
+        check(cudaStreamSynchronize(stream), "Z matrix upload");
+        entries.push_back(e);
+        return entries.back();
     }
 };
 static thread_local ZMatrixCache t_zmat;
 
 // Applies the all-levels Z analysis (or synthesis) matrix to a z-major float
-// or double field of nx*ny columns on the tensor cores; `out.group` takes
-// every result. nz <= 128, nx*ny a multiple of 4.
+// or double field of nx*ny columns on the tensor cores, in the arithmetic of
+// split form `zsplit`; `out.group` takes every result. nz <= 128 (96 for the
+// exact slices), nx*ny a multiple of 4.
+template <class K>
+static void zmatrix_launch(K kernel, uint32_t smem, uint32_t smem_max, uint64_t ncols, cudaStream_t stream,
+                           unsigned& grid) {
+    static thread_local std::vector<std::pair<const void*, int>> configured;
+    int dev = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    const void* key = reinterpret_cast<const void*>(kernel);
+    bool seen = false;
+    for (auto& c : configured)
+        if (c.first == key && c.second == dev) seen = true;
+    if (!seen) {
+        check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_max)),
+              "matrix kernel shared memory");
+        configured.emplace_back(key, dev);
+    }
+    const uint64_t tiles = (ncols + kZmCols - 1) / kZmCols;
+    // resident CTAs at this column length's shared memory (one or two per SM)
+    int sms = 0, occ = 0;
+    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kZmThreads, smem), "occupancy");
+    const uint64_t slots = uint64_t(sms) * uint64_t(occ > 0 ? occ : 1);
+    grid = unsigned(std::min<uint64_t>(tiles, slots));
+}
+
 template <class T, class Out>
-static void zmatrix_apply(const T* x, uint32_t nx, uint32_t ny, uint32_t nz, bool inverse, const Out& out,
+static void zmatrix_apply(const T* x, uint32_t nx, uint32_t ny, uint32_t nz, bool inverse, int zsplit, const Out& out,
                           uint32_t* status, bool check_finite, Sink& sink) {
     need(nz >= 1 && nz <= uint32_t(kZmMaxK), "Waltz: matrix form needs 1 <= nz <= 128");
+    need(zsplit != kZsExact || nz <= uint32_t(kZsExactMaxK), "Waltz: the exact slice form needs nz <= 96");
     const uint64_t ncols = uint64_t(nx) * ny;
-    const ZmPlan P = ZmPlan::make(nz);
-    const float* bhi = t_zmat.get(nz, inverse, false, sink.stream);
-    const float* blo = t_zmat.get(nz, inverse, true, sink.stream);
+    const ZMatrixCache::Entry& e = t_zmat.get(nz, zsplit, sink.stream);
+    const unsigned char* base = static_cast<const unsigned char*>(e.dev);
+    const int dir = inverse ? 1 : 0;
+    const uint32_t cf = check_finite ? 1u : 0u;
     // no batched form: every field keeps its own persistent launch
+    if (zsplit == kZsTf32x3) {
+        const ZmPlan P = ZmPlan::make(nz);
+        const float* bhi = reinterpret_cast<const float*>(base + e.off[dir][0]);
+        const float* blo = bhi + size_t(P.np) * P.kp;
+        sink.direct([=](cudaStream_t stream) {
+            auto kernel = zmatrix_kernel<T, Out>;
+            unsigned grid = 0;
+            zmatrix_launch(kernel, P.smem(), ZmPlan::make(kZmMaxK).smem(), ncols, stream, grid);
+            kernel<<<grid, kZmThreads, P.smem(), stream>>>(x, bhi, blo, nz, ncols, out, status, cf);
+            note_launch();
+            check(cudaGetLastError(), "matrix kernel launch");
+        });
+        return;
+    }
+    const bool exact = zsplit == kZsExact;
+    need(zsplit == kZsBf16x3 || exact, "Waltz: unknown matrix split form");
+    const ZsPlan P = ZsPlan::make(nz, exact ? kZsExactSlices : 3);
+    const uint16_t* bsl = reinterpret_cast<const uint16_t*>(base + e.off[dir][0]);
+    const double* bscale = reinterpret_cast<const double*>(base + e.off[dir][1]);
     sink.direct([=](cudaStream_t stream) {
-        auto kernel = zmatrix_kernel<T, Out>;
-        const uint32_t smem_max = ZmPlan::make(kZmMaxK).smem();
-        static thread_local int configured_device = -1;
-        int dev = 0;
-        check(cudaGetDevice(&dev), "cudaGetDevice");
-        if (configured_device != dev) {
-            check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_max)),
-                  "matrix kernel shared memory");
-            configured_device = dev;
+        unsigned grid = 0;
+        if (exact) {
+            auto kernel = zmatrix_slices_kernel<T, Out, true>;
+            zmatrix_launch(kernel, P.smem(), ZsPlan::make(kZsExactMaxK, kZsExactSlices).smem(), ncols, stream, grid);
+            kernel<<<grid, kZmThreads, P.smem(), stream>>>(x, bsl, bscale, nz, ncols, out, status, cf);
+        } else {
+            auto kernel = zmatrix_slices_kernel<T, Out, false>;
+            zmatrix_launch(kernel, P.smem(), ZsPlan::make(kZmMaxK, 3).smem(), ncols, stream, grid);
+            kernel<<<grid, kZmThreads, P.smem(), stream>>>(x, bsl, bscale, nz, ncols, out, status, cf);
         }
-        const uint64_t tiles = (ncols + kZmCols - 1) / kZmCols;
-        // resident CTAs at this column length's shared memory (one or two per SM)
-        int sms = 0, occ = 0;
-        check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
-        check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kZmThreads, P.smem()), "occupancy");
-        const uint64_t slots = uint64_t(sms) * uint64_t(occ > 0 ? occ : 1);
-        const unsigned grid = unsigned(std::min<uint64_t>(tiles, slots));
-        kernel<<<grid, kZmThreads, P.smem(), stream>>>(x, bhi, blo, nz, ncols, out, status, check_finite ? 1u : 0u);
         note_launch();
         check(cudaGetLastError(), "matrix kernel launch");
     });
@@ -837,19 +949,32 @@ static uint64_t* pinned() {
 struct EncodeOptions {
     uint32_t spin_cap = 1u << 22;
     uint32_t skip_publish = 0xffffffffu;
-    bool matrix = false; // precision form: tensor-core Z transform, header flag bit 6
+    int zsplit = kZsNone; // precision form: tensor-core Z transform in this split form (header flag bits)
 };
 
-// Header flag bit 6: the archive's Z stage is the tensor-core matrix form
-// (a reserved bit of the reference header, include/utils/Blob.hpp:46-53, so
-// the reference decoders reject such archives and the default bytes stay).
+// Header flag bit 6: the archive's Z stage is the tensor-core matrix form;
+// bits 5 and 7 then give its split form (0 TF32x3, 1 BF16x3, 2 exact bf16
+// slices). All three are reserved bits of the reference header
+// (include/utils/Blob.hpp:46-53), so the reference decoders reject such
+// archives and the default bytes stay.
 constexpr uint8_t kMatrixFlag = 0x40;
+static uint8_t split_flags(int zsplit) {
+    if (!zsplit) return 0;
+    const unsigned code = unsigned(zsplit - 1);
+    return uint8_t(kMatrixFlag | ((code & 1u) << 5) | ((code >> 1) << 7));
+}
+// Split form of an archive (kZsNone for lifting; 4 for the undefined code).
+static int split_of_flags(uint8_t flags) {
+    if (!(flags & kMatrixFlag)) return kZsNone;
+    return 1 + int(((flags >> 5) & 1u) | ((flags >> 6) & 2u));
+}
 
 // Fields the matrix form serves: float or double, plane schedule with Z
-// levels, 1 <= nz <= 128 and nx*ny a multiple of 4.
-static bool matrix_form_ok(const Geometry& g, size_t width) {
-    return (width == 4 || width == 8) && !g.dyadic && g.lz >= 1 && g.nz <= uint32_t(kZmMaxK) &&
-           (uint64_t(g.nx) * g.ny) % 4 == 0;
+// levels, 1 <= nz <= 128 (96 for the exact slices) and nx*ny a multiple of 4.
+static bool matrix_form_ok(const Geometry& g, size_t width, int zsplit = kZsTf32x3) {
+    const uint32_t kmax = zsplit == kZsExact ? uint32_t(kZsExactMaxK) : uint32_t(kZmMaxK);
+    return zsplit >= kZsTf32x3 && zsplit <= kZsExact && (width == 4 || width == 8) && !g.dyadic && g.lz >= 1 &&
+           g.nz <= kmax && (uint64_t(g.nx) * g.ny) % 4 == 0;
 }
 
 // ------------------------------------------------------------------ encode
@@ -891,8 +1016,9 @@ template <class T> struct CompressJob {
         }
         need(capacity >= 32 + wzp_header(uint32_t(n)), "Waltz: archive capacity too small");
         CompressJob j{d_in, nx, ny, nz, eb, d_out, capacity, opt, Geometry::make(nx, ny, nz), n};
-        need(!opt.matrix || matrix_form_ok(j.g, sizeof(T)),
-             "Waltz: the matrix form needs the plane schedule with 1 <= nz <= 128 and nx*ny a multiple of 4");
+        need(!opt.zsplit || matrix_form_ok(j.g, sizeof(T), opt.zsplit),
+             "Waltz: the matrix form needs the plane schedule with 1 <= nz <= 128 (96 for the exact slices) and nx*ny "
+             "a multiple of 4");
         return j;
     }
 
@@ -946,7 +1072,7 @@ template <class T> struct CompressJob {
         if (!sink.rec) stage_clock().begin(sink.stream);
         // 1. forward transform
         sink.phase(PH_FORWARD);
-        forward<T>(g, in, P.C, P.lowA, P.lowB, P.inter, P.status, sink, opt.matrix);
+        forward<T>(g, in, P.C, P.lowA, P.lowB, P.inter, P.status, sink, opt.zsplit);
         // 2. quantisation + Morton reorder: a field made of whole bricks (2^k
         // samples each) is quantised inside the WZP encoder, chunk by chunk;
         // otherwise a separate pass writes the Morton-packed magnitudes and
@@ -987,7 +1113,7 @@ template <class T> struct CompressJob {
             T safe = T(eb * (1.0 - std::ldexp(1.0, -21)));
             if (double(safe) > eb * (1.0 - std::ldexp(1.0, -21))) safe = std::nextafter(safe, T(0));
             RepairOut<T> fin{in, nx, size_t(nx) * ny, eb, T(eb), P.pbits, P.perr, P.status, safe};
-            inverse<T>(g, P.C, P.inter, P.bank2, fin, P.status, sink, "inv_l0_repair", opt.matrix);
+            inverse<T>(g, P.C, P.inter, P.bank2, fin, P.status, sink, "inv_l0_repair", opt.zsplit);
         }
         // 5. ordered side records
         sink.phase(PH_SIDE);
@@ -997,7 +1123,7 @@ template <class T> struct CompressJob {
                                  both);
         sink.run<ScanLayoutOp>(ScanLayoutOp::Params{P.counts_p, P.counts_q, uint32_t(cblocks), P.wzp_total, P.status,
                                                     out, capacity, uint32_t(sizeof(T)),
-                                                    uint8_t(g.flags(sizeof(T)) | (opt.matrix ? kMatrixFlag : 0)),
+                                                    uint8_t(g.flags(sizeof(T)) | split_flags(opt.zsplit)),
                                                     uint8_t(g.lxy), uint8_t(g.lz), uint8_t(g.bz), quantum, layout},
                                1);
         sink.run<CompactWriteOp<T>>(typename CompactWriteOp<T>::Params{P.pbits, P.qbits, words, P.counts_p,
@@ -1083,8 +1209,10 @@ template <class T>
 static Layout validate_header(const Header& h, const Geometry& g, size_t bytes, bool canonical) {
     const uint64_t n = g.n;
     need(bytes >= 32, "invalid Waltz archive header");
-    need(!(h.flags & 0xa0) && (h.flags & 0x18) && ((h.flags & 4) ? 8u : 4u) == sizeof(T), "invalid Waltz archive header");
-    need(!(h.flags & kMatrixFlag) || matrix_form_ok(g, sizeof(T)), "invalid Waltz archive header");
+    const int zsplit = split_of_flags(h.flags);
+    need((zsplit || !(h.flags & 0xa0)) && (h.flags & 0x18) && ((h.flags & 4) ? 8u : 4u) == sizeof(T),
+         "invalid Waltz archive header");
+    need(!zsplit || matrix_form_ok(g, sizeof(T), zsplit), "invalid Waltz archive header");
     need(((h.flags >> 3) & 3) == 3, "unsupported Waltz synthesis mode");
     need(!(h.flags & 2), "compact repair archives are not supported by this decoder");
     const bool dyadic = h.flags & 1;
@@ -1203,7 +1331,7 @@ static DecodeJob decode_job(const uint8_t* d_in, const Header& h, const Layout& 
 // `job.ptr` set (graph capture) the side-record kernels are always launched
 // on a fixed grid, as the counts are only known on the device.
 template <class T, class Final, class Patch>
-static void decode_launch(const JobRef& job, bool matrix, const Geometry& g, const uint16_t* irank,
+static void decode_launch(const JobRef& job, int zsplit, const Geometry& g, const uint16_t* irank,
                           const uint16_t* frank, T* C, T* bank1,
                           T* bank2, const Final& fin, const Patch& patch, uint32_t* status, Sink& sink) {
     const uint32_t n = uint32_t(g.n);
@@ -1230,7 +1358,7 @@ static void decode_launch(const JobRef& job, bool matrix, const Geometry& g, con
     }
     sink.mark("qpatch");
     sink.phase(PH_DINVERSE);
-    inverse<T>(g, C, bank1, bank2, fin, status, sink, "inv_l0", matrix);
+    inverse<T>(g, C, bank1, bank2, fin, status, sink, "inv_l0", zsplit);
     if (job.ptr || job.val.np) {
         sink.phase(PH_RPATCH);
         sink.run<RPatchOp<T, Patch>>(typename RPatchOp<T, Patch>::Params{job, g.n, patch, status},
@@ -1324,7 +1452,7 @@ static void decompress(const uint8_t* d_in, size_t bytes, uint32_t nx, uint32_t 
     check(cudaMemsetAsync(P.status, 0, 4, stream), "memset");
     FinalOut<T> fin{d_out, nx, size_t(nx) * ny, P.status};
     Sink sink{stream};
-    decode_launch<T>(JobRef{nullptr, decode_job(d_in, h, L)}, (h.flags & kMatrixFlag) != 0, g, irank, frank, P.C, P.bank1,
+    decode_launch<T>(JobRef{nullptr, decode_job(d_in, h, L)}, split_of_flags(h.flags), g, irank, frank, P.C, P.bank1,
                      P.bank2, fin, RowPatch<T>{d_out}, P.status, sink);
     check(cudaMemcpyAsync(pin + 8, P.status, 4, cudaMemcpyDeviceToHost, stream), "readback");
     check(cudaStreamSynchronize(stream), "decompress");
@@ -1759,7 +1887,7 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
         append_key(key, items[i].nz);
         append_key(key, list[i].sy);
         append_key(key, list[i].sz);
-        key.push_back(list[i].h.flags & kMatrixFlag);
+        key.push_back(split_of_flags(list[i].h.flags));
     }
     if (!st.graph.valid(key)) {
         std::vector<const uint16_t*> irank(count), frank(count);
@@ -1767,7 +1895,7 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
             const Geometry& g = list[i].g;
             irank[i] = st.tables.get(g.nx, g.ny, g.nz, g.bz, true, bs.cap);
             frank[i] = st.tables.get(g.nx, g.ny, g.nz, g.bz, false, bs.cap);
-            if (list[i].h.flags & kMatrixFlag) t_zmat.get(g.nz, true, false, bs.cap); // upload before capture
+            if (split_of_flags(list[i].h.flags)) t_zmat.get(g.nz, split_of_flags(list[i].h.flags), bs.cap); // upload before capture
         }
         auto enqueue = [&](uint32_t i, Sink& sink) {
             const uint32_t k = lane_of(i);
@@ -1775,7 +1903,7 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
             const DecodeJob* job = P.jobs + i;
             JobOut<T> fin{job, list[i].sy, list[i].sz, P.status + i};
             JobPatch<T> patch{job, g.nx, g.ny, list[i].sy, list[i].sz};
-            decode_launch<T>(JobRef{job, {}}, (list[i].h.flags & kMatrixFlag) != 0, g, irank[i], frank[i], P.C[k], P.b1[k],
+            decode_launch<T>(JobRef{job, {}}, split_of_flags(list[i].h.flags), g, irank[i], frank[i], P.C[k], P.b1[k],
                              P.b2[k], fin, patch, P.status + i, sink);
         };
         if (staged) {
@@ -1846,9 +1974,9 @@ int waltz_b200_compress_form(const void* d_input, int width, uint32_t nx, uint32
         need(written != nullptr, "null argument");
         *written = 0;
         need(width == 4 || width == 8, "type must be FP32 or FP64");
-        need(form == WALTZ_B200_FORM_PLAIN || form == WALTZ_B200_FORM_MATRIX, "unknown transform form");
+        need(form >= WALTZ_B200_FORM_PLAIN && form <= WALTZ_B200_FORM_MATRIX_EXACT, "unknown transform form");
         EncodeOptions opt;
-        opt.matrix = form == WALTZ_B200_FORM_MATRIX;
+        opt.zsplit = form; // the form values are the split codes
         auto s = reinterpret_cast<cudaStream_t>(stream);
         auto* out = static_cast<uint8_t*>(d_archive);
         *written = width == 4
@@ -2148,8 +2276,9 @@ extern "C" int waltz_b200_wzp_encode_noalloc(const uint16_t* d_mag, const uint32
 
 // Diagnostic entries of the tensor-core Z transform (declared in include/waltz_b200.h).
 template <class T>
-static void zmatrix_in_place(T* d_data, uint32_t nx, uint32_t ny, uint32_t nz, int inverse, void* stream) {
+static void zmatrix_in_place(T* d_data, uint32_t nx, uint32_t ny, uint32_t nz, int inverse, int zsplit, void* stream) {
     need(d_data && nx && ny && nz, "invalid matrix transform arguments");
+    need(zsplit >= kZsTf32x3 && zsplit <= kZsExact, "unknown matrix split form");
     auto s = reinterpret_cast<cudaStream_t>(stream);
     const uint64_t n = uint64_t(nx) * ny * nz;
     Carver cv{nullptr};
@@ -2164,7 +2293,7 @@ static void zmatrix_in_place(T* d_data, uint32_t nx, uint32_t ny, uint32_t nz, i
     auto P = plan(real);
     check(cudaMemsetAsync(P.status, 0, 4, s), "memset");
     Sink sink{s};
-    zmatrix_apply<T>(d_data, nx, ny, nz, inverse != 0, ZmStore<T>{P.out}, P.status, false, sink);
+    zmatrix_apply<T>(d_data, nx, ny, nz, inverse != 0, zsplit, ZmStore<T>{P.out}, P.status, false, sink);
     check(cudaMemcpyAsync(d_data, P.out, n * sizeof(T), cudaMemcpyDeviceToDevice, s), "copy");
     uint32_t st = 0;
     check(cudaMemcpyAsync(&st, P.status, 4, cudaMemcpyDeviceToHost, s), "readback");
@@ -2174,7 +2303,7 @@ static void zmatrix_in_place(T* d_data, uint32_t nx, uint32_t ny, uint32_t nz, i
 
 extern "C" int waltz_b200_zmatrix(float* d_data, uint32_t nx, uint32_t ny, uint32_t nz, int inverse, void* stream) {
     try {
-        zmatrix_in_place<float>(d_data, nx, ny, nz, inverse, stream);
+        zmatrix_in_place<float>(d_data, nx, ny, nz, inverse, kZsTf32x3, stream);
         return 0;
     } catch (const std::exception& e) {
         return fail(e);
@@ -2184,7 +2313,20 @@ extern "C" int waltz_b200_zmatrix(float* d_data, uint32_t nx, uint32_t ny, uint3
 extern "C" int waltz_b200_zmatrix_f64(double* d_data, uint32_t nx, uint32_t ny, uint32_t nz, int inverse,
                                       void* stream) {
     try {
-        zmatrix_in_place<double>(d_data, nx, ny, nz, inverse, stream);
+        zmatrix_in_place<double>(d_data, nx, ny, nz, inverse, kZsTf32x3, stream);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+extern "C" int waltz_b200_zmatrix_split(void* d_data, int width, uint32_t nx, uint32_t ny, uint32_t nz, int inverse,
+                                        int form, void* stream) {
+    try {
+        need(width == 4 || width == 8, "type must be FP32 or FP64");
+        need(form >= WALTZ_B200_FORM_MATRIX && form <= WALTZ_B200_FORM_MATRIX_EXACT, "unknown matrix form");
+        if (width == 4) zmatrix_in_place<float>(static_cast<float*>(d_data), nx, ny, nz, inverse, form, stream);
+        else zmatrix_in_place<double>(static_cast<double*>(d_data), nx, ny, nz, inverse, form, stream);
         return 0;
     } catch (const std::exception& e) {
         return fail(e);
