@@ -431,10 +431,15 @@ def bound_entry(lib, field, eb, steps, hbm, host_field=None):
     return entry
 
 
+# the precision form's tensor-core splits (WALTZ_B200_FORM_MATRIX*)
+SPLIT_FORMS = (("matrix_tf32x3", 1), ("matrix_bf16x3", 2), ("matrix_exact", 3))
+
+
 def _form_entries(dev, lib, f, eb, steps, ref_gpu):
-    """Plain lifting and the precision form on one device-resident field at
-    one absolute bound: compress / decompress GB/s (median of `steps` after
-    one warm-up), ratio, repair records, worst error; beside them the
+    """Plain lifting and every split of the precision form on one
+    device-resident field at one absolute bound: compress / decompress GB/s
+    (median of `steps` after one warm-up), ratio, repair records, worst error,
+    and each split's ratio change against the plain form; beside them the
     reference's own CUDA library (the plain form's bytes)."""
     import torch
     import waltz_b200
@@ -450,7 +455,7 @@ def _form_entries(dev, lib, f, eb, steps, ref_gpu):
     written = C.c_size_t()
     entry = {}
     plain_arch = None
-    for form, code in (("plain", 0), ("matrix", 1)):
+    for form, code in (("plain", 0),) + SPLIT_FORMS:
         def comp():
             _lib.checked(lib.waltz_b200_compress_form(C.c_void_p(f.data_ptr()), width, nx, ny, nz, eb, code,
                                                       C.c_void_p(arch.data_ptr()), cap, C.byref(written), sp))
@@ -486,9 +491,10 @@ def _form_entries(dev, lib, f, eb, steps, ref_gpu):
                        "max_abs_error": err, "abs_bound": eb}
         if form == "plain":
             plain_arch = arch[:size].clone()
-    if "compression_ratio" in entry["matrix"] and "compression_ratio" in entry["plain"]:
-        entry["ratio_change"] = round(entry["matrix"]["compression_ratio"] / entry["plain"]["compression_ratio"] - 1,
-                                      5)
+    if "compression_ratio" in entry["plain"]:
+        entry["ratio_change"] = {form: round(entry[form]["compression_ratio"] / entry["plain"]["compression_ratio"] - 1,
+                                             5)
+                                 for form, _ in SPLIT_FORMS if "compression_ratio" in entry[form]}
     if ref_gpu and plain_arch is not None:
         entry["reference_gpu"] = gpu_baseline(f, eb, plain_arch, max(1, steps))
     del plain_arch, arch, out
@@ -496,9 +502,9 @@ def _form_entries(dev, lib, f, eb, steps, ref_gpu):
 
 
 def _z_coefficient_error(dev, lib, f):
-    """Largest error of the tensor-core Z stage against the float64 lifting on
-    up to 16384 columns of the field (absolute, and relative to the largest
-    coefficient of each column)."""
+    """Largest error of the tensor-core Z stage, in every split, against the
+    float64 lifting on up to 16384 columns of the field (absolute, and
+    relative to the largest coefficient of each column)."""
     import torch
     from waltz_b200 import _lib
     nz, ny, nx = f.shape
@@ -512,18 +518,23 @@ def _z_coefficient_error(dev, lib, f):
         _lib.checked(lib.waltz_b200_transform(C.c_void_p(e.data_ptr()), 8, 1, 1, nz, 0, sp))
         m[:, k] = e.reshape(nz)
     ref = m @ x.double()
-    tcx = x.clone()
-    entry = lib.waltz_b200_zmatrix if f.element_size() == 4 else lib.waltz_b200_zmatrix_f64
-    _lib.checked(entry(C.c_void_p(tcx.data_ptr()), cols, 1, nz, 0, sp))
-    diff = (tcx.double() - ref).abs()
-    return {"max_abs": float(diff.max()),
-            "max_rel_to_column_max": float((diff.max(0).values / ref.abs().max(0).values.clamp_min(1e-30)).max()),
-            "columns": cols}
+    report = {"columns": cols}
+    for form, code in SPLIT_FORMS:
+        tcx = x.clone()
+        rc = lib.waltz_b200_zmatrix_split(C.c_void_p(tcx.data_ptr()), f.element_size(), cols, 1, nz, 0, code, sp)
+        if rc != 0:
+            report[form] = {"error": _lib.last_error()}
+            continue
+        diff = (tcx.double() - ref).abs()
+        report[form] = {"max_abs": float(diff.max()),
+                        "max_rel_to_column_max": float((diff.max(0).values /
+                                                        ref.abs().max(0).values.clamp_min(1e-30)).max())}
+    return report
 
 
 def tc_form_comparison(dev, lib, steps, shape=(64, 1024, 1024), ref_gpu=True):
-    """Plain lifting against the precision form (tensor-core Z stage) on the
-    tensor-core configuration: float32 1024x1024x64 (z=64) k^-11/3 random field
+    """Plain lifting against every split of the precision form (tensor-core Z
+    stage) on the tensor-core configuration: float32 1024x1024x64 (z=64) k^-11/3 random field
     (seed 3) with 1 % salt spikes of magnitude 50, REL 1e-3 and 1e-5; device
     resident, CUDA events, median of `steps` after one warm-up; beside them the
     reference's own CUDA library (its default profile, the plain form's bytes)
@@ -547,7 +558,8 @@ def tc_form_comparison(dev, lib, steps, shape=(64, 1024, 1024), ref_gpu=True):
 def tc_form_f64(dev, lib, steps, shape=(96, 256, 384), ref_gpu=True):
     """The same comparison on the double configuration: float64 384x256x96
     (z=96) k^-5/3 random field (seed 2) plus a front 10*tanh((z-48)/2) along
-    z, ABS 1e-4, 1e-5 and 1e-6. The precision form's Z stage is fp32-accurate; its
+    z, ABS 1e-4, 1e-5 and 1e-6, every split of the precision form: TF32x3 and
+    BF16x3 are fp32-accurate, the exact bf16 slices double-accurate; the
     quantisation and repair decisions stay in double, and the repair pass
     restores the bound."""
     import torch

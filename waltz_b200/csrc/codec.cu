@@ -758,42 +758,49 @@ static double host_bf16_value(uint16_t h) {
     return f;
 }
 
-// bf16 slices of a matrix in the K-major no-swizzle core layout of
-// zmatrix_slices_kernel (core (n/8, k/8) at ((n/8) * kp/8 + k/8) * 64
-// elements, element (n%8, k%8) at (n%8) * 8 + k%8), slice after slice.
-// BF16x3: m = b0 + b1 + b2 (+ residual), each bf16 of the remaining residual.
-// Exact: row n scaled by 2^-f_n (|m| < 2^f_n over the row) and cut into
-// 7-bit integer slices; scale[n] = 2^(f_n - 14), the epilogue's row factor.
-static void pack_bf16_slices(const std::vector<double>& m, uint32_t nz, bool exact, std::vector<uint16_t>& out,
-                             std::vector<double>& scale) {
-    const uint32_t S = exact ? kZsExactSlices : 3;
-    const ZsPlan P = ZsPlan::make(nz, S);
+// Slices of a matrix in the K-major no-swizzle core layouts of the slice
+// kernels, slice after slice.
+// BF16x3 (zmatrix_bf16_kernel): m = b0 + b1 + b2 (+ residual), each the bf16
+//   of the remaining residual; core (n/8, k/8) at ((n/8) * kp/8 + k/8) * 64
+//   elements, element (n%8, k%8) at (n%8) * 8 + k%8.
+// Exact (zmatrix_exact_kernel): row n scaled by 2^-(f_n+1) (|m| < 2^f_n over
+//   the row) and cut into five 7-bit integer slices (int8, |a| <= 64); core
+//   (n/8, k/16) at ((n/8) * kp/16 + k/16) * 128 bytes, element (n%8, k%16) at
+//   (n%8) * 16 + k%16; scale[n] = 2^(f_n + 1 - 14), the epilogue's row factor.
+static void pack_bf16_slices(const std::vector<double>& m, uint32_t nz, std::vector<uint16_t>& out) {
+    const ZsPlan P = ZsPlan::make(nz, false);
     const size_t per = size_t(P.np) * P.kp;
-    out.assign(S * per, 0);
+    out.assign(P.S * per, 0);
+    for (uint32_t n = 0; n < P.np; ++n)
+        for (uint32_t k = 0; k < P.kp; ++k) {
+            const size_t at = (size_t(n / 8) * (P.kp / 8) + k / 8) * 64 + (n % 8) * 8 + (k % 8);
+            double r = (n < nz && k < nz) ? m[size_t(n) * nz + k] : 0.0;
+            for (uint32_t sl = 0; sl < P.S; ++sl) {
+                const uint16_t h = host_bf16(r);
+                out[sl * per + at] = h;
+                r -= host_bf16_value(h);
+            }
+        }
+}
+static void pack_exact_slices(const std::vector<double>& m, uint32_t nz, std::vector<int8_t>& out,
+                              std::vector<double>& scale) {
+    const ZsPlan P = ZsPlan::make(nz, true);
+    const size_t per = size_t(P.np) * P.kp;
+    out.assign(P.S * per, 0);
     scale.assign(P.np, 0.0);
-    for (uint32_t n = 0; n < P.np; ++n) {
+    for (uint32_t n = 0; n < nz; ++n) {
         double rmax = 0.0;
-        for (uint32_t k = 0; k < nz && n < nz; ++k) rmax = std::max(rmax, std::fabs(m[size_t(n) * nz + k]));
+        for (uint32_t k = 0; k < nz; ++k) rmax = std::max(rmax, std::fabs(m[size_t(n) * nz + k]));
         int f = 0;
         if (rmax > 0) std::frexp(rmax, &f); // rmax < 2^f
-        scale[n] = n < nz ? std::ldexp(1.0, f - 14) : 0.0;
-        for (uint32_t k = 0; k < P.kp; ++k) {
-            const double v = (n < nz && k < nz) ? m[size_t(n) * nz + k] : 0.0;
-            const size_t at = (size_t(n / 8) * (P.kp / 8) + k / 8) * 64 + (n % 8) * 8 + (k % 8);
-            if (exact) {
-                double u = std::ldexp(v, -f);
-                for (uint32_t sl = 0; sl < S; ++sl) {
-                    const double a = std::nearbyint(u * 128.0);
-                    u = u * 128.0 - a;
-                    out[sl * per + at] = host_bf16(a);
-                }
-            } else {
-                double r = v;
-                for (uint32_t sl = 0; sl < S; ++sl) {
-                    const uint16_t h = host_bf16(r);
-                    out[sl * per + at] = h;
-                    r -= host_bf16_value(h);
-                }
+        scale[n] = std::ldexp(1.0, f + 1 - 14);
+        for (uint32_t k = 0; k < nz; ++k) {
+            const size_t at = (size_t(n / 8) * (P.kp / 16) + k / 16) * 128 + (n % 8) * 16 + (k % 16);
+            double u = std::ldexp(m[size_t(n) * nz + k], -(f + 1));
+            for (uint32_t sl = 0; sl < P.S; ++sl) {
+                const double a = std::nearbyint(u * 128.0);
+                u = u * 128.0 - a;
+                out[sl * per + at] = int8_t(a);
             }
         }
     }
@@ -841,11 +848,15 @@ struct ZMatrixCache {
                 pack_tf32_halves(mat, n, hi, lo);
                 hi.insert(hi.end(), lo.begin(), lo.end());
                 e.off[inv][0] = append(hi.data(), hi.size() * 4);
-            } else {
+            } else if (split == kZsBf16x3) {
                 std::vector<uint16_t> sl;
-                std::vector<double> sc;
-                pack_bf16_slices(mat, n, split == kZsExact, sl, sc);
+                pack_bf16_slices(mat, n, sl);
                 e.off[inv][0] = append(sl.data(), sl.size() * 2);
+            } else {
+                std::vector<int8_t> sl;
+                std::vector<double> sc;
+                pack_exact_slices(mat, n, sl, sc);
+                e.off[inv][0] = append(sl.data(), sl.size());
                 e.off[inv][1] = append(sc.data(), sc.size() * 8);
             }
         }
@@ -913,19 +924,21 @@ static void zmatrix_apply(const T* x, uint32_t nx, uint32_t ny, uint32_t nz, boo
     }
     const bool exact = zsplit == kZsExact;
     need(zsplit == kZsBf16x3 || exact, "Waltz: unknown matrix split form");
-    const ZsPlan P = ZsPlan::make(nz, exact ? kZsExactSlices : 3);
-    const uint16_t* bsl = reinterpret_cast<const uint16_t*>(base + e.off[dir][0]);
+    const ZsPlan P = ZsPlan::make(nz, exact);
+    const unsigned char* bsl = base + e.off[dir][0];
     const double* bscale = reinterpret_cast<const double*>(base + e.off[dir][1]);
     sink.direct([=](cudaStream_t stream) {
         unsigned grid = 0;
         if (exact) {
-            auto kernel = zmatrix_slices_kernel<T, Out, true>;
-            zmatrix_launch(kernel, P.smem(), ZsPlan::make(kZsExactMaxK, kZsExactSlices).smem(), ncols, stream, grid);
-            kernel<<<grid, kZmThreads, P.smem(), stream>>>(x, bsl, bscale, nz, ncols, out, status, cf);
+            auto kernel = zmatrix_exact_kernel<T, Out>;
+            zmatrix_launch(kernel, P.smem(), ZsPlan::make(kZsExactMaxK, true).smem(), ncols, stream, grid);
+            kernel<<<grid, kZmThreads, P.smem(), stream>>>(x, reinterpret_cast<const int8_t*>(bsl), bscale, nz, ncols,
+                                                           out, status, cf);
         } else {
-            auto kernel = zmatrix_slices_kernel<T, Out, false>;
-            zmatrix_launch(kernel, P.smem(), ZsPlan::make(kZmMaxK, 3).smem(), ncols, stream, grid);
-            kernel<<<grid, kZmThreads, P.smem(), stream>>>(x, bsl, bscale, nz, ncols, out, status, cf);
+            auto kernel = zmatrix_bf16_kernel<T, Out>;
+            zmatrix_launch(kernel, P.smem(), ZsPlan::make(kZmMaxK, false).smem(), ncols, stream, grid);
+            kernel<<<grid, kZmThreads, P.smem(), stream>>>(x, reinterpret_cast<const uint16_t*>(bsl), nz, ncols, out,
+                                                           status, cf);
         }
         note_launch();
         check(cudaGetLastError(), "matrix kernel launch");

@@ -281,61 +281,80 @@ __global__ void __launch_bounds__(kZmThreads, 2)
 
 
 // ---------------------------------------------------------------------------
-// BF16 slice forms (tcgen05.mma kind::f16, bf16 operands, fp32 accumulation
-// in tensor memory), same GEMM D = X^T * Mz^T, same tiling and epilogue:
-//   * BF16x3: every value is split into three bf16 slices (x = b0 + b1 + b2
-//     + r with |r| ~ 2^-24 |x|: b0 = bf16(x), b1 = bf16(x - b0),
-//     b2 = bf16(x - b0 - b1), each residual exact in fp32) and the six
-//     slice products of order <= 2 accumulate into one fp32 tile;
-//   * exact slices (double fields, nz <= 96): every field column c is scaled
-//     by 2^-e_c (|x| < 2^e_c over the column) and every matrix row n by
-//     2^-f_n, then cut into five 7-bit integer slices (u = sum_s a_s 2^-7(s+1),
-//     |a_s| <= 128, exact in bf16). A product of two slices summed over
-//     K <= 96 planes is an integer below 2^21 and the at most five products
-//     of one order d = s + t below 2^24, so each order accumulates EXACTLY in
-//     its own fp32 tile; the epilogue recombines the five tiles in double
-//     (Horner in 2^-7, exact) and scales by 2^(e_c + f_n - 14). The result is
-//     the exact sum of every slice product of order <= 4: a truncation error
-//     near 2^-35 of (column max x row max x K), far below fp32 rounding.
-// Operands are K-major without swizzle: core matrices of 8 rows x 16 bytes
-// (8 bf16 along K), cores 128 B apart along K (LBO), 8-row groups kc/8
-// (A) or kp/8 (B) cores apart (SBO); one MMA (K = 16) is two cores.
+// Slice forms, same GEMM D = X^T * Mz^T, same tiling and epilogue layout.
+//
+// BF16x3 (tcgen05.mma kind::f16, bf16 operands, fp32 accumulation): every
+// value is split into three bf16 slices (x = b0 + b1 + b2 + r with
+// |r| ~ 2^-24 |x|: b0 = bf16(x), b1 = bf16(x - b0), b2 = bf16(x - b0 - b1),
+// each residual exact in fp32) and the six slice products of order <= 2
+// accumulate into one fp32 tile. Operands K-major without swizzle: core
+// matrices of 8 rows x 16 bytes (8 bf16 along K), cores 128 B apart along K
+// (LBO), 8-row groups kc/8 (A) or kp/8 (B) cores apart (SBO); one MMA
+// (K = 16) is two cores.
+//
+// Exact slices (tcgen05.mma kind::i8, signed 8-bit operands, s32
+// accumulation; double fields, nz <= 96): every field column c is scaled by
+// 2^-(e_c+1) (|x| < 2^e_c over the column) and every matrix row n by
+// 2^-(f_n+1), so all values lie in (-1/2, 1/2), then cut into five 7-bit
+// integer slices u = sum_s a_s 2^-7(s+1) with |a_s| <= 64. Every product
+// order d = s + t accumulates exactly (integers) in its own s32 tile; the
+// epilogue recombines the five tiles in double (Horner in 2^-7, exact) and
+// scales by 2^(e_c + f_n + 2 - 14). The result is the exact sum of every
+// slice product of order <= 4: a truncation error near 2^-34 of (column max
+// x row max x K), far below fp32 rounding. One MMA (K = 32) is two cores of
+// 16 int8 along K; the int8 operands keep a CTA at 110 KB of shared memory
+// (two per SM).
 
 constexpr int kZsExactSlices = 5;
 constexpr int kZsExactMaxK = 96; // five accumulators of 96 columns fit the 512 TMEM columns
 
 struct ZsPlan {
     uint32_t S;       // slices per operand
-    uint32_t kp, np;  // K and N padded to multiples of 16
-    uint32_t kc;      // planes per A chunk (multiple of 16, <= 64)
-    uint32_t a_bytes; // one A slice: 128 x kc bf16
-    uint32_t b_bytes; // one B slice: np x kp bf16
-    __host__ __device__ static ZsPlan make(uint32_t nz, uint32_t slices) {
+    uint32_t eb;      // bytes per element: 2 (bf16) or 1 (int8)
+    uint32_t kp, np;  // K padded to the MMA K (16 or 32), N to a multiple of 16
+    uint32_t kc;      // planes per A chunk
+    uint32_t a_bytes; // one A slice: 128 x kc elements
+    uint32_t b_bytes; // one B slice: np x kp elements
+    __host__ __device__ static ZsPlan make(uint32_t nz, bool exact) {
         ZsPlan p;
-        p.S = slices;
-        p.kp = (nz + 15) / 16 * 16;
-        p.np = p.kp;
-        p.kc = p.kp < 64u ? p.kp : 64u;
-        p.a_bytes = 128 * p.kc * 2;
-        p.b_bytes = p.np * p.kp * 2;
+        p.S = exact ? uint32_t(kZsExactSlices) : 3u;
+        p.eb = exact ? 1u : 2u;
+        const uint32_t kstep = exact ? 32u : 16u;
+        p.kp = (nz + kstep - 1) / kstep * kstep;
+        p.np = (nz + 15) / 16 * 16;
+        // the exact form stages the whole column (nz <= 96) in one chunk
+        p.kc = exact ? p.kp : (p.kp < 64u ? p.kp : 64u);
+        p.a_bytes = 128 * p.kc * p.eb;
+        p.b_bytes = p.np * p.kp * p.eb;
         return p;
     }
     // A slices, B slices, 2 x 128 column maxima / exponents, barrier, TMEM slot
     __host__ __device__ uint32_t smem() const { return 1024 + S * (a_bytes + b_bytes) + 2 * 128 * 8 + 64; }
 };
 
-// Instruction descriptor of tcgen05.mma kind::f16: D f32, A and B bf16, both
-// K-major, M = 128, N = np.
-__host__ __device__ constexpr uint32_t zs_idesc(uint32_t np) {
+// Instruction descriptors: kind::f16 with D f32, A and B bf16; kind::i8 with
+// D s32, A and B signed 8-bit; both K-major, M = 128, N = np.
+__host__ __device__ constexpr uint32_t zs_idesc_bf16(uint32_t np) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((np >> 3) << 17) | ((128u >> 4) << 24);
 }
+__host__ __device__ constexpr uint32_t zs_idesc_s8(uint32_t np) {
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((np >> 3) << 17) | ((128u >> 4) << 24);
+}
 
-__device__ __forceinline__ void zs_mma(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                       uint32_t accumulate) {
+__device__ __forceinline__ void zs_mma_bf16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                            uint32_t accumulate) {
     const uint32_t mask = 0;
     asm volatile(
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(dtmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(mask), "r"(mask), "r"(mask), "r"(mask));
+}
+__device__ __forceinline__ void zs_mma_s8(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+    const uint32_t mask = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(dtmem),
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(mask), "r"(mask), "r"(mask), "r"(mask));
 }
 
@@ -345,25 +364,11 @@ __device__ __forceinline__ float bf16_value(uint16_t b) { return __bfloat162floa
 // 2^e as a double (normal range).
 __device__ __forceinline__ double pow2(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
 
-template <class T, class Out, bool Exact>
-__global__ void __launch_bounds__(kZmThreads, 1)
-    zmatrix_slices_kernel(const T* x, const uint16_t* bsl, const double* bscale, uint32_t nz, uint64_t ncols,
-                          Out out, uint32_t* status, uint32_t check_finite) {
-    constexpr int S = Exact ? kZsExactSlices : 3;
-    extern __shared__ __align__(1024) unsigned char zs_smem[];
-    const ZsPlan P = ZsPlan::make(nz, S);
-    unsigned char* base = zs_smem + ((1024 - (smem_u32(zs_smem) & 1023)) & 1023);
-    unsigned char* A = base;                        // S slices of a_bytes
-    unsigned char* B = A + S * P.a_bytes;           // S slices of b_bytes
-    double* cmax = reinterpret_cast<double*>(B + S * P.b_bytes); // [2][128] partial maxima
-    int* cexp = reinterpret_cast<int*>(cmax);        // [128] column exponents (after the maxima)
-    uint64_t* mma_bar = reinterpret_cast<uint64_t*>(cmax + 2 * 128);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_bar + 1);
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const uint64_t tiles = (ncols + kZmCols - 1) / kZmCols;
-    const uint32_t tcols = Exact ? 512u : (P.np <= 32 ? 32u : (P.np <= 64 ? 64u : 128u));
-
-    if (warp == 0) {
+// Common set-up of the slice kernels: TMEM allocation, mbarrier, operand B
+// copied into shared memory.
+__device__ __forceinline__ uint32_t zs_setup(unsigned char* B, const void* bsrc, uint32_t bbytes, uint64_t* mma_bar,
+                                             uint32_t* tmem_slot, uint32_t tcols, int tid) {
+    if ((tid >> 5) == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                      "r"(tcols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -372,14 +377,44 @@ __global__ void __launch_bounds__(kZmThreads, 1)
         mbar_init(mma_bar, 1);
         fence_barrier_init();
     }
-    for (uint32_t i = tid; i < S * P.b_bytes / 16; i += kZmThreads)
-        reinterpret_cast<uint4*>(B)[i] = reinterpret_cast<const uint4*>(bsl)[i];
+    for (uint32_t i = tid; i < bbytes / 16; i += kZmThreads)
+        reinterpret_cast<uint4*>(B)[i] = reinterpret_cast<const uint4*>(bsrc)[i];
     fence_proxy_async();
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const uint32_t tmem = *tmem_slot;
-    const uint32_t idesc = zs_idesc(P.np);
+    return *tmem_slot;
+}
+
+__device__ __forceinline__ void zs_teardown(uint32_t tmem, uint32_t tcols, bool bad, bool range_bad,
+                                            uint32_t check_finite, uint32_t* status, int tid) {
+    if (check_finite && __syncthreads_or(bad) && tid == 0) atomicOr(status, ST_NONFINITE_INPUT);
+    if (check_finite && __syncthreads_or(range_bad) && tid == 0) atomicOr(status, ST_MATRIX_RANGE);
+    __syncthreads();
+    if ((tid >> 5) == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tcols));
+    }
+}
+
+// BF16x3. bsl: the three B slices of np x kp bf16 each, in the core layout.
+template <class T, class Out>
+__global__ void __launch_bounds__(kZmThreads, 2)
+    zmatrix_bf16_kernel(const T* x, const uint16_t* bsl, uint32_t nz, uint64_t ncols, Out out, uint32_t* status,
+                        uint32_t check_finite) {
+    constexpr int S = 3;
+    extern __shared__ __align__(1024) unsigned char zs_smem[];
+    const ZsPlan P = ZsPlan::make(nz, false);
+    unsigned char* base = zs_smem + ((1024 - (smem_u32(zs_smem) & 1023)) & 1023);
+    unsigned char* A = base;              // S slices of a_bytes
+    unsigned char* B = A + S * P.a_bytes; // S slices of b_bytes
+    uint64_t* mma_bar = reinterpret_cast<uint64_t*>(B + S * P.b_bytes + 2 * 128 * 8);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_bar + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint64_t tiles = (ncols + kZmCols - 1) / kZmCols;
+    const uint32_t tcols = P.np <= 32 ? 32u : (P.np <= 64 ? 64u : 128u);
+    const uint32_t tmem = zs_setup(B, bsl, S * P.b_bytes, mma_bar, tmem_slot, tcols, tid);
+    const uint32_t idesc = zs_idesc_bf16(P.np);
     const uint32_t sbo_b = (P.kp / 8) * 128;
 
     uint32_t phase = 0;
@@ -389,62 +424,38 @@ __global__ void __launch_bounds__(kZmThreads, 1)
         const uint64_t col = tile * kZmCols + c;
         const bool live = col < ncols;
         const T* xcol = x + col;
-        double scale = 1.0; // 2^-e_c (exact form)
-        if constexpr (Exact) {
-            // column maxima: the two threads of a column take alternate planes
-            double m = 0.0;
-            if (live)
-                for (uint32_t k = half; k < nz; k += 2) {
-                    const double w = double(xcol[size_t(k) * ncols]);
-                    if (check_finite) bad |= !finite_bits(w);
-                    m = fmax(m, fabs(w));
-                }
-            cmax[half * 128 + c] = m;
-            __syncthreads();
-            const double amax = fmax(cmax[c], cmax[128 + c]);
-            // |x| < 2^e over the column; e clamped so that 2^-e and 2^e stay
-            // normal doubles (columns below 2^-1000 become zero, beyond 2^1000
-            // are refused)
-            int e = amax > 0.0 ? int((__double_as_longlong(amax) >> 52) & 0x7ff) - 1022 : -1000;
-            if (amax != amax || amax >= 0x1p1000) range_bad = true;
-            e = e < -1000 ? -1000 : (e > 1000 ? 1000 : e);
-            scale = pow2(-e);
-            __syncthreads();
-            if (half == 0) cexp[c] = e;
-        }
         for (uint32_t k0 = 0; k0 < P.kp; k0 += P.kc) {
             const uint32_t kc = min(P.kc, P.kp - k0);
             const uint32_t sbo_a = (kc / 8) * 128, kh = kc / 2;
+            // every plane this thread slices is loaded first (all loads in
+            // flight at once): planes half * kh .. half * kh + kh - 1 of the chunk
+            constexpr int MAXH = kZmChunk / 2;
+            T v[MAXH];
+#pragma unroll
+            for (int j = 0; j < MAXH; ++j) {
+                const uint32_t k = k0 + half * kh + j;
+                v[j] = (uint32_t(j) < kh && k < nz && live) ? xcol[size_t(k) * ncols] : T(0);
+            }
             // slice and transpose: element (c, kk) of slice s goes to core
             // (c/8, kk/8) of that slice, row c % 8, 2-byte column kk % 8
             unsigned char* row0 = A + (c / 8) * sbo_a + (c % 8) * 16;
-            for (uint32_t j = 0; j < kh; j += 8) {
+#pragma unroll
+            for (int j = 0; j < MAXH; j += 8) {
+                if (uint32_t(j) >= kh) break;
                 uint32_t pk[S][4];
 #pragma unroll
                 for (int q = 0; q < 8; ++q) {
-                    const uint32_t k = k0 + half * kh + j + q;
-                    T w = T(0);
-                    if (k < nz && live) w = xcol[size_t(k) * ncols];
-                    uint16_t sl[S];
-                    if constexpr (Exact) {
-                        double u = double(w) * scale;
-#pragma unroll
-                        for (int s2 = 0; s2 < S; ++s2) {
-                            const double a = rint(u * 128.0);
-                            u = u * 128.0 - a;
-                            sl[s2] = bf16_bits(float(a));
-                        }
-                    } else {
-                        if (check_finite) {
-                            bad |= !finite_bits(w);
-                            if constexpr (sizeof(T) == 8) range_bad |= finite_bits(w) && fabs(w) > double(FLT_MAX);
-                        }
-                        const float xf = float(w);
-                        sl[0] = bf16_bits(xf);
-                        const float r1 = __fsub_rn(xf, bf16_value(sl[0]));
-                        sl[1] = bf16_bits(r1);
-                        sl[2] = bf16_bits(__fsub_rn(r1, bf16_value(sl[1])));
+                    const T w = v[j + q];
+                    if (check_finite) {
+                        bad |= !finite_bits(w);
+                        if constexpr (sizeof(T) == 8) range_bad |= finite_bits(w) && fabs(w) > double(FLT_MAX);
                     }
+                    const float xf = float(w);
+                    uint16_t sl[S];
+                    sl[0] = bf16_bits(xf);
+                    const float r1 = __fsub_rn(xf, bf16_value(sl[0]));
+                    sl[1] = bf16_bits(r1);
+                    sl[2] = bf16_bits(__fsub_rn(r1, bf16_value(sl[1])));
 #pragma unroll
                     for (int s2 = 0; s2 < S; ++s2) {
                         if (q & 1) pk[s2][q >> 1] |= uint32_t(sl[s2]) << 16;
@@ -464,18 +475,15 @@ __global__ void __launch_bounds__(kZmThreads, 1)
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t a0 = smem_u32(A), b0 = smem_u32(B) + (k0 / 8) * 128;
                 for (uint32_t st = 0; st < kc / 16; ++st) {
-                    // products of order d = s + t: the exact form keeps each
-                    // order in its own accumulator, BF16x3 sums orders 0..2
+                    // the six slice products of order <= 2, one accumulator
 #pragma unroll
-                    for (int d = 0; d < (Exact ? S : 3); ++d) {
-                        const uint32_t dt = tmem + (Exact ? uint32_t(d) * P.np : 0u);
+                    for (int d = 0; d < 3; ++d) {
 #pragma unroll
                         for (int s2 = 0; s2 <= d; ++s2) {
-                            const int t2 = d - s2;
                             const uint64_t da = zm_sdesc(a0 + s2 * P.a_bytes + st * 256, 128, sbo_a, 0);
-                            const uint64_t db = zm_sdesc(b0 + t2 * P.b_bytes + st * 256, 128, sbo_b, 0);
-                            const bool first = k0 == 0 && st == 0 && s2 == 0 && (Exact || d == 0);
-                            zs_mma(dt, da, db, idesc, first ? 0u : 1u);
+                            const uint64_t db = zm_sdesc(b0 + (d - s2) * P.b_bytes + st * 256, 128, sbo_b, 0);
+                            const bool first = k0 == 0 && st == 0 && d == 0;
+                            zs_mma_bf16(tmem, da, db, idesc, first ? 0u : 1u);
                         }
                     }
                 }
@@ -491,44 +499,148 @@ __global__ void __launch_bounds__(kZmThreads, 1)
         if (stop) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t sub = warp % 4;
-        const uint32_t lc = 32 * sub + lane;
-        const uint64_t ocol = tile * kZmCols + lc;
+        const uint64_t ocol = tile * kZmCols + 32 * sub + lane;
         for (uint32_t c0 = 16 * (warp / 4); c0 < P.np; c0 += 32) {
             uint32_t r[16];
-            if constexpr (Exact) {
-                double v[16];
+            tmem_ld16(tmem + (uint32_t(32 * sub) << 16) + c0, r);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            float f[16];
 #pragma unroll
-                for (int d = S - 1; d >= 0; --d) {
-                    tmem_ld16(tmem + (uint32_t(32 * sub) << 16) + uint32_t(d) * P.np + c0, r);
-                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-                    for (int j = 0; j < 16; ++j)
-                        v[j] = d == S - 1 ? double(__uint_as_float(r[j]))
-                                          : fma(v[j], 0x1p-7, double(__uint_as_float(r[j])));
-                }
-                const double cs = pow2(cexp[lc]);
-#pragma unroll
-                for (int j = 0; j < 16; ++j) v[j] = v[j] * cs * (c0 + j < P.np ? bscale[c0 + j] : 0.0);
-                if (ocol < ncols) out.group(uint32_t(ocol), c0, nz, ncols, v);
-            } else {
-                tmem_ld16(tmem + (uint32_t(32 * sub) << 16) + c0, r);
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                float f[16];
-#pragma unroll
-                for (int j = 0; j < 16; ++j) f[j] = __uint_as_float(r[j]);
-                if (ocol < ncols) out.group(uint32_t(ocol), c0, nz, ncols, f);
-            }
+            for (int j = 0; j < 16; ++j) f[j] = __uint_as_float(r[j]);
+            if (ocol < ncols) out.group(uint32_t(ocol), c0, nz, ncols, f);
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads(); // tensor memory read out: the next tile's MMAs may overwrite it
     }
-    if (check_finite && __syncthreads_or(bad) && tid == 0) atomicOr(status, ST_NONFINITE_INPUT);
-    if (check_finite && __syncthreads_or(range_bad) && tid == 0) atomicOr(status, ST_MATRIX_RANGE);
-    __syncthreads();
-    if (warp == 0) {
+    zs_teardown(tmem, tcols, bad, range_bad, check_finite, status, tid);
+}
+
+// Exact slices. bsl: the five B slices of np x kp int8 each, in the core
+// layout (core (n/8, k/16) at ((n/8) * kp/16 + k/16) * 128 B, element
+// (n%8, k%16) at (n%8) * 16 + k%16); bscale[n] = 2^(f_n + 1 - 14).
+template <class T, class Out>
+__global__ void __launch_bounds__(kZmThreads, 2)
+    zmatrix_exact_kernel(const T* x, const int8_t* bsl, const double* bscale, uint32_t nz, uint64_t ncols, Out out,
+                         uint32_t* status, uint32_t check_finite) {
+    constexpr int S = kZsExactSlices;
+    extern __shared__ __align__(1024) unsigned char zs_smem[];
+    const ZsPlan P = ZsPlan::make(nz, true);
+    unsigned char* base = zs_smem + ((1024 - (smem_u32(zs_smem) & 1023)) & 1023);
+    unsigned char* A = base;              // S slices of a_bytes
+    unsigned char* B = A + S * P.a_bytes; // S slices of b_bytes
+    double* cmax = reinterpret_cast<double*>(B + S * P.b_bytes); // [2][128] partial maxima
+    int* cexp = reinterpret_cast<int*>(cmax);                     // [128] column exponents, after the maxima
+    uint64_t* mma_bar = reinterpret_cast<uint64_t*>(cmax + 2 * 128);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_bar + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint64_t tiles = (ncols + kZmCols - 1) / kZmCols;
+    const uint32_t tmem = zs_setup(B, bsl, S * P.b_bytes, mma_bar, tmem_slot, 512u, tid);
+    const uint32_t idesc = zs_idesc_s8(P.np);
+    const uint32_t kc = P.kp, kh = kc / 2;
+    const uint32_t sbo_a = (kc / 16) * 128, sbo_b = (P.kp / 16) * 128;
+
+    uint32_t phase = 0;
+    bool bad = false, range_bad = false;
+    for (uint64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int c = tid % kZmCols, half = tid / kZmCols;
+        const uint64_t col = tile * kZmCols + c;
+        const bool live = col < ncols;
+        const T* xcol = x + col;
+        // column maximum over both threads' planes (half * kh .. + kh - 1)
+        double m = 0.0;
+#pragma unroll 8
+        for (uint32_t j = 0; j < kh; ++j) {
+            const uint32_t k = half * kh + j;
+            const double w = (k < nz && live) ? double(xcol[size_t(k) * ncols]) : 0.0;
+            if (check_finite) bad |= !finite_bits(w);
+            m = fmax(m, fabs(w));
+        }
+        cmax[half * 128 + c] = m;
+        __syncthreads();
+        const double amax = fmax(cmax[c], cmax[128 + c]);
+        // |x| < 2^e over the column; e clamped so that the scalings stay
+        // normal doubles (columns below 2^-1000 become zero, beyond 2^1000
+        // are refused)
+        int e = amax > 0.0 ? int((__double_as_longlong(amax) >> 52) & 0x7ff) - 1022 : -1000;
+        if (amax >= 0x1p1000) range_bad = true;
+        e = e < -1000 ? -1000 : (e > 1000 ? 1000 : e);
+        const double scale = pow2(-(e + 1));
+        __syncthreads();
+        if (half == 0) cexp[c] = e;
+        // slice and transpose: element (c, kk) of slice s goes to core
+        // (c/8, kk/16) of that slice, row c % 8, byte kk % 16
+        unsigned char* row0 = A + (c / 8) * sbo_a + (c % 8) * 16;
+        for (uint32_t j = 0; j < kh; j += 16) {
+            uint32_t pk[S][4];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                const uint32_t k = half * kh + j + q;
+                const double w = (k < nz && live) ? double(xcol[size_t(k) * ncols]) : 0.0;
+                double u = w * scale;
+#pragma unroll
+                for (int s2 = 0; s2 < S; ++s2) {
+                    const double a = rint(u * 128.0);
+                    u = u * 128.0 - a;
+                    const uint32_t b = uint32_t(int32_t(a)) & 0xffu;
+                    if (q & 3) pk[s2][q >> 2] |= b << (8 * (q & 3));
+                    else pk[s2][q >> 2] = b;
+                }
+            }
+            const uint32_t kq = (half * kh + j) / 16;
+#pragma unroll
+            for (int s2 = 0; s2 < S; ++s2)
+                *reinterpret_cast<uint4*>(row0 + s2 * P.a_bytes + kq * 128) =
+                    make_uint4(pk[s2][0], pk[s2][1], pk[s2][2], pk[s2][3]);
+        }
+        fence_proxy_async();
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t a0 = smem_u32(A), b0 = smem_u32(B);
+            for (uint32_t st = 0; st < kc / 32; ++st) {
+                // products of order d = s + t, each order in its own accumulator
+#pragma unroll
+                for (int d = 0; d < S; ++d) {
+#pragma unroll
+                    for (int s2 = 0; s2 <= d; ++s2) {
+                        const uint64_t da = zm_sdesc(a0 + s2 * P.a_bytes + st * 256, 128, sbo_a, 0);
+                        const uint64_t db = zm_sdesc(b0 + (d - s2) * P.b_bytes + st * 256, 128, sbo_b, 0);
+                        zs_mma_s8(tmem + uint32_t(d) * P.np, da, db, idesc, (st == 0 && s2 == 0) ? 0u : 1u);
+                    }
+                }
+            }
+            zm_commit(mma_bar);
+        }
+        if (!__syncthreads_and(warp != 0 || mbar_wait(mma_bar, phase, kWaitBound))) {
+            if (tid == 0) atomicOr(status, ST_WAIT_TIMEOUT);
+            break;
+        }
+        phase ^= 1;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tcols));
+        const uint32_t sub = warp % 4;
+        const uint32_t lc = 32 * sub + lane;
+        const uint64_t ocol = tile * kZmCols + lc;
+        const double cs = pow2(cexp[lc] + 1);
+        for (uint32_t c0 = 16 * (warp / 4); c0 < P.np; c0 += 32) {
+            double v[16];
+#pragma unroll
+            for (int d = S - 1; d >= 0; --d) {
+                uint32_t r[16];
+                tmem_ld16(tmem + (uint32_t(32 * sub) << 16) + uint32_t(d) * P.np + c0, r);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                    v[j] = d == S - 1 ? double(int32_t(r[j])) : fma(v[j], 0x1p-7, double(int32_t(r[j])));
+            }
+#pragma unroll
+            for (int j = 0; j < 16; ++j) v[j] = v[j] * cs * (c0 + j < P.np ? bscale[c0 + j] : 0.0);
+            if (ocol < ncols) out.group(uint32_t(ocol), c0, nz, ncols, v);
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads(); // tensor memory read out: the next tile's MMAs may overwrite it
     }
+    zs_teardown(tmem, 512u, bad, range_bad, check_finite, status, tid);
 }
 
 } // namespace wb
