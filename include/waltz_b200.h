@@ -47,8 +47,9 @@ int waltz_b200_compress(const void* d_input, int width, uint32_t nx, uint32_t ny
  *                 (power-of-two scaled), every product order accumulated
  *                 exactly in its own FP32 tile and recombined in double:
  *                 about 2^-35 relative error, for double fields (nz <= 96).
- * Such archives set header flag bit 6 and record the form in bits 5 and 7,
- * which the reference's decoders reject. The matrix forms need the plane
+ * Such archives set header flag bit 6 (which the reference's decoders
+ * reject) and record the form in the two top bits of header byte 3, the z
+ * band (0 TF32x3, 1 BF16x3, 2 exact slices). The matrix forms need the plane
  * schedule (Z levels differ from XY levels) with 1 <= nz <= 128 (96 for
  * MATRIX_EXACT) and nx*ny a multiple of 4; float and double fields (TF32x3
  * and BF16x3 round double samples to float first; a double field's

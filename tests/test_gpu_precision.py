@@ -19,8 +19,8 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 SPLITS = {"matrix": 1, "matrix-bf16": 2, "matrix-exact": 3}
-# header flag bits of each form: bit 6, and the split code in bits 5 and 7
-FLAG_BITS = {"matrix": 0x40, "matrix-bf16": 0x60, "matrix-exact": 0xC0}
+# the split code of each form, in the top two bits of header byte 3 (the z band)
+BAND_CODE = {"matrix": 0, "matrix-bf16": 1, "matrix-exact": 2}
 
 
 def _lib():
@@ -98,16 +98,18 @@ def _spiky_field(shape):
 @pytest.mark.parametrize("shape,dtype,eb", [((64, 128, 128), np.float32, 1e-3), ((33, 24, 40), np.float32, 1e-5),
                                             ((96, 32, 48), np.float64, 1e-6), ((24, 64, 64), np.float64, 1e-4)])
 def test_split_form_round_trip(form, shape, dtype, eb):
-    """Each split form: header bit 6 with the split code in bits 5 and 7, the
-    reference decoder (the oracle) rejects the archive, the GPU decoder
-    restores every sample within the bound, twice identically."""
+    """Each split form: header flag bit 6, the split code in the top bits of
+    the z-band byte, the reference decoder (the oracle) rejects the archive,
+    the GPU decoder restores every sample within the bound, twice
+    identically."""
     import waltz_b200
     a = _spiky_field(shape) if dtype == np.float32 else _front_field(shape)
     if dtype == np.float32:
         eb = float(eb * (a.max() - a.min()))
     plain = waltz_b200.compress(a, abs_error=eb)
     arc = waltz_b200.compress(a, abs_error=eb, form=form)
-    assert arc[0] == plain[0] | FLAG_BITS[form]
+    assert arc[0] == plain[0] | 0x40
+    assert arc[3] == plain[3] | (BAND_CODE[form] << 6)
     with pytest.raises(Exception):
         O.decompress(arc, a.shape, dtype)
     out1 = waltz_b200.decompress(arc, shape=a.shape, dtype=dtype)
@@ -134,16 +136,18 @@ def test_exact_form_keeps_the_plain_ratio_on_double_fields():
 
 
 def test_undefined_split_code_rejected():
-    """Bits 5 and 7 mean nothing without bit 6, and bit 6 with both of them
-    set is an undefined split: the decoder refuses either archive."""
+    """Flag bits 5 and 7 are refused (bit 5 is the reference's CUDA fused
+    plane-Z profile), band bits 6-7 mean nothing without flag bit 6, and the
+    band code 3 is an undefined split: the decoder refuses each archive."""
     import waltz_b200
     a = _spiky_field((24, 64, 64))
     eb = float(1e-3 * (a.max() - a.min()))
     plain = bytearray(waltz_b200.compress(a, abs_error=eb))
     exact = bytearray(waltz_b200.compress(a, abs_error=eb, form="matrix-exact"))
-    for arc, flip in ((plain, 0x20), (plain, 0x80), (exact, 0x20)):
+    for arc, byte, flip in ((plain, 0, 0x20), (plain, 0, 0x80), (exact, 0, 0x20), (plain, 3, 0x40),
+                            (exact, 3, 0xc0)):
         bad = bytearray(arc)
-        bad[0] |= flip
+        bad[byte] |= flip
         with pytest.raises(waltz_b200.WaltzError):
             waltz_b200.decompress(bytes(bad), shape=a.shape, dtype=np.float32)
     # the exact form is refused above nz = 96, the other splits are not

@@ -965,21 +965,22 @@ struct EncodeOptions {
     int zsplit = kZsNone; // precision form: tensor-core Z transform in this split form (header flag bits)
 };
 
-// Header flag bit 6: the archive's Z stage is the tensor-core matrix form;
-// bits 5 and 7 then give its split form (0 TF32x3, 1 BF16x3, 2 exact bf16
-// slices). All three are reserved bits of the reference header
-// (include/utils/Blob.hpp:46-53), so the reference decoders reject such
-// archives and the default bytes stay.
+// Header flag bit 6 (reserved in the reference header,
+// include/utils/Blob.hpp:38-53, so the reference decoders reject such
+// archives and the default bytes stay): the archive's Z stage is the
+// tensor-core matrix form. Its split form (0 TF32x3, 1 BF16x3, 2 exact
+// slices) is then stored in the two top bits of header byte 3, the z band,
+// which needs six bits (1..32). Flag bit 5 keeps the reference's meaning (its
+// CUDA fused plane-Z profile, which this decoder does not take).
 constexpr uint8_t kMatrixFlag = 0x40;
-static uint8_t split_flags(int zsplit) {
-    if (!zsplit) return 0;
-    const unsigned code = unsigned(zsplit - 1);
-    return uint8_t(kMatrixFlag | ((code & 1u) << 5) | ((code >> 1) << 7));
+static uint8_t split_flags(int zsplit) { return zsplit ? kMatrixFlag : uint8_t(0); }
+static uint8_t split_band(int zsplit, uint32_t bz) {
+    return uint8_t(bz | (zsplit ? uint32_t(zsplit - 1) << 6 : 0u));
 }
 // Split form of an archive (kZsNone for lifting; 4 for the undefined code).
-static int split_of_flags(uint8_t flags) {
+static int split_of(uint8_t flags, uint8_t band) {
     if (!(flags & kMatrixFlag)) return kZsNone;
-    return 1 + int(((flags >> 5) & 1u) | ((flags >> 6) & 2u));
+    return 1 + int(band >> 6);
 }
 
 // Fields the matrix form serves: float or double, plane schedule with Z
@@ -1137,7 +1138,7 @@ template <class T> struct CompressJob {
         sink.run<ScanLayoutOp>(ScanLayoutOp::Params{P.counts_p, P.counts_q, uint32_t(cblocks), P.wzp_total, P.status,
                                                     out, capacity, uint32_t(sizeof(T)),
                                                     uint8_t(g.flags(sizeof(T)) | split_flags(opt.zsplit)),
-                                                    uint8_t(g.lxy), uint8_t(g.lz), uint8_t(g.bz), quantum, layout},
+                                                    uint8_t(g.lxy), uint8_t(g.lz), split_band(opt.zsplit, g.bz), quantum, layout},
                                1);
         sink.run<CompactWriteOp<T>>(typename CompactWriteOp<T>::Params{P.pbits, P.qbits, words, P.counts_p,
                                                                        P.counts_q, P.perr, P.qval, out, layout, n,
@@ -1187,6 +1188,7 @@ static size_t compress(const T* d_in, uint32_t nx, uint32_t ny, uint32_t nz, dou
 // ------------------------------------------------------------------ decode
 struct Header {
     uint8_t flags, lxy, lz, bz;
+    int split;
     uint32_t pwe_bytes;
     double q;
     uint64_t wzp;
@@ -1194,6 +1196,9 @@ struct Header {
     static Header parse(const uint8_t* p) {
         Header h;
         h.flags = p[0]; h.lxy = p[1]; h.lz = p[2]; h.bz = p[3];
+        // matrix-form archives keep their split code in the band's top bits
+        h.split = split_of(h.flags, h.bz);
+        if (h.split) h.bz &= 0x3f;
         std::memcpy(&h.pwe_bytes, p + 4, 4);
         std::memcpy(&h.q, p + 8, 8);
         std::memcpy(&h.wzp, p + 16, 8);
@@ -1222,8 +1227,8 @@ template <class T>
 static Layout validate_header(const Header& h, const Geometry& g, size_t bytes, bool canonical) {
     const uint64_t n = g.n;
     need(bytes >= 32, "invalid Waltz archive header");
-    const int zsplit = split_of_flags(h.flags);
-    need((zsplit || !(h.flags & 0xa0)) && (h.flags & 0x18) && ((h.flags & 4) ? 8u : 4u) == sizeof(T),
+    const int zsplit = h.split;
+    need(!(h.flags & 0xa0) && (h.flags & 0x18) && ((h.flags & 4) ? 8u : 4u) == sizeof(T),
          "invalid Waltz archive header");
     need(!zsplit || matrix_form_ok(g, sizeof(T), zsplit), "invalid Waltz archive header");
     need(((h.flags >> 3) & 3) == 3, "unsupported Waltz synthesis mode");
@@ -1465,7 +1470,7 @@ static void decompress(const uint8_t* d_in, size_t bytes, uint32_t nx, uint32_t 
     check(cudaMemsetAsync(P.status, 0, 4, stream), "memset");
     FinalOut<T> fin{d_out, nx, size_t(nx) * ny, P.status};
     Sink sink{stream};
-    decode_launch<T>(JobRef{nullptr, decode_job(d_in, h, L)}, split_of_flags(h.flags), g, irank, frank, P.C, P.bank1,
+    decode_launch<T>(JobRef{nullptr, decode_job(d_in, h, L)}, h.split, g, irank, frank, P.C, P.bank1,
                      P.bank2, fin, RowPatch<T>{d_out}, P.status, sink);
     check(cudaMemcpyAsync(pin + 8, P.status, 4, cudaMemcpyDeviceToHost, stream), "readback");
     check(cudaStreamSynchronize(stream), "decompress");
@@ -1900,7 +1905,7 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
         append_key(key, items[i].nz);
         append_key(key, list[i].sy);
         append_key(key, list[i].sz);
-        key.push_back(split_of_flags(list[i].h.flags));
+        key.push_back(list[i].h.split);
     }
     if (!st.graph.valid(key)) {
         std::vector<const uint16_t*> irank(count), frank(count);
@@ -1908,7 +1913,7 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
             const Geometry& g = list[i].g;
             irank[i] = st.tables.get(g.nx, g.ny, g.nz, g.bz, true, bs.cap);
             frank[i] = st.tables.get(g.nx, g.ny, g.nz, g.bz, false, bs.cap);
-            if (split_of_flags(list[i].h.flags)) t_zmat.get(g.nz, split_of_flags(list[i].h.flags), bs.cap); // upload before capture
+            if (list[i].h.split) t_zmat.get(g.nz, list[i].h.split, bs.cap); // upload before capture
         }
         auto enqueue = [&](uint32_t i, Sink& sink) {
             const uint32_t k = lane_of(i);
@@ -1916,7 +1921,7 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
             const DecodeJob* job = P.jobs + i;
             JobOut<T> fin{job, list[i].sy, list[i].sz, P.status + i};
             JobPatch<T> patch{job, g.nx, g.ny, list[i].sy, list[i].sz};
-            decode_launch<T>(JobRef{job, {}}, split_of_flags(list[i].h.flags), g, irank[i], frank[i], P.C[k], P.b1[k],
+            decode_launch<T>(JobRef{job, {}}, list[i].h.split, g, irank[i], frank[i], P.C[k], P.b1[k],
                              P.b2[k], fin, patch, P.status + i, sink);
         };
         if (staged) {
