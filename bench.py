@@ -845,17 +845,17 @@ def batch_only(dev, lib, args, count=512):
             "gbs": round(nbytes / (statistics.median(ms) / 1e3) / 1e9, 3)}
 
 
-# DRAM bytes (read + write) per launch of the finest-level kernels at f32
-# 512^3: dram__bytes_read.sum + dram__bytes_write.sum of the ncu capture of the
-# 256x384x384 case (profiles/kernels_f32_256x384x384_and_64x768x768_sections.md)
-# scaled by the sample ratio 512^3 / (256*384*384) = 3.5556; traffic grows in
-# proportion to the samples processed.
+# DRAM bytes (read + write) per launch of the finest-level kernels on this
+# workload (f32 512^3, REL 1e-3): dram__bytes_read.sum + dram__bytes_write.sum
+# of one ncu capture of each kernel's first launch at 512^3
+# (profiles/dram_traffic_f32_512cubed_rel1e-3.md). A run on another shape
+# reports no traffic.
 TRAFFIC_512 = {
-    "compress:fwd_l0": 1010748985,
-    "compress:wzp_encode": 974181717,
-    "compress:inv_l0_repair": 1288321252,
-    "decompress:wzp_decode": 453289756,
-    "decompress:inv_l0": 968155136,
+    "compress:fwd_l0": 1045993984,
+    "compress:wzp_encode": 1110756608,
+    "compress:inv_l0_repair": 1309071616,
+    "decompress:wzp_decode": 576808704,
+    "decompress:inv_l0": 1053336576,
 }
 
 
