@@ -128,6 +128,17 @@ int waltz_b200_decompress_batch(const waltz_b200_archive* archives, uint32_t cou
 #define WALTZ_B200_OPT_ZMARCH_PLANES 2
 #define WALTZ_B200_OPT_SMALL_LEVEL 3
 #define WALTZ_B200_OPT_SMALL_FWD 4
+/* WALTZ_B200_OPT_COMPACT_REPAIRS (0 default, 16 or 64): not a performance
+ *   knob but an opt-in archive profile, the reference's compact repair
+ *   section (WPW1, src/small_pwe.cuh:21-152; its CUDA library selects it with
+ *   WALTZ_SMALL_PWE_SCALE): the calling thread's later compressions store
+ *   their repair errors as int8 multiples of step = eb / value where that
+ *   provably keeps the sample within step of the original, in groups of 32,
+ *   when that section is smaller than the native errors (header flag bit 1).
+ *   Such archives decode with waltz_b200_decompress(_batch) and the reference
+ *   CPU decoder; the canonical decoders (waltz_cuda_decode_chunk,
+ *   waltz_gpu_decode_batch) refuse them, as the reference's do. */
+#define WALTZ_B200_OPT_COMPACT_REPAIRS 5
 int waltz_b200_set_option(int option, int value);
 
 #define WALTZ_B200_BATCH_STAGES 0

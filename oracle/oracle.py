@@ -71,6 +71,7 @@ def oracle_lib():
         "wo_max_compressed_bytes": (sz, [C.POINTER(WoConfig)]),
         "wo_compress": (C.c_int, [C.POINTER(WoConfig), p, p, sz, C.POINTER(sz), C.c_char_p, sz]),
         "wo_decompress": (C.c_int, [C.POINTER(WoConfig), p, sz, p, sz, C.c_char_p, sz]),
+        "wo_compact_repairs": (C.c_int, [p, sz, C.c_int, p, C.c_double, p, sz, C.POINTER(sz), C.c_char_p, sz]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -257,6 +258,20 @@ def decompress(archive: bytes, shape, dtype) -> np.ndarray:
     if oracle_lib().wo_decompress(C.byref(cfg), _ptr(src), len(archive), _ptr(out), out.nbytes, err, 256):
         raise CodecError(err.value.decode())
     return out
+
+
+def compact_repairs(archive: bytes, field: np.ndarray, step: float) -> bytes:
+    """The archive with its repair section in the compact WPW1 form (groups in
+    order, as the GPU encoder writes it) where that is smaller, else itself."""
+    a = np.ascontiguousarray(field)
+    src = np.frombuffer(archive, np.uint8).copy()
+    out = np.zeros(len(archive), np.uint8)
+    written = C.c_size_t()
+    err = C.create_string_buffer(256)
+    if oracle_lib().wo_compact_repairs(_ptr(src), len(archive), a.itemsize, _ptr(a), step, _ptr(out), out.size,
+                                       C.byref(written), err, 256):
+        raise CodecError(err.value.decode())
+    return out[:written.value].tobytes()
 
 
 # --------------------------------------------------------------- reference

@@ -8,6 +8,7 @@
  */
 #include "waltz_oracle.h"
 
+#include <fenv.h>
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -418,6 +419,32 @@ static int within_bound(double value, double original, double bound) {
     return !((diff > 0 && err > 0) || (diff < 0 && err < 0));
 }
 
+/* Compact repair section checks (cpu/src/codec.cpp:305-316): header,
+ * groups, step and every group's span inside the payload. */
+static int popc32(uint32_t v) { int c = 0; while (v) { v &= v - 1; ++c; } return c; }
+static int wpw_validate(const uint8_t* sec, size_t bytes, uint32_t np, size_t width, char* err, size_t errlen) {
+    const uint32_t groups = (np + 31) / 32;
+    const size_t prefix = 24 + 8 * (size_t)groups;
+    double step;
+    size_t payload;
+    uint32_t g;
+    if (bytes < prefix || get32(sec) != 0x31575057u || get32(sec + 4) != groups || get64(sec + 8) != bytes - prefix) {
+        say(err, errlen, "invalid WPW1 directory"); return -1;
+    }
+    payload = bytes - prefix;
+    { uint64_t u = get64(sec + 16); memcpy(&step, &u, 8); }
+    if (!(step > 0) || !isfinite(step)) { say(err, errlen, "invalid compact repair step"); return -1; }
+    for (g = 0; g < groups; ++g) {
+        const uint32_t off = get32(sec + 24 + 8 * (size_t)g), mask = get32(sec + 28 + 8 * (size_t)g);
+        const uint32_t count = np - g * 32 < 32 ? np - g * 32 : 32;
+        const size_t start = off & 0x7fffffffu;
+        const size_t span = (off >> 31) ? count * width : (count + width - 1) / width * width + (size_t)popc32(mask) * width;
+        if (count < 32 && (mask >> count)) { say(err, errlen, "invalid compact repair mask"); return -1; }
+        if (start % 8 || start > payload || span > payload - start) { say(err, errlen, "invalid compact repair group span"); return -1; }
+    }
+    return 0;
+}
+
 /* ------------------------------------------------------ typed codec parts */
 
 #define REAL float
@@ -497,4 +524,42 @@ int wo_decompress(const wo_config* c, const uint8_t* archive, size_t bytes, void
     if (output_bytes < (size_t)c->nx * c->ny * c->nz * (size_t)c->width) { say(err, errlen, "output capacity too small"); return -1; }
     return c->width == 4 ? decode_f32(c, archive, bytes, (float*)output, err, errlen)
                          : decode_f64(c, archive, bytes, (double*)output, err, errlen);
+}
+
+int wo_compact_repairs(const uint8_t* archive, size_t bytes, int width, const void* original, double step,
+                       uint8_t* out, size_t capacity, size_t* written, char* err, size_t errlen) {
+    uint32_t np, nq;
+    size_t pi, pv, qi, qv, end, section, sec8, qb;
+    uint64_t wb;
+    uint8_t* tmp;
+    if (written) *written = 0;
+    if (!archive || !original || !out || !written || bytes < 32 || (width != 4 && width != 8) || !(step > 0)) {
+        say(err, errlen, "invalid argument"); return -1;
+    }
+    wb = get64(archive + 16); np = get32(archive + 24); nq = get32(archive + 28);
+    pi = 32 + pad8((size_t)wb); pv = pi + pad8((size_t)np * 4); qi = pv + pad8((size_t)np * width);
+    qv = qi + pad8((size_t)nq * 4); end = qv + pad8((size_t)nq * 4);
+    if ((archive[0] & 2) || end != bytes || capacity < bytes) { say(err, errlen, "not a native archive"); return -1; }
+    tmp = (uint8_t*)calloc((size_t)np * width + 64, 1);
+    if (!tmp) { say(err, errlen, "out of memory"); return -1; }
+    section = np ? (width == 4 ? wpw_pack_f32(archive + pi, archive + pv, np, (const float*)original, step, tmp)
+                               : wpw_pack_f64(archive + pi, archive + pv, np, (const double*)original, step, tmp))
+                 : 0;
+    if (!section) {
+        memcpy(out, archive, bytes);
+        *written = bytes;
+        free(tmp);
+        return 0;
+    }
+    sec8 = pad8(section);
+    qb = pad8((size_t)nq * 4);
+    memmove(out, archive, pv);
+    out[0] |= 2;
+    put32(out + 4, (uint32_t)section);
+    memcpy(out + pv, tmp, section);
+    memset(out + pv + section, 0, sec8 - section);
+    memmove(out + pv + sec8, archive + qi, 2 * qb);
+    *written = pv + sec8 + 2 * qb;
+    free(tmp);
+    return 0;
 }

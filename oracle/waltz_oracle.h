@@ -17,7 +17,11 @@
  *   wo_wzp_encode       cpu/src/wzp_cpu.cpp:769-867
  *   wo_wzp_decode       cpu/src/wzp_cpu.cpp:869-949
  *   wo_compress         cpu/src/codec.cpp:177-258 (scalar backend)
- *   wo_decompress       cpu/src/codec.cpp:276-336 (native repairs only)
+ *   wo_decompress       cpu/src/codec.cpp:276-336 (native and compact repairs)
+ *   wo_compact_repairs  src/small_pwe.cuh:21-105 (the compact WPW1 repair
+ *                       section; groups placed in order, as this library's
+ *                       encoder does, where the reference's CUDA packer
+ *                       places them by an atomic counter)
  */
 #ifndef WALTZ_ORACLE_H
 #define WALTZ_ORACLE_H
@@ -63,6 +67,11 @@ int wo_compress(const wo_config* c, const void* input, uint8_t* archive, size_t 
                 size_t* written, char* err, size_t errlen);
 int wo_decompress(const wo_config* c, const uint8_t* archive, size_t bytes, void* output,
                   size_t output_bytes, char* err, size_t errlen);
+/* The archive with its native repair section replaced by the compact one
+ * (step, the originals of the compressed field), when that is smaller; else
+ * a copy. out may not overlap archive. Returns 0 or -1. */
+int wo_compact_repairs(const uint8_t* archive, size_t bytes, int width, const void* original, double step,
+                       uint8_t* out, size_t capacity, size_t* written, char* err, size_t errlen);
 
 #ifdef __cplusplus
 }

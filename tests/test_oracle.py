@@ -159,3 +159,27 @@ def test_golden_fixtures():
         assert archive == case["archive"], case["name"]
         out = O.decompress(archive, field.shape, field.dtype)
         assert hashlib.sha256(out.tobytes()).hexdigest() == case["decoded_sha256"], case["name"]
+
+
+@pytest.mark.parametrize("scale", [16, 64])
+@pytest.mark.parametrize("nxyz,dtype,rel", [((40, 44, 52), np.float32, 1e-3), ((33, 24, 40), np.float64, 1e-5),
+                                            ((64, 64, 64), np.float32, 1e-5)])
+def test_oracle_compact_repairs_decode_like_the_reference(nxyz, dtype, rel, scale):
+    """The oracle's compact (WPW1) repair sections decode bit for bit like the
+    reference CPU codec decodes them, within the bound (cpu/src/codec.cpp:
+    305-325 reads the section; src/small_pwe.cuh:21-94 defines it)."""
+    if not O.ref_available():
+        pytest.skip("reference CPU codec not built")
+    from waltz_b200 import synthetic as S
+    a = S.power_law_field(P.zyx(nxyz), 7, dtype=dtype)
+    eb = rel * (float(a.max()) - float(a.min()))
+    plain = O.compress(a, eb)
+    arc = O.compact_repairs(plain, a, eb / scale)
+    assert arc[0] & 2 and len(arc) < len(plain)
+    ours = O.decompress(arc, a.shape, dtype)
+    assert ours.tobytes() == O.RefCodec(O.SCALAR).decompress(arc, a.shape, dtype).tobytes()
+    assert float(np.abs(ours.astype(np.float64) - a.astype(np.float64)).max()) <= eb
+    bad = bytearray(arc)
+    bad[4:8] = (len(plain)).to_bytes(4, "little")  # section length inconsistent with the layout
+    with pytest.raises(O.CodecError):
+        O.decompress(bytes(bad), a.shape, dtype)

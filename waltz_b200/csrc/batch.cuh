@@ -116,7 +116,7 @@ static void decode_batch(const waltz_batch_shape& d, const uint8_t* host, const 
         }
         FrameOut<T> fin{dst, d.fx, d.fy, d.fz, ox, oy, oz, status};
         FramePatch<T> patch{dst, d.x, d.y, d.fx, d.fy, d.fz, ox, oy, oz};
-        decode_launch<T>(JobRef{nullptr, decode_job(packed + job.at, job.h, job.L)}, (job.h.flags & kMatrixFlag) != 0,
+        decode_launch<T>(JobRef{nullptr, decode_job(packed + job.at, job.h, job.L)}, job.h.split,
                          g, irank, nullptr, C, bank1, bank2, fin, patch, status, sink);
     }
     check(cudaGetLastError(), "batch launch");

@@ -10,6 +10,7 @@
 // lifting -> repair patches. Every status is gathered in one device word and
 // read at the call's single synchronisation point.
 #include "common.cuh"
+#include "compact.cuh"
 #include "inverse.cuh"
 #include "launch.cuh"
 #include "ops.cuh"
@@ -204,6 +205,7 @@ struct Options {
     uint64_t small_level = uint64_t(1) << 15; // inverse levels of at most this many samples: direct staging
     uint64_t small_fwd = uint64_t(1) << 20;   // forward levels of at most this many samples: direct staging,
                                               // short z ranges (measured on 128^3 .. 512^3 fields)
+    uint32_t repair_scale = 0; // compact repair section (WPW1) with step eb / scale: 0 (off), 16 or 64
 };
 static thread_local Options t_opt;
 
@@ -963,6 +965,7 @@ struct EncodeOptions {
     uint32_t spin_cap = 1u << 22;
     uint32_t skip_publish = 0xffffffffu;
     int zsplit = kZsNone; // precision form: tensor-core Z transform in this split form (header flag bits)
+    uint32_t repair_scale = t_opt.repair_scale; // the calling thread's compact repair setting
 };
 
 // Header flag bit 6 (reserved in the reference header,
@@ -1011,7 +1014,13 @@ template <class T> struct CompressJob {
         uint16_t* mag;
         uint32_t *sign, *qbits, *qval, *pbits, *status, *ticket, *counts_p, *counts_q;
         uint64_t *state, *sizes, *wzp_total, *layout; // layout[8] = status copy
+        uint32_t* wpw_groups;  // compact repairs: per group bytes, then offsets
+        uint64_t* wpw_state;
+        uint8_t* wpw_tail;     // the compact section and the moved q-outlier sections
     };
+    // Compact repairs: record and group capacities of this field.
+    uint64_t repair_cap() const { return std::min<uint64_t>(n, uint64_t(1) << 22); }
+    uint64_t outlier_cap() const { return std::min<uint64_t>(n, uint64_t(1) << 20); }
 
     static CompressJob make(const T* d_in, uint32_t nx, uint32_t ny, uint32_t nz, double eb, uint8_t* d_out,
                             size_t capacity, const EncodeOptions& opt) {
@@ -1061,6 +1070,14 @@ template <class T> struct CompressJob {
         p.sizes = c.take<uint64_t>(chunks);
         p.wzp_total = c.take<uint64_t>(1);
         p.layout = c.take<uint64_t>(9);
+        p.wpw_groups = nullptr;
+        p.wpw_state = nullptr;
+        p.wpw_tail = nullptr;
+        if (opt.repair_scale) {
+            p.wpw_groups = c.take<uint32_t>((repair_cap() + 31) / 32 + 1);
+            p.wpw_state = c.take<uint64_t>(8);
+            p.wpw_tail = c.take<uint8_t>(repair_cap() * sizeof(T) + 2 * pad8(outlier_cap() * 4) + 64);
+        }
         return p;
     }
     size_t scratch_bytes() const {
@@ -1144,6 +1161,24 @@ template <class T> struct CompressJob {
                                                                        P.counts_q, P.perr, P.qval, out, layout, n,
                                                                        uint32_t(cblocks)},
                                     both);
+        // 6. compact repair section (opt-in WPW1 profile), from the ordered
+        // native records just written; every grid is fixed by the field's
+        // record capacity (the counts are on the device)
+        if (opt.repair_scale) {
+            const double step = eb / double(opt.repair_scale);
+            const uint64_t groups = (repair_cap() + 31) / 32;
+            const uint32_t gblocks = uint32_t(std::min<uint64_t>((groups + 7) / 8, 148 * 8));
+            sink.run<WpwSizeOp<T>>(typename WpwSizeOp<T>::Params{layout, out, in, step, P.wpw_groups},
+                                   std::max(gblocks, 1u));
+            sink.run<WpwScanOp>(WpwScanOp::Params{layout, out, P.wpw_groups, P.wpw_state, uint32_t(sizeof(T)), step},
+                                1);
+            sink.run<WpwWriteOp<T>>(typename WpwWriteOp<T>::Params{layout, out, in, step, P.wpw_groups, P.wpw_state,
+                                                                   P.wpw_tail},
+                                    std::max(gblocks, 1u));
+            const uint64_t tail = repair_cap() * sizeof(T) + 2 * pad8(outlier_cap() * 4);
+            sink.run<WpwMoveOp>(WpwMoveOp::Params{layout, P.wpw_state, P.wpw_tail, out},
+                                uint32_t(std::min<uint64_t>((tail / 8 + 255) / 256 + 1, 148 * 8)));
+        }
         sink.mark("side_records");
     }
 
@@ -1232,7 +1267,7 @@ static Layout validate_header(const Header& h, const Geometry& g, size_t bytes, 
          "invalid Waltz archive header");
     need(!zsplit || matrix_form_ok(g, sizeof(T), zsplit), "invalid Waltz archive header");
     need(((h.flags >> 3) & 3) == 3, "unsupported Waltz synthesis mode");
-    need(!(h.flags & 2), "compact repair archives are not supported by this decoder");
+    const bool compact = (h.flags & 2) != 0; // WPW1 repair section (cpu/src/codec.cpp:280-293)
     const bool dyadic = h.flags & 1;
     need(h.lxy <= 5 && h.lz <= 5 && h.bz >= 1 && h.bz <= 32 && !(dyadic && h.lxy != h.lz), "invalid levels or z band");
     need(h.lxy == g.lxy && h.lz == g.lz, "dimensions/levels mismatch");
@@ -1247,7 +1282,12 @@ static Layout validate_header(const Header& h, const Geometry& g, size_t bytes, 
     L.qv = L.qi + pad8(uint64_t(h.nq) * 4);
     L.end = L.qv + pad8(uint64_t(h.nq) * 4);
     need(L.end == bytes, "truncated archive or trailing data");
-    need(uint64_t(h.pwe_bytes) == uint64_t(h.np) * sizeof(T), "invalid native correction section");
+    if (compact)
+        need(h.np > 0 && uint64_t(h.pwe_bytes) >= kWpwHeader + uint64_t(kWpwEntry) * ((uint64_t(h.np) + 31) / 32) &&
+                 uint64_t(h.pwe_bytes) < uint64_t(h.np) * sizeof(T),
+             "invalid compact correction section");
+    else
+        need(uint64_t(h.pwe_bytes) == uint64_t(h.np) * sizeof(T), "invalid native correction section");
     need(h.wzp >= wzp_header(uint32_t(n)) && h.wzp <= wzp_max_bytes(uint32_t(n)), "WZP archive size is outside its valid bounds");
     need(h.bz == g.bz, "invalid Waltz reorder z-band");
     if (canonical) {
@@ -1341,7 +1381,7 @@ static void host_directory_check(const uint8_t* in, uint32_t n, uint64_t payload
 }
 
 static DecodeJob decode_job(const uint8_t* d_in, const Header& h, const Layout& L, void* out = nullptr) {
-    return DecodeJob{d_in, h.wzp, L.pi, L.pv, L.qi, L.qv, h.q, h.np, h.nq, out};
+    return DecodeJob{d_in, h.wzp, L.pi, L.pv, L.qi, L.qv, h.q, h.np, h.nq, out, h.pwe_bytes, (h.flags & 2u) != 0 ? 1u : 0u};
 }
 
 // Decoder kernels of one archive, launched without synchronising. Scratch:
@@ -2041,6 +2081,10 @@ int waltz_b200_set_option(int option, int value) {
     case WALTZ_B200_OPT_SMALL_FWD:
         if (value < 0) break;
         t_opt.small_fwd = uint64_t(value);
+        return 0;
+    case WALTZ_B200_OPT_COMPACT_REPAIRS:
+        if (value != 0 && value != 16 && value != 64) break;
+        t_opt.repair_scale = uint32_t(value);
         return 0;
     default:
         break;

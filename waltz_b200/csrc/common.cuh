@@ -260,6 +260,8 @@ struct DecodeJob {
     double q;
     uint32_t np, nq;
     void* out; // where the samples go (read by JobOut / JobPatch)
+    uint32_t pwe_bytes; // repair section bytes
+    uint32_t compact;   // the repair section is a compact (WPW1) section
 };
 
 // A decode kernel's archive parameters: by value (one archive decoded by

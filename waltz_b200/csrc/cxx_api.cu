@@ -12,6 +12,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -60,9 +61,21 @@ size_t d_WALTZ_compress(T* d_oridata, char* d_cmpData, const Config& config, con
         throw std::invalid_argument("Waltz: input and output buffers overlap");
     const double eb = config.absErrorBound;
     if (!(eb > 0) || !std::isfinite(1.5 * eb)) throw std::invalid_argument("Waltz: invalid bound or rounding mode");
+    // the reference's compact repair profile switch (src/waltz.cu:162-172):
+    // WALTZ_SMALL_PWE_SCALE = 0 (default), 16 or 64, for this call
+    int scale = 0;
+    if (const char* v = std::getenv("WALTZ_SMALL_PWE_SCALE")) {
+        char* end = nullptr;
+        const double d = std::strtod(v, &end);
+        if (end == v || *end != '\0' || (d != 0.0 && d != 16.0 && d != 64.0))
+            throw std::invalid_argument("Waltz: WALTZ_SMALL_PWE_SCALE must be 0, 16 or 64");
+        scale = int(d);
+    }
+    waltz_b200_set_option(WALTZ_B200_OPT_COMPACT_REPAIRS, scale);
     size_t written = 0;
-    if (waltz_b200_compress(d_oridata, int(sizeof(T)), nx, ny, nz, eb, d_cmpData, capacity, &written, stream))
-        fail_runtime("Waltz compress");
+    const int rc = waltz_b200_compress(d_oridata, int(sizeof(T)), nx, ny, nz, eb, d_cmpData, capacity, &written, stream);
+    waltz_b200_set_option(WALTZ_B200_OPT_COMPACT_REPAIRS, 0);
+    if (rc) fail_runtime("Waltz compress");
     return written;
 }
 

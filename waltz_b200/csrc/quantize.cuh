@@ -2,6 +2,7 @@
 // side-record kernels (ordered compaction, decode patches, extrema).
 #pragma once
 #include "common.cuh"
+#include "compact.cuh"
 #include "scan.cuh"
 
 namespace wb {
@@ -525,12 +526,18 @@ __device__ __forceinline__ void RPatchOp<T, Patch>::run(const Params P, uint32_t
         T err;
         if (aligned) {
             at = reinterpret_cast<const uint32_t*>(pi)[i];
-            err = reinterpret_cast<const T*>(pv)[i];
+            if (!J.compact) err = reinterpret_cast<const T*>(pv)[i];
             if (i) prev = reinterpret_cast<const uint32_t*>(pi)[i - 1];
         } else {
             memcpy(&at, pi + 4 * uint64_t(i), 4);
-            memcpy(&err, pv + sizeof(T) * uint64_t(i), sizeof(T));
+            if (!J.compact) memcpy(&err, pv + sizeof(T) * uint64_t(i), sizeof(T));
             if (i) memcpy(&prev, pi + 4 * uint64_t(i - 1), 4);
+        }
+        // compact section: the record's correction from its group (validated
+        // header, directory entry and span; never a trap)
+        if (J.compact && !wpw_correction<T>(pv, J.pwe_bytes, J.np, i, err)) {
+            atomicOr(status, ST_BAD_REPAIR);
+            continue;
         }
         if (at >= n) { atomicOr(status, ST_BAD_INDEX); continue; }
         if (i && prev >= at) atomicOr(status, ST_UNORDERED);
