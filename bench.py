@@ -823,8 +823,8 @@ def batch_only(dev, lib, args, count=512):
                       device=dev)
     dec = torch.empty(sum(f.numel() for f in fields), dtype=torch.float32, device=dev)
     if args.batch_config:
-        mode, width = (int(v) for v in args.batch_config.split(":"))
-        knobs = {"mode": mode, "width": width, "stage_kernels": 1}
+        parts = [int(v) for v in args.batch_config.split(":")]
+        knobs = {"mode": parts[0], "width": parts[1], "stage_kernels": parts[2] if len(parts) > 2 else 1}
     else:
         knobs = autotune.lookup(autotune.batch_class(shapes, 4))
     lib.waltz_b200_batch_config(knobs["mode"], knobs["width"])
@@ -1074,8 +1074,9 @@ def main():
                     help="run only the batched form on the uneven-chunk workload (profiler captures)")
     ap.add_argument("--tc-only", action="store_true",
                     help="run only the plain vs tensor-core form comparison at --tc-shape (profiler captures)")
-    ap.add_argument("--batch-config", default=None, metavar="MODE:WIDTH",
-                    help="batch execution form instead of the tuning table's (0 = stage-batched, 1 = field chains)")
+    ap.add_argument("--batch-config", default=None, metavar="MODE:WIDTH[:STAGE]",
+                    help="batch execution form instead of the tuning table's (0 = stage-batched, 1 = field chains, "
+                         "2 = work queues; STAGE: whole-stage plane kernels 1 or 0)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

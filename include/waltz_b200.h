@@ -110,6 +110,9 @@ int waltz_b200_decompress_batch(const waltz_b200_archive* archives, uint32_t cou
  *   chunk-tile work list); groups run as parallel graph branches.
  * WALTZ_B200_BATCH_FIELDS: each field's own launches, fields round-robin on
  *   `width` parallel graph branches. Default, width 32.
+ * WALTZ_B200_BATCH_QUEUE: as STAGES, but every stage launch is a persistent
+ *   work queue: a grid of resident CTAs pulling chunk-tile items (a field's
+ *   block of that stage) from a device ticket, reset by the graph itself.
  * width 1..64. Returns 0, or -1 for an invalid configuration. */
 /* Tuning options of the calling thread (performance knobs: results do not
  * depend on them). Returns 0, or -1 for an unknown option or value.
@@ -143,6 +146,7 @@ int waltz_b200_set_option(int option, int value);
 
 #define WALTZ_B200_BATCH_STAGES 0
 #define WALTZ_B200_BATCH_FIELDS 1
+#define WALTZ_B200_BATCH_QUEUE 2
 int waltz_b200_batch_config(int mode, int width);
 
 /* Decode an archive of `bytes` bytes into nx*ny*nz samples (the archive does

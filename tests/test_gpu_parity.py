@@ -371,7 +371,7 @@ def test_matrix_form_round_trip_float64(shape, eb):
     assert err <= np.longdouble(eb)
 
 
-BATCH_FORMS = [(0, 1), (0, 3), (1, 32)]  # (stage-batched | field chains, width)
+BATCH_FORMS = [(0, 1), (0, 3), (1, 32), (2, 1), (2, 4)]  # (stage-batched | field chains | work queue, width)
 
 
 @pytest.fixture(params=BATCH_FORMS, ids=lambda f: f"mode{f[0]}w{f[1]}")
@@ -486,7 +486,7 @@ def test_batch_decompress_f64_and_errors(batch_form):
 
 def test_batch_config_rejects_invalid_forms():
     lib = _lib()
-    assert lib.waltz_b200_batch_config(2, 4) == -1
+    assert lib.waltz_b200_batch_config(3, 4) == -1
     assert lib.waltz_b200_batch_config(0, 0) == -1
     assert lib.waltz_b200_batch_config(1, 65) == -1
     assert b"invalid batch configuration" in lib.waltz_b200_last_error()

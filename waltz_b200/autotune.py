@@ -9,9 +9,9 @@ question and the table can be applied blindly):
    and the level sizes below which dyadic and XY levels stage tiles with
    reflecting loads instead of tensor-map copies (WALTZ_B200_OPT_SMALL_LEVEL /
    _FWD);
- * batches: the execution form of the batch graph (stage-batched groups or
-   per-field chains, and their width, waltz_b200_batch_config) and the stage
-   kernels knob;
+ * batches: the execution form of the batch graph (stage-batched groups,
+   the same as persistent work queues, or per-field chains, and their width,
+   waltz_b200_batch_config) and the stage kernels knob;
  * the transform form (lifting or the tensor-core matrix form) of fields the
    matrix form serves: recorded per class and used only when a caller asks
    for form="auto", since the matrix form sets its own header flag.
@@ -35,7 +35,7 @@ from pathlib import Path
 TABLE = Path(__file__).with_name("tuning.json")
 
 OPT_STAGE_KERNELS, OPT_ZMARCH_PLANES, OPT_SMALL_LEVEL, OPT_SMALL_FWD = 1, 2, 3, 4
-BATCH_STAGES, BATCH_FIELDS = 0, 1
+BATCH_STAGES, BATCH_FIELDS, BATCH_QUEUE = 0, 1, 2
 DEFAULT_SINGLE = {"stage_kernels": 1, "zmarch": 0, "small_inv": 1 << 15, "small_fwd": 1 << 20}
 MATRIX_MARGIN = 0.97  # the matrix form changes the header flag: take it only for a clear gain
 DEFAULT_BATCH = {"mode": BATCH_FIELDS, "width": 32, "stage_kernels": 1}
@@ -44,6 +44,7 @@ SINGLE_CANDIDATES = [{"stage_kernels": s, "zmarch": z, "small_inv": i, "small_fw
                      for s in (1, 0) for z in (0, 32) for i in (1 << 15, 1 << 18, 1 << 21)
                      for f in (1 << 20, 1 << 21, 1 << 24, 1 << 26)]
 BATCH_CANDIDATES = ([{"mode": BATCH_STAGES, "width": w, "stage_kernels": s} for w in (1, 4, 16) for s in (1, 0)] +
+                    [{"mode": BATCH_QUEUE, "width": w, "stage_kernels": s} for w in (1, 4, 16) for s in (1, 0)] +
                     [{"mode": BATCH_FIELDS, "width": w, "stage_kernels": s} for w in (16, 32, 64) for s in (1, 0)])
 
 

@@ -1698,7 +1698,8 @@ struct BatchCompressState {
 // the capture stream; the parameter table is uploaded first and kept.
 template <class Enqueue>
 static void capture_stage_batched(BatchStreams& bs, int groups, CachedGraph& cg, Arena& table_arena,
-                                  std::vector<unsigned char>&& key, uint32_t count, Enqueue enqueue) {
+                                  std::vector<unsigned char>&& key, uint32_t count, Enqueue enqueue,
+                                  bool queue = false) {
     groups = int(std::min<uint32_t>(uint32_t(groups), count));
     std::vector<Recorder> recs(groups);
     for (uint32_t i = 0; i < count; ++i) {
@@ -1720,7 +1721,7 @@ static void capture_stage_batched(BatchStreams& bs, int groups, CachedGraph& cg,
         check(cudaMemcpy(table + at[g], plans[g].host.data(), plans[g].bytes(), cudaMemcpyHostToDevice),
               "batch table upload");
     capture_batch(bs, groups == 1 ? 0 : groups, cg, std::move(key), [&](cudaStream_t* s) {
-        for (size_t g = 0; g < plans.size(); ++g) plans[g].execute(table + at[g], s[g]);
+        for (size_t g = 0; g < plans.size(); ++g) plans[g].execute(table + at[g], s[g], queue, uint32_t(plans.size()));
     });
 }
 static thread_local BatchCompressState t_bc;
@@ -1768,11 +1769,12 @@ static void compress_batch(const waltz_b200_chunk* items, uint32_t count, uint64
         std::vector<const uint16_t*> rank(count);
         for (uint32_t i = 0; i < count; ++i)
             rank[i] = st.tables.get(jobs[i].nx, jobs[i].ny, jobs[i].nz, jobs[i].g.bz, false, bs.cap);
-        if (cfg.mode == WALTZ_B200_BATCH_STAGES) {
+        if (cfg.mode == WALTZ_B200_BATCH_STAGES || cfg.mode == WALTZ_B200_BATCH_QUEUE) {
             capture_stage_batched(bs, cfg.width, st.graph, st.table, std::move(key), count,
                                   [&](uint32_t i, Sink& sink) {
                                       jobs[i].enqueue(base + offset[i], rank[i], sink, results + 9 * size_t(i));
-                                  });
+                                  },
+                                  cfg.mode == WALTZ_B200_BATCH_QUEUE);
         } else {
             capture_batch(bs, cfg.width, st.graph, std::move(key), [&](cudaStream_t* work) {
                 for (uint32_t i = 0; i < count; ++i) {
@@ -1857,7 +1859,7 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
     // per field when stage-batched (all fields run at once), else one per
     // branch sized by the largest field on it.
     const BatchConfig cfg = t_batch_cfg;
-    const bool staged = cfg.mode == WALTZ_B200_BATCH_STAGES;
+    const bool staged = cfg.mode == WALTZ_B200_BATCH_STAGES || cfg.mode == WALTZ_B200_BATCH_QUEUE;
     const uint32_t lanes = staged ? count : uint32_t(cfg.width);
     auto lane_of = [&](uint32_t i) { return staged ? i : i % uint32_t(cfg.width); };
     std::vector<uint64_t> lane_n(lanes, 0);
@@ -1965,7 +1967,8 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
                              P.b2[k], fin, patch, P.status + i, sink);
         };
         if (staged) {
-            capture_stage_batched(bs, cfg.width, st.graph, st.table, std::move(key), count, enqueue);
+            capture_stage_batched(bs, cfg.width, st.graph, st.table, std::move(key), count, enqueue,
+                                  cfg.mode == WALTZ_B200_BATCH_QUEUE);
         } else {
             capture_batch(bs, cfg.width, st.graph, std::move(key), [&](cudaStream_t* work) {
                 for (uint32_t i = 0; i < count; ++i) {
@@ -2095,7 +2098,8 @@ int waltz_b200_set_option(int option, int value) {
 
 int waltz_b200_batch_config(int mode, int width) {
     using namespace wb;
-    if ((mode != WALTZ_B200_BATCH_STAGES && mode != WALTZ_B200_BATCH_FIELDS) || width < 1 || width > kMaxBranches) {
+    if ((mode != WALTZ_B200_BATCH_STAGES && mode != WALTZ_B200_BATCH_FIELDS && mode != WALTZ_B200_BATCH_QUEUE) ||
+        width < 1 || width > kMaxBranches) {
         std::snprintf(t_error, sizeof(t_error), "invalid batch configuration (mode %d, width %d)", mode, width);
         return -1;
     }

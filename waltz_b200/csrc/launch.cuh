@@ -54,6 +54,33 @@ static void launch_op_batch(const void* table, const uint32_t* starts, uint32_t 
     check(cudaGetLastError(), "batched kernel launch");
 }
 
+// Resident CTAs of a kernel on this device (occupancy at its block size and
+// shared memory, times the SM count).
+template <class K> static uint32_t resident_ctas(K kernel, int threads, size_t smem) {
+    int dev = 0, sms = 0, occ = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem), "occupancy");
+    return uint32_t(std::max(sms, 1) * std::max(occ, 1));
+}
+
+template <class Op>
+static void launch_op_queue(const void* table, const uint32_t* starts, uint32_t count, uint32_t blocks, size_t smem,
+                            uint32_t* ticket, uint32_t share, cudaStream_t s) {
+    if (!blocks) return;
+    static thread_local int device = -1;
+    static thread_local size_t granted = 0;
+    opt_in_smem(op_queue_kernel<Op>, smem, device, granted);
+    // one share of the resident CTAs: the parallel branches of the batch
+    // graph each keep their queues on their share of the GPU
+    const uint32_t slots = resident_ctas(op_queue_kernel<Op>, Op::kThreads, smem);
+    const uint32_t grid = std::min(blocks, std::max(1u, (slots + share - 1) / share));
+    op_queue_kernel<Op><<<grid, Op::kThreads, smem, s>>>(static_cast<const typename Op::Params*>(table), starts,
+                                                         count, ticket);
+    note_launch();
+    check(cudaGetLastError(), "queued kernel launch");
+}
+
 // One recorded stage of one field.
 struct OpRecord {
     virtual ~OpRecord() = default;
@@ -67,6 +94,13 @@ struct OpRecord {
     // records that cannot be batched, one launch each)
     virtual void launch_group(const std::vector<const OpRecord*>& group, const void* table, const uint32_t* starts,
                               uint32_t blocks, size_t smem, cudaStream_t s) const = 0;
+    // the same group as a persistent work queue (ticket zeroed beforehand)
+    virtual void launch_queue(const std::vector<const OpRecord*>& group, const void* table, const uint32_t* starts,
+                              uint32_t blocks, size_t smem, uint32_t* ticket, uint32_t share, cudaStream_t s) const {
+        (void)ticket;
+        (void)share;
+        launch_group(group, table, starts, blocks, smem, s);
+    }
 };
 
 template <class Op> struct OpRec final : OpRecord {
@@ -87,6 +121,10 @@ template <class Op> struct OpRec final : OpRecord {
     void launch_group(const std::vector<const OpRecord*>& group, const void* table, const uint32_t* starts,
                       uint32_t blocks, size_t smem, cudaStream_t s) const override {
         launch_op_batch<Op>(table, starts, uint32_t(group.size()), blocks, smem, s);
+    }
+    void launch_queue(const std::vector<const OpRecord*>& group, const void* table, const uint32_t* starts,
+                      uint32_t blocks, size_t smem, uint32_t* ticket, uint32_t share, cudaStream_t s) const override {
+        launch_op_queue<Op>(table, starts, uint32_t(group.size()), blocks, smem, ticket, share, s);
     }
 };
 
@@ -170,9 +208,12 @@ struct BatchPlan {
         size_t table_off = 0, starts_off = 0;
         uint32_t blocks = 0;
         size_t smem = 0;
+        uint32_t ticket = 0; // work-queue form: index of its ticket word
     };
     std::vector<std::vector<Group>> steps;
     std::vector<unsigned char> host; // the table image
+    size_t tickets_off = 0;          // work-queue tickets, one u32 per group
+    uint32_t tickets = 0;
     size_t bytes() const { return host.size(); }
 
     static BatchPlan make(const Recorder& r) {
@@ -207,8 +248,10 @@ struct BatchPlan {
                     g.blocks += rec->blocks();
                 }
             }
+            for (Group& g : groups) g.ticket = plan.tickets++;
             plan.steps.push_back(std::move(groups));
         }
+        plan.tickets_off = place(4 * size_t(plan.tickets + 1), 256);
         plan.host.assign(at, 0);
         for (auto& groups : plan.steps)
             for (Group& g : groups) {
@@ -226,13 +269,19 @@ struct BatchPlan {
     }
 
     // Launches every step on `s`, reading the parameters from `table` (the
-    // device copy of `host`).
-    void execute(const unsigned char* table, cudaStream_t s) const {
+    // device copy of `host`); `queue`: each step as a persistent work queue
+    // on 1/`share` of the resident CTAs (`share` plans run side by side),
+    // its tickets zeroed first (a memset node of the captured graph).
+    void execute(unsigned char* table, cudaStream_t s, bool queue = false, uint32_t share = 1) const {
+        uint32_t* tick = reinterpret_cast<uint32_t*>(table + tickets_off);
+        if (queue) check(cudaMemsetAsync(tick, 0, 4 * size_t(tickets), s), "ticket reset");
         for (const auto& groups : steps)
-            for (const Group& g : groups)
-                g.recs.front()->launch_group(g.recs, table + g.table_off,
-                                             reinterpret_cast<const uint32_t*>(table + g.starts_off), g.blocks, g.smem,
-                                             s);
+            for (const Group& g : groups) {
+                const uint32_t* starts = reinterpret_cast<const uint32_t*>(table + g.starts_off);
+                if (queue) g.recs.front()->launch_queue(g.recs, table + g.table_off, starts, g.blocks, g.smem,
+                                                        tick + g.ticket, share, s);
+                else g.recs.front()->launch_group(g.recs, table + g.table_off, starts, g.blocks, g.smem, s);
+            }
     }
 };
 

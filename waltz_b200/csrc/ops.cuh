@@ -60,6 +60,39 @@ __global__ void __launch_bounds__(Op::kThreads, Op::kMinBlocks)
     Op::run(table[lo], b - first, __ldg(starts + lo + 1) - first);
 }
 
+// The same stage as a persistent work queue: a grid of resident CTAs, each
+// pulling chunk-tile items (a field's block) from a device ticket until the
+// stage's items run out; an item runs the body exactly as op_batch_kernel
+// runs it, and the CTA synchronises before its next item reuses shared
+// memory. Items are taken in increasing order, so a stage whose blocks wait
+// on earlier blocks of the same field (the WZP lookback) only waits on items
+// already running on resident CTAs. The ticket is zeroed before each launch.
+template <class Op>
+__global__ void __launch_bounds__(Op::kThreads, Op::kMinBlocks)
+    op_queue_kernel(const typename Op::Params* __restrict__ table, const uint32_t* __restrict__ starts,
+                    uint32_t count, uint32_t* ticket) {
+    __shared__ uint32_t item;
+    const uint32_t total = __ldg(starts + count);
+    for (;;) {
+        if (threadIdx.x == 0) item = atomicAdd(ticket, 1u);
+        __syncthreads();
+        const uint32_t b = item;
+        if (b >= total) break;
+        uint32_t lo = 0, hi = count;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(starts + mid) <= b) lo = mid;
+            else hi = mid;
+        }
+        const uint32_t first = __ldg(starts + lo);
+        if constexpr (GridConstant<Op>::value) {
+            if (threadIdx.x == 0) Op::acquire_maps(table[lo]);
+        }
+        Op::run(table[lo], b - first, __ldg(starts + lo + 1) - first);
+        __syncthreads(); // the item's shared memory and `item` are free again
+    }
+}
+
 // Zero fill of one byte range (16-byte stores for the aligned bulk).
 struct ZeroOp {
     static constexpr int kThreads = 256, kMinBlocks = 0; // no occupancy floor: the compiler picks the register budget
