@@ -40,3 +40,33 @@ def test_committed_table_is_well_formed():
         assert e["measured"] and all(r["compress_ms"] > 0 and r["decompress_ms"] > 0 for r in e["measured"])
         best = min(e["measured"], key=lambda r: r["compress_ms"] + r["decompress_ms"])["knobs"]
         assert all(e["choice"][k] == v for k, v in best.items())
+
+
+def test_matrix_choice_follows_the_rule():
+    """Entries that timed the precision-form splits choose the fastest one
+    that beats the plain knobs by the margin with an archive at most 2 %
+    larger than the plain one, or none; matrix_choice reads it back."""
+    t = A.load()
+    for e in t.get("entries", []):
+        if "matrix_forms" not in e:
+            continue
+        best = min(e["measured"], key=lambda r: r["compress_ms"] + r["decompress_ms"])
+        limit = A.MATRIX_MARGIN * (best["compress_ms"] + best["decompress_ms"])
+        ok = sorted((m["compress_ms"] + m["decompress_ms"], f) for f, m in e["matrix_forms"].items()
+                    if m["compress_ms"] + m["decompress_ms"] < limit
+                    and m["archive_bytes"] * A.MATRIX_RATIO <= e["plain_archive_bytes"])
+        assert e["choice"]["matrix"] == (ok[0][1] if ok else False)
+
+
+def test_matrix_choice_lookup(tmp_path):
+    table = {"entries": [
+        {"class": {"kind": "single", "dtype": "f32", "schedule": "plane", "log2n": 26},
+         "choice": {"stage_kernels": 1, "matrix": "matrix-bf16"}},
+        {"class": {"kind": "single", "dtype": "f64", "schedule": "plane", "log2n": 23},
+         "choice": {"stage_kernels": 1, "matrix": False}},
+    ]}
+    path = tmp_path / "t.json"
+    path.write_text(json.dumps(table))
+    assert A.matrix_choice((64, 1024, 1024), 4, path) == "matrix-bf16"
+    assert A.matrix_choice((96, 256, 384), 8, path) is None
+    assert A.matrix_choice((512, 512, 512), 4, path) is None  # dyadic: no entry of that schedule

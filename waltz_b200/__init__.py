@@ -70,15 +70,14 @@ def _matrix_ok(shape, itemsize, form="matrix"):
 
 
 def auto_form(shape, itemsize):
-    """The form form="auto" takes: the precision form where it applies and
-    the tuning table measured it faster, in its most accurate split for the
-    field's type (exact slices for double fields with nz <= 96, BF16x3
-    otherwise); the plain form elsewhere."""
-    if not (_matrix_ok(shape, itemsize) and autotune.matrix_preferred(tuple(shape), itemsize)):
+    """The form form="auto" takes: the precision-form split the tuning table
+    chose for the field's class (the fastest split that beat the plain form
+    by 3 % with an archive within 2 % of the plain one's size), where the
+    matrix form applies to this field; the plain form elsewhere."""
+    if not _matrix_ok(shape, itemsize):
         return "plain"
-    if itemsize == 8 and _matrix_ok(shape, itemsize, "matrix-exact"):
-        return "matrix-exact"
-    return "matrix-bf16"
+    form = autotune.matrix_choice(tuple(shape), itemsize)
+    return form if form and _matrix_ok(shape, itemsize, form) else "plain"
 
 
 def compress_tensor(field, abs_error: float, *, form: str = "plain", stream=None, tuned=True):

@@ -12,9 +12,11 @@ question and the table can be applied blindly):
  * batches: the execution form of the batch graph (stage-batched groups,
    the same as persistent work queues, or per-field chains, and their width,
    waltz_b200_batch_config) and the stage kernels knob;
- * the transform form (lifting or the tensor-core matrix form) of fields the
-   matrix form serves: recorded per class and used only when a caller asks
-   for form="auto", since the matrix form sets its own header flag.
+ * the transform form (lifting or one split of the tensor-core matrix form)
+   of fields the matrix form serves: every split is timed and the fastest
+   one that beats lifting by 3 % with a compression ratio at most 2 % lower
+   is recorded per class; it is used only when a caller asks for
+   form="auto", since the matrix form sets its own header flag.
 The WZP group size (16 chunks of 8192 samples) is part of the archive
 format the reference decoders read, so it is not a knob.
 
@@ -38,6 +40,8 @@ OPT_STAGE_KERNELS, OPT_ZMARCH_PLANES, OPT_SMALL_LEVEL, OPT_SMALL_FWD = 1, 2, 3, 
 BATCH_STAGES, BATCH_FIELDS, BATCH_QUEUE = 0, 1, 2
 DEFAULT_SINGLE = {"stage_kernels": 1, "zmarch": 0, "small_inv": 1 << 15, "small_fwd": 1 << 20}
 MATRIX_MARGIN = 0.97  # the matrix form changes the header flag: take it only for a clear gain
+MATRIX_RATIO = 0.98   # ... and only when its archive stays within 2 % of the plain one's size
+MATRIX_SPLITS = ("matrix-tf32", "matrix-bf16", "matrix-exact")
 DEFAULT_BATCH = {"mode": BATCH_FIELDS, "width": 32, "stage_kernels": 1}
 
 SINGLE_CANDIDATES = [{"stage_kernels": s, "zmarch": z, "small_inv": i, "small_fwd": f}
@@ -119,9 +123,11 @@ def apply_batch(lib, shapes, itemsize):
     return k
 
 
-def matrix_preferred(shape, itemsize):
-    """Whether the measured class prefers the matrix form (form="auto")."""
-    return bool(lookup(single_class(shape, itemsize)).get("matrix", False))
+def matrix_choice(shape, itemsize, path=TABLE):
+    """The precision-form split the measured class takes under form="auto"
+    (a form name), or None for the plain form."""
+    m = lookup(single_class(shape, itemsize), path).get("matrix")
+    return m if isinstance(m, str) and m in MATRIX_SPLITS else None
 
 
 # ------------------------------------------------------------------ tuning
@@ -157,16 +163,28 @@ def _tune_single(torch, lib, shape, dtype, reps, rel=1e-3):
              "measured": results}
     choice = min(results, key=lambda r: r["compress_ms"] + r["decompress_ms"])["knobs"]
     entry["choice"] = dict(choice)
-    # the matrix form where it applies: timed with the chosen knobs
-    nz, ny, nx = shape
-    if entry["class"]["schedule"] == "plane" and nz <= 128 and (nx * ny) % 4 == 0:
+    # every precision-form split where it applies, timed with the chosen
+    # knobs: form="auto" takes the fastest split that beats the plain form by
+    # the margin and keeps the archive within 2 % of the plain one's size
+    if waltz_b200._matrix_ok(shape, itemsize):
         set_single(lib, choice)
-        arc = waltz_b200.compress_tensor(f, eb, form="matrix", tuned=False)
-        tc = _time(torch, lambda: waltz_b200.compress_tensor(f, eb, form="matrix", tuned=False), reps)
-        td = _time(torch, lambda: waltz_b200.decompress_tensor(arc, shape, dtype, tuned=False), reps)
         best = min(results, key=lambda r: r["compress_ms"] + r["decompress_ms"])
-        entry["matrix_form"] = {"compress_ms": round(tc, 4), "decompress_ms": round(td, 4)}
-        entry["choice"]["matrix"] = tc + td < MATRIX_MARGIN * (best["compress_ms"] + best["decompress_ms"])
+        plain_bytes = int(waltz_b200.compress_tensor(f, eb, tuned=False).numel())
+        entry["plain_archive_bytes"] = plain_bytes
+        forms = {}
+        for form in MATRIX_SPLITS:
+            if not waltz_b200._matrix_ok(shape, itemsize, form):
+                continue
+            arc = waltz_b200.compress_tensor(f, eb, form=form, tuned=False)
+            tc = _time(torch, lambda: waltz_b200.compress_tensor(f, eb, form=form, tuned=False), reps)
+            td = _time(torch, lambda: waltz_b200.decompress_tensor(arc, shape, dtype, tuned=False), reps)
+            forms[form] = {"compress_ms": round(tc, 4), "decompress_ms": round(td, 4),
+                           "archive_bytes": int(arc.numel())}
+        entry["matrix_forms"] = forms
+        ok = [(m["compress_ms"] + m["decompress_ms"], form) for form, m in forms.items()
+              if m["compress_ms"] + m["decompress_ms"] < MATRIX_MARGIN * (best["compress_ms"] + best["decompress_ms"])
+              and m["archive_bytes"] * MATRIX_RATIO <= plain_bytes]  # compression ratio at most 2 % lower
+        entry["choice"]["matrix"] = min(ok)[1] if ok else False
     set_single(lib, {})
     return entry
 
@@ -225,7 +243,9 @@ def tune(quick=False, reps=5, path=TABLE):
         torch.cuda.empty_cache()
     table = {"device": torch.cuda.get_device_name(), "reps": reps,
              "note": "median CUDA-event times per candidate through the Python API (same call overhead for "
-                     "every candidate); choice = least compress + decompress time",
+                     "every candidate); choice = least compress + decompress time; matrix = the fastest "
+                     "precision-form split at least 3 % faster than the chosen plain knobs whose archive is at "
+                     "most 2 % larger than the plain one (false: none)",
              "entries": entries}
     Path(path).write_text(json.dumps(table, indent=1) + "\n")
     _cache.pop(str(path), None)

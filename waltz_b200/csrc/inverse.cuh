@@ -42,7 +42,7 @@ template <class T, int UX, int UY, int UZ> struct InvShape {
     static constexpr int BX = (HX + PADX + V - 1) / V * V;
     static constexpr int BOX = HZ * HY * BX;             // elements per parity box
     static constexpr int FX = UX + 8, FY = UY + 8, FZ = UZ + 8;
-    static constexpr size_t smem = size_t(8) * BOX * sizeof(T) + 128 + 16;
+    static constexpr size_t smem = size_t(8) * BOX * sizeof(T) + 128 + 32; // + alignment + four barriers
     static_assert((BOX * sizeof(T)) % 128 == 0, "parity boxes must stay 128-byte aligned");
     static_assert(UX % (2 * V) == 0 && UZ == (sizeof(T) == 4 ? 16 : 8) && UY % 8 == 0, "tile shape");
 };
@@ -97,30 +97,43 @@ __device__ __forceinline__ void InvTileOp<T, UX, UY, UZ, Out>::run(const Params&
                (fx >> 1) + S::PADX;
     };
 
-    // ---- stage the eight parity boxes
+    // ---- stage the eight parity boxes, the z-even and z-odd box of one x/y
+    // parity on one barrier each (bar[par], par = x parity + 2 * y parity),
+    // so the Z pass of a parity starts as soon as its two boxes have landed
     if (tid == 0) {
-        mbar_init(bar, 1);
+#pragma unroll 1
+        for (int p = 0; p < 4; ++p) mbar_init(bar + p, 1);
         fence_barrier_init();
-        mbar_expect_tx(bar, uint32_t(8 * S::BOX * sizeof(T)));
         const int x0 = int(ox / 2) - 2 - S::PADX, y0 = int(oy / 2) - 2, z0 = int(oz / 2) - 2;
 #pragma unroll 1
-        for (int b = 0; b < 8; ++b) {
-            const int xp = b & 1, yp = (b >> 1) & 1, zp = b >> 2;
-            const bool from_low = b == 0 && lv.low != nullptr;
-            tma_load_3d(Bx + b * S::BOX, from_low ? &P.lmap : &P.cmap, x0 + (xp ? int(hx) : 0), y0 + (yp ? int(hy) : 0),
-                        z0 + (zp ? int(hz) : 0), bar);
+        for (int p = 0; p < 4; ++p) {
+            mbar_expect_tx(bar + p, uint32_t(2 * S::BOX * sizeof(T)));
+            const int xp = p & 1, yp = p >> 1;
+#pragma unroll 1
+            for (int zp = 0; zp < 2; ++zp) {
+                const int b = p + 4 * zp;
+                const bool from_low = b == 0 && lv.low != nullptr;
+                tma_load_3d(Bx + b * S::BOX, from_low ? &P.lmap : &P.cmap, x0 + (xp ? int(hx) : 0),
+                            y0 + (yp ? int(hy) : 0), z0 + (zp ? int(hz) : 0), bar + p);
+            }
         }
     }
-    {
-        const bool ok = __syncthreads_and(warp != 0 || mbar_wait(bar, 0, kWaitBound));
-        if (!ok) {
-            if (tid == 0) atomicOr(status, ST_WAIT_TIMEOUT);
-            return;
-        }
-    }
-    // ---- edge tiles: out-of-range cells from their reflections
+    __syncthreads(); // the barriers are initialised before any thread polls them
+    // ---- edge tiles: every box first, then the out-of-range cells from
+    // their reflections
     const bool edge = ox < 4 || ox + UX + 4 > a.x || oy < 4 || oy + UY + 4 > a.y || oz < 4 || oz + UZ + 4 > a.z;
     if (edge) {
+        {
+            bool landed = true;
+            if (warp == 0) {
+#pragma unroll 1
+                for (int p = 0; p < 4; ++p) landed = landed && mbar_wait(bar + p, 0, kWaitBound);
+            }
+            if (!__syncthreads_and(landed)) {
+                if (tid == 0) atomicOr(status, ST_WAIT_TIMEOUT);
+                return;
+            }
+        }
         // only the cells outside the array: the in-range footprint is the box
         // [f*_lo, f*_hi); cells of in-range rows left or right of it (A), and
         // whole rows outside it in y or z (B), as one flat list
@@ -177,10 +190,16 @@ __device__ __forceinline__ void InvTileOp<T, UX, UY, UZ, Out>::run(const Params&
     constexpr int ZS = S::HY * S::BX; // z-slot stride inside a box
     {
         constexpr int P = UZ / 2 + 4;
+        bool failed = false; // a copy that never landed: skip the work, the status fails the call
         for (int L = tid; L < S::FX * S::FY; L += kThreads) {
             // x index fastest inside one (x parity, y parity) box
             const int i = L % (S::FX / 2), k = (L / (S::FX / 2)) % (S::FY / 2);
             const int par = L / ((S::FX / 2) * (S::FY / 2)); // x parity + 2 * y parity
+            if (!edge && !failed && !mbar_wait(bar + par, 0, kWaitBound)) { // edge tiles waited above
+                failed = true;
+                atomicOr(status, ST_WAIT_TIMEOUT);
+            }
+            if (failed) continue;
             T* pe = Bx + par * S::BOX + k * S::BX + i + S::PADX;
             T* po = pe + 4 * S::BOX;
             T e[P], o[P];
