@@ -323,6 +323,30 @@ def gpu_arm(args, rank, world, local_rank):
     e2e_ms = dist_max(streamed(steps_e2e), world) / steps_e2e
     worst = max(float((sl["hout"].double() - host_in.double()).abs().max()) for sl in slots)
     assert worst <= eb, f"streamed end-to-end result violates the bound: {worst} > {eb}"
+
+    # the copy ceiling of that pipeline: a field's bytes up and a field's
+    # bytes down at the same time, no kernels (per-direction GB/s, best of 3)
+    def both_ways(reps=3):
+        best = None
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0.record(comp)
+            up.wait_event(t0)
+            down.wait_event(t0)
+            with torch.cuda.stream(up):
+                slots[0]["field"].copy_(host_in, non_blocking=True)
+            with torch.cuda.stream(down):
+                slots[1]["hout"].copy_(slots[1]["out"], non_blocking=True)
+            comp.wait_stream(up)
+            comp.wait_stream(down)
+            t1.record(comp)
+            torch.cuda.synchronize()
+            ms = t0.elapsed_time(t1)
+            best = ms if best is None else min(best, ms)
+        return nbytes / (best / 1e3) / 1e9
+
+    pcie_gbs = both_ways()
     del slots
 
     hbm, peak_kind = peaks()
@@ -358,6 +382,9 @@ def gpu_arm(args, rank, world, local_rank):
                 "form": f"streamed: {steps_e2e} steps, three-deep pipeline; field uploads, archive round trips, "
                         "kernels and downloads on their own streams, three buffer sets",
                 "ms_per_step": round(e2e_ms, 4),
+                # a step's copies alone at the measured two-way rate: the ceiling of `value`
+                "pcie_both_ways_gbs": round(pcie_gbs, 3),
+                "copy_ceiling": round(world * nbytes / ((nbytes + a_bytes) / (pcie_gbs * 1e9)) / 1e9, 3),
                 "serial": {"value": round(world * nbytes / (e2e_serial / 1e3) / 1e9, 3), "compress_ms": round(e2e_c, 4),
                            "decompress_ms": round(e2e_d, 4)}},
         "gpu_launches": int(launches),

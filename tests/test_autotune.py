@@ -43,19 +43,24 @@ def test_committed_table_is_well_formed():
 
 
 def test_matrix_choice_follows_the_rule():
-    """Entries that timed the precision-form splits choose the fastest one
-    that beats the plain knobs by the margin with an archive at most 2 %
-    larger than the plain one, or none; matrix_choice reads it back."""
+    """Entries that timed the precision-form splits choose the fastest
+    candidate (double fields: the exact slices only) that beats the plain
+    knobs by the margin with an archive at most 2 % larger than the plain
+    one, or none."""
     t = A.load()
     for e in t.get("entries", []):
         if "matrix_forms" not in e:
             continue
+        itemsize = 4 if e["class"]["dtype"] == "f32" else 8
         best = min(e["measured"], key=lambda r: r["compress_ms"] + r["decompress_ms"])
         limit = A.MATRIX_MARGIN * (best["compress_ms"] + best["decompress_ms"])
         ok = sorted((m["compress_ms"] + m["decompress_ms"], f) for f, m in e["matrix_forms"].items()
-                    if m["compress_ms"] + m["decompress_ms"] < limit
+                    if f in A.matrix_candidates(itemsize) and m["compress_ms"] + m["decompress_ms"] < limit
                     and m["archive_bytes"] * A.MATRIX_RATIO <= e["plain_archive_bytes"])
         assert e["choice"]["matrix"] == (ok[0][1] if ok else False)
+        assert A.choose_matrix(e, itemsize) == e["choice"]["matrix"]
+        if itemsize == 8:
+            assert e["choice"]["matrix"] in (False, "matrix-exact")
 
 
 def test_matrix_choice_lookup(tmp_path):
