@@ -19,6 +19,7 @@
 #include "stream.cuh"
 #include "transform.cuh"
 #include "wzp.cuh"
+#include "zlevel.cuh"
 #include "zmatrix.cuh"
 
 #include "../../include/waltz_b200.h"
@@ -227,6 +228,26 @@ static void level(const Src& src, Dims a, const Out& out, Sink& sink) {
         launch_level<T, Inverse, Mask, Tiles<T>::XY[0], Tiles<T>::XY[1], Tiles<T>::XY[2]>(src, a, out, sink);
     else
         launch_level<T, Inverse, Mask, Tiles<T>::Z[0], Tiles<T>::Z[1], Tiles<T>::Z[2]>(src, a, out, sink);
+}
+
+// One Z level of the plane schedule as a per-column register march
+// (ZMarchOp): a warp per 32 columns and run of windows. A single field's
+// runs are halved until the level has about 32 warps per SM (a run's first
+// window reloads the 4 pairs it shares with the run before); many fields fill
+// the GPU together, so each keeps whole columns.
+template <class T, bool Inverse, class Src, class Out>
+static void level_z(const Src& src, Dims a, const Out& out, Sink& sink) {
+    using Op = ZMarchOp<T, Inverse, Src, Out>;
+    using Sh = ZMarchShape<T, Inverse>;
+    const uint32_t wins = (a.z + Sh::W - 1) / Sh::W, tx = (a.x + 31) / 32;
+    const uint64_t cols = uint64_t(tx) * a.y;
+    uint32_t seg = wins;
+    if (!sink.many)
+        while (seg > 1 && cols * ((wins + seg - 1) / seg) < 148ull * 32) seg = (seg + 1) / 2;
+    const uint64_t warps = cols * ((wins + seg - 1) / seg);
+    const uint64_t blocks = (warps + Op::kThreads / 32 - 1) / (Op::kThreads / 32);
+    need(blocks < (1ull << 31), "Waltz: level grid too large");
+    sink.run<Op>(typename Op::Params{src, a, out, seg, tx}, uint32_t(blocks));
 }
 
 // Resident CTAs of a kernel per SM times the SM count, cached per device.
@@ -528,7 +549,7 @@ static void forward(const Geometry& g, const T* in, T* C, T* lowA, T* lowB, T* i
         const Dims a = g.zl[l], lo = halve(a, AZ);
         const bool last = l + 1 == g.lz;
         FwdOut<T> out{zdst, sy, sz, last ? nullptr : lows[l & 1], lo, a, AZ};
-        level<T, false, AZ>(src, a, out, sink);
+        level_z<T, false>(src, a, out, sink);
         src = FwdSrc<T>{lows[l & 1], lo.x, size_t(lo.x) * lo.y};
     }
     if (g.lz) sink.mark("fwd_z");
@@ -641,10 +662,10 @@ static void inverse(const Geometry& g, T* C, T* bank1, T* bank2, const Final& fi
             InvSrc<T> src{zbase, sy, sz, low, halve(a, AZ)};
             if (l > 0) {
                 T* dst = zping[l & 1];
-                level<T, true, AZ>(src, a, StoreOut<T>{dst, a.x, size_t(a.x) * a.y}, sink);
+                level_z<T, true>(src, a, StoreOut<T>{dst, a.x, size_t(a.x) * a.y}, sink);
                 low = dst;
             } else {
-                level<T, true, AZ>(src, a, fin, sink);
+                level_z<T, true>(src, a, fin, sink);
             }
         }
         sink.mark("inv_z");
