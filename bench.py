@@ -870,11 +870,13 @@ def batch_only(dev, lib, args, count=512):
     dec = torch.empty(sum(f.numel() for f in fields), dtype=torch.float32, device=dev)
     if args.batch_config:
         parts = [int(v) for v in args.batch_config.split(":")]
-        knobs = {"mode": parts[0], "width": parts[1], "stage_kernels": parts[2] if len(parts) > 2 else 1}
+        knobs = {"mode": parts[0], "width": parts[1], "stage_kernels": parts[2] if len(parts) > 2 else 1,
+                 "zmarch": parts[3] if len(parts) > 3 else 0}
     else:
         knobs = autotune.lookup(autotune.batch_class(shapes, 4))
     lib.waltz_b200_batch_config(knobs["mode"], knobs["width"])
     lib.waltz_b200_set_option(autotune.OPT_STAGE_KERNELS, int(knobs.get("stage_kernels", 1)))
+    lib.waltz_b200_set_option(autotune.OPT_ZMARCH_PLANES, int(knobs.get("zmarch", 0)))
     ms = []
     for k in range(args.warmup + max(1, args.steps)):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -1120,7 +1122,7 @@ def main():
                     help="run only the batched form on the uneven-chunk workload (profiler captures)")
     ap.add_argument("--tc-only", action="store_true",
                     help="run only the plain vs tensor-core form comparison at --tc-shape (profiler captures)")
-    ap.add_argument("--batch-config", default=None, metavar="MODE:WIDTH[:STAGE]",
+    ap.add_argument("--batch-config", default=None, metavar="MODE:WIDTH[:STAGE[:ZMARCH]]",
                     help="batch execution form instead of the tuning table's (0 = stage-batched, 1 = field chains, "
                          "2 = work queues; STAGE: whole-stage plane kernels 1 or 0)")
     args = ap.parse_args()

@@ -11,7 +11,9 @@ question and the table can be applied blindly):
    _FWD);
  * batches: the execution form of the batch graph (stage-batched groups,
    the same as persistent work queues, or per-field chains, and their width,
-   waltz_b200_batch_config) and the stage kernels knob;
+   waltz_b200_batch_config), the stage kernels knob and, for stage-batched
+   groups, the forward z-march depth (short ranges give small chunks more
+   CTAs for the price of re-read z halos);
  * the transform form (lifting or one split of the tensor-core matrix form)
    of fields the matrix form serves: every split is timed and the fastest
    one that beats lifting by 3 % with a compression ratio at most 2 % lower
@@ -69,7 +71,8 @@ DEFAULT_BATCH = {"mode": BATCH_FIELDS, "width": 32, "stage_kernels": 1}
 SINGLE_CANDIDATES = [{"stage_kernels": s, "zmarch": z, "small_inv": i, "small_fwd": f}
                      for s in (1, 0) for z in (0, 32) for i in (1 << 15, 1 << 18, 1 << 21)
                      for f in (1 << 20, 1 << 21, 1 << 24, 1 << 26)]
-BATCH_CANDIDATES = ([{"mode": BATCH_STAGES, "width": w, "stage_kernels": s} for w in (1, 4, 16) for s in (1, 0)] +
+BATCH_CANDIDATES = ([{"mode": BATCH_STAGES, "width": w, "stage_kernels": s, "zmarch": z}
+                     for w in (1, 4, 16) for s in (1, 0) for z in (0, 16, 32)] +
                     [{"mode": BATCH_QUEUE, "width": w, "stage_kernels": s} for w in (1, 4, 16) for s in (1, 0)] +
                     [{"mode": BATCH_FIELDS, "width": w, "stage_kernels": s} for w in (16, 32, 64) for s in (1, 0)])
 
@@ -141,7 +144,7 @@ def apply_single(lib, shape, itemsize):
 def apply_batch(lib, shapes, itemsize):
     k = lookup(batch_class(shapes, itemsize))
     lib.waltz_b200_batch_config(int(k["mode"]), int(k["width"]))
-    set_single(lib, {"stage_kernels": int(k.get("stage_kernels", 1))})
+    set_single(lib, {"stage_kernels": int(k.get("stage_kernels", 1)), "zmarch": int(k.get("zmarch", 0))})
     return k
 
 
@@ -220,7 +223,7 @@ def _tune_batch(torch, lib, fields, label, reps, rel=1e-3):
     results = []
     for cand in BATCH_CANDIDATES:
         lib.waltz_b200_batch_config(cand["mode"], cand["width"])
-        set_single(lib, {"stage_kernels": cand["stage_kernels"]})
+        set_single(lib, {"stage_kernels": cand["stage_kernels"], "zmarch": cand.get("zmarch", 0)})
         arcs = waltz_b200.compress_batch(fields, bounds, out=out, tuned=False)
         tc = _time(torch, lambda: waltz_b200.compress_batch(fields, bounds, out=out, tuned=False), reps)
         td = _time(torch, lambda: waltz_b200.decompress_batch(arcs, shapes, fields[0].dtype, out=dec, tuned=False),
