@@ -527,6 +527,17 @@ def _form_entries(dev, lib, f, eb, steps, ref_gpu):
             torch.cuda.synchronize()
             tc.append(ev[0].elapsed_time(ev[1]))
             td.append(ev[1].elapsed_time(ev[2]))
+        # per-stage device times of one more compress + decompress (profiling on)
+        lib.waltz_b200_profile(1)
+        stage = {}
+        times, names = (C.c_double * 16)(), (C.c_char_p * 16)()
+        size = comp()
+        for i in range(lib.waltz_b200_stage_times(times, names, 16)):
+            stage["compress:" + names[i].decode()] = round(times[i], 4)
+        dec(size)
+        for i in range(lib.waltz_b200_stage_times(times, names, 16)):
+            stage["decompress:" + names[i].decode()] = round(times[i], 4)
+        lib.waltz_b200_profile(0)
         header = arch[:32].cpu().numpy().tobytes()
         err = float((out.double() - f.double()).abs().max())
         assert err <= eb, f"{form} form violates the bound: {err} > {eb}"
@@ -534,7 +545,7 @@ def _form_entries(dev, lib, f, eb, steps, ref_gpu):
                        "decompress_gbs": round(nbytes / (statistics.median(td) / 1e3) / 1e9, 3),
                        "compression_ratio": round(nbytes / size, 4),
                        "repair_records": int.from_bytes(header[24:28], "little"),
-                       "max_abs_error": err, "abs_bound": eb}
+                       "max_abs_error": err, "abs_bound": eb, "stage_ms": stage}
         if form == "plain":
             plain_arch = arch[:size].clone()
     if "compression_ratio" in entry["plain"]:

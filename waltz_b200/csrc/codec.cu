@@ -935,6 +935,23 @@ static void zmatrix_apply(const T* x, uint32_t nx, uint32_t ny, uint32_t nz, boo
         const ZmPlan P = ZmPlan::make(nz);
         const float* bhi = reinterpret_cast<const float*>(base + e.off[dir][0]);
         const float* blo = bhi + size_t(P.np) * P.kp;
+        // float fields: planes staged by TMA (the plane stride meets the copy
+        // engine's 16-byte rule because nx * ny is a multiple of 4)
+        if constexpr (sizeof(T) == 4) {
+            const ZmTmaPlan Q = ZmTmaPlan::make(nz);
+            CUtensorMap xmap;
+            if (make_map_3d<float>(&xmap, x, ncols, nz, 1, ncols, ncols * nz, kZmCols, Q.kc, 1)) {
+                sink.direct([=](cudaStream_t stream) {
+                    auto kernel = zmatrix_tma_kernel<Out>;
+                    unsigned grid = 0;
+                    zmatrix_launch(kernel, Q.smem(), ZmTmaPlan::make(kZmMaxK).smem(), ncols, stream, grid);
+                    kernel<<<grid, kZmThreads, Q.smem(), stream>>>(xmap, bhi, blo, nz, ncols, out, status, cf);
+                    note_launch();
+                    check(cudaGetLastError(), "matrix kernel launch");
+                });
+                return;
+            }
+        }
         sink.direct([=](cudaStream_t stream) {
             auto kernel = zmatrix_kernel<T, Out>;
             unsigned grid = 0;

@@ -281,6 +281,188 @@ __global__ void __launch_bounds__(kZmThreads, 2)
 
 
 // ---------------------------------------------------------------------------
+// TF32x3 for float fields with the planes staged by TMA. The field (or the
+// coefficients) is a 2-D tensor of nz planes of ncols floats; a work item is
+// (tile of 128 columns, chunk of up to 32 planes), and its box of planes is
+// copied into one of two raw buffers two items ahead of its use, so the
+// copies run while the threads split, the MMAs run and the epilogue stores.
+// The split reads a column of the raw box (consecutive threads on
+// consecutive columns), and from there on every step is zmatrix_kernel's:
+// the same TF32 halves in the same core layout, the same three products per
+// K step into one fp32 tile, the same epilogue, so the output is identical.
+// 97 KB of shared memory at nz <= 64 (two CTAs per SM).
+constexpr int kZmTmaChunk = 32;
+
+struct ZmTmaPlan {
+    uint32_t kp, np, kc;
+    uint32_t raw_bytes, a_bytes, b_bytes;
+    __host__ __device__ static ZmTmaPlan make(uint32_t nz) {
+        ZmTmaPlan p;
+        p.kp = (nz + 7) / 8 * 8;
+        p.np = (nz + 15) / 16 * 16;
+        p.kc = p.kp < uint32_t(kZmTmaChunk) ? p.kp : uint32_t(kZmTmaChunk);
+        p.raw_bytes = p.kc * kZmCols * 4;
+        p.a_bytes = kZmCols * p.kc * 4;
+        p.b_bytes = p.np * p.kp * 4;
+        return p;
+    }
+    // raw boxes, A halves, B halves, four barriers + TMEM slot
+    __host__ __device__ uint32_t smem() const { return 1024 + 2 * raw_bytes + 2 * a_bytes + 2 * b_bytes + 64; }
+};
+
+template <class Out>
+__global__ void __launch_bounds__(kZmThreads, 2)
+    zmatrix_tma_kernel(const __grid_constant__ CUtensorMap xmap, const float* bhi, const float* blo, uint32_t nz,
+                       uint64_t ncols, Out out, uint32_t* status, uint32_t check_finite) {
+    extern __shared__ __align__(1024) unsigned char zt_smem[];
+    const ZmTmaPlan P = ZmTmaPlan::make(nz);
+    unsigned char* base = zt_smem + ((1024 - (smem_u32(zt_smem) & 1023)) & 1023);
+    float* raw = reinterpret_cast<float*>(base);                       // 2 boxes of kc x 128
+    unsigned char* Ahi = base + 2 * P.raw_bytes;
+    unsigned char* Alo = Ahi + P.a_bytes;
+    unsigned char* Bhi = Alo + P.a_bytes;
+    unsigned char* Blo = Bhi + P.b_bytes;
+    uint64_t* mma_bar = reinterpret_cast<uint64_t*>(Blo + P.b_bytes);
+    uint64_t* raw_bar = mma_bar + 1;                                    // two
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_bar + 3);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint64_t tiles = (ncols + kZmCols - 1) / kZmCols;
+    const uint32_t ncols_alloc = P.np <= 32 ? 32 : (P.np <= 64 ? 64 : 128);
+    const uint32_t nch = (P.kp + P.kc - 1) / P.kc;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(ncols_alloc));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    // item i of this CTA: tile blockIdx.x + (i / nch) * gridDim.x, chunk i % nch
+    auto item_tile = [&](uint64_t i) { return uint64_t(blockIdx.x) + (i / nch) * gridDim.x; };
+    auto stage = [&](uint64_t i) { // thread 0: copy item i's planes into raw box i % 2
+        const uint32_t b = uint32_t(i & 1);
+        mbar_expect_tx(raw_bar + b, P.raw_bytes);
+        tma_load_3d(reinterpret_cast<unsigned char*>(raw) + b * P.raw_bytes, &xmap, int(item_tile(i) * kZmCols),
+                    int((i % nch) * P.kc), 0, raw_bar + b);
+    };
+    if (tid == 0) {
+        mbar_init(mma_bar, 1);
+        mbar_init(raw_bar, 1);
+        mbar_init(raw_bar + 1, 1);
+        fence_barrier_init();
+        if (item_tile(0) < tiles) stage(0);
+        if (item_tile(1) < tiles) stage(1);
+    }
+    for (uint32_t i = tid; i < P.b_bytes / 16; i += kZmThreads) {
+        reinterpret_cast<uint4*>(Bhi)[i] = reinterpret_cast<const uint4*>(bhi)[i];
+        reinterpret_cast<uint4*>(Blo)[i] = reinterpret_cast<const uint4*>(blo)[i];
+    }
+    fence_proxy_async();
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t idesc = zm_idesc(P.np);
+    const uint32_t sbo_b = (P.kp / 4) * 128;
+    const int c = tid % kZmCols, half = tid / kZmCols;
+
+    uint32_t mphase = 0;
+    uint64_t staged = 2;   // next item to stage (thread 0)
+    uint64_t consumed = 0; // items whose copy was waited for
+    bool bad = false, stop = false;
+    for (uint64_t i = 0; item_tile(i) < tiles; ++i) {
+        const uint64_t tile = item_tile(i);
+        const uint32_t k0 = uint32_t(i % nch) * P.kc;
+        const uint32_t kc = min(P.kc, P.kp - k0); // planes of this chunk (multiple of 8)
+        const uint32_t sbo_a = (kc / 4) * 128, kh = kc / 2;
+        const uint32_t b = uint32_t(i & 1);
+        if (!__syncthreads_and(warp != 0 || mbar_wait(raw_bar + b, uint32_t((i >> 1) & 1), kWaitBound))) {
+            if (tid == 0) atomicOr(status, ST_WAIT_TIMEOUT);
+            stop = true;
+            break;
+        }
+        consumed = i + 1;
+        // split and transpose from the raw box: element (c, k) of the box
+        // (plane k0 + k) goes to core (c/8, k/4), row c%8, as in zmatrix_kernel
+        {
+            const float* box = raw + size_t(b) * (P.raw_bytes / 4);
+            const uint64_t col = tile * kZmCols + c;
+            unsigned char* hrow = Ahi + (c / 8) * sbo_a + (c % 8) * 16;
+            unsigned char* lrow = Alo + (c / 8) * sbo_a + (c % 8) * 16;
+#pragma unroll
+            for (int j = 0; j < kZmTmaChunk / 2; j += 4) {
+                if (j < int(kh)) {
+                    uint32_t h[4], l[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const uint32_t k = half * kh + j + q;
+                        const float w = box[k * kZmCols + c]; // zero past the field (the copy's fill)
+                        if (check_finite && col < ncols && k0 + k < nz) bad |= !finite_bits(w);
+                        h[q] = __float_as_uint(w) & 0xffffe000u;
+                        l[q] = __float_as_uint(__fsub_rn(w, __uint_as_float(h[q])));
+                    }
+                    const uint32_t kq = (half * kh + j) / 4;
+                    *reinterpret_cast<uint4*>(hrow + kq * 128) = make_uint4(h[0], h[1], h[2], h[3]);
+                    *reinterpret_cast<uint4*>(lrow + kq * 128) = make_uint4(l[0], l[1], l[2], l[3]);
+                }
+            }
+        }
+        fence_proxy_async(); // the raw box's reads before the copy that refills it
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            if (item_tile(staged) < tiles) stage(staged); // item i + 2 into the box just read
+            ++staged;
+            const uint32_t a0 = smem_u32(Ahi), a1 = smem_u32(Alo);
+            const uint32_t b0 = smem_u32(Bhi) + (k0 / 8) * 256, b1 = smem_u32(Blo) + (k0 / 8) * 256;
+            for (uint32_t st = 0; st < kc / 8; ++st) {
+                const uint64_t dah = zm_sdesc(a0 + st * 256, 128, sbo_a, 0);
+                const uint64_t dal = zm_sdesc(a1 + st * 256, 128, sbo_a, 0);
+                const uint64_t dbh = zm_sdesc(b0 + st * 256, 128, sbo_b, 0);
+                const uint64_t dbl = zm_sdesc(b1 + st * 256, 128, sbo_b, 0);
+                zm_mma(tmem, dah, dbh, idesc, (k0 > 0 || st > 0) ? 1u : 0u);
+                zm_mma(tmem, dah, dbl, idesc, 1);
+                zm_mma(tmem, dal, dbh, idesc, 1);
+            }
+            zm_commit(mma_bar);
+        }
+        if (!__syncthreads_and(warp != 0 || mbar_wait(mma_bar, mphase, kWaitBound))) {
+            if (tid == 0) atomicOr(status, ST_WAIT_TIMEOUT);
+            stop = true;
+            break;
+        }
+        mphase ^= 1;
+        if (k0 + P.kc >= P.kp) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t sub = warp % 4;
+            const uint64_t ocol = tile * kZmCols + 32 * sub + lane;
+            for (uint32_t c0 = 16 * (warp / 4); c0 < P.np; c0 += 32) {
+                uint32_t r[16];
+                tmem_ld16(tmem + (uint32_t(32 * sub) << 16) + c0, r);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                float f[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) f[j] = __uint_as_float(r[j]);
+                if (ocol < ncols) out.group(uint32_t(ocol), c0, nz, ncols, f);
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncthreads(); // tensor memory read out: the next tile's MMAs may overwrite it
+        }
+    }
+    if (stop && tid == 0) {
+        // copies still in flight (items consumed .. staged - 1 that exist)
+        // land before the block leaves, each wait bounded
+        for (uint64_t j = consumed; j < staged && item_tile(j) < tiles; ++j)
+            mbar_wait(raw_bar + (j & 1), uint32_t((j >> 1) & 1), kWaitBound);
+    }
+    if (check_finite && __syncthreads_or(bad) && tid == 0) atomicOr(status, ST_NONFINITE_INPUT);
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols_alloc));
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Slice forms, same GEMM D = X^T * Mz^T, same tiling and epilogue layout.
 //
 // BF16x3 (tcgen05.mma kind::f16, bf16 operands, fp32 accumulation): every
