@@ -898,7 +898,7 @@ static thread_local ZMatrixCache t_zmat;
 // exact slices), nx*ny a multiple of 4.
 template <class K>
 static void zmatrix_launch(K kernel, uint32_t smem, uint32_t smem_max, uint64_t ncols, cudaStream_t stream,
-                           unsigned& grid) {
+                           unsigned& grid, uint32_t tmem_cols) {
     static thread_local std::vector<std::pair<const void*, int>> configured;
     int dev = 0;
     check(cudaGetDevice(&dev), "cudaGetDevice");
@@ -909,14 +909,29 @@ static void zmatrix_launch(K kernel, uint32_t smem, uint32_t smem_max, uint64_t 
     if (!seen) {
         check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_max)),
               "matrix kernel shared memory");
+        // the whole unified L1 as shared memory, so that two CTAs of up to
+        // ~113 KB share an SM
+        check(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   int(cudaSharedmemCarveoutMaxShared)),
+              "matrix kernel carveout");
         configured.emplace_back(key, dev);
     }
     const uint64_t tiles = (ncols + kZmCols - 1) / kZmCols;
-    // resident CTAs at this column length's shared memory (one or two per SM)
-    int sms = 0, occ = 0;
+    // resident CTAs at this column length's shared memory: the runtime's
+    // answer, or the count the SM's shared memory and the two-CTA register
+    // budget allow (__launch_bounds__(256, 2)), whichever is larger. A CTA
+    // that does not fit waits for a free SM: the CTAs never wait on one
+    // another, so a larger grid costs nothing but a second wave.
+    int sms = 0, occ = 0, smem_sm = 0, reserved = 0;
     check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
     check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kZmThreads, smem), "occupancy");
-    const uint64_t slots = uint64_t(sms) * uint64_t(occ > 0 ? occ : 1);
+    check(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev), "shared memory per SM");
+    check(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev), "reserved shared memory");
+    const int by_smem = smem_sm / int(smem + uint32_t(reserved));
+    // ... and never more CTAs than the SM's 512 tensor-memory columns hold
+    const int by_tmem = int(512 / std::max<uint32_t>(tmem_cols, 32));
+    const int per_sm = std::min(std::max(occ, std::min(by_smem, 2)), std::max(by_tmem, 1));
+    const uint64_t slots = uint64_t(sms) * uint64_t(per_sm > 0 ? per_sm : 1);
     grid = unsigned(std::min<uint64_t>(tiles, slots));
 }
 
@@ -944,7 +959,8 @@ static void zmatrix_apply(const T* x, uint32_t nx, uint32_t ny, uint32_t nz, boo
                 sink.direct([=](cudaStream_t stream) {
                     auto kernel = zmatrix_tma_kernel<Out>;
                     unsigned grid = 0;
-                    zmatrix_launch(kernel, Q.smem(), ZmTmaPlan::make(kZmMaxK).smem(), ncols, stream, grid);
+                    zmatrix_launch(kernel, Q.smem(), ZmTmaPlan::make(kZmMaxK).smem(), ncols, stream, grid,
+                                   Q.np <= 32 ? 32u : (Q.np <= 64 ? 64u : 128u));
                     kernel<<<grid, kZmThreads, Q.smem(), stream>>>(xmap, bhi, blo, nz, ncols, out, status, cf);
                     note_launch();
                     check(cudaGetLastError(), "matrix kernel launch");
@@ -955,7 +971,8 @@ static void zmatrix_apply(const T* x, uint32_t nx, uint32_t ny, uint32_t nz, boo
         sink.direct([=](cudaStream_t stream) {
             auto kernel = zmatrix_kernel<T, Out>;
             unsigned grid = 0;
-            zmatrix_launch(kernel, P.smem(), ZmPlan::make(kZmMaxK).smem(), ncols, stream, grid);
+            zmatrix_launch(kernel, P.smem(), ZmPlan::make(kZmMaxK).smem(), ncols, stream, grid,
+                           P.np <= 32 ? 32u : (P.np <= 64 ? 64u : 128u));
             kernel<<<grid, kZmThreads, P.smem(), stream>>>(x, bhi, blo, nz, ncols, out, status, cf);
             note_launch();
             check(cudaGetLastError(), "matrix kernel launch");
@@ -971,12 +988,13 @@ static void zmatrix_apply(const T* x, uint32_t nx, uint32_t ny, uint32_t nz, boo
         unsigned grid = 0;
         if (exact) {
             auto kernel = zmatrix_exact_kernel<T, Out>;
-            zmatrix_launch(kernel, P.smem(), ZsPlan::make(kZsExactMaxK, true).smem(), ncols, stream, grid);
+            zmatrix_launch(kernel, P.smem(), ZsPlan::make(kZsExactMaxK, true).smem(), ncols, stream, grid, 512u);
             kernel<<<grid, kZmThreads, P.smem(), stream>>>(x, reinterpret_cast<const int8_t*>(bsl), bscale, nz, ncols,
                                                            out, status, cf);
         } else {
             auto kernel = zmatrix_bf16_kernel<T, Out>;
-            zmatrix_launch(kernel, P.smem(), ZsPlan::make(kZmMaxK, false).smem(), ncols, stream, grid);
+            zmatrix_launch(kernel, P.smem(), ZsPlan::make(kZmMaxK, false).smem(), ncols, stream, grid,
+                           P.np <= 32 ? 32u : (P.np <= 64 ? 64u : 128u));
             kernel<<<grid, kZmThreads, P.smem(), stream>>>(x, reinterpret_cast<const uint16_t*>(bsl), nz, ncols, out,
                                                            status, cf);
         }
