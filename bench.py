@@ -886,8 +886,7 @@ def batch_only(dev, lib, args, count=512):
     else:
         knobs = autotune.lookup(autotune.batch_class(shapes, 4))
     lib.waltz_b200_batch_config(knobs["mode"], knobs["width"])
-    lib.waltz_b200_set_option(autotune.OPT_STAGE_KERNELS, int(knobs.get("stage_kernels", 1)))
-    lib.waltz_b200_set_option(autotune.OPT_ZMARCH_PLANES, int(knobs.get("zmarch", 0)))
+    autotune.set_single(lib, autotune.batch_single_knobs(knobs))
     ms = []
     for k in range(args.warmup + max(1, args.steps)):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -519,7 +519,7 @@ def test_tuning_knobs_never_change_the_bytes():
         ref = [waltz_b200.compress_tensor(f, eb, tuned=False) for f, eb in zip(fields, bounds)]
         for k in A.BATCH_CANDIDATES:
             assert lib.waltz_b200_batch_config(k["mode"], k["width"]) == 0
-            assert lib.waltz_b200_set_option(A.OPT_STAGE_KERNELS, k["stage_kernels"]) == 0
+            A.set_single(lib, A.batch_single_knobs(k))
             arcs = waltz_b200.compress_batch(fields, bounds, tuned=False)
             assert all(torch.equal(a, r) for a, r in zip(arcs, ref)), k
             dec = waltz_b200.decompress_batch(arcs, [tuple(f.shape) for f in fields], torch.float32, tuned=False)

@@ -13,7 +13,8 @@ question and the table can be applied blindly):
    the same as persistent work queues, or per-field chains, and their width,
    waltz_b200_batch_config), the stage kernels knob and, for stage-batched
    groups, the forward z-march depth (short ranges give small chunks more
-   CTAs for the price of re-read z halos);
+   CTAs for the price of re-read z halos) and tensor-map staging on every
+   level (the small-level thresholds at 0);
  * the transform form (lifting or one split of the tensor-core matrix form)
    of fields the matrix form serves: every split is timed and the fastest
    one that beats lifting by 3 % with a compression ratio at most 2 % lower
@@ -71,8 +72,9 @@ DEFAULT_BATCH = {"mode": BATCH_FIELDS, "width": 32, "stage_kernels": 1}
 SINGLE_CANDIDATES = [{"stage_kernels": s, "zmarch": z, "small_inv": i, "small_fwd": f}
                      for s in (1, 0) for z in (0, 32) for i in (1 << 15, 1 << 18, 1 << 21)
                      for f in (1 << 20, 1 << 21, 1 << 24, 1 << 26)]
-BATCH_CANDIDATES = ([{"mode": BATCH_STAGES, "width": w, "stage_kernels": s, "zmarch": z}
-                     for w in (1, 4, 16) for s in (1, 0) for z in (0, 16, 32)] +
+BATCH_CANDIDATES = ([{"mode": BATCH_STAGES, "width": w, "stage_kernels": s, "zmarch": z, "small_inv": si, "small_fwd": sf}
+                     for w in (1, 4, 16) for s in (1, 0) for z in (0, 16, 32)
+                     for si, sf in ((1 << 15, 1 << 20), (0, 0))] +
                     [{"mode": BATCH_QUEUE, "width": w, "stage_kernels": s} for w in (1, 4, 16) for s in (1, 0)] +
                     [{"mode": BATCH_FIELDS, "width": w, "stage_kernels": s} for w in (16, 32, 64) for s in (1, 0)])
 
@@ -144,8 +146,15 @@ def apply_single(lib, shape, itemsize):
 def apply_batch(lib, shapes, itemsize):
     k = lookup(batch_class(shapes, itemsize))
     lib.waltz_b200_batch_config(int(k["mode"]), int(k["width"]))
-    set_single(lib, {"stage_kernels": int(k.get("stage_kernels", 1)), "zmarch": int(k.get("zmarch", 0))})
+    set_single(lib, batch_single_knobs(k))
     return k
+
+
+def batch_single_knobs(k):
+    """The single-field knobs a batch entry sets (missing ones: defaults)."""
+    return {"stage_kernels": int(k.get("stage_kernels", 1)), "zmarch": int(k.get("zmarch", 0)),
+            "small_inv": int(k.get("small_inv", DEFAULT_SINGLE["small_inv"])),
+            "small_fwd": int(k.get("small_fwd", DEFAULT_SINGLE["small_fwd"]))}
 
 
 def matrix_choice(shape, itemsize, path=TABLE):
@@ -223,7 +232,7 @@ def _tune_batch(torch, lib, fields, label, reps, rel=1e-3):
     results = []
     for cand in BATCH_CANDIDATES:
         lib.waltz_b200_batch_config(cand["mode"], cand["width"])
-        set_single(lib, {"stage_kernels": cand["stage_kernels"], "zmarch": cand.get("zmarch", 0)})
+        set_single(lib, batch_single_knobs(cand))
         arcs = waltz_b200.compress_batch(fields, bounds, out=out, tuned=False)
         tc = _time(torch, lambda: waltz_b200.compress_batch(fields, bounds, out=out, tuned=False), reps)
         td = _time(torch, lambda: waltz_b200.decompress_batch(arcs, shapes, fields[0].dtype, out=dec, tuned=False),
