@@ -42,11 +42,32 @@ template <class T, bool Inverse, class Src, class Out> struct ZMarchOp {
 // coefficient (inverse: even positions from the low half, odd ones from the
 // high half) of spatial position z after reflection; `m` is the level's z
 // length.
+// pairs(p0, from, e, o) fills pairs from .. PP-1 of the window whose pair 0
+// starts at spatial position p0: windows inside the column read with one
+// pointer per half and no reflection, edge windows through at().
 template <class T> struct ZColFwd {
     const T* p;   // column base
     size_t s;     // z stride
     uint32_t m;
     __device__ __forceinline__ T at(int64_t z) const { return p[size_t(mirror(z, m)) * s]; }
+    template <int PP> __device__ __forceinline__ void pairs(int64_t p0, int from, T (&e)[PP], T (&o)[PP]) const {
+        if (p0 >= 0 && p0 + 2 * PP <= int64_t(m)) {
+            const T* b = p + size_t(p0) * s;
+#pragma unroll
+            for (int j = 0; j < PP; ++j) {
+                if (j < from) continue;
+                e[j] = b[size_t(2 * j) * s];
+                o[j] = b[size_t(2 * j + 1) * s];
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < PP; ++j) {
+                if (j < from) continue;
+                e[j] = at(p0 + 2 * j);
+                o[j] = at(p0 + 2 * j + 1);
+            }
+        }
+    }
 };
 template <class T> struct ZColInv {
     const T* lo;  // low coefficients: index i at lo[i * ls]
@@ -57,6 +78,27 @@ template <class T> struct ZColInv {
     __device__ __forceinline__ T at(int64_t z) const {
         const uint32_t r = mirror(z, m);
         return (r & 1) ? hi[size_t(r >> 1) * s] : lo[size_t(r >> 1) * ls];
+    }
+    template <int PP> __device__ __forceinline__ void pairs(int64_t p0, int from, T (&e)[PP], T (&o)[PP]) const {
+        if (p0 >= 0 && p0 + 2 * PP <= int64_t(m)) {
+            // p0 is even: pair j's even sample is low coefficient p0/2 + j,
+            // its odd one high coefficient p0/2 + j
+            const T* lb = lo + size_t(p0 >> 1) * ls;
+            const T* hb = hi + size_t(p0 >> 1) * s;
+#pragma unroll
+            for (int j = 0; j < PP; ++j) {
+                if (j < from) continue;
+                e[j] = lb[size_t(j) * ls];
+                o[j] = hb[size_t(j) * s];
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < PP; ++j) {
+                if (j < from) continue;
+                e[j] = at(p0 + 2 * j);
+                o[j] = at(p0 + 2 * j + 1);
+            }
+        }
     }
 };
 
@@ -105,22 +147,14 @@ __device__ __forceinline__ void ZMarchOp<T, Inverse, Src, Out>::run(const Params
         const int64_t p0 = int64_t(w) * W - 4; // spatial position of pair 0's even sample
         T e[PP], o[PP];
         if (w == w0) {
-#pragma unroll
-            for (int j = 0; j < PP; ++j) {
-                e[j] = col.at(p0 + 2 * j);
-                o[j] = col.at(p0 + 2 * j + 1);
-            }
+            col.template pairs<PP>(p0, 0, e, o);
         } else {
 #pragma unroll
             for (int j = 0; j < KEEP; ++j) {
                 e[j] = ke[j];
                 o[j] = ko[j];
             }
-#pragma unroll
-            for (int j = KEEP; j < PP; ++j) {
-                e[j] = col.at(p0 + 2 * j);
-                o[j] = col.at(p0 + 2 * j + 1);
-            }
+            col.template pairs<PP>(p0, KEEP, e, o);
         }
 #pragma unroll
         for (int j = 0; j < KEEP; ++j) {
