@@ -509,7 +509,9 @@ def test_tuning_knobs_never_change_the_bytes():
             f = torch.from_numpy(S.power_law_field(shape, 3).astype(dt)).cuda()
             ref = waltz_b200.compress_tensor(f, 1e-3, tuned=False)
             dref = waltz_b200.decompress_tensor(ref, shape, f.dtype, tuned=False)
-            for k in A.SINGLE_CANDIDATES + [{"small_inv": 0, "small_fwd": 0}, {"small_inv": 1 << 30, "small_fwd": 1 << 30}]:
+            extra = [{"small_inv": 0, "small_fwd": 0}, {"small_inv": 1 << 30, "small_fwd": 1 << 30},
+                     {"xy_march": 1}, {"xy_march": 1, "stage_kernels": 0}, {"xy_march": 1, "small_inv": 0}]
+            for k in A.SINGLE_CANDIDATES + extra:
                 A.set_single(lib, k)
                 arc = waltz_b200.compress_tensor(f, 1e-3, tuned=False)
                 assert torch.equal(arc, ref), (shape, k)

@@ -13,8 +13,9 @@ question and the table can be applied blindly):
    the same as persistent work queues, or per-field chains, and their width,
    waltz_b200_batch_config), the stage kernels knob and, for stage-batched
    groups, the forward z-march depth (short ranges give small chunks more
-   CTAs for the price of re-read z halos) and tensor-map staging on every
-   level (the small-level thresholds at 0);
+   CTAs for the price of re-read z halos), tensor-map staging on every
+   level (the small-level thresholds at 0) and the plane XY levels as the
+   warp march (WALTZ_B200_OPT_XY_MARCH; single plane fields try it too);
  * the transform form (lifting or one split of the tensor-core matrix form)
    of fields the matrix form serves: every split is timed and the fastest
    one that beats lifting by 3 % with a compression ratio at most 2 % lower
@@ -40,8 +41,9 @@ from pathlib import Path
 TABLE = Path(__file__).with_name("tuning.json")
 
 OPT_STAGE_KERNELS, OPT_ZMARCH_PLANES, OPT_SMALL_LEVEL, OPT_SMALL_FWD = 1, 2, 3, 4
+OPT_XY_MARCH = 6
 BATCH_STAGES, BATCH_FIELDS, BATCH_QUEUE = 0, 1, 2
-DEFAULT_SINGLE = {"stage_kernels": 1, "zmarch": 0, "small_inv": 1 << 15, "small_fwd": 1 << 20}
+DEFAULT_SINGLE = {"stage_kernels": 1, "zmarch": 0, "small_inv": 1 << 15, "small_fwd": 1 << 20, "xy_march": 0}
 MATRIX_MARGIN = 0.97  # the matrix form changes the header flag: take it only for a clear gain
 MATRIX_RATIO = 0.98   # ... and only when its archive stays within 2 % of the plain one's size
 MATRIX_SPLITS = ("matrix-tf32", "matrix-bf16", "matrix-exact")
@@ -72,9 +74,10 @@ DEFAULT_BATCH = {"mode": BATCH_FIELDS, "width": 32, "stage_kernels": 1}
 SINGLE_CANDIDATES = [{"stage_kernels": s, "zmarch": z, "small_inv": i, "small_fwd": f}
                      for s in (1, 0) for z in (0, 32) for i in (1 << 15, 1 << 18, 1 << 21)
                      for f in (1 << 20, 1 << 21, 1 << 24, 1 << 26)]
-BATCH_CANDIDATES = ([{"mode": BATCH_STAGES, "width": w, "stage_kernels": s, "zmarch": z, "small_inv": si, "small_fwd": sf}
+BATCH_CANDIDATES = ([{"mode": BATCH_STAGES, "width": w, "stage_kernels": s, "zmarch": z, "small_inv": si, "small_fwd": sf,
+                      "xy_march": xy}
                      for w in (1, 4, 16) for s in (1, 0) for z in (0, 16, 32)
-                     for si, sf in ((1 << 15, 1 << 20), (0, 0))] +
+                     for si, sf in ((1 << 15, 1 << 20), (0, 0)) for xy in (0, 1)] +
                     [{"mode": BATCH_QUEUE, "width": w, "stage_kernels": s} for w in (1, 4, 16) for s in (1, 0)] +
                     [{"mode": BATCH_FIELDS, "width": w, "stage_kernels": s} for w in (16, 32, 64) for s in (1, 0)])
 
@@ -136,6 +139,7 @@ def set_single(lib, k):
     lib.waltz_b200_set_option(OPT_ZMARCH_PLANES, int(k["zmarch"]))
     lib.waltz_b200_set_option(OPT_SMALL_LEVEL, int(k["small_inv"]))
     lib.waltz_b200_set_option(OPT_SMALL_FWD, int(k["small_fwd"]))
+    lib.waltz_b200_set_option(OPT_XY_MARCH, int(k["xy_march"]))
     return k
 
 
@@ -154,7 +158,8 @@ def batch_single_knobs(k):
     """The single-field knobs a batch entry sets (missing ones: defaults)."""
     return {"stage_kernels": int(k.get("stage_kernels", 1)), "zmarch": int(k.get("zmarch", 0)),
             "small_inv": int(k.get("small_inv", DEFAULT_SINGLE["small_inv"])),
-            "small_fwd": int(k.get("small_fwd", DEFAULT_SINGLE["small_fwd"]))}
+            "small_fwd": int(k.get("small_fwd", DEFAULT_SINGLE["small_fwd"])),
+            "xy_march": int(k.get("xy_march", 0))}
 
 
 def matrix_choice(shape, itemsize, path=TABLE):
@@ -187,7 +192,11 @@ def _tune_single(torch, lib, shape, dtype, reps, rel=1e-3):
     eb = rel * (hi - lo)
     itemsize = f.element_size()
     results = []
-    for cand in SINGLE_CANDIDATES:
+    # plane fields also try their XY levels as the warp march
+    cands = SINGLE_CANDIDATES
+    if single_class(shape, itemsize)["schedule"] == "plane":
+        cands = cands + [{**c, "xy_march": 1} for c in SINGLE_CANDIDATES]
+    for cand in cands:
         set_single(lib, cand)
         arc = waltz_b200.compress_tensor(f, eb, tuned=False)
         tc = _time(torch, lambda: waltz_b200.compress_tensor(f, eb, tuned=False), reps)

@@ -19,6 +19,7 @@
 #include "stream.cuh"
 #include "transform.cuh"
 #include "wzp.cuh"
+#include "xylevel.cuh"
 #include "zlevel.cuh"
 #include "zmatrix.cuh"
 
@@ -207,6 +208,7 @@ struct Options {
     uint64_t small_fwd = uint64_t(1) << 20;   // forward levels of at most this many samples: direct staging,
                                               // short z ranges (measured on 128^3 .. 512^3 fields)
     uint32_t repair_scale = 0; // compact repair section (WPW1) with step eb / scale: 0 (off), 16 or 64
+    bool xy_march = false;     // plane schedule: XY levels as the warp march instead of the staged kernels
 };
 static thread_local Options t_opt;
 
@@ -245,6 +247,25 @@ static void level_z(const Src& src, Dims a, const Out& out, Sink& sink) {
     if (!sink.many)
         while (seg > 1 && cols * ((wins + seg - 1) / seg) < 148ull * 32) seg = (seg + 1) / 2;
     const uint64_t warps = cols * ((wins + seg - 1) / seg);
+    const uint64_t blocks = (warps + Op::kThreads / 32 - 1) / (Op::kThreads / 32);
+    need(blocks < (1ull << 31), "Waltz: level grid too large");
+    sink.run<Op>(typename Op::Params{src, a, out, seg, tx}, uint32_t(blocks));
+}
+
+// One XY level of the plane schedule as a warp march (XYMarchOp, taken with
+// WALTZ_B200_OPT_XY_MARCH): a warp per strip of 24 x, plane and run of Y
+// windows; runs halved for a single field until the level has about 32
+// warps per SM, as for the Z levels.
+template <class T, bool Inverse, class Src, class Out>
+static void level_xy(const Src& src, Dims a, const Out& out, Sink& sink) {
+    using Op = XYMarchOp<T, Inverse, Src, Out>;
+    using Sh = XYMarchShape<T, Inverse>;
+    const uint32_t wins = (a.y + Sh::W - 1) / Sh::W, tx = (a.x + Sh::U - 1) / Sh::U;
+    const uint64_t strips = uint64_t(tx) * a.z;
+    uint32_t seg = wins;
+    if (!sink.many)
+        while (seg > 1 && strips * ((wins + seg - 1) / seg) < 148ull * 32) seg = (seg + 1) / 2;
+    const uint64_t warps = strips * ((wins + seg - 1) / seg);
     const uint64_t blocks = (warps + Op::kThreads / 32 - 1) / (Op::kThreads / 32);
     need(blocks < (1ull << 31), "Waltz: level grid too large");
     sink.run<Op>(typename Op::Params{src, a, out, seg, tx}, uint32_t(blocks));
@@ -563,7 +584,8 @@ static void forward(const Geometry& g, const T* in, T* C, T* lowA, T* lowB, T* i
         const Dims a = g.xyl[l], lo = halve(a, AX | AY);
         const bool last = l + 1 == g.lxy;
         FwdOut<T> out{C, sy, sz, last ? nullptr : lows[l & 1], lo, a, AX | AY};
-        level_fwd_stream<T, false>(src, a, out, status, sink);
+        if (t_opt.xy_march) level_xy<T, false>(src, a, out, sink);
+        else level_fwd_stream<T, false>(src, a, out, status, sink);
         src = FwdSrc<T>{lows[l & 1], lo.x, size_t(lo.x) * lo.y};
     }
     if (g.lxy) sink.mark("fwd_xy");
@@ -635,14 +657,19 @@ static void inverse(const Geometry& g, T* C, T* bank1, T* bank2, const Final& fi
             InvSrc<T> src{C, sy, sz, low, halve(a, AX | AY)};
             if (l > 0) {
                 T* dst = halves[l & 1];
-                level_inv_xy<T>(src, a, StoreOut<T>{dst, a.x, size_t(a.x) * a.y}, status, sink);
+                const StoreOut<T> to{dst, a.x, size_t(a.x) * a.y};
+                if (t_opt.xy_march) level_xy<T, true>(src, a, to, sink);
+                else level_inv_xy<T>(src, a, to, status, sink);
                 low = dst;
             } else if (g.lz) {
-                level_inv_xy<T>(src, a, StoreOut<T>{bank1, sy, sz}, status, sink);
+                const StoreOut<T> to{bank1, sy, sz};
+                if (t_opt.xy_march) level_xy<T, true>(src, a, to, sink);
+                else level_inv_xy<T>(src, a, to, status, sink);
                 zbase = bank1;
                 zping[1] = C; // the coefficients are no longer read
             } else {
-                level_inv_xy<T>(src, a, fin, status, sink);
+                if (t_opt.xy_march) level_xy<T, true>(src, a, fin, sink);
+                else level_inv_xy<T>(src, a, fin, status, sink);
             }
         }
         sink.mark("inv_xy");
@@ -1818,6 +1845,7 @@ static void compress_batch(const waltz_b200_chunk* items, uint32_t count, uint64
     append_key(key, t_opt.zmarch);
     append_key(key, t_opt.small_level);
     append_key(key, t_opt.small_fwd);
+    append_key(key, t_opt.xy_march);
     char* base = st.scratch.reserve(total);
     append_key(key, base); // the scratch must not have moved since the graph was captured
     uint64_t* results = reinterpret_cast<uint64_t*>(base + results_at);
@@ -1995,6 +2023,7 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
     append_key(key, t_opt.zmarch);
     append_key(key, t_opt.small_level);
     append_key(key, t_opt.small_fwd);
+    append_key(key, t_opt.xy_march);
     append_key(key, count);
     append_key(key, static_cast<const void*>(P.jobs));
     for (uint32_t i = 0; i < count; ++i) {
@@ -2144,6 +2173,10 @@ int waltz_b200_set_option(int option, int value) {
     case WALTZ_B200_OPT_COMPACT_REPAIRS:
         if (value != 0 && value != 16 && value != 64) break;
         t_opt.repair_scale = uint32_t(value);
+        return 0;
+    case WALTZ_B200_OPT_XY_MARCH:
+        if (value != 0 && value != 1) break;
+        t_opt.xy_march = value != 0;
         return 0;
     default:
         break;
