@@ -4,8 +4,8 @@
 // Device side: one elected thread arms the barrier with the expected byte
 // count and issues the copies; every thread waits on the barrier's phase with
 // an iteration bound, after which the block agrees (barrier vote) to stop and
-// records ST_WAIT_TIMEOUT instead of hanging. Copies are plain (no cluster
-// multicast): every CTA reads its own boxes.
+// records ST_WAIT_TIMEOUT instead of hanging. Copies are plain, one CTA
+// each: every CTA reads its own boxes into its own shared memory.
 // Host side: tensor maps are encoded with the driver's cuTensorMapEncodeTiled,
 // reached through the runtime's driver entry point (no link-time libcuda).
 #pragma once

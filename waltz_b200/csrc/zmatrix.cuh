@@ -22,7 +22,7 @@
 //     coefficient) and writes it back z-major, or hands it to an emitter.
 // One thread issues the MMAs and commits them to an mbarrier; every wait is
 // bounded and a block that gives up records ST_WAIT_TIMEOUT, frees its tensor
-// memory and returns. Nothing here multicasts.
+// memory and returns. Every copy and load targets only this CTA.
 #pragma once
 #include "common.cuh"
 
