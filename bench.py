@@ -1069,7 +1069,8 @@ def reference_arm(args):
     from oracle import oracle as O
     from waltz_b200.synthetic import power_law_field
     kind = "reference" if O.ref_available() else "port"
-    field = power_law_field(SHAPE, SEED)
+    shape = tuple(args.shape)
+    field = power_law_field(shape, SEED)
     eb = REL * (float(field.max()) - float(field.min()))
     codec = _codec(kind)
     times = []
@@ -1103,13 +1104,14 @@ def reference_arm(args):
         done = sum(pool.map(work, range(len(blocks))))
         par = done / (time.perf_counter() - t0) / 1e9
     backend = "AVX2 backend" if kind == "reference" else "C port"
-    sample = (f"f32 512^3 field as one archive, one compress + decompress per step, reference CPU codec "
+    dims = "x".join(str(d) for d in shape[::-1])
+    sample = (f"f32 {dims} field as one archive, one compress + decompress per step, reference CPU codec "
               f"({backend}), 1 thread (the codec has none of its own)")
     return {"metric": METRIC, "value": round(value, 4), "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(step * 1e3, 2), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "f32 512x512x512 (z,y,x) k^-11/3 GRF seed 1, REL 1e-3, one archive, "
-                                   "step = compress + decompress",
+            "config": {"workload": f"f32 {'x'.join(str(d) for d in shape)} (z,y,x) k^-11/3 GRF seed 1, REL 1e-3, "
+                                   "one archive, step = compress + decompress",
                        "parallelism": "1 host thread"},
             "impl": "reference",
             "cpu_baseline": {"value": round(value, 4), "unit": "GB/s", "cores": 1, "kind": kind, "sample": sample},
