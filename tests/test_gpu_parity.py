@@ -561,14 +561,16 @@ def test_unaligned_archive_addresses():
             assert torch.equal(out, waltz_b200.decompress_tensor(ref, shape, f.dtype))
 
 
+@pytest.mark.parametrize("xy_march", [0, 1])
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 @pytest.mark.parametrize("nxyz", [(64, 40, 100), (200, 17, 9), (9, 11, 65), (48, 32, 9), (33, 31, 130),
                                   (72, 80, 24), (40, 36, 257)])
-def test_plane_schedule_per_level_z_matches_oracle(nxyz, dtype):
+def test_plane_schedule_per_level_z_matches_oracle(nxyz, dtype, xy_march):
     """Plane-schedule fields with the whole-stage kernels off: every Z level
     runs as the per-column register march (forward and inverse, ragged last
-    windows, reflection at both ends); transforms, archives and decodes equal
-    the oracle's."""
+    windows, reflection at both ends), and the XY levels as the staged
+    kernels or, with the knob, the warp march (X across lanes); transforms,
+    archives and decodes equal the oracle's."""
     import torch
     import waltz_b200
     from waltz_b200 import autotune as A
@@ -579,6 +581,7 @@ def test_plane_schedule_per_level_z_matches_oracle(nxyz, dtype):
     g = S.power_law_field(P.zyx(nxyz), 7).astype(dtype)
     eb = 1e-4 * (float(g.max()) - float(g.min()))
     assert lib.waltz_b200_set_option(A.OPT_STAGE_KERNELS, 0) == 0
+    assert lib.waltz_b200_set_option(A.OPT_XY_MARCH, xy_march) == 0
     try:
         f = gpu_transform(a, inverse=False)
         assert f.tobytes() == O.transform(a, inverse=False).tobytes()
@@ -591,3 +594,4 @@ def test_plane_schedule_per_level_z_matches_oracle(nxyz, dtype):
         assert out.tobytes() == O.decompress(host, g.shape, dtype).tobytes()
     finally:
         lib.waltz_b200_set_option(A.OPT_STAGE_KERNELS, 1)
+        lib.waltz_b200_set_option(A.OPT_XY_MARCH, 0)
