@@ -510,7 +510,8 @@ def test_tuning_knobs_never_change_the_bytes():
             ref = waltz_b200.compress_tensor(f, 1e-3, tuned=False)
             dref = waltz_b200.decompress_tensor(ref, shape, f.dtype, tuned=False)
             extra = [{"small_inv": 0, "small_fwd": 0}, {"small_inv": 1 << 30, "small_fwd": 1 << 30},
-                     {"xy_march": 1}, {"xy_march": 1, "stage_kernels": 0}, {"xy_march": 1, "small_inv": 0}]
+                     {"xy_march": 1}, {"xy_march": 2}, {"xy_march": 3, "stage_kernels": 0},
+                     {"xy_march": 3, "small_inv": 0}]
             for k in A.SINGLE_CANDIDATES + extra:
                 A.set_single(lib, k)
                 arc = waltz_b200.compress_tensor(f, 1e-3, tuned=False)
@@ -561,7 +562,7 @@ def test_unaligned_archive_addresses():
             assert torch.equal(out, waltz_b200.decompress_tensor(ref, shape, f.dtype))
 
 
-@pytest.mark.parametrize("xy_march", [0, 1])
+@pytest.mark.parametrize("xy_march", [0, 3])
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 @pytest.mark.parametrize("nxyz", [(64, 40, 100), (200, 17, 9), (9, 11, 65), (48, 32, 9), (33, 31, 130),
                                   (72, 80, 24), (40, 36, 257)])

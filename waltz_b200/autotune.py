@@ -15,7 +15,8 @@ question and the table can be applied blindly):
    groups, the forward z-march depth (short ranges give small chunks more
    CTAs for the price of re-read z halos), tensor-map staging on every
    level (the small-level thresholds at 0) and the plane XY levels as the
-   warp march (WALTZ_B200_OPT_XY_MARCH; single plane fields try it too);
+   warp march, forward and inverse levels separately
+   (WALTZ_B200_OPT_XY_MARCH bits 0 and 1; single plane fields try it too);
  * the transform form (lifting or one split of the tensor-core matrix form)
    of fields the matrix form serves: every split is timed and the fastest
    one that beats lifting by 3 % with a compression ratio at most 2 % lower
@@ -77,7 +78,7 @@ SINGLE_CANDIDATES = [{"stage_kernels": s, "zmarch": z, "small_inv": i, "small_fw
 BATCH_CANDIDATES = ([{"mode": BATCH_STAGES, "width": w, "stage_kernels": s, "zmarch": z, "small_inv": si, "small_fwd": sf,
                       "xy_march": xy}
                      for w in (1, 4, 16) for s in (1, 0) for z in (0, 16, 32)
-                     for si, sf in ((1 << 15, 1 << 20), (0, 0)) for xy in (0, 1)] +
+                     for si, sf in ((1 << 15, 1 << 20), (0, 0)) for xy in (0, 1, 2, 3)] +
                     [{"mode": BATCH_QUEUE, "width": w, "stage_kernels": s} for w in (1, 4, 16) for s in (1, 0)] +
                     [{"mode": BATCH_FIELDS, "width": w, "stage_kernels": s} for w in (16, 32, 64) for s in (1, 0)])
 
@@ -195,7 +196,7 @@ def _tune_single(torch, lib, shape, dtype, reps, rel=1e-3):
     # plane fields also try their XY levels as the warp march
     cands = SINGLE_CANDIDATES
     if single_class(shape, itemsize)["schedule"] == "plane":
-        cands = cands + [{**c, "xy_march": 1} for c in SINGLE_CANDIDATES]
+        cands = cands + [{**c, "xy_march": xy} for xy in (1, 2, 3) for c in SINGLE_CANDIDATES]
     for cand in cands:
         set_single(lib, cand)
         arc = waltz_b200.compress_tensor(f, eb, tuned=False)

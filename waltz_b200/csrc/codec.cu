@@ -208,7 +208,8 @@ struct Options {
     uint64_t small_fwd = uint64_t(1) << 20;   // forward levels of at most this many samples: direct staging,
                                               // short z ranges (measured on 128^3 .. 512^3 fields)
     uint32_t repair_scale = 0; // compact repair section (WPW1) with step eb / scale: 0 (off), 16 or 64
-    bool xy_march = false;     // plane schedule: XY levels as the warp march instead of the staged kernels
+    uint32_t xy_march = 0;     // plane schedule: XY levels as the warp march instead of the staged kernels
+                               // (bit 0: forward levels, bit 1: inverse levels)
 };
 static thread_local Options t_opt;
 
@@ -584,7 +585,7 @@ static void forward(const Geometry& g, const T* in, T* C, T* lowA, T* lowB, T* i
         const Dims a = g.xyl[l], lo = halve(a, AX | AY);
         const bool last = l + 1 == g.lxy;
         FwdOut<T> out{C, sy, sz, last ? nullptr : lows[l & 1], lo, a, AX | AY};
-        if (t_opt.xy_march) level_xy<T, false>(src, a, out, sink);
+        if (t_opt.xy_march & 1u) level_xy<T, false>(src, a, out, sink);
         else level_fwd_stream<T, false>(src, a, out, status, sink);
         src = FwdSrc<T>{lows[l & 1], lo.x, size_t(lo.x) * lo.y};
     }
@@ -658,17 +659,17 @@ static void inverse(const Geometry& g, T* C, T* bank1, T* bank2, const Final& fi
             if (l > 0) {
                 T* dst = halves[l & 1];
                 const StoreOut<T> to{dst, a.x, size_t(a.x) * a.y};
-                if (t_opt.xy_march) level_xy<T, true>(src, a, to, sink);
+                if (t_opt.xy_march & 2u) level_xy<T, true>(src, a, to, sink);
                 else level_inv_xy<T>(src, a, to, status, sink);
                 low = dst;
             } else if (g.lz) {
                 const StoreOut<T> to{bank1, sy, sz};
-                if (t_opt.xy_march) level_xy<T, true>(src, a, to, sink);
+                if (t_opt.xy_march & 2u) level_xy<T, true>(src, a, to, sink);
                 else level_inv_xy<T>(src, a, to, status, sink);
                 zbase = bank1;
                 zping[1] = C; // the coefficients are no longer read
             } else {
-                if (t_opt.xy_march) level_xy<T, true>(src, a, fin, sink);
+                if (t_opt.xy_march & 2u) level_xy<T, true>(src, a, fin, sink);
                 else level_inv_xy<T>(src, a, fin, status, sink);
             }
         }
@@ -2175,8 +2176,8 @@ int waltz_b200_set_option(int option, int value) {
         t_opt.repair_scale = uint32_t(value);
         return 0;
     case WALTZ_B200_OPT_XY_MARCH:
-        if (value != 0 && value != 1) break;
-        t_opt.xy_march = value != 0;
+        if (value < 0 || value > 3) break;
+        t_opt.xy_march = uint32_t(value);
         return 0;
     default:
         break;
