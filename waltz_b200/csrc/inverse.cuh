@@ -119,6 +119,16 @@ __device__ __forceinline__ void InvTileOp<T, UX, UY, UZ, Out>::run(const Params&
         }
     }
     __syncthreads(); // the barriers are initialised before any thread polls them
+    // the emitter's own operands (the originals, for repairs): one thread per
+    // tile row of UX samples (one 128-byte line) asks L2 for it now, so the
+    // Y pass's fetches find it there
+    if constexpr (Out::kPrefetch) {
+        static_assert(UZ * UY <= kThreads && UX * sizeof(T) == 128, "one line per tile row and thread");
+        if (tid < UZ * UY) {
+            const uint32_t gy = oy + tid % UY, gz = oz + tid / UY;
+            if (gy < a.y && gz < a.z) out.warm(ox, gy, gz);
+        }
+    }
     // ---- edge tiles: every box first, then the out-of-range cells from
     // their reflections
     const bool edge = ox < 4 || ox + UX + 4 > a.x || oy < 4 || oy + UY + 4 > a.y || oz < 4 || oz + UZ + 4 > a.z;

@@ -199,6 +199,10 @@ template <class T> struct RepairOut {
     __device__ __forceinline__ T fetch(uint32_t x, uint32_t y, uint32_t z) const {
         return __ldg(orig + size_t(z) * sz + size_t(y) * sy + x);
     }
+    // asks L2 for the line holding original (x, y, z) ahead of its fetch
+    __device__ __forceinline__ void warm(uint32_t x, uint32_t y, uint32_t z) const {
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(orig + size_t(z) * sz + size_t(y) * sy + x));
+    }
     __device__ __forceinline__ void emit(uint32_t x, uint32_t y, uint32_t z, T v, T o) const {
         const T err = Lift<T>::sub(v, o);
         const bool patched = fabs(err) > nb;
