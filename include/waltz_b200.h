@@ -144,10 +144,11 @@ int waltz_b200_decompress_batch(const waltz_b200_archive* archives, uint32_t cou
 #define WALTZ_B200_OPT_COMPACT_REPAIRS 5
 /* WALTZ_B200_OPT_XY_MARCH (0 default; bit 0: forward levels, bit 1:
  *   inverse levels): plane schedule, run those XY levels that the
- *   whole-stage kernels do not take as a warp march (a warp per strip of 24 x
- *   and plane walking down y in registers, X lifted across its lanes by
- *   shuffles) instead of the shared-memory staged kernels. A performance
- *   knob like the others: the bytes do not change. */
+ *   whole-stage kernels do not take as a warp march (a warp per strip of 56 x
+ *   and plane walking down y in registers, each lane holding an even/odd pair
+ *   and X lifted across the lanes by shuffles) instead of the shared-memory
+ *   staged kernels. A performance knob like the others: the bytes do not
+ *   change. */
 #define WALTZ_B200_OPT_XY_MARCH 6
 int waltz_b200_set_option(int option, int value);
 

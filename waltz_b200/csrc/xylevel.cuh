@@ -1,15 +1,18 @@
 // One XY level of the plane schedule as a warp march in registers.
 //
-// A warp owns a strip of 32 consecutive x (24 outputs and a 4-sample halo
+// A warp owns a strip of 64 consecutive x (56 outputs and a 4-sample halo
 // per side) on one z plane, and marches down y through a run of Y windows;
-// a lane keeps its column's window in registers, exactly as the Z march
-// (zlevel.cuh) does along z, and the X lifting of a row runs across the
-// warp's lanes with shuffles: lane l holds spatial x = x0 + l (x0 even), so
-// even lanes hold the even samples and odd lanes the odd ones, and every
-// lifting step reads the two neighbours with one shuffle each way. After the
-// four steps lanes 4..27 hold exact results (each output depends only on its
-// 4-sample neighbourhood, the reason the forward analysis and the inverse X
-// synthesis are window independent); lanes 0-3 and 28-31 are the halo.
+// a lane keeps its two columns' windows in registers, exactly as the Z march
+// (zlevel.cuh) does along z. Lane l holds the pair of spatial x = x0 + 2l
+// (even) and x0 + 2l + 1 (odd), x0 even: in the split-band layout that pair
+// is low-half and high-half coefficient x0/2 + l, so a warp reads a
+// coefficient row as two contiguous 128-byte runs. The X lifting of a row
+// runs across the lanes: every lifting step updates one sample of each pair
+// from the other sample of its own pair and one of the neighbouring lane's,
+// one shuffle per step. After the four steps pairs 2..29 hold exact results
+// (each output depends only on its 4-sample neighbourhood, the reason the
+// forward analysis and the inverse X synthesis are window independent);
+// lanes 0-1 and 30-31 are the halo.
 //  * forward (order Y, X): a window's rows are lifted along Y in registers
 //    (windows of 16, any origin gives the same bits), then each output row
 //    along X across the lanes;
@@ -17,9 +20,9 @@
 //    lifted along X across the lanes, then the window along Y in the
 //    canonical folded windows of 8 (origins at multiples of 8,
 //    cpu/src/transform.cpp:110-147).
-// Each lane reads its column of every row it needs once per window (the 4
-// pairs shared with the next window stay in registers); a warp's loads and
-// stores of a row are contiguous, nothing is staged in shared memory.
+// Each lane reads its columns of every row it needs once per window (the 4
+// pairs of rows shared with the next window stay in registers); nothing is
+// staged in shared memory.
 #pragma once
 #include "transform.cuh"
 
@@ -27,44 +30,51 @@ namespace wb {
 
 template <class T, bool Inverse> struct XYMarchShape {
     static constexpr int W = Inverse ? 8 : 16; // Y outputs per window
-    static constexpr int P = W / 2 + 4;        // pairs per window
-    static constexpr int KEEP = 4;             // pairs shared with the next window
-    static constexpr int U = 24;               // x outputs per warp
+    static constexpr int P = W / 2 + 4;        // pairs of rows per window
+    static constexpr int KEEP = 4;             // pairs of rows shared with the next window
+    static constexpr int U = 56;               // x outputs per warp (lanes 2..29, two each)
 };
 
-// Lane-wise lifting of one row held one sample per lane (lane l = spatial
-// x0 + l, x0 even). The step order, operands and operand order are those of
-// lift_forward / lift_inverse<..., false> (common.cuh).
-template <class T> __device__ __forceinline__ T lane_step(T v, T c, bool mine) {
-    const T left = __shfl_up_sync(0xffffffffu, v, 1), right = __shfl_down_sync(0xffffffffu, v, 1);
-    return mine ? Lift<T>::fma(c, Lift<T>::add(left, right), v) : v;
+// Lane-wise lifting of one row held as one (even, odd) pair per lane (lane l
+// = pair x0/2 + l). The step order, operands and operand order are those of
+// lift_forward / lift_inverse<..., false> (common.cuh): an odd update adds
+// the pair's own even sample and the next lane's, an even update the
+// previous lane's odd sample and the pair's own.
+template <class T> __device__ __forceinline__ void pair_odd(T& o, T e, T c) {
+    const T next = __shfl_down_sync(0xffffffffu, e, 1);
+    o = Lift<T>::fma(c, Lift<T>::add(e, next), o);
 }
-template <class T> __device__ __forceinline__ T lane_forward(T v, bool odd) {
-    using L = Lift<T>;
-    v = lane_step(v, K97<T>::a, odd);
-    v = lane_step(v, K97<T>::b, !odd);
-    v = lane_step(v, K97<T>::g, odd);
-    v = lane_step(v, K97<T>::d, !odd);
-    return odd ? L::mul(v, -K97<T>::ik) : L::mul(v, K97<T>::k);
+template <class T> __device__ __forceinline__ void pair_even(T& e, T o, T c) {
+    const T prev = __shfl_up_sync(0xffffffffu, o, 1);
+    e = Lift<T>::fma(c, Lift<T>::add(prev, o), e);
 }
-template <class T> __device__ __forceinline__ T lane_inverse(T v, bool odd) {
+template <class T> __device__ __forceinline__ void pair_forward(T& e, T& o) {
     using L = Lift<T>;
-    v = odd ? L::mul(v, -K97<T>::k) : L::mul(v, K97<T>::ik);
-    v = lane_step(v, -K97<T>::d, !odd);
-    v = lane_step(v, -K97<T>::g, odd);
-    v = lane_step(v, -K97<T>::b, !odd);
-    v = lane_step(v, -K97<T>::a, odd);
-    return v;
+    pair_odd(o, e, K97<T>::a);
+    pair_even(e, o, K97<T>::b);
+    pair_odd(o, e, K97<T>::g);
+    pair_even(e, o, K97<T>::d);
+    e = L::mul(e, K97<T>::k);
+    o = L::mul(o, -K97<T>::ik);
+}
+template <class T> __device__ __forceinline__ void pair_inverse(T& e, T& o) {
+    using L = Lift<T>;
+    e = L::mul(e, K97<T>::ik);
+    o = L::mul(o, -K97<T>::k);
+    pair_even(e, o, -K97<T>::d);
+    pair_odd(o, e, -K97<T>::g);
+    pair_even(e, o, -K97<T>::b);
+    pair_odd(o, e, -K97<T>::a);
 }
 
 template <class T, bool Inverse, class Src, class Out> struct XYMarchOp {
-    static constexpr int kThreads = 256, kMinBlocks = 0; // no occupancy floor: the compiler picks the register budget
+    static constexpr int kThreads = 256, kMinBlocks = 0; // no occupancy floor: a 64-register cap spills
     struct Params {
         Src src;
         Dims a;   // level dims (x, y lifted; z planes)
         Out out;
         uint32_t seg; // Y windows per warp
-        uint32_t tx;  // strips of 24 x
+        uint32_t tx;  // strips of 56 x
     };
     static __device__ __forceinline__ void run(const Params& P, uint32_t block, uint32_t);
 };
@@ -83,94 +93,115 @@ __device__ __forceinline__ void XYMarchOp<T, Inverse, Src, Out>::run(const Param
     const uint32_t xs = uint32_t(warp % Pm.tx);
     const uint64_t rest = warp / Pm.tx;
     const uint32_t sg = uint32_t(rest % nseg), z = uint32_t(rest / nseg);
-    const int64_t x = int64_t(xs) * Sh::U - 4 + lane; // x0 = 24 xs - 4 is even: odd lanes hold odd x
-    const bool odd = (lane & 1) != 0;
-    const bool live = lane >= 4 && lane < 4 + Sh::U && x < int64_t(a.x);
-    const uint32_t mx = mirror(x, a.x);
+    const int64_t xe = int64_t(xs) * Sh::U - 4 + 2 * lane; // this lane's even x; the odd one is xe + 1
+    const bool live = lane >= 2 && lane < 2 + Sh::U / 2;
+    const bool live_e = live && xe < int64_t(a.x), live_o = live && xe + 1 < int64_t(a.x);
+    // columns read for this lane: split-band positions (inverse) or spatial
+    // ones (forward), reflected at the row's ends; inside the row the pair is
+    // low / high coefficient xe / 2 (inverse) or samples xe, xe + 1 (forward)
+    const bool inside = xe >= 0 && xe + 1 < int64_t(a.x);
+    const uint32_t me = inside ? uint32_t(xe) : mirror(xe, a.x), mo = inside ? uint32_t(xe + 1) : mirror(xe + 1, a.x);
+    const uint32_t ce = Inverse ? split_of(me, a.x) : me, co = Inverse ? split_of(mo, a.x) : mo;
     const uint32_t w0 = sg * Pm.seg, w1 = min(w0 + Pm.seg, wins);
 
-    // sample (forward) or coefficient (inverse) of this lane's column at
-    // spatial row p, reflected into the level
-    auto row = [&](int64_t p) -> T {
+    // row p (spatial, reflected into the level) of this lane's two columns
+    auto row = [&](int64_t p, T& ve, T& vo) {
         const uint32_t my = mirror(p, a.y);
         if constexpr (Inverse) {
-            const uint32_t cx = split_of(mx, a.x), cy = split_of(my, a.y);
-            if (src.low && cx < src.lo.x && cy < src.lo.y)
-                return src.low[(size_t(z) * src.lo.y + cy) * src.lo.x + cx];
-            return src.base[size_t(z) * src.sz + size_t(cy) * src.sy + cx];
+            const uint32_t cy = split_of(my, a.y);
+            const T* b = src.base + size_t(z) * src.sz + size_t(cy) * src.sy;
+            const T* l = (src.low && cy < src.lo.y) ? src.low + (size_t(z) * src.lo.y + cy) * src.lo.x : nullptr;
+            ve = (l && ce < src.lo.x) ? l[ce] : b[ce];
+            vo = (l && co < src.lo.x) ? l[co] : b[co];
         } else {
-            return src.p[size_t(z) * src.sz + size_t(my) * src.sy + mx];
+            const T* b = src.p + size_t(z) * src.sz + size_t(my) * src.sy;
+            ve = b[ce];
+            vo = b[co];
         }
     };
     bool bad = false;
-    T ke[KEEP], ko[KEEP]; // pairs the next window shares (inverse: already lifted along X)
+    T ke[KEEP][2], ko[KEEP][2]; // pairs of rows the next window shares (inverse: already lifted along X)
     for (uint32_t w = w0; w < w1; ++w) {
         const int64_t p0 = int64_t(w) * W - 4; // spatial row of pair 0's even row
-        T e[PP], o[PP];
+        T e[PP][2], o[PP][2];                  // [row pair][even / odd column]
         const int from = w == w0 ? 0 : KEEP;
         if (from) {
 #pragma unroll
             for (int j = 0; j < KEEP; ++j) {
-                e[j] = ke[j];
-                o[j] = ko[j];
+                e[j][0] = ke[j][0], e[j][1] = ke[j][1];
+                o[j][0] = ko[j][0], o[j][1] = ko[j][1];
             }
         }
 #pragma unroll
         for (int j = 0; j < PP; ++j) {
             if (j < from) continue;
-            e[j] = row(p0 + 2 * j);
-            o[j] = row(p0 + 2 * j + 1);
+            row(p0 + 2 * j, e[j][0], e[j][1]);
+            row(p0 + 2 * j + 1, o[j][0], o[j][1]);
         }
         if constexpr (Inverse) {
             // X first: every newly loaded coefficient row across the lanes
 #pragma unroll
             for (int j = 0; j < PP; ++j) {
                 if (j < from) continue;
-                e[j] = lane_inverse(e[j], odd);
-                o[j] = lane_inverse(o[j], odd);
+                pair_inverse(e[j][0], e[j][1]);
+                pair_inverse(o[j][0], o[j][1]);
             }
         } else if (src.status) {
 #pragma unroll
             for (int j = 0; j < PP; ++j) {
                 if (j < from) continue;
-                bad |= !finite_bits(e[j]) || !finite_bits(o[j]);
+                bad |= !finite_bits(e[j][0]) || !finite_bits(e[j][1]) || !finite_bits(o[j][0]) ||
+                       !finite_bits(o[j][1]);
             }
         }
 #pragma unroll
         for (int j = 0; j < KEEP; ++j) {
-            ke[j] = e[PP - KEEP + j];
-            ko[j] = o[PP - KEEP + j];
+            ke[j][0] = e[PP - KEEP + j][0], ke[j][1] = e[PP - KEEP + j][1];
+            ko[j][0] = o[PP - KEEP + j][0], ko[j][1] = o[PP - KEEP + j][1];
         }
         const uint32_t y0 = w * W;
-        if constexpr (Inverse) {
-            T pre[W];
-            if constexpr (Out::kPrefetch) {
 #pragma unroll
-                for (int k = 0; k < W; ++k)
-                    pre[k] = (live && y0 + k < a.y) ? out.fetch(uint32_t(x), y0 + k, z) : T(0);
-            }
-            lift_inverse<T, PP, true>(e, o);
+        for (int c = 0; c < 2; ++c) {
+            // one column of the pair along Y, in registers
+            T ye[PP], yo[PP];
+#pragma unroll
+            for (int j = 0; j < PP; ++j) ye[j] = e[j][c], yo[j] = o[j][c];
+            if constexpr (Inverse) lift_inverse<T, PP, true>(ye, yo);
+            else lift_forward<T, PP>(ye, yo);
+#pragma unroll
+            for (int j = 0; j < PP; ++j) e[j][c] = ye[j], o[j][c] = yo[j];
+        }
+        if constexpr (Inverse) {
+            const uint32_t x = uint32_t(xe);
             if (live) {
 #pragma unroll
                 for (int j = 2; j < PP - 2; ++j) {
                     const uint32_t y = y0 + 2 * (j - 2);
-                    if constexpr (Out::kPrefetch) {
-                        if (y < a.y) out.emit(uint32_t(x), y, z, e[j], pre[2 * (j - 2)]);
-                        if (y + 1 < a.y) out.emit(uint32_t(x), y + 1, z, o[j], pre[2 * (j - 2) + 1]);
-                    } else {
-                        if (y < a.y) out(uint32_t(x), y, z, e[j]);
-                        if (y + 1 < a.y) out(uint32_t(x), y + 1, z, o[j]);
+                    if (y < a.y) {
+                        if (live_e) out(x, y, z, e[j][0]);
+                        if (live_o) out(x + 1, y, z, e[j][1]);
+                    }
+                    if (y + 1 < a.y) {
+                        if (live_e) out(x, y + 1, z, o[j][0]);
+                        if (live_o) out(x + 1, y + 1, z, o[j][1]);
                     }
                 }
             }
         } else {
-            lift_forward<T, PP>(e, o); // Y, in registers
+            const uint32_t x = uint32_t(xe);
 #pragma unroll
             for (int j = 2; j < PP - 2; ++j) {
                 const uint32_t y = y0 + 2 * (j - 2);
-                const T ve = lane_forward(e[j], odd), vo = lane_forward(o[j], odd); // X, across the lanes
-                if (live && y < a.y) out(uint32_t(x), y, z, ve);
-                if (live && y + 1 < a.y) out(uint32_t(x), y + 1, z, vo);
+                pair_forward(e[j][0], e[j][1]); // X, across the lanes
+                pair_forward(o[j][0], o[j][1]);
+                if (y < a.y) {
+                    if (live_e) out(x, y, z, e[j][0]);
+                    if (live_o) out(x + 1, y, z, e[j][1]);
+                }
+                if (y + 1 < a.y) {
+                    if (live_e) out(x, y + 1, z, o[j][0]);
+                    if (live_o) out(x + 1, y + 1, z, o[j][1]);
+                }
             }
         }
     }
