@@ -14,8 +14,9 @@
 // forward analysis and the inverse X synthesis are window independent);
 // lanes 0-1 and 30-31 are the halo.
 //  * forward (order Y, X): a window's rows are lifted along Y in registers
-//    (windows of 16, any origin gives the same bits), then each output row
-//    along X across the lanes;
+//    (windows of 8, any size and origin give the same bits; 8 keeps the
+//    registers to about 80, three CTAs per SM), then each output row along X
+//    across the lanes;
 //  * inverse (order X, Y): every coefficient row a window loads is first
 //    lifted along X across the lanes, then the window along Y in the
 //    canonical folded windows of 8 (origins at multiples of 8,
@@ -24,12 +25,14 @@
 // pairs of rows shared with the next window stay in registers); nothing is
 // staged in shared memory.
 #pragma once
+#include <limits>
+
 #include "transform.cuh"
 
 namespace wb {
 
 template <class T, bool Inverse> struct XYMarchShape {
-    static constexpr int W = Inverse ? 8 : 16; // Y outputs per window
+    static constexpr int W = 8;                // Y outputs per window
     static constexpr int P = W / 2 + 4;        // pairs of rows per window
     static constexpr int KEEP = 4;             // pairs of rows shared with the next window
     static constexpr int U = 56;               // x outputs per warp (lanes 2..29, two each)
@@ -68,7 +71,7 @@ template <class T> __device__ __forceinline__ void pair_inverse(T& e, T& o) {
 }
 
 template <class T, bool Inverse, class Src, class Out> struct XYMarchOp {
-    static constexpr int kThreads = 256, kMinBlocks = 0; // no occupancy floor: a 64-register cap spills
+    static constexpr int kThreads = 256, kMinBlocks = 0; // no occupancy floor: about 80 registers, three CTAs per SM
     struct Params {
         Src src;
         Dims a;   // level dims (x, y lifted; z planes)
@@ -78,6 +81,18 @@ template <class T, bool Inverse, class Src, class Out> struct XYMarchOp {
     };
     static __device__ __forceinline__ void run(const Params& P, uint32_t block, uint32_t);
 };
+
+// Emitters that store a level row as one contiguous run take per-row
+// pointers; the others take each sample through their own operator().
+template <class Out> struct RowStore {
+    static constexpr bool value = false;
+};
+template <class T> struct RowStore<StoreOut<T>> {
+    static constexpr bool value = true;
+};
+
+// Not finite (NaN or infinite): one compare of the magnitude.
+template <class T> __device__ __forceinline__ bool nonfinite(T v) { return !(fabs(v) <= std::numeric_limits<T>::max()); }
 
 template <class T, bool Inverse, class Src, class Out>
 __device__ __forceinline__ void XYMarchOp<T, Inverse, Src, Out>::run(const Params& Pm, uint32_t block, uint32_t) {
@@ -96,25 +111,43 @@ __device__ __forceinline__ void XYMarchOp<T, Inverse, Src, Out>::run(const Param
     const int64_t xe = int64_t(xs) * Sh::U - 4 + 2 * lane; // this lane's even x; the odd one is xe + 1
     const bool live = lane >= 2 && lane < 2 + Sh::U / 2;
     const bool live_e = live && xe < int64_t(a.x), live_o = live && xe + 1 < int64_t(a.x);
+    const uint32_t hx = half_len(a.x), hy = half_len(a.y);
     // columns read for this lane: split-band positions (inverse) or spatial
     // ones (forward), reflected at the row's ends; inside the row the pair is
-    // low / high coefficient xe / 2 (inverse) or samples xe, xe + 1 (forward)
+    // low / high coefficient xe / 2 (inverse) or samples xe, xe + 1 (forward).
+    // Reflection keeps parity, so the even column is always a low-half
+    // coefficient and the odd one a high-half one.
     const bool inside = xe >= 0 && xe + 1 < int64_t(a.x);
     const uint32_t me = inside ? uint32_t(xe) : mirror(xe, a.x), mo = inside ? uint32_t(xe + 1) : mirror(xe + 1, a.x);
     const uint32_t ce = Inverse ? split_of(me, a.x) : me, co = Inverse ? split_of(mo, a.x) : mo;
     const uint32_t w0 = sg * Pm.seg, w1 = min(w0 + Pm.seg, wins);
 
-    // row p (spatial, reflected into the level) of this lane's two columns
+    // the plane's rows: inverse, coefficient row cy of the base array (and of
+    // the compact low band for cy < hy, the even rows); forward, sample row y
+    const T* plane;
+    const T* lplane = nullptr;
+    size_t rs, lrs = 0; // row strides
+    if constexpr (Inverse) {
+        plane = src.base + size_t(z) * src.sz;
+        rs = src.sy;
+        if (src.low) {
+            lplane = src.low + size_t(z) * src.lo.y * src.lo.x;
+            lrs = src.lo.x;
+        }
+    } else {
+        plane = src.p + size_t(z) * src.sz;
+        rs = src.sy;
+    }
+    // the two columns of spatial row p, reflected into the level
     auto row = [&](int64_t p, T& ve, T& vo) {
         const uint32_t my = mirror(p, a.y);
         if constexpr (Inverse) {
             const uint32_t cy = split_of(my, a.y);
-            const T* b = src.base + size_t(z) * src.sz + size_t(cy) * src.sy;
-            const T* l = (src.low && cy < src.lo.y) ? src.low + (size_t(z) * src.lo.y + cy) * src.lo.x : nullptr;
-            ve = (l && ce < src.lo.x) ? l[ce] : b[ce];
-            vo = (l && co < src.lo.x) ? l[co] : b[co];
+            const T* b = plane + size_t(cy) * rs;
+            ve = (lplane && cy < hy) ? lplane[size_t(cy) * lrs + ce] : b[ce];
+            vo = b[co];
         } else {
-            const T* b = src.p + size_t(z) * src.sz + size_t(my) * src.sy;
+            const T* b = plane + size_t(my) * rs;
             ve = b[ce];
             vo = b[co];
         }
@@ -132,11 +165,40 @@ __device__ __forceinline__ void XYMarchOp<T, Inverse, Src, Out>::run(const Param
                 o[j][0] = ko[j][0], o[j][1] = ko[j][1];
             }
         }
+        if (p0 >= 0 && p0 + 2 * PP <= int64_t(a.y)) {
+            // a window inside the level: no reflection; inverse, pair j's even
+            // row is coefficient row p0/2 + j and its odd row hy + p0/2 + j
+            if constexpr (Inverse) {
+                const uint32_t r0 = uint32_t(p0) >> 1;
+                const T* be = plane + size_t(r0) * rs;
+                const T* bo = plane + size_t(hy + r0) * rs;
+                const T* le = lplane ? lplane + size_t(r0) * lrs : nullptr;
 #pragma unroll
-        for (int j = 0; j < PP; ++j) {
-            if (j < from) continue;
-            row(p0 + 2 * j, e[j][0], e[j][1]);
-            row(p0 + 2 * j + 1, o[j][0], o[j][1]);
+                for (int j = 0; j < PP; ++j) {
+                    if (j < from) continue;
+                    e[j][0] = le ? le[size_t(j) * lrs + ce] : be[size_t(j) * rs + ce];
+                    e[j][1] = be[size_t(j) * rs + co];
+                    o[j][0] = bo[size_t(j) * rs + ce];
+                    o[j][1] = bo[size_t(j) * rs + co];
+                }
+            } else {
+                const T* b = plane + size_t(p0) * rs;
+#pragma unroll
+                for (int j = 0; j < PP; ++j) {
+                    if (j < from) continue;
+                    e[j][0] = b[size_t(2 * j) * rs + ce];
+                    e[j][1] = b[size_t(2 * j) * rs + co];
+                    o[j][0] = b[size_t(2 * j + 1) * rs + ce];
+                    o[j][1] = b[size_t(2 * j + 1) * rs + co];
+                }
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < PP; ++j) {
+                if (j < from) continue;
+                row(p0 + 2 * j, e[j][0], e[j][1]);
+                row(p0 + 2 * j + 1, o[j][0], o[j][1]);
+            }
         }
         if constexpr (Inverse) {
             // X first: every newly loaded coefficient row across the lanes
@@ -150,8 +212,7 @@ __device__ __forceinline__ void XYMarchOp<T, Inverse, Src, Out>::run(const Param
 #pragma unroll
             for (int j = 0; j < PP; ++j) {
                 if (j < from) continue;
-                bad |= !finite_bits(e[j][0]) || !finite_bits(e[j][1]) || !finite_bits(o[j][0]) ||
-                       !finite_bits(o[j][1]);
+                bad |= nonfinite(e[j][0]) || nonfinite(e[j][1]) || nonfinite(o[j][0]) || nonfinite(o[j][1]);
             }
         }
 #pragma unroll
@@ -171,29 +232,42 @@ __device__ __forceinline__ void XYMarchOp<T, Inverse, Src, Out>::run(const Param
 #pragma unroll
             for (int j = 0; j < PP; ++j) e[j][c] = ye[j], o[j][c] = yo[j];
         }
-        if constexpr (Inverse) {
-            const uint32_t x = uint32_t(xe);
-            if (live) {
+        const uint32_t x = uint32_t(xe);
 #pragma unroll
-                for (int j = 2; j < PP - 2; ++j) {
-                    const uint32_t y = y0 + 2 * (j - 2);
-                    if (y < a.y) {
-                        if (live_e) out(x, y, z, e[j][0]);
-                        if (live_o) out(x + 1, y, z, e[j][1]);
-                    }
-                    if (y + 1 < a.y) {
-                        if (live_e) out(x, y + 1, z, o[j][0]);
-                        if (live_o) out(x + 1, y + 1, z, o[j][1]);
-                    }
-                }
-            }
-        } else {
-            const uint32_t x = uint32_t(xe);
-#pragma unroll
-            for (int j = 2; j < PP - 2; ++j) {
-                const uint32_t y = y0 + 2 * (j - 2);
+        for (int j = 2; j < PP - 2; ++j) {
+            const uint32_t y = y0 + 2 * (j - 2); // even; the pair's odd row is y + 1
+            if constexpr (!Inverse) {
                 pair_forward(e[j][0], e[j][1]); // X, across the lanes
                 pair_forward(o[j][0], o[j][1]);
+                // an XY level's split positions: x even -> xe / 2, odd ->
+                // hx + xe / 2; y even -> y / 2 (the all-even corner to the
+                // compact low band when there is one), odd -> hy + y / 2
+                const size_t ye_row = size_t(z) * out.sz + size_t(y >> 1) * out.sy;
+                const size_t yo_row = size_t(z) * out.sz + size_t(hy + (y >> 1)) * out.sy;
+                const uint32_t cxe = x >> 1, cxo = hx + (x >> 1);
+                if (y < a.y) {
+                    if (live_e) {
+                        if (out.low) out.low[(size_t(z) * out.lo.y + (y >> 1)) * out.lo.x + cxe] = e[j][0];
+                        else out.dst[ye_row + cxe] = e[j][0];
+                    }
+                    if (live_o) out.dst[ye_row + cxo] = e[j][1];
+                }
+                if (y + 1 < a.y) {
+                    if (live_e) out.dst[yo_row + cxe] = o[j][0];
+                    if (live_o) out.dst[yo_row + cxo] = o[j][1];
+                }
+            } else if constexpr (RowStore<Out>::value) {
+                T* re = out.dst + size_t(z) * out.sz + size_t(y) * out.sy + x;
+                T* ro = re + out.sy;
+                if (y < a.y) {
+                    if (live_e) re[0] = e[j][0];
+                    if (live_o) re[1] = e[j][1];
+                }
+                if (y + 1 < a.y) {
+                    if (live_e) ro[0] = o[j][0];
+                    if (live_o) ro[1] = o[j][1];
+                }
+            } else {
                 if (y < a.y) {
                     if (live_e) out(x, y, z, e[j][0]);
                     if (live_o) out(x + 1, y, z, e[j][1]);
