@@ -214,12 +214,12 @@ __device__ __forceinline__ void lift_inverse(T (&e)[P], T (&o)[P]) {
     for (int j = 2; j < P - 2; ++j) o[j] = L::fma(-K97<T>::a, L::add(e[j], e[j + 1]), o[j]);
 }
 
+// Finite (neither NaN nor infinite): the magnitude compares at most the
+// largest finite value, one compare (a NaN compares false).
 template <class T> __device__ __forceinline__ bool finite_bits(T v);
-template <> __device__ __forceinline__ bool finite_bits<float>(float v) {
-    return (__float_as_uint(v) & 0x7f800000u) != 0x7f800000u;
-}
+template <> __device__ __forceinline__ bool finite_bits<float>(float v) { return fabsf(v) <= 3.40282346638528859812e+38f; }
 template <> __device__ __forceinline__ bool finite_bits<double>(double v) {
-    return (__double_as_longlong(v) & 0x7ff0000000000000ll) != 0x7ff0000000000000ll;
+    return fabs(v) <= 1.79769313486231570815e+308;
 }
 
 // |value - original| <= bound on the exact difference: the double difference

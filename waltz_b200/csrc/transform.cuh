@@ -91,6 +91,16 @@ template <class T> struct StoreOut {
     }
 };
 
+// Emitters whose samples sit at dst + z * sz + y * sy + x take pointers
+// computed once per row or column; the others take each sample through
+// their own operator().
+template <class Out> struct RowStore {
+    static constexpr bool value = false;
+};
+template <class T> struct RowStore<StoreOut<T>> {
+    static constexpr bool value = true;
+};
+
 template <int Mask, int U, int Axis> struct Ext {
     static constexpr int value = (Mask & Axis) ? U + 8 : U;
 };

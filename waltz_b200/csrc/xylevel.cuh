@@ -25,8 +25,6 @@
 // pairs of rows shared with the next window stay in registers); nothing is
 // staged in shared memory.
 #pragma once
-#include <limits>
-
 #include "transform.cuh"
 
 namespace wb {
@@ -81,18 +79,6 @@ template <class T, bool Inverse, class Src, class Out> struct XYMarchOp {
     };
     static __device__ __forceinline__ void run(const Params& P, uint32_t block, uint32_t);
 };
-
-// Emitters that store a level row as one contiguous run take per-row
-// pointers; the others take each sample through their own operator().
-template <class Out> struct RowStore {
-    static constexpr bool value = false;
-};
-template <class T> struct RowStore<StoreOut<T>> {
-    static constexpr bool value = true;
-};
-
-// Not finite (NaN or infinite): one compare of the magnitude.
-template <class T> __device__ __forceinline__ bool nonfinite(T v) { return !(fabs(v) <= std::numeric_limits<T>::max()); }
 
 template <class T, bool Inverse, class Src, class Out>
 __device__ __forceinline__ void XYMarchOp<T, Inverse, Src, Out>::run(const Params& Pm, uint32_t block, uint32_t) {
@@ -212,7 +198,8 @@ __device__ __forceinline__ void XYMarchOp<T, Inverse, Src, Out>::run(const Param
 #pragma unroll
             for (int j = 0; j < PP; ++j) {
                 if (j < from) continue;
-                bad |= nonfinite(e[j][0]) || nonfinite(e[j][1]) || nonfinite(o[j][0]) || nonfinite(o[j][1]);
+                bad |= !finite_bits(e[j][0]) || !finite_bits(e[j][1]) || !finite_bits(o[j][0]) ||
+                       !finite_bits(o[j][1]);
             }
         }
 #pragma unroll

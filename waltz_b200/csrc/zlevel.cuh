@@ -186,6 +186,10 @@ __device__ __forceinline__ void ZMarchOp<T, Inverse, Src, Out>::run(const Params
                     if constexpr (Out::kPrefetch) {
                         if (z < m) out.emit(x, y, z, e[j], pre[2 * (j - 2)]);
                         if (z + 1 < m) out.emit(x, y, z + 1, o[j], pre[2 * (j - 2) + 1]);
+                    } else if constexpr (RowStore<Out>::value) {
+                        T* const c = out.dst + size_t(z) * out.sz + size_t(y) * out.sy + x;
+                        if (z < m) c[0] = e[j];
+                        if (z + 1 < m) c[out.sz] = o[j];
                     } else {
                         if (z < m) out(x, y, z, e[j]);
                         if (z + 1 < m) out(x, y, z + 1, o[j]);
@@ -195,11 +199,21 @@ __device__ __forceinline__ void ZMarchOp<T, Inverse, Src, Out>::run(const Params
         } else {
             lift_forward<T, PP>(e, o);
             if (live) {
+                // a Z level's split positions (the output's mask is AZ):
+                // even z -> z / 2, in the compact low band when there is
+                // one; odd z -> hz + z / 2
+                T* const cd = out.dst + size_t(y) * out.sy + x;
+                T* const cl = out.low ? out.low + size_t(y) * out.lo.x + x : nullptr;
+                const size_t ls = size_t(out.lo.x) * out.lo.y;
+                const uint32_t hz = half_len(m);
 #pragma unroll
                 for (int j = 2; j < PP - 2; ++j) {
                     const uint32_t z = z0 + 2 * (j - 2);
-                    if (z < m) out(x, y, z, e[j]);
-                    if (z + 1 < m) out(x, y, z + 1, o[j]);
+                    if (z < m) {
+                        if (cl) cl[size_t(z >> 1) * ls] = e[j];
+                        else cd[size_t(z >> 1) * out.sz] = e[j];
+                    }
+                    if (z + 1 < m) cd[size_t(hz + (z >> 1)) * out.sz] = o[j];
                 }
             }
         }
