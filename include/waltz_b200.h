@@ -150,6 +150,12 @@ int waltz_b200_decompress_batch(const waltz_b200_archive* archives, uint32_t cou
  *   staged kernels. A performance knob like the others: the bytes do not
  *   change. */
 #define WALTZ_B200_OPT_XY_MARCH 6
+/* WALTZ_B200_OPT_SMALL_MARCH (samples, default 0 = none): dyadic inverse
+ *   levels of at most this many samples run as two register marches (the Z
+ *   synthesis, then the X and Y synthesis) instead of the tile inverse, whose
+ *   tiles cannot fill the GPU on small levels. A performance knob like the
+ *   others: the bytes do not change. */
+#define WALTZ_B200_OPT_SMALL_MARCH 7
 int waltz_b200_set_option(int option, int value);
 
 #define WALTZ_B200_BATCH_STAGES 0

@@ -511,7 +511,7 @@ def test_tuning_knobs_never_change_the_bytes():
             dref = waltz_b200.decompress_tensor(ref, shape, f.dtype, tuned=False)
             extra = [{"small_inv": 0, "small_fwd": 0}, {"small_inv": 1 << 30, "small_fwd": 1 << 30},
                      {"xy_march": 1}, {"xy_march": 2}, {"xy_march": 3, "stage_kernels": 0},
-                     {"xy_march": 3, "small_inv": 0}]
+                     {"xy_march": 3, "small_inv": 0}, {"small_march": 1 << 21}, {"small_march": 1 << 30}]
             for k in A.SINGLE_CANDIDATES + extra:
                 A.set_single(lib, k)
                 arc = waltz_b200.compress_tensor(f, 1e-3, tuned=False)
@@ -560,6 +560,38 @@ def test_unaligned_archive_addresses():
             L.checked(lib.waltz_b200_decompress(C.c_void_p(buf.data_ptr() + off), written.value, w, nx, ny, nz,
                                                 C.c_void_p(out.data_ptr()), out.numel() * w, _stream()))
             assert torch.equal(out, waltz_b200.decompress_tensor(ref, shape, f.dtype))
+
+
+@pytest.mark.parametrize("small_march", [1 << 15, 1 << 40])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("nxyz", [(64, 64, 64), (37, 41, 50), (96, 80, 72), (130, 129, 128)])
+def test_dyadic_small_levels_as_marches_match_oracle(nxyz, dtype, small_march):
+    """Dyadic fields whose small inverse levels (every level, with the
+    largest threshold, the finest one's repair and final emitters included)
+    run as a Z march then an XY march instead of the tile inverse:
+    transforms, archives and decodes equal the oracle's."""
+    import torch
+    import waltz_b200
+    from waltz_b200 import autotune as A
+    from waltz_b200 import synthetic as S
+    lib = _lib()
+    rng = np.random.default_rng(sum(nxyz) + 9)
+    a = rng.standard_normal(P.zyx(nxyz)).astype(dtype)
+    g = S.power_law_field(P.zyx(nxyz), 8).astype(dtype)
+    eb = 1e-4 * (float(g.max()) - float(g.min()))
+    assert lib.waltz_b200_set_option(A.OPT_SMALL_MARCH, small_march) == 0
+    try:
+        f = gpu_transform(a, inverse=False)
+        assert f.tobytes() == O.transform(a, inverse=False).tobytes()
+        assert gpu_transform(f, inverse=True).tobytes() == O.transform(f, inverse=True).tobytes()
+        d = torch.from_numpy(g).cuda()
+        arc = waltz_b200.compress_tensor(d, eb, tuned=False)
+        host = arc.cpu().numpy().tobytes()
+        assert host == O.compress(g, eb)
+        out = waltz_b200.decompress_tensor(arc, g.shape, dtype, tuned=False).cpu().numpy()
+        assert out.tobytes() == O.decompress(host, g.shape, dtype).tobytes()
+    finally:
+        lib.waltz_b200_set_option(A.OPT_SMALL_MARCH, 0)
 
 
 @pytest.mark.parametrize("xy_march", [0, 3])

@@ -210,6 +210,7 @@ struct Options {
     uint32_t repair_scale = 0; // compact repair section (WPW1) with step eb / scale: 0 (off), 16 or 64
     uint32_t xy_march = 0;     // plane schedule: XY levels as the warp march instead of the staged kernels
                                // (bit 0: forward levels, bit 1: inverse levels)
+    uint64_t small_march = 0;  // dyadic inverse levels of at most this many samples: Z march + XY march
 };
 static thread_local Options t_opt;
 
@@ -395,6 +396,18 @@ static void level_inv(const InvSrc<T>& src, Dims a, const Out& out, uint32_t* st
     p.out = out;
     p.status = status;
     sink.run<Op>(p, uint32_t(blocks), S::smem);
+}
+
+// One small dyadic inverse level as two register marches: the Z synthesis
+// (ZMarchOp, canonical folded windows) into `tmp` in the level's x/y split
+// layout, then the X and Y synthesis (XYMarchOp, canonical Y windows of 8)
+// to `out`. The passes are the tile inverse's Z, X and Y passes, sample for
+// sample, so the bits are the same; a level whose tiles cannot fill the GPU
+// takes thousands of short warps instead.
+template <class T, class Out>
+static void level_inv_march(const InvSrc<T>& src, Dims a, const Out& out, T* tmp, Sink& sink) {
+    level_z<T, true>(src, a, StoreOut<T>{tmp, a.x, size_t(a.x) * a.y}, sink);
+    level_xy<T, true>(InvSrc<T>{tmp, a.x, size_t(a.x) * a.y, nullptr, Dims{}}, a, out, sink);
 }
 
 // One inverse XY level of the plane schedule from TMA-staged parity boxes
@@ -627,14 +640,20 @@ static void inverse(const Geometry& g, T* C, T* bank1, T* bank2, const Final& fi
         for (int l = int(g.lxy) - 1; l >= 0; --l) {
             const Dims a = g.dyad[l];
             InvSrc<T> src{C, sy, sz, low, halve(a, AX | AY | AZ)};
+            // small levels: two marches through bank1 (unused by the dyadic
+            // schedule) instead of the tile inverse
+            const bool march = vol(a) <= t_opt.small_march;
             if (l > 0) {
                 T* dst = halves[l & 1];
-                level_inv<T>(src, a, StoreOut<T>{dst, a.x, size_t(a.x) * a.y}, status, sink);
+                const StoreOut<T> to{dst, a.x, size_t(a.x) * a.y};
+                if (march) level_inv_march<T>(src, a, to, bank1, sink);
+                else level_inv<T>(src, a, to, status, sink);
                 low = dst;
                 static const char* const kInvNames[5] = {"inv_l0", "inv_l1", "inv_l2", "inv_l3", "inv_l4"};
                 sink.mark(kInvNames[l]);
             } else {
-                level_inv<T>(src, a, fin, status, sink);
+                if (march) level_inv_march<T>(src, a, fin, bank1, sink);
+                else level_inv<T>(src, a, fin, status, sink);
                 sink.mark(final_stage);
             }
         }
@@ -1847,6 +1866,7 @@ static void compress_batch(const waltz_b200_chunk* items, uint32_t count, uint64
     append_key(key, t_opt.small_level);
     append_key(key, t_opt.small_fwd);
     append_key(key, t_opt.xy_march);
+    append_key(key, t_opt.small_march);
     char* base = st.scratch.reserve(total);
     append_key(key, base); // the scratch must not have moved since the graph was captured
     uint64_t* results = reinterpret_cast<uint64_t*>(base + results_at);
@@ -2025,6 +2045,7 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
     append_key(key, t_opt.small_level);
     append_key(key, t_opt.small_fwd);
     append_key(key, t_opt.xy_march);
+    append_key(key, t_opt.small_march);
     append_key(key, count);
     append_key(key, static_cast<const void*>(P.jobs));
     for (uint32_t i = 0; i < count; ++i) {
@@ -2178,6 +2199,10 @@ int waltz_b200_set_option(int option, int value) {
     case WALTZ_B200_OPT_XY_MARCH:
         if (value < 0 || value > 3) break;
         t_opt.xy_march = uint32_t(value);
+        return 0;
+    case WALTZ_B200_OPT_SMALL_MARCH:
+        if (value < 0) break;
+        t_opt.small_march = uint64_t(value);
         return 0;
     default:
         break;

@@ -124,7 +124,10 @@ __device__ __forceinline__ void ZMarchOp<T, Inverse, Src, Out>::run(const Params
             const Src& s = Pm.src;
             const size_t off = size_t(y) * s.sy + xs;
             ZColInv<T> c;
-            if (s.low) {
+            // the compact low band holds the z-even half of the columns it
+            // covers: every column of a plane-schedule Z level, the x/y-low
+            // corner of a dyadic level
+            if (s.low && xs < s.lo.x && y < s.lo.y) {
                 c.lo = s.low + size_t(y) * s.lo.x + xs;
                 c.ls = size_t(s.lo.x) * s.lo.y;
             } else {
