@@ -156,6 +156,10 @@ int waltz_b200_decompress_batch(const waltz_b200_archive* archives, uint32_t cou
  *   tiles cannot fill the GPU on small levels. A performance knob like the
  *   others: the bytes do not change. */
 #define WALTZ_B200_OPT_SMALL_MARCH 7
+/* WALTZ_B200_OPT_SMALL_MARCH_FWD (samples, default 0 = none): the same for
+ *   dyadic forward levels (the Y and X analysis as the warp march, then the
+ *   Z analysis as the register march). */
+#define WALTZ_B200_OPT_SMALL_MARCH_FWD 8
 int waltz_b200_set_option(int option, int value);
 
 #define WALTZ_B200_BATCH_STAGES 0

@@ -511,7 +511,8 @@ def test_tuning_knobs_never_change_the_bytes():
             dref = waltz_b200.decompress_tensor(ref, shape, f.dtype, tuned=False)
             extra = [{"small_inv": 0, "small_fwd": 0}, {"small_inv": 1 << 30, "small_fwd": 1 << 30},
                      {"xy_march": 1}, {"xy_march": 2}, {"xy_march": 3, "stage_kernels": 0},
-                     {"xy_march": 3, "small_inv": 0}, {"small_march": 1 << 21}, {"small_march": 1 << 30}]
+                     {"xy_march": 3, "small_inv": 0}, {"small_march": 1 << 21}, {"small_march": 1 << 30},
+                     {"small_march_fwd": 1 << 21}, {"small_march_fwd": 1 << 30, "small_march": 1 << 30}]
             for k in A.SINGLE_CANDIDATES + extra:
                 A.set_single(lib, k)
                 arc = waltz_b200.compress_tensor(f, 1e-3, tuned=False)
@@ -566,10 +567,11 @@ def test_unaligned_archive_addresses():
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 @pytest.mark.parametrize("nxyz", [(64, 64, 64), (37, 41, 50), (96, 80, 72), (130, 129, 128)])
 def test_dyadic_small_levels_as_marches_match_oracle(nxyz, dtype, small_march):
-    """Dyadic fields whose small inverse levels (every level, with the
-    largest threshold, the finest one's repair and final emitters included)
-    run as a Z march then an XY march instead of the tile inverse:
-    transforms, archives and decodes equal the oracle's."""
+    """Dyadic fields whose small levels (every level, with the largest
+    threshold, the finest one's repair and final emitters included) run as
+    marches: the inverse as a Z march then an XY march instead of the tile
+    inverse, the forward as an XY march then a Z march instead of the
+    z-march. Transforms, archives and decodes equal the oracle's."""
     import torch
     import waltz_b200
     from waltz_b200 import autotune as A
@@ -580,6 +582,7 @@ def test_dyadic_small_levels_as_marches_match_oracle(nxyz, dtype, small_march):
     g = S.power_law_field(P.zyx(nxyz), 8).astype(dtype)
     eb = 1e-4 * (float(g.max()) - float(g.min()))
     assert lib.waltz_b200_set_option(A.OPT_SMALL_MARCH, small_march) == 0
+    assert lib.waltz_b200_set_option(A.OPT_SMALL_MARCH_FWD, small_march) == 0
     try:
         f = gpu_transform(a, inverse=False)
         assert f.tobytes() == O.transform(a, inverse=False).tobytes()
@@ -592,6 +595,7 @@ def test_dyadic_small_levels_as_marches_match_oracle(nxyz, dtype, small_march):
         assert out.tobytes() == O.decompress(host, g.shape, dtype).tobytes()
     finally:
         lib.waltz_b200_set_option(A.OPT_SMALL_MARCH, 0)
+        lib.waltz_b200_set_option(A.OPT_SMALL_MARCH_FWD, 0)
 
 
 @pytest.mark.parametrize("xy_march", [0, 3])

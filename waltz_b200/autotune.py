@@ -18,8 +18,9 @@ question and the table can be applied blindly):
    warp march, forward and inverse levels separately
    (WALTZ_B200_OPT_XY_MARCH bits 0 and 1; single plane fields try it too),
    and the size up to which dyadic inverse levels run as a Z march and an
-   XY march instead of the tile inverse (WALTZ_B200_OPT_SMALL_MARCH; single
-   dyadic fields try it too);
+   XY march instead of the tile inverse (WALTZ_B200_OPT_SMALL_MARCH), and
+   dyadic forward levels as an XY march and a Z march instead of the
+   z-march (WALTZ_B200_OPT_SMALL_MARCH_FWD); single dyadic fields try both;
  * the transform form (lifting or one split of the tensor-core matrix form)
    of fields the matrix form serves: every split is timed and the fastest
    one that beats lifting by 3 % with a compression ratio at most 2 % lower
@@ -46,11 +47,12 @@ TABLE = Path(__file__).with_name("tuning.json")
 
 OPT_STAGE_KERNELS, OPT_ZMARCH_PLANES, OPT_SMALL_LEVEL, OPT_SMALL_FWD = 1, 2, 3, 4
 OPT_XY_MARCH = 6
-OPT_SMALL_MARCH = 7
+OPT_SMALL_MARCH, OPT_SMALL_MARCH_FWD = 7, 8
 BATCH_STAGES, BATCH_FIELDS, BATCH_QUEUE = 0, 1, 2
 DEFAULT_SINGLE = {"stage_kernels": 1, "zmarch": 0, "small_inv": 1 << 15, "small_fwd": 1 << 20, "xy_march": 0,
-                  "small_march": 0}
+                  "small_march": 0, "small_march_fwd": 0}
 SMALL_MARCH_CHOICES = (0, 1 << 21, 1 << 24, 1 << 27)  # dyadic inverse levels as Z + XY marches up to this size
+SMALL_MARCH_FWD_CHOICES = (0, 1 << 21, 1 << 24)       # the same for dyadic forward levels
 MATRIX_MARGIN = 0.97  # the matrix form changes the header flag: take it only for a clear gain
 MATRIX_RATIO = 0.98   # ... and only when its archive stays within 2 % of the plain one's size
 MATRIX_SPLITS = ("matrix-tf32", "matrix-bf16", "matrix-exact")
@@ -86,8 +88,8 @@ BATCH_CANDIDATES = ([{"mode": BATCH_STAGES, "width": w, "stage_kernels": s, "zma
                      for w in (1, 4, 16) for s in (1, 0) for z in (0, 16, 32)
                      for si, sf in ((1 << 15, 1 << 20), (0, 0)) for xy in (0, 1, 2, 3)] +
                     [{"mode": BATCH_STAGES, "width": w, "stage_kernels": s, "zmarch": z, "small_inv": 0, "small_fwd": 0,
-                      "xy_march": xy, "small_march": 1 << 24}
-                     for w in (4, 16) for s in (1, 0) for z in (0, 32) for xy in (0, 3)] +
+                      "xy_march": xy, "small_march": 1 << 24, "small_march_fwd": mf}
+                     for w in (4, 16) for s in (1, 0) for z in (0, 32) for xy in (0, 3) for mf in (0, 1 << 24)] +
                     [{"mode": BATCH_QUEUE, "width": w, "stage_kernels": s} for w in (1, 4, 16) for s in (1, 0)] +
                     [{"mode": BATCH_FIELDS, "width": w, "stage_kernels": s} for w in (16, 32, 64) for s in (1, 0)])
 
@@ -151,6 +153,7 @@ def set_single(lib, k):
     lib.waltz_b200_set_option(OPT_SMALL_FWD, int(k["small_fwd"]))
     lib.waltz_b200_set_option(OPT_XY_MARCH, int(k["xy_march"]))
     lib.waltz_b200_set_option(OPT_SMALL_MARCH, int(k["small_march"]))
+    lib.waltz_b200_set_option(OPT_SMALL_MARCH_FWD, int(k["small_march_fwd"]))
     return k
 
 
@@ -170,7 +173,8 @@ def batch_single_knobs(k):
     return {"stage_kernels": int(k.get("stage_kernels", 1)), "zmarch": int(k.get("zmarch", 0)),
             "small_inv": int(k.get("small_inv", DEFAULT_SINGLE["small_inv"])),
             "small_fwd": int(k.get("small_fwd", DEFAULT_SINGLE["small_fwd"])),
-            "xy_march": int(k.get("xy_march", 0)), "small_march": int(k.get("small_march", 0))}
+            "xy_march": int(k.get("xy_march", 0)), "small_march": int(k.get("small_march", 0)),
+            "small_march_fwd": int(k.get("small_march_fwd", 0))}
 
 
 def matrix_choice(shape, itemsize, path=TABLE):
@@ -209,7 +213,8 @@ def _tune_single(torch, lib, shape, dtype, reps, rel=1e-3):
         cands = cands + [{**c, "xy_march": xy} for xy in (1, 2, 3) for c in SINGLE_CANDIDATES]
     else:
         # dyadic fields also try their small inverse levels as marches
-        cands = [{**c, "small_march": sm} for sm in SMALL_MARCH_CHOICES for c in SINGLE_CANDIDATES]
+        cands = [{**c, "small_march": sm, "small_march_fwd": mf} for sm in SMALL_MARCH_CHOICES
+                 for mf in SMALL_MARCH_FWD_CHOICES for c in SINGLE_CANDIDATES]
     for cand in cands:
         set_single(lib, cand)
         arc = waltz_b200.compress_tensor(f, eb, tuned=False)

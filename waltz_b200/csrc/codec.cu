@@ -211,6 +211,7 @@ struct Options {
     uint32_t xy_march = 0;     // plane schedule: XY levels as the warp march instead of the staged kernels
                                // (bit 0: forward levels, bit 1: inverse levels)
     uint64_t small_march = 0;  // dyadic inverse levels of at most this many samples: Z march + XY march
+    uint64_t small_march_fwd = 0; // dyadic forward levels of at most this many samples: XY march + Z march
 };
 static thread_local Options t_opt;
 
@@ -564,8 +565,18 @@ static void forward(const Geometry& g, const T* in, T* C, T* lowA, T* lowB, T* i
         for (unsigned l = 0; l < g.lxy; ++l) {
             const Dims a = g.dyad[l], lo = halve(a, AX | AY | AZ);
             const bool last = l + 1 == g.lxy;
-            FwdOut<T> out{C, sy, sz, last ? nullptr : lows[l & 1], lo, a, AX | AY | AZ};
-            level_fwd_stream<T>(src, a, out, status, sink);
+            if (vol(a) <= t_opt.small_march_fwd) {
+                // a small level as two marches: the Y and X analysis into
+                // `inter` (x/y split, z spatial), then the Z analysis to C
+                // and the compact low band (the z-march's Y, X, Z order)
+                const size_t isy = a.x, isz = size_t(a.x) * a.y;
+                level_xy<T, false>(src, a, FwdOut<T>{inter, isy, isz, nullptr, halve(a, AX | AY), a, AX | AY}, sink);
+                level_z<T, false>(FwdSrc<T>{inter, isy, isz}, a,
+                                  FwdOut<T>{C, sy, sz, last ? nullptr : lows[l & 1], lo, a, AZ}, sink);
+            } else {
+                FwdOut<T> out{C, sy, sz, last ? nullptr : lows[l & 1], lo, a, AX | AY | AZ};
+                level_fwd_stream<T>(src, a, out, status, sink);
+            }
             static const char* const kFwdNames[5] = {"fwd_l0", "fwd_l1", "fwd_l2", "fwd_l3", "fwd_l4"};
             sink.mark(kFwdNames[l]);
             src = FwdSrc<T>{lows[l & 1], lo.x, size_t(lo.x) * lo.y};
@@ -1867,6 +1878,7 @@ static void compress_batch(const waltz_b200_chunk* items, uint32_t count, uint64
     append_key(key, t_opt.small_fwd);
     append_key(key, t_opt.xy_march);
     append_key(key, t_opt.small_march);
+    append_key(key, t_opt.small_march_fwd);
     char* base = st.scratch.reserve(total);
     append_key(key, base); // the scratch must not have moved since the graph was captured
     uint64_t* results = reinterpret_cast<uint64_t*>(base + results_at);
@@ -2046,6 +2058,7 @@ static void decompress_batch(const waltz_b200_archive* items, uint32_t count, cu
     append_key(key, t_opt.small_fwd);
     append_key(key, t_opt.xy_march);
     append_key(key, t_opt.small_march);
+    append_key(key, t_opt.small_march_fwd);
     append_key(key, count);
     append_key(key, static_cast<const void*>(P.jobs));
     for (uint32_t i = 0; i < count; ++i) {
@@ -2203,6 +2216,10 @@ int waltz_b200_set_option(int option, int value) {
     case WALTZ_B200_OPT_SMALL_MARCH:
         if (value < 0) break;
         t_opt.small_march = uint64_t(value);
+        return 0;
+    case WALTZ_B200_OPT_SMALL_MARCH_FWD:
+        if (value < 0) break;
+        t_opt.small_march_fwd = uint64_t(value);
         return 0;
     default:
         break;

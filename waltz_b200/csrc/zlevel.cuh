@@ -203,10 +203,11 @@ __device__ __forceinline__ void ZMarchOp<T, Inverse, Src, Out>::run(const Params
             lift_forward<T, PP>(e, o);
             if (live) {
                 // a Z level's split positions (the output's mask is AZ):
-                // even z -> z / 2, in the compact low band when there is
-                // one; odd z -> hz + z / 2
+                // even z -> z / 2, in the compact low band for the columns
+                // it covers (all of a plane-schedule level, the x/y-low
+                // corner of a dyadic level); odd z -> hz + z / 2
                 T* const cd = out.dst + size_t(y) * out.sy + x;
-                T* const cl = out.low ? out.low + size_t(y) * out.lo.x + x : nullptr;
+                T* const cl = (out.low && x < out.lo.x && y < out.lo.y) ? out.low + size_t(y) * out.lo.x + x : nullptr;
                 const size_t ls = size_t(out.lo.x) * out.lo.y;
                 const uint32_t hz = half_len(m);
 #pragma unroll
