@@ -60,6 +60,11 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32
     return false;
 }
 
+// Poll bound of every wait for a TMA copy or an MMA. A CTA whose wait runs
+// out records ST_WAIT_TIMEOUT and returns, and the host rejects the call. The
+// bulk copy it waited on may still be in flight into the CTA's shared memory
+// at that point. A healthy device lands a tile in microseconds, far inside
+// 2^22 polls, so this path only runs on a device that has already failed.
 constexpr uint32_t kWaitBound = 1u << 22;
 
 // A tensor map read from global memory (a batched launch's parameter table)
