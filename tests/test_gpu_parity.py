@@ -385,16 +385,18 @@ def batch_form(request):
 def test_batch_compress_equals_single_calls(batch_form):
     """Batched compress of uneven chunks (one CUDA graph): every archive is
     byte-identical to the single-call archive of its chunk, on the first call
-    and on the replay; per-chunk bounds differ."""
+    and on the replay, and a few archives equal the oracle's directly;
+    per-chunk bounds differ."""
     torch = _torch()
     import waltz_b200
     from waltz_b200 import synthetic as S
     rng = np.random.default_rng(4)
     sides = [16, 17, 32, 48, 64]
-    fields, bounds = [], []
+    fields, bounds, hosts = [], [], []
     for k in range(14):
         shape = tuple(int(rng.choice(sides)) for _ in range(3))
         a = S.power_law_field(shape, 40 + k) * float(10 ** rng.uniform(-2, 3))
+        hosts.append(a)
         fields.append(torch.from_numpy(a).cuda())
         bounds.append(1e-3 * float(a.max() - a.min()))
     out = torch.empty(sum(waltz_b200.compressed_capacity(f.numel(), 4) + 16 for f in fields), dtype=torch.uint8,
@@ -404,6 +406,8 @@ def test_batch_compress_equals_single_calls(batch_form):
         for f, eb, arc in zip(fields, bounds, archives):
             single = waltz_b200.compress_tensor(f, eb)
             assert torch.equal(arc, single)
+    for a, eb, arc in list(zip(hosts, bounds, archives))[::5]:
+        assert arc.cpu().numpy().tobytes() == O.compress(a, eb)
     # a failing item is reported with its index
     bad = fields[:3] + [torch.full((8, 8, 8), float("nan"), device="cuda")]
     with pytest.raises(waltz_b200.WaltzError, match="batch item 3"):
