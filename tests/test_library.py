@@ -71,3 +71,28 @@ def test_api_rejects_without_cuda():
     import waltz_b200
     with pytest.raises(waltz_b200.WaltzError):
         waltz_b200.compress(np.zeros((4, 4, 4), np.float32), abs_error=1e-3)
+
+
+def test_noalloc_encoder_host_checks_without_a_device():
+    """The allocation-free WZP encoder refuses bad arguments on the host,
+    before it touches a device: null pointers, an empty input, unaligned
+    magnitudes and inputs beyond its static array (16384 chunks of 8192
+    magnitudes). The pointers are never dereferenced on these paths."""
+    from waltz_b200 import _lib
+    lib = _lib.lib()
+    fn = lib.waltz_b200_wzp_encode_noalloc
+    base = 0x10000  # a 16-byte aligned stand-in address
+    cases = [
+        ((None, base, 64, base, 1 << 20), "null argument"),
+        ((base, base, 0, base, 1 << 20), "must be positive"),
+        ((base + 2, base, 64, base, 1 << 20), "16-byte aligned"),
+        ((base, base, 16384 * 8192 + 1, base, 1 << 30), "allocation-free limit"),
+    ]
+    for (dm, ds, n, out, cap), message in cases:
+        written = ctypes.c_size_t(7)
+        rc = fn(ctypes.c_void_p(dm), ctypes.c_void_p(ds), ctypes.c_uint32(n), ctypes.c_void_p(out),
+                ctypes.c_size_t(cap), ctypes.byref(written), None)
+        assert rc != 0
+        assert message in _lib.last_error()
+        if dm is not None:
+            assert written.value == 0
